@@ -1,0 +1,381 @@
+// Oracle harness around the reference's own C++ classes (test infrastructure).
+//
+// Linked with the reference objects into oracle/_ref/libvmref.so.  It drives the
+// reference through its public element interface, the same calls System makes:
+//   - FixedPositions : InitialState   places walker at caller-given coordinates
+//                                     (the reference's InitialState API,
+//                                     src/InitialStates/initialstate.h:6-32)
+//   - ReplayRNG : RandomNumberGenerator  returns a caller-given stream of numbers
+//                                     in call order (src/RNG/rng.h:6-22), so the
+//                                     reference and the GPU engine consume the
+//                                     same uniforms and normals.
+//   nextInt(n)        = floor(u * n)
+//   nextDouble(lo,hi) = lo + (hi - lo) * u
+//   nextGaussian(m,s) = m + s * z
+// Private members of System/Sampler are reached by compiling this one file with
+// the access keywords widened; the reference sources are unchanged.
+#include <Eigen/Dense>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <unistd.h>
+
+#define private public
+#define protected public
+#include "system.h"
+#include "sampler.h"
+#include "InitialStates/initialstate.h"
+#include "Metropolis/metropolis.h"
+#include "RNG/rng.h"
+#include "WaveFunctions/wavefunction.h"
+#include "Hamiltonians/hamiltonian.h"
+#include "Interaction/interaction.h"
+#include "Optimization/optimization.h"
+#include "block/blocker.h"
+#undef private
+#undef protected
+
+namespace {
+
+class ReplayRNG : public RandomNumberGenerator
+{
+public:
+    std::vector<double> stream;
+    size_t pos = 0;
+    bool exhausted = false;
+    double next()
+    {
+        if (pos >= stream.size()) {
+            exhausted = true;
+            return 0.5;
+        }
+        return stream[pos++];
+    }
+    void setSeed(int) override {}
+    int nextInt(int upperLimit) override { return int(std::floor(next() * upperLimit)); }
+    double nextDouble(double lo, double hi) override { return lo + (hi - lo) * next(); }
+    double nextGaussian(double mean, double sd) override { return mean + sd * next(); }
+    std::string getLabel() override { return "replay"; }
+    Eigen::MatrixXd randomUniformMatrix(Eigen::Index r, Eigen::Index c, double lo,
+                                        double hi) override
+    {
+        Eigen::MatrixXd m(r, c);
+        for (Eigen::Index i = 0; i < m.size(); i++) m.data()[i] = lo + (hi - lo) * next();
+        return m;
+    }
+    Eigen::MatrixXd randomNormalMatrix(Eigen::Index r, Eigen::Index c, double mean,
+                                       double sd) override
+    {
+        Eigen::MatrixXd m(r, c);
+        for (Eigen::Index i = 0; i < m.size(); i++) m.data()[i] = mean + sd * next();
+        return m;
+    }
+};
+
+class FixedPositions : public InitialState
+{
+public:
+    FixedPositions(System *s, const Eigen::VectorXd &p) : InitialState(s), fixed(p) {}
+    Eigen::VectorXd fixed;
+    std::string getLabel() override { return "fixed positions"; }
+    void setupInitialState() override
+    {
+        m_numberOfDimensions = m_system->getNumberOfDimensions();
+        m_numberOfParticles = m_system->getNumberOfParticles();
+        m_degreesOfFreedom = m_system->getNumberOfFreeDimensions();
+        m_positions = fixed;
+        calculateDistanceMatrix();
+        calculateRadialVector();
+        for (auto &e : m_system->getWaveFunctionElements()) {
+            e->initializeArrays(m_positions, m_radialVector, m_distanceMatrix);
+            e->setArrays();
+        }
+    }
+};
+
+struct Handle
+{
+    System *sys = nullptr;
+    FixedPositions *init = nullptr;
+    ReplayRNG *rng = nullptr;
+    std::string cfgPath;
+    // snapshot for vmref_move / vmref_reset
+    Eigen::VectorXd posOld;
+    Eigen::MatrixXd distOld;
+    Eigen::VectorXd radOld;
+};
+
+void syncFromInitialState(Handle *h)
+{
+    System *s = h->sys;
+    s->m_positions = s->m_initialState->getParticles();
+    s->m_distanceMatrix = s->m_initialState->getDistanceMatrix();
+    s->m_radialVector = s->m_initialState->getRadialVector();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Build a System from input.in text.  pos: D coordinates (particle-major).
+// params: E x Pmax row-major (n_params entries) or NULL for the reference's own
+// initial weights.  stream: the replayed random numbers.
+void *vmref_create(const char *config_text, const double *pos, int n_pos, const double *params,
+                   int n_params, const double *stream, long stream_len)
+{
+    Handle *h = new Handle();
+    char tmpl[] = "/tmp/vmref_cfg_XXXXXX";
+    int fd = mkstemp(tmpl);
+    if (fd < 0) {
+        delete h;
+        return nullptr;
+    }
+    FILE *f = fdopen(fd, "w");
+    fputs(config_text, f);
+    fclose(f);
+    h->cfgPath = tmpl;
+
+    System *s = new System();
+    h->sys = s;
+    // main.cpp:8-10 defaults, applied before the configuration file is parsed
+    s->setNumberOfParticles(2);
+    s->setNumberOfDimensions(2);
+    s->setEquilibrationFraction(0.001);
+
+    Eigen::VectorXd p(n_pos);
+    for (int i = 0; i < n_pos; i++) p(i) = pos[i];
+    delete s->m_initialState;
+    h->init = new FixedPositions(s, p);
+    s->setInitialState(h->init);
+    delete s->m_randomNumberGenerator;
+    h->rng = new ReplayRNG();
+    if (stream && stream_len > 0) h->rng->stream.assign(stream, stream + stream_len);
+    s->setRandomNumberGenerator(h->rng);
+
+    char arg0[] = "vmachine";
+    std::vector<char> arg1(h->cfgPath.begin(), h->cfgPath.end());
+    arg1.push_back('\0');
+    char *argv[2] = {arg0, arg1.data()};
+    s->initializeFromConfig(2, argv);
+    s->initializeSystem();
+    unlink(h->cfgPath.c_str());
+
+    if (params) {
+        int E = s->m_numberOfElements, P = s->m_maxParameters;
+        if (n_params != E * P) {
+            fprintf(stderr, "vmref_create: expected %d parameters, got %d\n", E * P, n_params);
+            return nullptr;
+        }
+        Eigen::MatrixXd m(E, P);
+        for (int i = 0; i < E; i++)
+            for (int j = 0; j < P; j++) m(i, j) = params[i * P + j];
+        s->m_parameters = m;
+        s->updateAllParameters(m);
+        s->m_initialState->setupInitialState();
+        syncFromInitialState(h);
+        s->m_metropolis->initialize();
+    }
+    // Initial weights of some element sets draw from the RNG (xavier.cpp:18,
+    // randomuniform.cpp:18); rewind so the Metropolis steps consume the stream
+    // from its first entry.
+    h->rng->pos = 0;
+    h->rng->exhausted = false;
+    return h;
+}
+
+void vmref_destroy(void *hp)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    if (!h) return;
+    // System's destructor frees the elements, the RNG and the initial state.
+    delete h->sys;
+    delete h;
+}
+
+// out: N, d, D, E, Pmax, numberOfBatches, stepsWOEqui, equilibrationSteps
+int vmref_info(void *hp, int *out)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    out[0] = s->m_numberOfParticles;
+    out[1] = s->m_numberOfDimensions;
+    out[2] = s->m_degreesOfFreedom;
+    out[3] = s->m_numberOfElements;
+    out[4] = s->m_maxParameters;
+    out[5] = s->m_optimization->getNumberOfBatches();
+    out[6] = s->m_stepsWOEqui;
+    out[7] = s->m_equilibriationSteps;
+    return 0;
+}
+
+int vmref_get_params(void *hp, double *out)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    const Eigen::MatrixXd &m = h->sys->m_parameters;
+    for (int i = 0; i < m.rows(); i++)
+        for (int j = 0; j < m.cols(); j++) out[i * m.cols() + j] = m(i, j);
+    return 0;
+}
+
+int vmref_get_positions(void *hp, double *out)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    const Eigen::VectorXd &p = h->sys->m_positions;
+    for (int i = 0; i < p.size(); i++) out[i] = p(i);
+    return 0;
+}
+
+// Per element: gradient[D], Laplacian, parameter gradient[Pmax]; then
+// energies = {T, V_ext, V_int} exactly as Sampler::sample forms them
+// (src/sampler.cpp:66-70).
+int vmref_eval(void *hp, double *grad, double *lap, double *pgrad, double *energies)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    int D = s->m_degreesOfFreedom, P = s->m_maxParameters, e = 0;
+    for (auto &el : s->m_waveFunctionElements) {
+        for (int k = 0; k < D; k++) grad[e * D + k] = el->computeGradient(k);
+        lap[e] = el->computeLaplacian();
+        Eigen::VectorXd g = el->computeParameterGradient();
+        for (int j = 0; j < P; j++) pgrad[e * P + j] = (j < g.size()) ? g(j) : 0.0;
+        e++;
+    }
+    energies[0] = s->getKineticEnergy();
+    energies[1] = s->m_hamiltonian->getExternalEnergy();
+    energies[2] = s->m_interactionStyle->getInteractionEnergy();
+    return 0;
+}
+
+// Move coordinate k to new_value the way Metropolis does (metropolis.cpp:21-39,
+// then System::updateAllArrays) and report each element's evaluateRatio().
+int vmref_move(void *hp, int k, double new_value, double *ratios)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    int d = s->m_numberOfDimensions, N = s->m_numberOfParticles;
+    h->posOld = s->m_positions;
+    h->distOld = s->m_distanceMatrix;
+    h->radOld = s->m_radialVector;
+    Eigen::VectorXd pos = s->m_positions;
+    pos(k) = new_value;
+    int p = k / d;
+    Eigen::MatrixXd dist = s->m_distanceMatrix;
+    auto pd = [&](int i, int j) {
+        double acc = 0;
+        for (int a = 0; a < d; a++) {
+            double diff = pos(d * i + a) - pos(d * j + a);
+            acc += diff * diff;
+        }
+        return std::sqrt(acc);
+    };
+    for (int i = 0; i < p; i++) dist(i, p) = pd(p, i);
+    for (int i = p + 1; i < N; i++) dist(p, i) = pd(p, i);
+    Eigen::VectorXd rad = s->m_radialVector;
+    if (rad.size() == N) {
+        double acc = 0;
+        for (int a = 0; a < d; a++) acc += pos(d * p + a) * pos(d * p + a);
+        rad(p) = std::sqrt(acc);
+    }
+    s->m_positions = pos;
+    s->m_distanceMatrix = dist;
+    s->m_radialVector = rad;
+    s->updateAllArrays(pos, rad, dist, k);
+    int e = 0;
+    for (auto &el : s->m_waveFunctionElements) ratios[e++] = el->evaluateRatio();
+    return 0;
+}
+
+int vmref_reset(void *hp)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    s->m_positions = h->posOld;
+    s->m_distanceMatrix = h->distOld;
+    s->m_radialVector = h->radOld;
+    s->resetAllArrays();
+    return 0;
+}
+
+// nsteps calls of Metropolis::acceptMove with the System copies refreshed as in
+// System::runMetropolisCycles (system.cpp:149-153).  Records per step the
+// accept flag, {T, V_ext, V_int}, and the parameter gradients (E x Pmax).
+// Returns the number of random numbers consumed, or -1 if the stream ran out.
+long vmref_steps(void *hp, int nsteps, unsigned char *accepted, double *energies, double *pgrads)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    int E = s->m_numberOfElements, P = s->m_maxParameters;
+    for (int i = 0; i < nsteps; i++) {
+        bool acc = s->m_metropolis->acceptMove();
+        s->m_positions = s->m_metropolis->updatePositions();
+        s->m_distanceMatrix = s->m_metropolis->updateDistanceMatrix();
+        s->m_radialVector = s->m_metropolis->updateRadialVector();
+        if (accepted) accepted[i] = acc ? 1 : 0;
+        if (energies) {
+            energies[3 * i + 0] = s->getKineticEnergy();
+            energies[3 * i + 1] = s->m_hamiltonian->getExternalEnergy();
+            energies[3 * i + 2] = s->m_interactionStyle->getInteractionEnergy();
+        }
+        if (pgrads) {
+            Eigen::MatrixXd g = s->getAllParameterGradients();
+            for (int a = 0; a < E; a++)
+                for (int b = 0; b < P; b++) pgrads[(size_t(i) * E + a) * P + b] = g(a, b);
+        }
+    }
+    return h->rng->exhausted ? -1 : long(h->rng->pos);
+}
+
+// One optimisation iteration as System::runSimulation runs it
+// (system.cpp:93-138) without files or terminal output:
+// runMetropolisCycles, computeTotals, computeAverages, theta -= update.
+// out: E, sigma_E, T, V_ext, V_int, acceptance ratio, then E*Pmax average
+// gradients, E*Pmax average E*gradients, E*Pmax new parameters.
+long vmref_iteration(void *hp, int iter, double *out)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    Sampler *sm = s->m_sampler;
+    s->m_iter = iter;
+    sm->m_iter = iter;
+    sm->setNumberOfSteps(s->m_stepsWOEqui, s->m_totalStepsWOEqui, s->m_totalStepsWEqui);
+    s->runMetropolisCycles();
+    sm->computeTotals();
+    sm->computeAverages();
+    s->m_parameters -= s->m_optimization->updateParameters();
+    s->updateAllParameters(s->m_parameters);
+    int E = s->m_numberOfElements, P = s->m_maxParameters;
+    out[0] = sm->m_averageEnergy;
+    out[1] = sm->m_stdError;
+    out[2] = sm->m_averageKineticEnergy;
+    out[3] = sm->m_averageExternalEnergy;
+    out[4] = sm->m_averageInteractionEnergy;
+    out[5] = double(sm->m_totalAcceptence) / sm->m_totalStepsWOEqui;
+    size_t o = 6;
+    for (int a = 0; a < E; a++)
+        for (int b = 0; b < P; b++) out[o++] = sm->m_averageGradients(a, b);
+    for (int a = 0; a < E; a++)
+        for (int b = 0; b < P; b++) out[o++] = sm->m_averageGradientsE(a, b);
+    for (int a = 0; a < E; a++)
+        for (int b = 0; b < P; b++) out[o++] = s->m_parameters(a, b);
+    return h->rng->exhausted ? -1 : long(h->rng->pos);
+}
+
+// Blocker on a series of length 2^k (include/block/blocker.cpp:15-33):
+// out = {mean, stdErr}.
+int vmref_blocking(const double *x, long n, double *out)
+{
+    std::vector<double> v(x, x + n);
+    Blocker b(v);
+    out[0] = b.mean;
+    out[1] = b.stdErr;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,129 @@
+"""Pin the C oracle (oracle/vmc_oracle.c) to the reference's own outputs.
+
+The golden vectors in tests/golden/ were produced by the reference's C++ sources
+(tests/golden/make_golden.py).  Bar: 1e-11 relative (max-abs over each array,
+relative to its max-abs) for FP64 values, identical accept/reject sequences.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle_bind import Oracle, load_cases, spec_from_case
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+TOL = 1e-11
+
+ORACLE = None
+
+
+def oracle():
+    global ORACLE
+    if ORACLE is None:
+        ORACLE = Oracle()
+    return ORACLE
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    scale = max(np.max(np.abs(b)) if b.size else 0.0, 1e-300)
+    return float(np.max(np.abs(a - b)) / scale) if b.size else 0.0
+
+
+EVAL = load_cases(os.path.join(GOLD, "eval_fixed.npz"))
+CHAINS = load_cases(os.path.join(GOLD, "chains.npz"))
+ITERS = load_cases(os.path.join(GOLD, "iterations.npz"))
+BLOCK = load_cases(os.path.join(GOLD, "blocking.npz"))
+
+
+@pytest.mark.parametrize("name", sorted(EVAL))
+def test_fixed_positions(name):
+    c = EVAL[name]
+    spec = spec_from_case(c)
+    O = oracle()
+    for t in range(len(c["pos"])):
+        pos = c["pos"][t]
+        g, lap, pg, en = O.eval(spec, c["theta"], pos)
+        assert rel(g, c["grad"][t]) < TOL
+        assert rel(lap, c["lap"][t]) < TOL
+        assert rel(pg, c["pgrad"][t]) < TOL
+        assert rel(en, c["energies"][t]) < TOL
+        k, xn = int(c["k"][t]), float(c["xnew"][t])
+        r = O.ratio(spec, c["theta"], pos, k, xn)
+        assert rel(r, c["ratios"][t]) < TOL
+        pos2 = pos.copy()
+        pos2[k] = xn
+        g, lap, pg, en = O.eval(spec, c["theta"], pos2)
+        assert rel(g, c["grad2"][t]) < TOL
+        assert rel(lap, c["lap2"][t]) < TOL
+        assert rel(pg, c["pgrad2"][t]) < TOL
+        assert rel(en, c["energies2"][t]) < TOL
+
+
+@pytest.mark.parametrize("name", sorted(CHAINS))
+def test_replayed_chain(name):
+    c = CHAINS[name]
+    spec = spec_from_case(c)
+    O = oracle()
+    steps = len(c["accepted"])
+    pos = c["pos"][None].copy()
+    f = O.quantum_force(spec, c["theta"], c["pos"])[None].copy()
+    out = O.run(spec, c["theta"], pos, f, steps, 0, 0, 1, stream=c["stream"][None])
+    assert np.array_equal(out["accepted"][0], c["accepted"])
+    assert rel(out["energies"][0], c["energies"]) < TOL
+    assert rel(pos[0], c["final_pos"]) < TOL
+
+
+def _run_iterations(c, spec, O):
+    from oracle.vmc_oracle_host import Adam, GradientDescent, averages, energy_gradient
+    theta = c["theta0"].copy()
+    E, P = theta.shape
+    burn, steps_wo, batches = int(c["burn_in"]), int(c["steps_wo"]), int(c["batches"])
+    per = burn + steps_wo
+    opt = spec.optimization.split()
+    if opt[0] == "adam":
+        optim = Adam(theta.shape, spec.learning_rate)
+    else:
+        gamma, power = (float(opt[1]), float(opt[2])) if len(opt) >= 3 else (0.0, 0.0)
+        optim = GradientDescent(theta.shape, spec.learning_rate, gamma, power)
+    assert optim.batches == batches
+    pos = c["pos"][None].copy()
+    f = O.quantum_force(spec, theta, c["pos"])[None].copy()
+    # Pade pair terms keep the gamma they were computed with until their particle moves
+    gpair = np.zeros((1, spec.N, spec.N))
+    if 2 in spec.elements:
+        gpair[:] = theta[list(spec.elements).index(2), 0]
+    res = []
+    for it in range(len(c["energy"])):
+        stream = c["stream"][it * per:(it + 1) * per][None]
+        out = O.run(spec, theta, pos, f, per, burn, it, batches, stream=stream, want_steps=False,
+                    gpair=gpair)
+        avg = averages(out["sums"].sum(0), steps_wo, steps_wo // batches, (E, P))
+        theta = theta - optim.update(energy_gradient(avg))
+        res.append((avg, theta.copy()))
+    return res
+
+
+@pytest.mark.parametrize("name", sorted(ITERS))
+def test_iterations(name):
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    c = ITERS[name]
+    spec = spec_from_case(c)
+    res = _run_iterations(c, spec, oracle())
+    for it, (avg, theta) in enumerate(res):
+        for key in ("energy", "kinetic", "external", "interaction", "acceptance"):
+            assert rel(avg[key], c[key][it]) < TOL, (key, it)
+        assert rel(avg["std_error"], c["std_error"][it]) < 1e-8
+        assert rel(avg["avg_grad"], c["avg_grad"][it]) < TOL
+        assert rel(avg["avg_grad_e"], c["avg_grad_e"][it]) < TOL
+        assert rel(theta, c["params"][it]) < TOL
+
+
+@pytest.mark.parametrize("name", sorted(BLOCK))
+def test_blocking(name):
+    c = BLOCK[name]
+    mean, var = oracle().blocking(c["x"])
+    assert abs(mean - float(c["mean"])) < 1e-12 * max(1.0, abs(float(c["mean"])))
+    assert abs(np.sqrt(var) - float(c["std_error"])) < 1e-9 * float(c["std_error"])
