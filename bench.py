@@ -1,0 +1,372 @@
+"""Benchmark: walker-moves/s of the B200 engine on the N=56 quantum dot.
+
+Workload (one "step" = one optimisation iteration of the whole walker population):
+  2D quantum dot, N=56 electrons (two 28x28 Hermite Slater blocks) x Gaussian x
+  Pade-Jastrow, omega=0.28, Coulomb, importance sampling dt=0.005, 16384 walkers x
+  (20000 + 20 burn-in) single-coordinate moves per iteration, E_L and dlnPsi/dtheta
+  sampled after every move (the reference's definition of a step), device-reduced
+  sums, ADAM update.  Mixed precision (FP32 sweep, FP64 rebuild every refresh
+  interval, compensated FP64 sums); an FP64 engine run of the same workload is
+  reported beside it.  Synthetic: walker start positions from per-walker Philox
+  streams, RandomNormal as in the reference.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+N > 1: one process per GPU (torchrun), walkers per GPU fixed (weak scaling), the
+only collective is the barrier and the max-over-ranks timing.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "N=56 dot walker-moves/s & E_L samples/s: mixed vs FP64 GPU at equal sigma_E"
+UNIT = "walker-moves/s"
+N_PART, OMEGA, DT = 56, 0.28, 0.005
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "vmachine_ref")
+
+
+def workload_text(walkers, steps_per_walker, precision, seed):
+    return "\n".join([
+        f"numParticles: {N_PART}", "numDimensions: 2", "hamiltonian: harmonicOscillator",
+        f"omega: {OMEGA}", "interactionStyle: coulomb",
+        "waveFunctionElement: slaterDeterminant", "waveFunctionElement: gaussian",
+        "waveFunctionElement: padeJastrow", "basis: hermite",
+        "sampling: importanceSampling", f"stepLength: {DT}", "optimization: adam",
+        "learningRate: 0.01", f"numSteps: {walkers * steps_per_walker}", "numIterations: 100",
+        f"numWalkers: {walkers}", f"precision: {precision}", f"rng: MersenneTwister {seed}",
+    ]) + "\n"
+
+
+def flops_per_step(N, d=2):
+    """Algorithmic flops of one accepted move plus one E_L / dlnPsi sample in the
+    engine's incremental scheme (FMA = 2, MUL/ADD = 1, div/sqrt/exp = 1); the count
+    is derived term by term in DESIGN.md."""
+    n = N // 2
+    K = {1: 1, 3: 2, 6: 3, 10: 4, 15: 5, 21: 6, 28: 7}[n]
+    tables = d * 4 * (K - 1)                     # Hermite recurrence at one point
+    ratio = tables + n * (d - 1) + 2 * n * n     # new orbital row, S_j = row . inv[:, j]
+    pairs = (N - 1) * (12 * d + 40)              # Pade/Coulomb terms of the moved particle
+    sm = 2 * n * n                               # Sherman-Morrison rank-1 update
+    deriv = n * (d * (4 * (K - 1) + 2 * K) + n * (10 if d == 2 else 18))  # d ln det refresh
+    kinetic = 7 * N * d
+    return ratio + pairs + sm + deriv + kinetic + 40
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def reference_sample(cores, steps_per_proc, seed0=11):
+    """Run `cores` concurrent single-rank reference processes on the workload's
+    input.in (numSteps scaled down) and return aggregate walker-moves/s from the
+    reference's own per-iteration CPU_time column."""
+    if not os.path.exists(REF_BIN):
+        return None, "oracle/_ref/vmachine_ref was not built"
+    tmp = tempfile.mkdtemp(prefix="vmref_")
+    procs = []
+    for i in range(cores):
+        d = os.path.join(tmp, f"p{i}")
+        os.makedirs(d)
+        txt = "\n".join([
+            f"numParticles: {N_PART}", "numDimensions: 2", "hamiltonian: harmonicOscillator",
+            f"omega: {OMEGA}", "interactionStyle: coulomb",
+            "waveFunctionElement: slaterDeterminant", "waveFunctionElement: gaussian",
+            "waveFunctionElement: padeJastrow", "basis: hermite",
+            "sampling: importanceSampling", f"stepLength: {DT}", "optimization: adam",
+            "learningRate: 0.01", f"numSteps: {steps_per_proc}", "numIterations: 2",
+            f"rng: MersenneTwister {seed0 + i}", f"path: {d}/"]) + "\n"
+        with open(os.path.join(d, "input.in"), "w") as f:
+            f.write(txt)
+        procs.append(subprocess.Popen([REF_BIN, "input.in"], cwd=d, stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True))
+    rates = []
+    for p in procs:
+        out, _ = p.communicate(timeout=900)
+        t = None
+        for ln in out.splitlines():
+            f = ln.split()
+            if len(f) == 11 and f[0] == "1":
+                t = float(f[-1])
+        if t:
+            rates.append((steps_per_proc + int(steps_per_proc * 0.001)) / t)
+    shutil.rmtree(tmp, ignore_errors=True)
+    if not rates:
+        return None, "reference runs printed no iteration timing"
+    return float(sum(rates)), None
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    cores = host_cores()
+    steps = args.ref_steps
+    values = []
+    for i in range(args.warmup + args.steps):
+        v, err = reference_sample(cores, steps, seed0=11 + 1000 * i)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return
+        if i >= args.warmup:
+            values.append(v)
+    value = statistics.median(values)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * (steps * cores) / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"2D quantum dot N={N_PART} omega={OMEGA}, Slater(Hermite) x "
+                               "Gaussian x Pade, importance sampling dt=0.005, one walker per "
+                               "process, E_L every move", "processes": cores,
+                   "steps_per_process": steps},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} concurrent one-rank runs of the reference built "
+                                   f"from its sources, {steps} moves each, CPU_time column"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- engine arm
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        t = torch.zeros(1, device=f"cuda:{local}")
+        pg.all_reduce(t)
+        torch.cuda.synchronize(local)
+
+
+def max_over_ranks(pg, local, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_engine_arm(args):
+    world, rank, local, pg = dist_setup(args)
+    from vmachine_b200 import Engine, measure_fma_peak
+    W, spw = args.walkers, args.steps_per_walker
+    seed = 1000 + rank
+    text = workload_text(W, spw, "mixed", seed)
+    eng = Engine(text, device=local)
+    eng.init_walkers(None, seed=seed)
+    burn = eng.info.burn_in
+    moves_per_step = W * (spw + burn)
+    for it in range(args.warmup):
+        eng.run_iteration(it)
+    barrier(pg, local)
+    sweep_s, launches, sig = 0.0, 0.0, []
+    with ClockSampler(local) as clk:
+        eng.stopwatch_start()
+        for it in range(args.steps):
+            a = eng.run_iteration(args.warmup + it)
+            sig.append(a.walker_std_error)
+        ms = eng.stopwatch_stop()
+    # per-launch sweep timing of one more iteration (same work, not in the timed region)
+    sums, _, _ = eng.sample(args.warmup + args.steps, spw + burn, burn)
+    sweep_s, launches = sums.sweep_seconds, sums.sweep_launches
+    ms = max_over_ranks(pg, local, ms)
+    total_moves = moves_per_step * args.steps * world
+    value = total_moves / (ms * 1e-3)
+    energy = a.energy
+
+    # e2e through the C ABI with host buffers: walkers uploaded, one iteration,
+    # walkers read back, every step
+    e2e = None
+    if not args.no_e2e:
+        pos = eng.positions()
+        h2d = pos.nbytes + 8 * eng.E * eng.P
+        d2h = pos.nbytes + 8 * 16
+        barrier(pg, local)
+        eng.stopwatch_start()
+        for it in range(args.e2e_steps):
+            eng.init_walkers(pos, seed=seed)
+            eng.run_iteration(1000 + it)
+            pos = eng.positions()
+        e2e_ms = max_over_ranks(pg, local, eng.stopwatch_stop())
+        e2e = {"value": moves_per_step * args.e2e_steps * world / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "path": "vmc_init_walkers(host positions) + vmc_run_iteration + "
+                       "vmc_get_positions per step"}
+
+    # FP64 engine on the same workload (same walkers, fewer steps per iteration)
+    fp64 = None
+    if not args.no_fp64:
+        eng64 = Engine(workload_text(W, args.fp64_steps_per_walker, "fp64", seed), device=local)
+        eng64.init_walkers(None, seed=seed)
+        eng64.run_iteration(0)
+        barrier(pg, local)
+        eng64.stopwatch_start()
+        a64 = eng64.run_iteration(1)
+        ms64 = max_over_ranks(pg, local, eng64.stopwatch_stop())
+        mv64 = W * (args.fp64_steps_per_walker + eng64.info.burn_in) * world
+        fp64 = {"value": mv64 / (ms64 * 1e-3), "ms_per_step": ms64,
+                "steps_per_walker": args.fp64_steps_per_walker, "energy": a64.energy,
+                "sigma_e_walkers": a64.walker_std_error}
+        eng64.close()
+
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    peak = measure_fma_peak(local, 1)
+    fl = flops_per_step(N_PART)
+    avg_launch = sweep_s / max(launches, 1)
+    steps_per_launch = (spw + burn) / max(launches, 1)
+    achieved = fl * W * steps_per_launch / avg_launch / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 rebuild and sums)",
+        "data": "synthetic (Philox RandomNormal starts, sigma = 1/omega)",
+        "config": {"workload": f"2D quantum dot N={N_PART} omega={OMEGA}: Slater(Hermite, 2 x "
+                               f"28x28) x Gaussian x Pade, Coulomb, importance sampling "
+                               f"dt={DT}, E_L + dlnPsi every move, ADAM",
+                   "walkers_per_gpu": W, "steps_per_walker": spw, "burn_in": burn,
+                   "precision": "mixed", "refresh_interval": eng.info.refresh_interval,
+                   "walkers_per_block": eng.info.walkers_per_block,
+                   "l2": "walker state %.0f MB per GPU > 126 MB L2, streamed every launch"
+                         % (W * (eng.info.n_coords * 5 * 4 + 2 * 28 * 28 * 4 + 56 * 8 + 64) / 1e6)},
+        "el_samples_per_s": value * spw / (spw + burn),
+        "energy": energy, "sigma_e_walkers": sig[-1] if sig else None,
+        "gpu_launches": int(args.steps * (2 * launches + 1)),
+        "roofline": {"bound": "fp32-pipe", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                     "traffic": None,
+                     "peak_source": "vmc_measure_fma_peak (FP32 FMA loop, this GPU, this run); "
+                                    "MEASURED_PEAKS.json has no FP32 pipe figure",
+                     "flops_per_move": fl, "kernel": "sweep_kernel<float,2,7>",
+                     "avg_launch_ms": avg_launch * 1e3},
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if fp64:
+        line["fp64"] = fp64
+        line["mixed_over_fp64"] = value / fp64["value"]
+    if not args.no_cpu_baseline and world == 1:
+        cores = host_cores()
+        v, err = reference_sample(cores, args.ref_steps)
+        line["cpu_baseline"] = ({"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                                 "sample": f"{cores} concurrent one-rank reference runs, "
+                                           f"{args.ref_steps} moves each"}
+                                if v else {"value": None, "unavailable": err})
+    line["clocks"] = clk.summary()
+    print(json.dumps(line))
+    eng.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--walkers", type=int, default=16384)
+    ap.add_argument("--steps-per-walker", type=int, default=20000)
+    ap.add_argument("--fp64-steps-per-walker", type=int, default=4000)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-steps", type=int, default=60000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args, int(os.environ.get("RANK", "0")))
+    else:
+        run_engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+// Device building blocks of the walker engine (sm_100a).
+//
+// One warp owns one walker.  Everything here is warp-synchronous: a value that is
+// the same in all 32 lanes ("uniform") is computed redundantly by every lane, which
+// costs one warp instruction, and lane-parallel work is spread over lanes by
+// particle or by orbital.  Reductions are xor-butterflies so that every lane ends
+// with the total.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vmc {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ------------------------------------------------------------------ flags
+enum : int {
+    F_GAUSS = 1 << 0,        // Gaussian element, exp(-omega alpha sum x^2 / 2)
+    F_SLATER = 1 << 1,       // Slater determinant (Hermite basis)
+    F_PADE = 1 << 2,         // Pade-Jastrow
+    F_COULOMB = 1 << 3,      // Coulomb interaction
+    F_ATOM = 1 << 4,         // atomic nucleus potential (else harmonic oscillator)
+    Q_PADE_RATIO = 1 << 5,   // Pade ratio over partners j > moved particle only
+    Q_PADE_DGAMMA = 1 << 6,  // dlnPsi/dgamma halved
+    Q_IS_GREEN = 1 << 7,     // importance-sampling Green's ratio with the cached force
+    Q_PADE_STALE = 1 << 8,   // Pade pairs keep the previous gamma until their particle moves
+    F_HYDROGENLIKE = 1 << 9, // exp(-alpha Z sum r_i)
+};
+
+enum : int { SAMPLER_IS = 0, SAMPLER_BF = 1 };
+
+// walker status bits
+enum : int {
+    ST_NAN_ENERGY = 1,
+    ST_BAD_RATIO = 2,
+    ST_SINGULAR = 4,
+};
+
+// ------------------------------------------------------------------ RNG
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+constexpr double TWO_M32 = 2.3283064365386963e-10;
+
+// ------------------------------------------------------------------ reductions
+template <typename R>
+__device__ __forceinline__ R warp_sum(R v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Neumaier-compensated accumulation (Neumaier 1974): s + c carries the sum.
+__device__ __forceinline__ void kadd(double &s, double &c, double v)
+{
+    const double t = s + v;
+    c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+    s = t;
+}
+
+// ------------------------------------------------------------------ math
+__device__ __forceinline__ float fast_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double fast_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float vsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double vsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float vexp(float x) { return expf(x); }
+__device__ __forceinline__ double vexp(double x) { return exp(x); }
+
+// Coefficients of the normalised Hermite functions h_m = H_m / sqrt(2^m m!):
+//   h_{m+1} = A_m x h_m - B_m h_{m-1},  A_m = sqrt(2/(m+1)), B_m = sqrt(m/(m+1))
+//   h'_m = C_m h_{m-1},  C_m = sqrt(2m);   h''_m = E_m h_{m-2},  E_m = 2 sqrt(m(m-1))
+// Filled once per device from the host (same double expressions as the CPU oracle).
+// Defined here: the engine is a single translation unit.
+constexpr int HMAX = 24;
+struct HermiteCoef {
+    double A[HMAX], B[HMAX], C[HMAX], E[HMAX];
+    float Af[HMAX], Bf[HMAX], Cf[HMAX], Ef[HMAX];
+};
+__constant__ HermiteCoef c_herm;
+
+template <typename R> __device__ __forceinline__ R hA(int m);
+template <> __device__ __forceinline__ double hA<double>(int m) { return c_herm.A[m]; }
+template <> __device__ __forceinline__ float hA<float>(int m) { return c_herm.Af[m]; }
+template <typename R> __device__ __forceinline__ R hB(int m);
+template <> __device__ __forceinline__ double hB<double>(int m) { return c_herm.B[m]; }
+template <> __device__ __forceinline__ float hB<float>(int m) { return c_herm.Bf[m]; }
+template <typename R> __device__ __forceinline__ R hC(int m);
+template <> __device__ __forceinline__ double hC<double>(int m) { return c_herm.C[m]; }
+template <> __device__ __forceinline__ float hC<float>(int m) { return c_herm.Cf[m]; }
+template <typename R> __device__ __forceinline__ R hE(int m);
+template <> __device__ __forceinline__ double hE<double>(int m) { return c_herm.E[m]; }
+template <> __device__ __forceinline__ float hE<float>(int m) { return c_herm.Ef[m]; }
+
+// h_0..h_{M-1} at x (registers; M is a compile-time count so indices stay static)
+template <int M, typename R>
+__device__ __forceinline__ void hermite_values(R x, R (&h)[M])
+{
+    h[0] = R(1);
+    if (M > 1) h[1] = hA<R>(0) * x;
+#pragma unroll
+    for (int m = 1; m + 1 < M; ++m) h[m + 1] = hA<R>(m) * x * h[m] - hB<R>(m) * h[m - 1];
+}
+
+template <int M, typename R>
+__device__ __forceinline__ void hermite_derivs(const R (&h)[M], R (&h1)[M], R (&h2)[M])
+{
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        h1[m] = m >= 1 ? hC<R>(m) * h[m - 1] : R(0);
+        h2[m] = m >= 2 ? hE<R>(m) * h[m - 2] : R(0);
+    }
+}
+
+// ------------------------------------------------------------------ orbitals
+// Closed-shell Hermite orbitals in the reference's order (basis.cpp:81-116):
+// 2D shell s: (s-j, j), j = 0..s;  3D shell s: (s-j-l, j, l).
+template <int DIM, int K> struct Shells;
+template <int K> struct Shells<2, K> { static constexpr int n = K * (K + 1) / 2; };
+template <int K> struct Shells<3, K> { static constexpr int n = K * (K + 1) * (K + 2) / 6; };
+
+// Calls f(o, mx, my, mz) for every orbital o, fully unrolled.
+template <int DIM, int K, typename F>
+__device__ __forceinline__ void for_each_orbital(F &&f)
+{
+    int o = 0;
+#pragma unroll
+    for (int s = 0; s < K; ++s) {
+        if (DIM == 2) {
+#pragma unroll
+            for (int j = 0; j <= s; ++j) { f(o, s - j, j, 0); ++o; }
+        } else {
+#pragma unroll
+            for (int j = 0; j <= s; ++j)
+#pragma unroll
+                for (int l = 0; l <= s - j; ++l) { f(o, s - j - l, j, l); ++o; }
+        }
+    }
+}
+
+}  // namespace vmc

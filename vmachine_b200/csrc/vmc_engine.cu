@@ -1,0 +1,978 @@
+// Host side of the walker engine: the C ABI declared in include/vmc_b200.h.
+//
+// Owns the device buffers and one CUDA stream per engine, selects the kernel
+// instantiation for (precision, dimension, Hermite shells), and runs the
+// reference's iteration semantics: burn-in, gradient window, averages, optimiser
+// step, parameter broadcast (src/system.cpp:81-139, src/sampler.cpp:52-226).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "vmc_b200.h"
+#include "vmc_config.hpp"
+#include "vmc_kernels.cuh"
+
+using namespace vmc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+    do {                                                                                 \
+        cudaError_t _e = (expr);                                                         \
+        if (_e != cudaSuccess)                                                           \
+            return fail(VMC_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+struct KernelSet {
+    const void *sweep = nullptr, *rebuild = nullptr, *eval = nullptr, *initpos = nullptr;
+};
+
+template <typename T, int DIM, int K>
+KernelSet make_set()
+{
+    KernelSet s;
+    s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K>);
+    s.rebuild = reinterpret_cast<const void *>(&rebuild_kernel<T, DIM, K>);
+    s.eval = reinterpret_cast<const void *>(&eval_kernel<T, DIM, K>);
+    s.initpos = reinterpret_cast<const void *>(&initial_positions_kernel<T>);
+    return s;
+}
+
+template <typename T>
+bool select_set_t(int dim, int K, KernelSet &out)
+{
+    if (dim == 2) {
+        switch (K) {
+        case 0: out = make_set<T, 2, 0>(); return true;
+        case 1: out = make_set<T, 2, 1>(); return true;
+        case 2: out = make_set<T, 2, 2>(); return true;
+        case 3: out = make_set<T, 2, 3>(); return true;
+        case 4: out = make_set<T, 2, 4>(); return true;
+        case 5: out = make_set<T, 2, 5>(); return true;
+        case 6: out = make_set<T, 2, 6>(); return true;
+        case 7: out = make_set<T, 2, 7>(); return true;
+        default: return false;
+        }
+    }
+    if (dim == 3) {
+        switch (K) {
+        case 0: out = make_set<T, 3, 0>(); return true;
+        case 1: out = make_set<T, 3, 1>(); return true;
+        case 2: out = make_set<T, 3, 2>(); return true;
+        case 3: out = make_set<T, 3, 3>(); return true;
+        case 4: out = make_set<T, 3, 4>(); return true;
+        default: return false;
+        }
+    }
+    return false;
+}
+
+bool select_set(int precision, int dim, int K, KernelSet &out)
+{
+    return precision == VMC_PRECISION_MIXED ? select_set_t<float>(dim, K, out)
+                                            : select_set_t<double>(dim, K, out);
+}
+
+uint4 host_philox(uint4 c, uint2 k)
+{
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
+        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k.x, (uint32_t)p1,
+                       (uint32_t)(p0 >> 32) ^ c.w ^ k.y, (uint32_t)p0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+int hermite_init_device(int device)
+{
+    static bool done[64] = {false};
+    if (device < 64 && done[device]) return VMC_OK;
+    HermiteCoef h;
+    for (int m = 0; m < HMAX; ++m) {
+        h.A[m] = std::sqrt(2.0 / (m + 1));
+        h.B[m] = std::sqrt((double)m / (m + 1));
+        h.C[m] = std::sqrt(2.0 * m);
+        h.E[m] = 2.0 * std::sqrt((double)m * (m - 1 > 0 ? m - 1 : 0));
+        h.Af[m] = (float)h.A[m];
+        h.Bf[m] = (float)h.B[m];
+        h.Cf[m] = (float)h.C[m];
+        h.Ef[m] = (float)h.E[m];
+    }
+    CUDA_TRY(cudaMemcpyToSymbol(c_herm, &h, sizeof(h)));
+    if (device < 64) done[device] = true;
+    return VMC_OK;
+}
+
+}  // namespace
+
+struct vmc_engine {
+    Config cfg;
+    int device = 0, num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int W = 0, N = 0, dim = 0, D = 0, n_orb = 0, K = 0, E = 0, Pmax = 0, EP = 0, nacc = 0;
+    int precision = 0, compat = 1, flags = 0, sampling = 0;
+    int steps_per_walker = 0, burn_in = 0, batches = 1;
+    int wpb = 0, refresh_interval = 0, sweep_chunk = 2048;
+    size_t elem_bytes = 8;
+    Layout L{};
+    KernelSet ks;
+    std::vector<double> theta;
+    double gamma_prev = 0.0;
+    bool have_walkers = false;
+    unsigned long long seed = 0;
+    // optimiser state (adam.cpp:12-37, gradientdescent.cpp/sgd.cpp)
+    std::vector<double> opt_m, opt_v;
+    int opt_step = 0;
+    // device buffers
+    void *d_state = nullptr;
+    double *d_scal = nullptr, *d_acc = nullptr, *d_out = nullptr, *d_drift = nullptr;
+    unsigned long long *d_mask = nullptr, *d_counter = nullptr;
+    unsigned *d_status = nullptr;
+    std::vector<cudaEvent_t> sweep_events;  // per-launch timing of the sweep kernel
+    cudaEvent_t sw0 = nullptr, sw1 = nullptr;  // vmc_stopwatch
+    // optional replayed random stream consumed by vmc_sample (W x replay_len x 3)
+    double *d_replay = nullptr;
+    int replay_len = 0, replay_pos = 0;
+    // last sampling pass
+    vmc_sums last{};
+    double last_samples_per_walker = 0.0;
+};
+
+namespace {
+
+void free_engine(vmc_engine *e)
+{
+    if (!e) return;
+    cudaSetDevice(e->device);
+    cudaFree(e->d_state);
+    cudaFree(e->d_scal);
+    cudaFree(e->d_acc);
+    cudaFree(e->d_out);
+    cudaFree(e->d_drift);
+    cudaFree(e->d_mask);
+    cudaFree(e->d_counter);
+    cudaFree(e->d_status);
+    cudaFree(e->d_replay);
+    for (cudaEvent_t ev : e->sweep_events) cudaEventDestroy(ev);
+    if (e->sw0) cudaEventDestroy(e->sw0);
+    if (e->sw1) cudaEventDestroy(e->sw1);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int closed_shells_2d(int N, int dim)
+{
+    // number of Hermite shells K with 2 * C(K-1+dim, dim) == N, or -1
+    for (int K = 1; K <= 9; ++K) {
+        long c = 1;
+        for (int i = 1; i <= dim; ++i) c = c * (K - 1 + i) / i;
+        if (2 * c == N) return K;
+        if (2 * c > N) return -1;
+    }
+    return -1;
+}
+
+Params make_params(const vmc_engine *e)
+{
+    Params P{};
+    P.L = e->L;
+    P.W = e->W;
+    P.N = e->N;
+    P.n_elem = e->E;
+    P.ep = e->EP;
+    P.nacc = e->nacc;
+    for (int i = 0; i < e->E && i < MAX_ELEM; ++i) P.elem_kind[i] = e->cfg.elements[i];
+    P.flags = e->flags;
+    P.sampling = e->sampling;
+    P.omega = e->cfg.omega;
+    P.Z = e->cfg.Z;
+    P.step = e->cfg.step_length;
+    P.alpha = 0.0;
+    P.gamma = 0.0;
+    P.alpha_h = 0.0;
+    P.idx_alpha = P.idx_gamma = P.idx_alpha_h = -1;
+    for (int i = 0; i < e->E; ++i) {
+        const double t0 = e->theta[(size_t)i * e->Pmax];
+        switch (e->cfg.elements[i]) {
+        case E_GAUSSIAN: P.alpha = t0; P.idx_alpha = i * e->Pmax; break;
+        case E_PADE: P.gamma = t0; P.idx_gamma = i * e->Pmax; break;
+        case E_HYDROGENLIKE: P.alpha_h = t0; P.idx_alpha_h = i * e->Pmax; break;
+        default: break;
+        }
+    }
+    P.gamma_prev = e->gamma_prev;
+    // Pade spin coefficients (padejastrow.cpp:140-170)
+    P.beta_same = e->dim == 2 ? 1.0 / 3 : e->dim == 3 ? 1.0 / 4 : 1.0 / 5;
+    P.beta_anti = e->dim == 2 ? 1.0 : e->dim == 3 ? 1.0 / 2 : 1.0 / 3;
+    P.state = e->d_state;
+    P.scal = e->d_scal;
+    P.mask = e->d_mask;
+    P.counter = e->d_counter;
+    P.acc = e->d_acc;
+    P.status = e->d_status;
+    return P;
+}
+
+int launch(const void *fn, int grid, int block, size_t smem, cudaStream_t st, void *args)
+{
+    void *argv[1] = {args};
+    CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(block), argv, smem, st));
+    return VMC_OK;
+}
+
+int sweep_smem_per_warp(const vmc_engine *e)
+{
+    return round_up(e->L.rec * (int)e->elem_bytes + e->N * 8, 16);
+}
+
+int run_rebuild(vmc_engine *e, int mode, double *drift)
+{
+    RebuildArgs a{};
+    a.P = make_params(e);
+    a.mode = mode;
+    a.drift = drift;
+    a.wpb = 4;
+    a.smem_per_warp = std::max(16, round_up(2 * e->n_orb * e->n_orb * 8, 16));
+    const size_t smem = (size_t)a.wpb * a.smem_per_warp;
+    CUDA_TRY(cudaFuncSetAttribute(e->ks.rebuild, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = (e->W + a.wpb - 1) / a.wpb;
+    return launch(e->ks.rebuild, grid, 32 * a.wpb, smem, e->stream, &a);
+}
+
+int run_sweep(vmc_engine *e, SweepArgs &a)
+{
+    a.P = make_params(e);
+    a.wpb = e->wpb;
+    a.smem_per_warp = sweep_smem_per_warp(e);
+    const size_t smem = (size_t)a.wpb * a.smem_per_warp;
+    CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = (e->W + a.wpb - 1) / a.wpb;
+    return launch(e->ks.sweep, grid, 32 * a.wpb, smem, e->stream, &a);
+}
+
+int choose_wpb(vmc_engine *e)
+{
+    if (e->cfg.walkers_per_block > 0) {
+        e->wpb = e->cfg.walkers_per_block;
+        return VMC_OK;
+    }
+    const int per_warp = sweep_smem_per_warp(e);
+    int best = 1, best_warps = -1;
+    for (int wpb : {8, 4, 2, 1}) {
+        const size_t smem = (size_t)wpb * per_warp;
+        if (smem > 227 * 1024) continue;
+        CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int blocks = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, e->ks.sweep, 32 * wpb, smem));
+        if (blocks * wpb > best_warps) {
+            best_warps = blocks * wpb;
+            best = wpb;
+        }
+    }
+    e->wpb = best;
+    return VMC_OK;
+}
+
+// Automatize::setupInitialWeights (automatize.cpp:55-105) with the configured
+// initialWeights method.  Random methods draw from host Philox (stream tag 2).
+int initial_weights(vmc_engine *e)
+{
+    const Config &c = e->cfg;
+    e->theta.assign((size_t)e->E * e->Pmax, 0.0);
+    std::string method = c.initial_weights;
+    double factor = c.weights_factor;
+    bool xavier = false;
+    if (method == "automatize") {
+        const std::string &t = c.trial_label;
+        if (t == "VMC" || t == "BVMC") { method = "constant"; factor = 1.0; }
+        else if (t == "RBM" || t == "RBMSJ" || t == "RBMPJ") { xavier = true; }
+        else if (t == "PRBM") { method = "constant"; factor = 0.0; }
+        else if (t == "SSJ") { method = "randomuniform"; factor = 0.2; }
+        else { method = "randomuniform"; factor = 0.01; }
+    }
+    const unsigned long long s = e->seed;
+    auto uniform = [&](uint32_t i) {
+        const uint4 v = host_philox(make_uint4(i, 0u, 0u, 2u), make_uint2((uint32_t)s, (uint32_t)(s >> 32)));
+        return v.x * 2.3283064365386963e-10;
+    };
+    if (xavier) {  // xavier.cpp:10-23
+        const double lim = 1.0 / std::sqrt((double)e->D);
+        for (size_t i = 0; i < e->theta.size(); ++i) e->theta[i] = -lim + 2 * lim * uniform((uint32_t)i);
+        if (e->E > 3)
+            for (int j = 0; j < e->Pmax; ++j) e->theta[3 * e->Pmax + j] = 0.2 * uniform((uint32_t)(e->theta.size() + j));
+    } else if (method == "constant") {  // constant.cpp:11-26
+        std::fill(e->theta.begin(), e->theta.end(), factor);
+    } else if (method == "randomuniform") {  // randomuniform.cpp (weights)
+        for (size_t i = 0; i < e->theta.size(); ++i) e->theta[i] = factor * uniform((uint32_t)i);
+    } else if (method == "fromfile") {  // fromfile.cpp:30-79
+        std::ifstream in(c.weights_file);
+        if (!in) return fail(VMC_E_CONFIG, "cannot open weights file '" + c.weights_file + "'");
+        std::vector<std::vector<double>> rows;
+        std::string line;
+        while (std::getline(in, line)) {
+            std::istringstream ls(line);
+            std::vector<double> r;
+            double v;
+            while (ls >> v) r.push_back(v);
+            if (!r.empty()) rows.push_back(r);
+        }
+        if ((int)rows.size() != e->E)
+            return fail(VMC_E_CONFIG, "weights file has " + std::to_string(rows.size()) + " rows, expected " + std::to_string(e->E));
+        for (int i = 0; i < e->E; ++i) {
+            if ((int)rows[i].size() != e->Pmax)
+                return fail(VMC_E_CONFIG, "weights file row " + std::to_string(i) + " has " + std::to_string(rows[i].size()) + " values, expected " + std::to_string(e->Pmax));
+            for (int j = 0; j < e->Pmax; ++j) e->theta[(size_t)i * e->Pmax + j] = rows[i][j];
+        }
+    }
+    return VMC_OK;
+}
+
+int refresh_all(vmc_engine *e)
+{
+    if (!e->have_walkers) return VMC_OK;
+    return run_rebuild(e, RB_REFRESH, nullptr);
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+
+extern "C" {
+
+int vmc_abi_version(void) { return VMC_ABI_VERSION; }
+
+const char *vmc_last_error(void) { return g_last_error.c_str(); }
+
+int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
+{
+    if (!text || !out) return fail(VMC_E_ARG, "null argument");
+    *out = nullptr;
+    vmc_engine *e = new vmc_engine();
+    std::string msg = parse_config(text, e->cfg);
+    if (!msg.empty()) {
+        delete e;
+        return fail(VMC_E_CONFIG, msg);
+    }
+    Config &c = e->cfg;
+    if (opt) {
+        e->device = opt->device;
+        if (opt->precision >= 0) c.precision = opt->precision;
+        if (opt->num_walkers > 0) c.walkers = opt->num_walkers;
+        if (opt->walkers_per_block > 0) c.walkers_per_block = opt->walkers_per_block;
+        if (opt->refresh_interval >= 0) c.refresh_interval = opt->refresh_interval;
+        if (opt->compat >= 0) c.compat = opt->compat;
+    }
+    auto reject = [&](const std::string &m) {
+        delete e;
+        return fail(VMC_E_UNSUPPORTED, m);
+    };
+    if (c.hamiltonian.empty()) return reject("no hamiltonian given (the reference requires one)");
+    if (c.hamiltonian != "harmonicOscillator" && c.hamiltonian != "atomicNucleus")
+        return reject("hamiltonian '" + c.hamiltonian + "' is not on the engine's path");
+    if (c.dim != 2 && c.dim != 3) return reject("numDimensions must be 2 or 3");
+    if (c.elements.empty()) return reject("no wave function elements");
+    if ((int)c.elements.size() > MAX_ELEM) return reject("too many elements");
+    if (c.N < 2 || c.N > MAX_N) return reject("numParticles must be in [2, 64]");
+    int flags = 0;
+    int K = 0;
+    for (int el : c.elements) {
+        switch (el) {
+        case E_GAUSSIAN: flags |= F_GAUSS; break;
+        case E_PADE: flags |= F_PADE; break;
+        case E_HYDROGENLIKE: flags |= F_HYDROGENLIKE; break;
+        case E_SLATER:
+            if (c.basis != "hermite") return reject("Slater determinant needs basis: hermite on this engine");
+            K = closed_shells_2d(c.N, c.dim);
+            if (K < 0) return reject("open shell: numParticles is not a closed shell");
+            if ((c.dim == 2 && K > 7) || (c.dim == 3 && K > 4)) return reject("too many shells");
+            flags |= F_SLATER;
+            break;
+        default: return reject("wave function element not implemented on the engine");
+        }
+    }
+    if (std::count(c.elements.begin(), c.elements.end(), (int)E_PADE) > 1 ||
+        std::count(c.elements.begin(), c.elements.end(), (int)E_GAUSSIAN) > 1 ||
+        std::count(c.elements.begin(), c.elements.end(), (int)E_SLATER) > 1)
+        return reject("repeated element");
+    if (c.coulomb) flags |= F_COULOMB;
+    if (c.hamiltonian == "atomicNucleus") flags |= F_ATOM;
+    if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
+    e->flags = flags;
+    e->K = K;
+    e->compat = c.compat;
+    e->sampling = c.sampling == "bruteForce" ? SAMPLER_BF : SAMPLER_IS;
+    e->precision = c.precision;
+    e->W = c.walkers;
+    if (e->W < 1) return reject("numWalkers must be >= 1");
+    e->N = c.N;
+    e->dim = c.dim;
+    e->D = c.N * c.dim;
+    e->n_orb = K > 0 ? c.N / 2 : 0;
+    e->E = (int)c.elements.size();
+    e->Pmax = 0;
+    for (int el : c.elements) e->Pmax = std::max(e->Pmax, element_parameters(c, el));
+    e->EP = e->E * e->Pmax;
+    e->nacc = 9 + 2 * e->EP;
+    if (e->nacc > 32) return reject("more than 11 parameters per walker is not supported");
+    // userinput.cpp:60-81 with walkers in place of ranks: numSteps is the total
+    // over walkers; each walker burns in its own share times the fraction.
+    e->steps_per_walker = (int)(c.num_steps / e->W);
+    if (e->steps_per_walker < 1) return reject("numSteps smaller than numWalkers");
+    e->burn_in = (int)(e->steps_per_walker * c.eq_fraction);
+    e->batches = c.optimization == "adam" ? 10 : 1;  // adam.h:15, gradientdescent.h:13
+    e->elem_bytes = e->precision == VMC_PRECISION_MIXED ? 4 : 8;
+    e->L = make_layout(e->N, e->dim, e->n_orb, (int)e->elem_bytes);
+    if (!select_set(e->precision, e->dim, K, e->ks)) return reject("no kernel for this shape");
+    e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
+                          : (e->precision == VMC_PRECISION_MIXED ? 4 * e->D : 0);
+    e->seed = c.have_seed ? (unsigned long long)c.seed : 0x5eedULL;
+
+    int rc;
+    if ((rc = [&]() -> int {
+            CUDA_TRY(cudaSetDevice(e->device));
+            CUDA_TRY(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->device));
+            int hrc = hermite_init_device(e->device);
+            if (hrc) return hrc;
+            CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreate(&e->ev0));
+            CUDA_TRY(cudaEventCreate(&e->ev1));
+            const size_t W = e->W;
+            CUDA_TRY(cudaMalloc(&e->d_state, W * e->L.rec * e->elem_bytes));
+            CUDA_TRY(cudaMalloc(&e->d_scal, W * NSCAL * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_acc, W * e->nacc * 2 * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_out, 64 * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_drift, W * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_mask, W * e->N * sizeof(unsigned long long)));
+            CUDA_TRY(cudaMalloc(&e->d_counter, W * sizeof(unsigned long long)));
+            CUDA_TRY(cudaMalloc(&e->d_status, W * sizeof(unsigned)));
+            CUDA_TRY(cudaMemsetAsync(e->d_state, 0, W * e->L.rec * e->elem_bytes, e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_scal, 0, W * NSCAL * sizeof(double), e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc * 2 * sizeof(double), e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_drift, 0, W * sizeof(double), e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_mask, 0xff, W * e->N * sizeof(unsigned long long), e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_counter, 0, W * sizeof(unsigned long long), e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_status, 0, W * sizeof(unsigned), e->stream));
+            return choose_wpb(e);
+        }())) {
+        free_engine(e);
+        return rc;
+    }
+    if ((rc = initial_weights(e))) {
+        free_engine(e);
+        return rc;
+    }
+    const size_t P = e->theta.size();
+    e->opt_m.assign(P, 1.0);  // adam.cpp:35-36 and gradientdescent.cpp/sgd.cpp: ones
+    e->opt_v.assign(P, 1.0);
+    e->gamma_prev = make_params(e).gamma;
+    *out = e;
+    return VMC_OK;
+}
+
+void vmc_destroy(vmc_engine *e) { free_engine(e); }
+
+int vmc_get_info(const vmc_engine *e, vmc_info *o)
+{
+    if (!e || !o) return fail(VMC_E_ARG, "null argument");
+    std::memset(o, 0, sizeof(*o));
+    o->n_particles = e->N;
+    o->n_dimensions = e->dim;
+    o->n_coords = e->D;
+    o->n_elements = e->E;
+    o->p_max = e->Pmax;
+    o->n_walkers = e->W;
+    o->precision = e->precision;
+    o->sampling = e->sampling;
+    o->steps_per_walker = e->steps_per_walker;
+    o->burn_in = e->burn_in;
+    o->batches = e->batches;
+    o->n_iterations = e->cfg.iterations;
+    o->compat = e->compat;
+    o->n_accumulators = e->nacc;
+    o->walkers_per_block = e->wpb;
+    o->refresh_interval = e->refresh_interval;
+    for (int i = 0; i < e->E && i < 8; ++i) o->element_kind[i] = e->cfg.elements[i];
+    return VMC_OK;
+}
+
+int vmc_set_parameters(vmc_engine *e, const double *theta, int n_elements, int p_max)
+{
+    if (!e || !theta) return fail(VMC_E_ARG, "null argument");
+    if (n_elements != e->E || p_max != e->Pmax) return fail(VMC_E_ARG, "parameter shape mismatch");
+    const double old_gamma = make_params(e).gamma;
+    e->theta.assign(theta, theta + (size_t)e->E * e->Pmax);
+    CUDA_TRY(cudaSetDevice(e->device));
+    if (e->have_walkers && (e->flags & Q_PADE_STALE)) {
+        // Pade pairs keep the gamma they were computed with until one of their
+        // particles moves (padejastrow.cpp:65-68 only stores gamma)
+        e->gamma_prev = old_gamma;
+        CUDA_TRY(cudaMemsetAsync(e->d_mask, 0, (size_t)e->W * e->N * sizeof(unsigned long long), e->stream));
+    } else {
+        e->gamma_prev = make_params(e).gamma;
+    }
+    return refresh_all(e);
+}
+
+int vmc_get_parameters(const vmc_engine *e, double *theta, int n_elements, int p_max)
+{
+    if (!e || !theta) return fail(VMC_E_ARG, "null argument");
+    if (n_elements != e->E || p_max != e->Pmax) return fail(VMC_E_ARG, "parameter shape mismatch");
+    std::copy(e->theta.begin(), e->theta.end(), theta);
+    return VMC_OK;
+}
+
+int vmc_init_walkers(vmc_engine *e, const double *pos, uint64_t seed)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    e->seed = seed;
+    const size_t W = e->W;
+    if (pos) {
+        std::vector<char> host(W * e->L.rec * e->elem_bytes, 0);
+        for (size_t w = 0; w < W; ++w)
+            for (int c = 0; c < e->D; ++c) {
+                const double v = pos[w * e->D + c];
+                char *dst = host.data() + (w * e->L.rec + e->L.off_x + c) * e->elem_bytes;
+                if (e->elem_bytes == 8) std::memcpy(dst, &v, 8);
+                else { const float f = (float)v; std::memcpy(dst, &f, 4); }
+            }
+        CUDA_TRY(cudaMemcpyAsync(e->d_state, host.data(), host.size(), cudaMemcpyHostToDevice, e->stream));
+    } else {
+        const bool normal = e->cfg.initial_state == "randomNormal";
+        const double sd = 1.0 / e->cfg.omega;  // randomnormal.cpp:19
+        const int n = e->W * e->D;
+        Layout L = e->L;
+        int Wi = e->W;
+        void *st = e->d_state;
+        unsigned long long sd_seed = seed;
+        int nrm = normal ? 1 : 0;
+        double sdv = sd;
+        void *args[] = {&L, &Wi, &st, &sd_seed, &nrm, &sdv};
+        CUDA_TRY(cudaLaunchKernel(e->ks.initpos, dim3((n + 255) / 256), dim3(256), args, 0, e->stream));
+    }
+    CUDA_TRY(cudaMemsetAsync(e->d_counter, 0, W * sizeof(unsigned long long), e->stream));
+    CUDA_TRY(cudaMemsetAsync(e->d_status, 0, W * sizeof(unsigned), e->stream));
+    CUDA_TRY(cudaMemsetAsync(e->d_mask, 0xff, W * e->N * sizeof(unsigned long long), e->stream));
+    e->gamma_prev = make_params(e).gamma;
+    int rc = run_rebuild(e, RB_INIT, nullptr);
+    if (rc) return rc;
+    std::vector<unsigned> st(W);
+    CUDA_TRY(cudaMemcpyAsync(st.data(), e->d_status, W * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (unsigned s : st)
+        if (s & ST_SINGULAR) return fail(VMC_E_SINGULAR, "singular Slater block at initialisation");
+    e->have_walkers = true;
+    return VMC_OK;
+}
+
+int vmc_get_positions(const vmc_engine *e, double *pos)
+{
+    if (!e || !pos) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    const size_t W = e->W;
+    std::vector<char> host(W * e->L.rec * e->elem_bytes);
+    CUDA_TRY(cudaMemcpyAsync(host.data(), e->d_state, host.size(), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (size_t w = 0; w < W; ++w)
+        for (int c = 0; c < e->D; ++c) {
+            const char *src = host.data() + (w * e->L.rec + e->L.off_x + c) * e->elem_bytes;
+            if (e->elem_bytes == 8) std::memcpy(&pos[w * e->D + c], src, 8);
+            else { float f; std::memcpy(&f, src, 4); pos[w * e->D + c] = f; }
+        }
+    return VMC_OK;
+}
+
+int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *out,
+               double *grad_sum, double *egrad_sum)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    if (!e->have_walkers) return fail(VMC_E_STATE, "vmc_init_walkers first");
+    if (steps < 1 || burn_in < 0 || burn_in >= steps) return fail(VMC_E_ARG, "bad step counts");
+    CUDA_TRY(cudaSetDevice(e->device));
+    const size_t W = e->W;
+    CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc * 2 * sizeof(double), e->stream));
+    const int bs = (steps - burn_in) / e->batches;
+    const int m = iteration % e->batches;
+    double max_drift = 0.0;
+    std::vector<double> drift;
+    CUDA_TRY(cudaMemsetAsync(e->d_drift, 0, W * sizeof(double), e->stream));
+    CUDA_TRY(cudaEventRecord(e->ev0, e->stream));
+    const int chunk = e->refresh_interval > 0 ? e->refresh_interval : e->sweep_chunk;
+    const int n_launch = (steps + chunk - 1) / chunk;
+    while ((int)e->sweep_events.size() < 2 * n_launch) {
+        cudaEvent_t ev;
+        CUDA_TRY(cudaEventCreate(&ev));
+        e->sweep_events.push_back(ev);
+    }
+    int n_refresh = 0, li = 0;
+    for (int off = 0; off < steps; off += chunk, ++li) {
+        SweepArgs a{};
+        a.steps = std::min(chunk, steps - off);
+        a.step_offset = off;
+        a.burn_in = burn_in;
+        a.win_lo = bs * m;
+        a.win_hi = bs * (m + 1);
+        a.seed = e->seed;
+        if (e->d_replay) {
+            if (e->replay_pos + steps > e->replay_len) return fail(VMC_E_ARG, "replay stream exhausted");
+            a.replay = e->d_replay;
+            a.replay_stride = e->replay_len;
+            a.replay_offset = e->replay_pos;
+        }
+        CUDA_TRY(cudaEventRecord(e->sweep_events[2 * li], e->stream));
+        int rc = run_sweep(e, a);
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(e->sweep_events[2 * li + 1], e->stream));
+        if (e->refresh_interval > 0) {
+            rc = run_rebuild(e, RB_REFRESH, e->d_drift);
+            if (rc) return rc;
+            ++n_refresh;
+        }
+    }
+    CUDA_TRY(cudaEventRecord(e->ev1, e->stream));
+    if (e->d_replay) e->replay_pos += steps;
+    reduce_acc_kernel<<<e->nacc, 256, 0, e->stream>>>(e->d_acc, e->W, e->nacc, e->d_out);
+    CUDA_TRY(cudaGetLastError());
+    std::vector<double> sums(e->nacc);
+    CUDA_TRY(cudaMemcpyAsync(sums.data(), e->d_out, e->nacc * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    std::vector<unsigned> st(W);
+    CUDA_TRY(cudaMemcpyAsync(st.data(), e->d_status, W * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    if (n_refresh) {
+        drift.resize(W);
+        CUDA_TRY(cudaMemcpyAsync(drift.data(), e->d_drift, W * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    double sweep_ms = 0.0;
+    for (int i = 0; i < n_launch; ++i) {
+        float t = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&t, e->sweep_events[2 * i], e->sweep_events[2 * i + 1]));
+        sweep_ms += t;
+    }
+    for (double d : drift) max_drift = std::max(max_drift, d);
+    vmc_sums s{};
+    s.energy = sums[0];
+    s.energy2 = sums[1];
+    s.kinetic = sums[2];
+    s.kinetic2 = sums[3];
+    s.external = sums[4];
+    s.external2 = sums[5];
+    s.interaction = sums[6];
+    s.interaction2 = sums[7];
+    s.accepts = sums[8];
+    s.n_samples = (double)W * (steps - burn_in);
+    s.n_window = (double)W * bs;
+    s.seconds = ms * 1e-3;
+    s.sweep_seconds = sweep_ms * 1e-3;
+    s.sweep_launches = n_launch;
+    s.max_drift = max_drift;
+    for (unsigned v : st) s.status |= v;
+    e->last = s;
+    e->last_samples_per_walker = steps - burn_in;
+    if (out) *out = s;
+    if (grad_sum) std::copy(sums.begin() + 9, sums.begin() + 9 + e->EP, grad_sum);
+    if (egrad_sum) std::copy(sums.begin() + 9 + e->EP, sums.begin() + 9 + 2 * e->EP, egrad_sum);
+    return VMC_OK;
+}
+
+int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy)
+{
+    if (!e || !mean_energy) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    std::vector<double> col((size_t)e->W * 2);
+    CUDA_TRY(cudaMemcpy2DAsync(col.data(), 2 * sizeof(double), e->d_acc, e->nacc * 2 * sizeof(double),
+                               2 * sizeof(double), e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    const double n = std::max(1.0, e->last_samples_per_walker);
+    for (int w = 0; w < e->W; ++w) mean_energy[w] = (col[2 * w] + col[2 * w + 1]) / n;
+    return VMC_OK;
+}
+
+int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    const int steps = e->steps_per_walker + e->burn_in;
+    std::vector<double> g(e->EP), ge(e->EP);
+    vmc_sums s{};
+    int rc = vmc_sample(e, iteration, steps, e->burn_in, &s, g.data(), ge.data());
+    if (rc) return rc;
+    // Sampler::computeAverages (sampler.cpp:194-226)
+    const double M = s.n_samples;
+    vmc_averages a{};
+    a.energy = s.energy / M;
+    a.kinetic = s.kinetic / M;
+    a.external = s.external / M;
+    a.interaction = s.interaction / M;
+    const double var = (s.energy2 / M - a.energy * a.energy) / M;
+    a.std_error = var > 0 ? std::sqrt(var) : 0.0;
+    a.acceptance = s.accepts / M;
+    if (e->W > 1) {
+        std::vector<double> we(e->W);
+        rc = vmc_get_walker_energies(e, we.data());
+        if (rc) return rc;
+        double mu = 0.0, v2 = 0.0;
+        for (double x : we) mu += x;
+        mu /= e->W;
+        for (double x : we) v2 += (x - mu) * (x - mu);
+        a.walker_std_error = std::sqrt(v2 / (e->W - 1) / e->W);
+    }
+    if (std::isnan(a.kinetic)) {
+        if (out) *out = a;
+        return fail(VMC_E_NAN, "Energy exploded, please decrease the learning rate");
+    }
+    // Optimization::getEnergyGradient (optimization.cpp:10-16)
+    const size_t P = e->theta.size();
+    std::vector<double> grad(P), delta(P);
+    for (size_t i = 0; i < P; ++i) {
+        const double dg = g[i] / s.n_window, dge = ge[i] / s.n_window;
+        grad[i] = 2.0 * (dge - a.energy * dg);
+    }
+    e->opt_step += 1;
+    const double eta = e->cfg.eta;
+    if (e->cfg.optimization == "adam") {  // adam.cpp:22-37
+        const double b1 = 0.89, b2 = 0.999, eps = 1e-8;
+        for (size_t i = 0; i < P; ++i) {
+            e->opt_m[i] = b1 * e->opt_m[i] + (1 - b1) * grad[i];
+            e->opt_v[i] = b2 * e->opt_v[i] + (1 - b2) * grad[i] * grad[i];
+            const double mh = e->opt_m[i] / (1 - std::pow(b1, e->opt_step));
+            const double vh = e->opt_v[i] / (1 - std::pow(b2, e->opt_step));
+            delta[i] = eta * mh / (std::sqrt(vh) + eps);
+        }
+    } else {  // gradientdescent.cpp:24-29, sgd.cpp:23-28
+        const double mono = 1.0 / std::pow((double)e->opt_step, e->cfg.opt_power);
+        for (size_t i = 0; i < P; ++i) {
+            e->opt_v[i] = e->cfg.opt_gamma * e->opt_v[i] + eta * grad[i] * mono;
+            delta[i] = e->opt_v[i];
+        }
+    }
+    std::vector<double> th(e->theta);
+    for (size_t i = 0; i < P; ++i) th[i] -= delta[i];  // system.cpp:114
+    rc = vmc_set_parameters(e, th.data(), e->E, e->Pmax);
+    if (rc) return rc;
+    if (out) *out = a;
+    return VMC_OK;
+}
+
+int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    if (!e->have_walkers) {
+        int rc = vmc_init_walkers(e, nullptr, e->seed);
+        if (rc) return rc;
+    }
+    for (int it = 0; it < e->cfg.iterations; ++it) {
+        vmc_averages a{};
+        int rc = vmc_run_iteration(e, it, &a);
+        if (history && it < n_history) history[it] = a;
+        if (rc) return rc;
+    }
+    return VMC_OK;
+}
+
+int vmc_eval(vmc_engine *e, double *grad, double *lap, double *pgrad, double *energies)
+{
+    if (!e || !grad || !lap || !pgrad || !energies) return fail(VMC_E_ARG, "null argument");
+    if (!e->have_walkers) return fail(VMC_E_STATE, "vmc_init_walkers first");
+    CUDA_TRY(cudaSetDevice(e->device));
+    const size_t W = e->W;
+    double *d = nullptr;
+    const size_t ng = W * e->E * e->D, nl = W * e->E, np = W * e->E * e->Pmax, ne = W * 3;
+    CUDA_TRY(cudaMalloc(&d, (ng + nl + np + ne) * sizeof(double)));
+    EvalArgs a{};
+    a.P = make_params(e);
+    a.p_max = e->Pmax;
+    a.grad = d;
+    a.lap = d + ng;
+    a.pgrad = d + ng + nl;
+    a.energies = d + ng + nl + np;
+    int rc = launch(e->ks.eval, (e->W + 3) / 4, 128, 0, e->stream, &a);
+    if (rc) { cudaFree(d); return rc; }
+    std::vector<double> h(ng + nl + np + ne);
+    cudaError_t ce = cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    cudaFree(d);
+    if (ce != cudaSuccess) return fail(VMC_E_CUDA, cudaGetErrorString(ce));
+    std::copy(h.begin(), h.begin() + ng, grad);
+    std::copy(h.begin() + ng, h.begin() + ng + nl, lap);
+    std::copy(h.begin() + ng + nl, h.begin() + ng + nl + np, pgrad);
+    std::copy(h.begin() + ng + nl + np, h.end(), energies);
+    return VMC_OK;
+}
+
+int vmc_probe_move(vmc_engine *e, const int *k, const double *xnew, double *ratios)
+{
+    if (!e || !k || !xnew || !ratios) return fail(VMC_E_ARG, "null argument");
+    if (!e->have_walkers) return fail(VMC_E_STATE, "vmc_init_walkers first");
+    CUDA_TRY(cudaSetDevice(e->device));
+    const size_t W = e->W;
+    for (size_t w = 0; w < W; ++w)
+        if (k[w] < 0 || k[w] >= e->D) return fail(VMC_E_ARG, "coordinate out of range");
+    int *dk = nullptr;
+    double *dx = nullptr, *dr = nullptr;
+    CUDA_TRY(cudaMalloc(&dk, W * sizeof(int)));
+    CUDA_TRY(cudaMalloc(&dx, W * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&dr, W * e->E * sizeof(double)));
+    CUDA_TRY(cudaMemcpyAsync(dk, k, W * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(dx, xnew, W * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    SweepArgs a{};
+    a.steps = 1;
+    a.step_offset = 0;
+    a.burn_in = 1 << 30;
+    a.win_lo = a.win_hi = 0;
+    a.seed = e->seed;
+    a.probe_k = dk;
+    a.probe_x = dx;
+    a.probe_ratio = dr;
+    int rc = run_sweep(e, a);
+    cudaError_t ce = cudaSuccess;
+    if (!rc) {
+        ce = cudaMemcpyAsync(ratios, dr, W * e->E * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    }
+    cudaFree(dk);
+    cudaFree(dx);
+    cudaFree(dr);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return fail(VMC_E_CUDA, cudaGetErrorString(ce));
+    return VMC_OK;
+}
+
+int vmc_set_replay(vmc_engine *e, const double *stream, int length)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    cudaFree(e->d_replay);
+    e->d_replay = nullptr;
+    e->replay_len = e->replay_pos = 0;
+    if (!stream) return VMC_OK;
+    if (length < 1) return fail(VMC_E_ARG, "bad replay length");
+    const size_t bytes = (size_t)e->W * length * 3 * sizeof(double);
+    CUDA_TRY(cudaMalloc(&e->d_replay, bytes));
+    CUDA_TRY(cudaMemcpyAsync(e->d_replay, stream, bytes, cudaMemcpyHostToDevice, e->stream));
+    e->replay_len = length;
+    return VMC_OK;
+}
+
+int vmc_replay(vmc_engine *e, const double *stream, int steps, uint8_t *accepted, double *energies)
+{
+    if (!e || steps < 1) return fail(VMC_E_ARG, "bad argument");
+    if (!e->have_walkers) return fail(VMC_E_STATE, "vmc_init_walkers first");
+    CUDA_TRY(cudaSetDevice(e->device));
+    const size_t W = e->W;
+    double *ds = nullptr, *den = nullptr;
+    unsigned char *dacc = nullptr;
+    if (stream) {
+        CUDA_TRY(cudaMalloc(&ds, W * steps * 3 * sizeof(double)));
+        CUDA_TRY(cudaMemcpyAsync(ds, stream, W * steps * 3 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    }
+    CUDA_TRY(cudaMalloc(&dacc, W * steps));
+    CUDA_TRY(cudaMalloc(&den, W * steps * 3 * sizeof(double)));
+    SweepArgs a{};
+    a.steps = steps;
+    a.step_offset = 0;
+    a.burn_in = 1 << 30;
+    a.seed = e->seed;
+    a.replay = ds;  // null: the engine's Philox streams
+    a.replay_stride = steps;
+    a.rec_acc = dacc;
+    a.rec_en = den;
+    a.rec_stride = steps;
+    int rc = run_sweep(e, a);
+    cudaError_t ce = cudaSuccess;
+    if (!rc) {
+        if (accepted) ce = cudaMemcpyAsync(accepted, dacc, W * steps, cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess && energies)
+            ce = cudaMemcpyAsync(energies, den, W * steps * 3 * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    }
+    cudaFree(ds);
+    cudaFree(dacc);
+    cudaFree(den);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return fail(VMC_E_CUDA, cudaGetErrorString(ce));
+    return VMC_OK;
+}
+
+int vmc_get_status(const vmc_engine *e, uint32_t *status)
+{
+    if (!e || !status) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    CUDA_TRY(cudaMemcpyAsync(status, e->d_status, e->W * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return VMC_OK;
+}
+
+int vmc_stopwatch(vmc_engine *e, int mode, double *ms)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    if (!e->sw0) {
+        CUDA_TRY(cudaEventCreate(&e->sw0));
+        CUDA_TRY(cudaEventCreate(&e->sw1));
+    }
+    if (mode == 0) {
+        CUDA_TRY(cudaEventRecord(e->sw0, e->stream));
+        return VMC_OK;
+    }
+    CUDA_TRY(cudaEventRecord(e->sw1, e->stream));
+    CUDA_TRY(cudaEventSynchronize(e->sw1));
+    float t = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&t, e->sw0, e->sw1));
+    if (ms) *ms = t;
+    return VMC_OK;
+}
+
+int vmc_measure_fma_peak(int device, int precision, double *tflops)
+{
+    if (!tflops) return fail(VMC_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(device));
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int threads = 256, blocks = sms * 8, iters = precision == VMC_PRECISION_MIXED ? 4096 : 1024;
+    float *out = nullptr;
+    CUDA_TRY(cudaMalloc(&out, (size_t)blocks * threads * sizeof(double)));
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    double best = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+        CUDA_TRY(cudaEventRecord(a));
+        if (precision == VMC_PRECISION_MIXED)
+            fma_peak_kernel<float><<<blocks, threads>>>(reinterpret_cast<float *>(out), iters, 1.0f + 1e-7f);
+        else
+            fma_peak_kernel<double><<<blocks, threads>>>(reinterpret_cast<double *>(out), iters, 1.0 + 1e-15);
+        CUDA_TRY(cudaEventRecord(b));
+        CUDA_TRY(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+        const double flops = 2.0 * FMA_CHAINS * (double)iters * blocks * threads;
+        if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    *tflops = best;
+    return VMC_OK;
+}
+
+}  // extern "C"
