@@ -12,8 +12,9 @@ Workload (one "step" = one optimisation iteration of the whole walker population
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
-N > 1: one process per GPU (torchrun), walkers per GPU fixed (weak scaling), the
-only collective is the barrier and the max-over-ranks timing.
+N > 1: one process per GPU (torchrun), walkers per GPU fixed (weak scaling); the
+only exchange per iteration is the NCCL all-reduce of the sampler totals
+(vmachine_b200.distributed), plus the barrier and the max-over-ranks timing.
 """
 import argparse
 import json
@@ -50,17 +51,18 @@ def workload_text(walkers, steps_per_walker, precision, seed):
 
 def flops_per_step(N, d=2):
     """Algorithmic flops of one accepted move plus one E_L / dlnPsi sample in the
-    engine's incremental scheme (FMA = 2, MUL/ADD = 1, div/sqrt/exp = 1); the count
-    is derived term by term in DESIGN.md."""
+    engine's incremental, degree-factorised scheme (FMA = 2, MUL/ADD = 1,
+    div/sqrt/exp = 1); derived term by term in DESIGN.md."""
     n = N // 2
-    K = {1: 1, 3: 2, 6: 3, 10: 4, 15: 5, 21: 6, 28: 7}[n]
-    tables = d * 4 * (K - 1)                     # Hermite recurrence at one point
-    ratio = tables + n * (d - 1) + 2 * n * n     # new orbital row, S_j = row . inv[:, j]
-    pairs = (N - 1) * (12 * d + 40)              # Pade/Coulomb terms of the moved particle
-    sm = 2 * n * n                               # Sherman-Morrison rank-1 update
-    deriv = n * (d * (4 * (K - 1) + 2 * K) + n * (10 if d == 2 else 18))  # d ln det refresh
+    K = next(k for k in range(1, 12) if (k * (k + 1) // 2 if d == 2 else k * (k + 1) * (k + 2) // 6) == n)
+    tables = d * 4 * (K - 1)                             # Hermite recurrence at one point
+    ratio = tables + n * (2 * n + 2 * K)                 # S_j = phi(r_p') . inv[:, j], all j
+    sm = 2 * n * n                                       # Sherman-Morrison rank-1 update
+    per_orbital = 4 if d == 2 else 9
+    deriv = n * (tables + per_orbital * n + 3 * d * (2 * K - 3))  # d ln det refresh of the block
+    pairs = (N - 1) * (10 * d + 38)                      # Pade / Coulomb terms of the moved particle
     kinetic = 7 * N * d
-    return ratio + pairs + sm + deriv + kinetic + 40
+    return ratio + sm + deriv + pairs + kinetic + 40
 
 
 class ClockSampler:
@@ -235,6 +237,7 @@ def max_over_ranks(pg, local, v):
 def run_engine_arm(args):
     world, rank, local, pg = dist_setup(args)
     from vmachine_b200 import Engine, measure_fma_peak
+    from vmachine_b200 import distributed as vd
     W, spw = args.walkers, args.steps_per_walker
     seed = 1000 + rank
     text = workload_text(W, spw, "mixed", seed)
@@ -243,18 +246,20 @@ def run_engine_arm(args):
     burn = eng.info.burn_in
     moves_per_step = W * (spw + burn)
     for it in range(args.warmup):
-        eng.run_iteration(it)
+        vd.run_iteration(eng, it)
     barrier(pg, local)
     sweep_s, launches, sig = 0.0, 0.0, []
     with ClockSampler(local) as clk:
         eng.stopwatch_start()
         for it in range(args.steps):
-            a = eng.run_iteration(args.warmup + it)
+            a = vd.run_iteration(eng, args.warmup + it)  # all-reduce of the sums when N > 1
             sig.append(a.walker_std_error)
         ms = eng.stopwatch_stop()
     # per-launch sweep timing of one more iteration (same work, not in the timed region)
     sums, _, _ = eng.sample(args.warmup + args.steps, spw + burn, burn)
     sweep_s, launches = sums.sweep_seconds, sums.sweep_launches
+    max_drift = sums.max_drift
+    refresh_now = eng.refresh_interval()
     ms = max_over_ranks(pg, local, ms)
     total_moves = moves_per_step * args.steps * world
     value = total_moves / (ms * 1e-3)
@@ -271,12 +276,12 @@ def run_engine_arm(args):
         eng.stopwatch_start()
         for it in range(args.e2e_steps):
             eng.init_walkers(pos, seed=seed)
-            eng.run_iteration(1000 + it)
+            vd.run_iteration(eng, 1000 + it)
             pos = eng.positions()
         e2e_ms = max_over_ranks(pg, local, eng.stopwatch_stop())
         e2e = {"value": moves_per_step * args.e2e_steps * world / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "vmc_init_walkers(host positions) + vmc_run_iteration + "
+               "path": "vmc_init_walkers(host positions) + vmc_sample + vmc_apply_sums + "
                        "vmc_get_positions per step"}
 
     # FP64 engine on the same workload (same walkers, fewer steps per iteration)
@@ -284,10 +289,10 @@ def run_engine_arm(args):
     if not args.no_fp64:
         eng64 = Engine(workload_text(W, args.fp64_steps_per_walker, "fp64", seed), device=local)
         eng64.init_walkers(None, seed=seed)
-        eng64.run_iteration(0)
+        vd.run_iteration(eng64, 0)
         barrier(pg, local)
         eng64.stopwatch_start()
-        a64 = eng64.run_iteration(1)
+        a64 = vd.run_iteration(eng64, 1)
         ms64 = max_over_ranks(pg, local, eng64.stopwatch_stop())
         mv64 = W * (args.fp64_steps_per_walker + eng64.info.burn_in) * world
         fp64 = {"value": mv64 / (ms64 * 1e-3), "ms_per_step": ms64,
@@ -313,7 +318,8 @@ def run_engine_arm(args):
                                f"28x28) x Gaussian x Pade, Coulomb, importance sampling "
                                f"dt={DT}, E_L + dlnPsi every move, ADAM",
                    "walkers_per_gpu": W, "steps_per_walker": spw, "burn_in": burn,
-                   "precision": "mixed", "refresh_interval": eng.info.refresh_interval,
+                   "precision": "mixed", "refresh_interval": refresh_now,
+                   "max_inverse_drift": max_drift,
                    "walkers_per_block": eng.info.walkers_per_block,
                    "l2": "walker state %.0f MB per GPU > 126 MB L2, streamed every launch"
                          % (W * (eng.info.n_coords * 5 * 4 + 2 * 28 * 28 * 4 + 56 * 8 + 64) / 1e6)},

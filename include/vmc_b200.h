@@ -127,6 +127,15 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
  * gradientdescent.cpp:24-29), parameter update.  Returns the averages. */
 int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out);
 
+/* The host half of an iteration, from totals that may be summed over several
+ * engines (one per GPU): averages (Sampler::computeAverages, sampler.cpp:194-226),
+ * the optimiser step and the parameter update (system.cpp:110-137).  Every engine
+ * that applies the same totals ends with the same parameters, which is what the
+ * reference's MPI_Reduce + MPI_Bcast achieve (sampler.cpp:111-187,
+ * system.cpp:130-135).  vmc_run_iteration = vmc_sample + vmc_apply_sums. */
+int vmc_apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum,
+                   const double *egrad_sum, vmc_averages *out);
+
 /* Per-walker sampled-energy means of the last vmc_sample (W values). */
 int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy);
 

@@ -3,11 +3,13 @@
     python -m vmachine_b200.build [--verbose-ptxas]
 
 nvcc cross-compiles without a GPU, so this runs in the build container; the
-resulting .so travels with the source tree.
+resulting .so travels with the source tree.  The translation units compile in
+parallel: the host engine, and the FP32 and FP64 kernel instantiations.
 """
 import os
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -15,8 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvmc_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["vmc_engine.cu", "vmc_config.cpp"]
-HEADERS = ["vmc_device.cuh", "vmc_kernels.cuh", "vmc_config.hpp"]
+SOURCES = ["vmc_engine.cu", "vmc_inst_f32.cu", "vmc_inst_f64.cu", "vmc_config.cpp"]
+HEADERS = ["vmc_device.cuh", "vmc_kernels.cuh", "vmc_sweep.cuh", "vmc_config.hpp"]
+FLAGS = ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 
 def _stale():
@@ -31,12 +34,19 @@ def _stale():
 def build(force=False, verbose_ptxas=False):
     if not force and not _stale():
         return LIB
-    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", LIB,
-           *[os.path.join(CSRC, f) for f in SOURCES]]
-    if verbose_ptxas:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    inc = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+    extra = ["-Xptxas=-v"] if verbose_ptxas else []
+    with tempfile.TemporaryDirectory(prefix="vmc_build_") as tmp:
+        procs, objs = [], []
+        for src in SOURCES:
+            obj = os.path.join(tmp, src + ".o")
+            objs.append(obj)
+            cmd = [NVCC, *ARCH, *FLAGS, *extra, *inc, "-c", os.path.join(CSRC, src), "-o", obj]
+            procs.append((src, subprocess.Popen(cmd)))
+        failed = [src for src, p in procs if p.wait() != 0]
+        if failed:
+            raise RuntimeError(f"nvcc failed on {failed}")
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], check=True)
     return LIB
 
 

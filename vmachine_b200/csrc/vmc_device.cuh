@@ -25,7 +25,14 @@ enum : int {
     Q_IS_GREEN = 1 << 7,     // importance-sampling Green's ratio with the cached force
     Q_PADE_STALE = 1 << 8,   // Pade pairs keep the previous gamma until their particle moves
     F_HYDROGENLIKE = 1 << 9, // exp(-alpha Z sum r_i)
+    F_IS = 1 << 10,          // importance sampling (else brute force)
 };
+
+// Flag sets with a compiled-in sweep: the 2D quantum dot, Slater x Gaussian x Pade
+// with Coulomb and importance sampling, with and without the reference quirks.
+constexpr int FX_DOT_COMPAT = F_GAUSS | F_SLATER | F_PADE | F_COULOMB | F_IS | Q_PADE_RATIO |
+                              Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
+constexpr int FX_DOT_CORRECTED = F_GAUSS | F_SLATER | F_PADE | F_COULOMB | F_IS;
 
 enum : int { SAMPLER_IS = 0, SAMPLER_BF = 1 };
 
@@ -82,13 +89,14 @@ __device__ __forceinline__ double vexp(double x) { return exp(x); }
 //   h_{m+1} = A_m x h_m - B_m h_{m-1},  A_m = sqrt(2/(m+1)), B_m = sqrt(m/(m+1))
 //   h'_m = C_m h_{m-1},  C_m = sqrt(2m);   h''_m = E_m h_{m-2},  E_m = 2 sqrt(m(m-1))
 // Filled once per device from the host (same double expressions as the CPU oracle).
-// Defined here: the engine is a single translation unit.
+// One copy per translation unit (internal linkage); each precision's kernel unit
+// uploads its own copy.
 constexpr int HMAX = 24;
 struct HermiteCoef {
     double A[HMAX], B[HMAX], C[HMAX], E[HMAX];
     float Af[HMAX], Bf[HMAX], Cf[HMAX], Ef[HMAX];
 };
-__constant__ HermiteCoef c_herm;
+static __constant__ HermiteCoef c_herm;
 
 template <typename R> __device__ __forceinline__ R hA(int m);
 template <> __device__ __forceinline__ double hA<double>(int m) { return c_herm.A[m]; }

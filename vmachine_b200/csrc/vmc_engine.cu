@@ -19,6 +19,32 @@
 
 using namespace vmc;
 
+namespace vmc {
+// Deterministic compensated reduction of the per-walker accumulators:
+// one block, thread group per accumulator, fixed summation order.
+__global__ void reduce_acc_kernel(const double *acc, int W, int nacc, double *out)
+{
+    const int a = blockIdx.x;  // accumulator index
+    double s = 0.0, c = 0.0;
+    for (int w = threadIdx.x; w < W; w += blockDim.x) {
+        kadd(s, c, acc[((size_t)w * nacc + a) * 2]);
+        kadd(s, c, acc[((size_t)w * nacc + a) * 2 + 1]);
+    }
+    __shared__ double ss[256], cc[256];
+    ss[threadIdx.x] = s;
+    cc[threadIdx.x] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S = 0.0, C = 0.0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            kadd(S, C, ss[t]);
+            kadd(S, C, cc[t]);
+        }
+        out[a] = S + C;
+    }
+}
+}  // namespace vmc
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -36,54 +62,21 @@ int fail(int code, const std::string &msg)
             return fail(VMC_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
     } while (0)
 
-struct KernelSet {
-    const void *sweep = nullptr, *rebuild = nullptr, *eval = nullptr, *initpos = nullptr;
-};
+}  // namespace
 
-template <typename T, int DIM, int K>
-KernelSet make_set()
-{
-    KernelSet s;
-    s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K>);
-    s.rebuild = reinterpret_cast<const void *>(&rebuild_kernel<T, DIM, K>);
-    s.eval = reinterpret_cast<const void *>(&eval_kernel<T, DIM, K>);
-    s.initpos = reinterpret_cast<const void *>(&initial_positions_kernel<T>);
-    return s;
-}
+namespace vmc {
+bool select_kernels_f32(int dim, int K, int flags, KernelSet &out);
+bool select_kernels_f64(int dim, int K, int flags, KernelSet &out);
+cudaError_t upload_hermite_f32(const HermiteCoef &h);
+cudaError_t upload_hermite_f64(const HermiteCoef &h);
+}  // namespace vmc
 
-template <typename T>
-bool select_set_t(int dim, int K, KernelSet &out)
-{
-    if (dim == 2) {
-        switch (K) {
-        case 0: out = make_set<T, 2, 0>(); return true;
-        case 1: out = make_set<T, 2, 1>(); return true;
-        case 2: out = make_set<T, 2, 2>(); return true;
-        case 3: out = make_set<T, 2, 3>(); return true;
-        case 4: out = make_set<T, 2, 4>(); return true;
-        case 5: out = make_set<T, 2, 5>(); return true;
-        case 6: out = make_set<T, 2, 6>(); return true;
-        case 7: out = make_set<T, 2, 7>(); return true;
-        default: return false;
-        }
-    }
-    if (dim == 3) {
-        switch (K) {
-        case 0: out = make_set<T, 3, 0>(); return true;
-        case 1: out = make_set<T, 3, 1>(); return true;
-        case 2: out = make_set<T, 3, 2>(); return true;
-        case 3: out = make_set<T, 3, 3>(); return true;
-        case 4: out = make_set<T, 3, 4>(); return true;
-        default: return false;
-        }
-    }
-    return false;
-}
+namespace {
 
-bool select_set(int precision, int dim, int K, KernelSet &out)
+bool select_set(int precision, int dim, int K, int flags, KernelSet &out)
 {
-    return precision == VMC_PRECISION_MIXED ? select_set_t<float>(dim, K, out)
-                                            : select_set_t<double>(dim, K, out);
+    return precision == VMC_PRECISION_MIXED ? select_kernels_f32(dim, K, flags, out)
+                                            : select_kernels_f64(dim, K, flags, out);
 }
 
 uint4 host_philox(uint4 c, uint2 k)
@@ -113,7 +106,8 @@ int hermite_init_device(int device)
         h.Cf[m] = (float)h.C[m];
         h.Ef[m] = (float)h.E[m];
     }
-    CUDA_TRY(cudaMemcpyToSymbol(c_herm, &h, sizeof(h)));
+    CUDA_TRY(upload_hermite_f32(h));
+    CUDA_TRY(upload_hermite_f64(h));
     if (device < 64) done[device] = true;
     return VMC_OK;
 }
@@ -129,6 +123,8 @@ struct vmc_engine {
     int precision = 0, compat = 1, flags = 0, sampling = 0;
     int steps_per_walker = 0, burn_in = 0, batches = 1;
     int wpb = 0, refresh_interval = 0, sweep_chunk = 2048;
+    bool refresh_auto = false;          // refreshInterval: auto (mixed precision)
+    double drift_tol = 1e-4;            // inverse drift that halves the interval
     size_t elem_bytes = 8;
     Layout L{};
     KernelSet ks;
@@ -152,6 +148,7 @@ struct vmc_engine {
     // last sampling pass
     vmc_sums last{};
     double last_samples_per_walker = 0.0;
+    double last_walker_std_error = 0.0;
 };
 
 namespace {
@@ -240,7 +237,8 @@ int launch(const void *fn, int grid, int block, size_t smem, cudaStream_t st, vo
 
 int sweep_smem_per_warp(const vmc_engine *e)
 {
-    return round_up(e->L.rec * (int)e->elem_bytes + e->N * 8, 16);
+    const int staged = e->L.rec;  // the whole record (InvInRegisters is off for every shape)
+    return round_up(staged * (int)e->elem_bytes + e->N * 8 + NSCAL * 8, 16);
 }
 
 int run_rebuild(vmc_engine *e, int mode, double *drift)
@@ -275,8 +273,11 @@ int choose_wpb(vmc_engine *e)
         return VMC_OK;
     }
     const int per_warp = sweep_smem_per_warp(e);
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, e->ks.sweep));
     int best = 1, best_warps = -1;
     for (int wpb : {8, 4, 2, 1}) {
+        if (32 * wpb > fa.maxThreadsPerBlock) continue;
         const size_t smem = (size_t)wpb * per_warp;
         if (smem > 227 * 1024) continue;
         CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -415,6 +416,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     if (c.coulomb) flags |= F_COULOMB;
     if (c.hamiltonian == "atomicNucleus") flags |= F_ATOM;
     if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
+    if (c.sampling != "bruteForce") flags |= F_IS;
     e->flags = flags;
     e->K = K;
     e->compat = c.compat;
@@ -440,9 +442,10 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     e->batches = c.optimization == "adam" ? 10 : 1;  // adam.h:15, gradientdescent.h:13
     e->elem_bytes = e->precision == VMC_PRECISION_MIXED ? 4 : 8;
     e->L = make_layout(e->N, e->dim, e->n_orb, (int)e->elem_bytes);
-    if (!select_set(e->precision, e->dim, K, e->ks)) return reject("no kernel for this shape");
+    if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) return reject("no kernel for this shape");
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
                           : (e->precision == VMC_PRECISION_MIXED ? 4 * e->D : 0);
+    e->refresh_auto = c.refresh_interval < 0 && e->precision == VMC_PRECISION_MIXED;
     e->seed = c.have_seed ? (unsigned long long)c.seed : 0x5eedULL;
 
     int rc;
@@ -669,6 +672,12 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         sweep_ms += t;
     }
     for (double d : drift) max_drift = std::max(max_drift, d);
+    if (e->refresh_auto && n_refresh) {
+        // FP64 re-inversion cadence against the measured drift of the FP32
+        // Sherman-Morrison inverse: halve past the tolerance, double well below it
+        if (max_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
+        else if (max_drift < e->drift_tol / 16) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
+    }
     vmc_sums s{};
     s.energy = sums[0];
     s.energy2 = sums[1];
@@ -688,6 +697,17 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
     for (unsigned v : st) s.status |= v;
     e->last = s;
     e->last_samples_per_walker = steps - burn_in;
+    e->last_walker_std_error = 0.0;
+    if (e->W > 1) {  // independent chains: spread of the per-walker means
+        std::vector<double> we(e->W);
+        const int rc = vmc_get_walker_energies(e, we.data());
+        if (rc) return rc;
+        double mu = 0.0, v2 = 0.0;
+        for (double x : we) mu += x;
+        mu /= e->W;
+        for (double x : we) v2 += (x - mu) * (x - mu);
+        e->last_walker_std_error = std::sqrt(v2 / (e->W - 1) / e->W);
+    }
     if (out) *out = s;
     if (grad_sum) std::copy(sums.begin() + 9, sums.begin() + 9 + e->EP, grad_sum);
     if (egrad_sum) std::copy(sums.begin() + 9 + e->EP, sums.begin() + 9 + 2 * e->EP, egrad_sum);
@@ -707,14 +727,12 @@ int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy)
     return VMC_OK;
 }
 
-int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
+int vmc_apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum,
+                   const double *egrad_sum, vmc_averages *out)
 {
-    if (!e) return fail(VMC_E_ARG, "null argument");
-    const int steps = e->steps_per_walker + e->burn_in;
-    std::vector<double> g(e->EP), ge(e->EP);
-    vmc_sums s{};
-    int rc = vmc_sample(e, iteration, steps, e->burn_in, &s, g.data(), ge.data());
-    if (rc) return rc;
+    if (!e || !total || !grad_sum || !egrad_sum) return fail(VMC_E_ARG, "null argument");
+    const vmc_sums &s = *total;
+    if (!(s.n_samples > 0) || !(s.n_window > 0)) return fail(VMC_E_ARG, "empty totals");
     // Sampler::computeAverages (sampler.cpp:194-226)
     const double M = s.n_samples;
     vmc_averages a{};
@@ -725,16 +743,7 @@ int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
     const double var = (s.energy2 / M - a.energy * a.energy) / M;
     a.std_error = var > 0 ? std::sqrt(var) : 0.0;
     a.acceptance = s.accepts / M;
-    if (e->W > 1) {
-        std::vector<double> we(e->W);
-        rc = vmc_get_walker_energies(e, we.data());
-        if (rc) return rc;
-        double mu = 0.0, v2 = 0.0;
-        for (double x : we) mu += x;
-        mu /= e->W;
-        for (double x : we) v2 += (x - mu) * (x - mu);
-        a.walker_std_error = std::sqrt(v2 / (e->W - 1) / e->W);
-    }
+    a.walker_std_error = e->last_walker_std_error;
     if (std::isnan(a.kinetic)) {
         if (out) *out = a;
         return fail(VMC_E_NAN, "Energy exploded, please decrease the learning rate");
@@ -743,7 +752,7 @@ int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
     const size_t P = e->theta.size();
     std::vector<double> grad(P), delta(P);
     for (size_t i = 0; i < P; ++i) {
-        const double dg = g[i] / s.n_window, dge = ge[i] / s.n_window;
+        const double dg = grad_sum[i] / s.n_window, dge = egrad_sum[i] / s.n_window;
         grad[i] = 2.0 * (dge - a.energy * dg);
     }
     e->opt_step += 1;
@@ -766,10 +775,21 @@ int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
     }
     std::vector<double> th(e->theta);
     for (size_t i = 0; i < P; ++i) th[i] -= delta[i];  // system.cpp:114
-    rc = vmc_set_parameters(e, th.data(), e->E, e->Pmax);
+    const int rc = vmc_set_parameters(e, th.data(), e->E, e->Pmax);
     if (rc) return rc;
     if (out) *out = a;
     return VMC_OK;
+}
+
+int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
+{
+    if (!e) return fail(VMC_E_ARG, "null argument");
+    const int steps = e->steps_per_walker + e->burn_in;
+    std::vector<double> g(e->EP), ge(e->EP);
+    vmc_sums s{};
+    const int rc = vmc_sample(e, iteration, steps, e->burn_in, &s, g.data(), ge.data());
+    if (rc) return rc;
+    return vmc_apply_sums(e, &s, g.data(), ge.data(), out);
 }
 
 int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)

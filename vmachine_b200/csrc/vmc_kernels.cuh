@@ -110,424 +110,11 @@ __device__ __forceinline__ bool same_spin(int i, int j, int N)
     return (i < h) == (j < h);
 }
 
-// ------------------------------------------------------------------ sweep kernel
+}  // namespace vmc
 
-template <typename T, int DIM, int K>
-__global__ void __launch_bounds__(256) sweep_kernel(const SweepArgs a)
-{
-    constexpr int NO = K > 0 ? Shells<DIM, K>::n : 0;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Params &P = a.P;
-    const Layout L = P.L;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    T *sm = reinterpret_cast<T *>(smem_raw + (size_t)wib * a.smem_per_warp);
-    unsigned long long *smask = reinterpret_cast<unsigned long long *>(sm + L.rec);
-    T *x = sm + L.off_x, *fc = sm + L.off_fc, *dd = sm + L.off_dd, *sdd = sm + L.off_sdd;
-    T *gj = sm + L.off_gj, *inv = sm + L.off_inv;
-    const int N = P.N, D = L.D, flags = P.flags;
-    const bool is = P.sampling == SAMPLER_IS;
-    const T wa = T(P.omega * P.alpha);
-    const T gam = T(P.gamma), gamp = T(P.gamma_prev);
-    const T az = T(P.alpha_h * P.Z);
-    const double half_dt = 0.5 * P.step, sq_dt = sqrt(P.step);
-    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+#include "vmc_sweep.cuh"
 
-    for (int w = blockIdx.x * a.wpb + wib; w < P.W; w += gridDim.x * a.wpb) {
-        T *g_rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
-        copy_in(sm, g_rec, L.rec, lane);
-        for (int j = lane; j < N; j += 32) smask[j] = P.mask[(size_t)w * N + j];
-        double sc[NSCAL];
-#pragma unroll
-        for (int i = 0; i < NSCAL; ++i) sc[i] = P.scal[(size_t)w * NSCAL + i];
-        double acc_s = 0.0, acc_c = 0.0;
-        if (lane < P.nacc) {
-            acc_s = P.acc[((size_t)w * P.nacc + lane) * 2];
-            acc_c = P.acc[((size_t)w * P.nacc + lane) * 2 + 1];
-        }
-        unsigned long long ctr = P.counter[w];
-        unsigned status = 0;
-        __syncwarp();
-
-        for (int s = 0; s < a.steps; ++s) {
-            const int it_step = a.step_offset + s;
-            // ---- random numbers: coordinate, displacement, acceptance
-            int k;
-            double r1, r2;
-            if (a.probe_k) {
-                k = a.probe_k[w];
-                r1 = 0.0;
-                r2 = 0.0;
-            } else if (a.replay) {
-                const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
-                k = (int)floor(q[0] * D);
-                r1 = q[1];
-                r2 = q[2];
-            } else {
-                const uint4 v = philox(
-                    make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)w, 0u), key);
-                ++ctr;
-                k = (int)__umulhi(v.x, (unsigned)D);
-                if (is) {
-                    if (sizeof(T) == 8) {
-                        const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
-                        r1 = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
-                    } else {
-                        const float u1 = ((float)v.y + 1.0f) * 2.3283064e-10f;
-                        const float u2 = (float)v.z * 2.3283064e-10f;
-                        r1 = (double)(sqrtf(-2.0f * __logf(u1)) * __cosf(6.2831853f * u2));
-                    }
-                } else {
-                    r1 = v.y * TWO_M32;
-                }
-                r2 = v.w * TWO_M32;
-            }
-            const int p = k / DIM, adim = k - p * DIM;
-            const T xo = x[k];
-            T xpo[DIM], xpn[DIM];
-#pragma unroll
-            for (int c = 0; c < DIM; ++c) xpo[c] = x[p * DIM + c];
-
-            // ---- gradient of ln Psi along k at the current point (QuantumForce)
-            T rpo = T(0);
-            if (flags & (F_HYDROGENLIKE | F_ATOM)) {
-                T r2s = T(0);
-#pragma unroll
-                for (int c = 0; c < DIM; ++c) r2s += xpo[c] * xpo[c];
-                rpo = vsqrt(r2s);
-            }
-            T Gk = T(0);
-            if (flags & F_GAUSS) Gk += -wa * xo;
-            if (K > 0) Gk += dd[k];
-            if (flags & F_PADE) Gk += gj[k];
-            if (flags & F_HYDROGENLIKE) Gk += -az * xo / rpo;
-
-            T dx, Fn = T(0), Fo = T(0);
-            if (a.probe_k) {
-                dx = T(a.probe_x[w]) - xo;
-            } else if (is) {
-                Fn = T(2) * Gk;
-                Fo = (flags & Q_IS_GREEN) ? fc[k] : Fn;
-                dx = T(half_dt) * Fn + T(r1) * T(sq_dt);
-            } else {
-                dx = T(10) * (T(r1) - T(0.5)) * T(P.step);
-            }
-            const T xn = a.probe_k ? T(a.probe_x[w]) : xo + dx;
-#pragma unroll
-            for (int c = 0; c < DIM; ++c) xpn[c] = (c == adim) ? xn : xpo[c];
-
-            // ---- Slater: S_j = phi(r_p') . inv[:, j]; R = S_pl
-            T Sj = T(0), R = T(1);
-            int b = 0, pl = 0;
-            if constexpr (K > 0) {
-                b = p / NO;
-                pl = p - b * NO;
-                T hv[DIM][K];
-#pragma unroll
-                for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
-                const T *invb = inv + b * NO * NO;
-                if (lane < NO) {
-                    for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
-                        T phi = hv[0][m0] * hv[1][m1];
-                        if (DIM == 3) phi *= hv[DIM - 1][m2];
-                        Sj += phi * invb[o * NO + lane];
-                    });
-                }
-                R = __shfl_sync(FULL, Sj, pl);
-            }
-
-            // ---- pair terms of the moved particle (Pade, Coulomb)
-            T sum_ratio = T(0), d_lap = T(0), d_bh2 = T(0), d_vint = T(0);
-            T gp_new[DIM], gdel[2][DIM];
-#pragma unroll
-            for (int c = 0; c < DIM; ++c) { gp_new[c] = T(0); gdel[0][c] = T(0); gdel[1][c] = T(0); }
-            if (flags & (F_PADE | F_COULOMB)) {
-                const unsigned long long mp = smask[p];
-#pragma unroll
-                for (int jj = 0; jj < 2; ++jj) {
-                    const int j = lane + 32 * jj;
-                    if (j < N && j != p) {
-                        T dxo[DIM], dxn[DIM], r2o = T(0), r2n = T(0);
-#pragma unroll
-                        for (int c = 0; c < DIM; ++c) {
-                            const T xj = x[j * DIM + c];
-                            dxo[c] = xpo[c] - xj;
-                            dxn[c] = xpn[c] - xj;
-                            r2o += dxo[c] * dxo[c];
-                            r2n += dxn[c] * dxn[c];
-                        }
-                        const T ro = vsqrt(r2o), rn = vsqrt(r2n);
-                        const T iro = T(1) / ro, irn = T(1) / rn;
-                        if (flags & F_PADE) {
-                            const T beta = same_spin(p, j, N) ? T(P.beta_same) : T(P.beta_anti);
-                            const T gpair = ((flags & Q_PADE_STALE) && !((mp >> j) & 1ull)) ? gamp : gam;
-                            const T fo1 = T(1) / (T(1) + gpair * ro), fo = beta * fo1 * fo1, ho = ro * fo1;
-                            const T fn1 = T(1) / (T(1) + gam * rn), fn = beta * fn1 * fn1, hn = rn * fn1;
-                            if (!(flags & Q_PADE_RATIO) || j > p) sum_ratio += beta * (hn - ho);
-#pragma unroll
-                            for (int c = 0; c < DIM; ++c) {
-                                const T tn = fn * dxn[c] * irn, to = fo * dxo[c] * iro;
-                                gp_new[c] += tn;
-                                gdel[jj][c] = to - tn;  // particle j sees -(x_p - x_j)
-                            }
-                            d_lap += T(2) * fn * (T(DIM) - (T(1) + T(2) * gam * hn)) * irn -
-                                     T(2) * fo * (T(DIM) - (T(1) + T(2) * gam * ho)) * iro;
-                            d_bh2 += beta * (hn * hn - ho * ho);
-                        }
-                        if (flags & F_COULOMB) d_vint += irn - iro;
-                    }
-                }
-                if (flags & F_PADE) {
-                    sum_ratio = warp_sum(sum_ratio);
-                    d_lap = warp_sum(d_lap);
-                    d_bh2 = warp_sum(d_bh2);
-#pragma unroll
-                    for (int c = 0; c < DIM; ++c) gp_new[c] = warp_sum(gp_new[c]);
-                }
-                if (flags & F_COULOMB) d_vint = warp_sum(d_vint);
-            }
-
-            // ---- element ratios, multiplied in configuration order
-            T rpn = T(0);
-            if (flags & (F_HYDROGENLIKE | F_ATOM)) {
-                T r2s = T(0);
-#pragma unroll
-                for (int c = 0; c < DIM; ++c) r2s += xpn[c] * xpn[c];
-                rpn = vsqrt(r2s);
-            }
-            double prob = 1.0;
-            double ratios[MAX_ELEM];
-            for (int e = 0; e < P.n_elem; ++e) {
-                double r = 1.0;
-                switch (P.elem_kind[e]) {
-                case 0: r = (double)vexp(wa * (xo * xo - xn * xn)); break;
-                case 1: r = (double)(R * R); break;
-                case 2: r = (double)vexp(T(2) * sum_ratio); break;
-                case 6: r = (double)vexp(T(2) * az * (rpo - rpn)); break;
-                default: break;
-                }
-                ratios[e] = r;
-                prob *= r;
-            }
-
-            bool accept;
-            if (a.probe_k) {
-                accept = true;
-                if (lane == 0)
-                    for (int e = 0; e < P.n_elem; ++e) a.probe_ratio[(size_t)w * P.n_elem + e] = ratios[e];
-            } else {
-                double wgt = prob;
-                if (is) {
-                    if (flags & Q_IS_GREEN) {
-                        wgt = (exp(0.5 * (double)(Fo - Fn) * (double)dx) + 1.0) * prob;
-                    } else {
-                        // Fokker-Planck Green's function ratio; needs F_k at the new point
-                        T gy = T(0);
-                        if (flags & F_GAUSS) gy += -wa * xn;
-                        if (flags & F_PADE) gy += gp_new[adim];
-                        if (flags & F_HYDROGENLIKE) gy += -az * xn / rpn;
-                        if constexpr (K > 0) {
-                            T hv[DIM][K], h1[DIM][K], h2u[DIM][K];
-#pragma unroll
-                            for (int c = 0; c < DIM; ++c) {
-                                hermite_values<K>(xpn[c], hv[c]);
-                                hermite_derivs<K>(hv[c], h1[c], h2u[c]);
-                            }
-                            T dphi = T(0);
-                            const T *invb = inv + b * NO * NO;
-                            if (lane < NO) {
-                                for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
-                                    if (o == lane) {
-                                        const int mm[3] = {m0, m1, m2};
-                                        T v = T(1);
-#pragma unroll
-                                        for (int c = 0; c < DIM; ++c) v *= (c == adim) ? h1[c][mm[c]] : hv[c][mm[c]];
-                                        dphi = v * invb[o * NO + pl];
-                                    }
-                                });
-                            }
-                            gy += warp_sum(dphi) / R;
-                        }
-                        const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
-                        wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
-                    }
-                }
-                if (wgt != wgt) status |= ST_BAD_RATIO;
-                accept = !(wgt < r2);
-            }
-
-            if (accept) {
-                // ---- positions and running scalars
-                __syncwarp();
-                if (lane == 0) {
-                    x[k] = xn;
-                    if (is) fc[k] = Fn;
-                }
-                sc[SC_SUMX2] += (double)xn * (double)xn - (double)xo * (double)xo;
-                if (flags & (F_HYDROGENLIKE | F_ATOM)) {
-                    sc[SC_INVR] += 1.0 / (double)rpn - 1.0 / (double)rpo;
-                    sc[SC_SUMR] += (double)rpn - (double)rpo;
-                }
-                // ---- Sherman-Morrison update of block b (slaterdeterminant.cpp:165-175)
-                if constexpr (K > 0) {
-                    T *invb = inv + b * NO * NO;
-                    const T rinv = T(1) / R;
-                    const T coef = Sj * rinv;
-                    const T colp = lane < NO ? invb[lane * NO + pl] : T(0);
-                    __syncwarp();
-#pragma unroll
-                    for (int o = 0; o < NO; ++o) {
-                        const T c = __shfl_sync(FULL, colp, o);
-                        if (lane < NO) {
-                            const T v = invb[o * NO + lane];
-                            invb[o * NO + lane] = (lane == pl) ? c * rinv : v - coef * c;
-                        }
-                    }
-                    sc[SC_LOGDET] += log(fabs((double)R));
-                    __syncwarp();
-                    // ---- derivative refresh of the block (slaterdeterminant.cpp:155-163)
-                    if (lane < NO) {
-                        const int q = b * NO + lane;
-                        T hv[DIM][K], h1[DIM][K], h2u[DIM][K];
-#pragma unroll
-                        for (int c = 0; c < DIM; ++c) {
-                            hermite_values<K>(x[q * DIM + c], hv[c]);
-                            hermite_derivs<K>(hv[c], h1[c], h2u[c]);
-                        }
-                        T gd[DIM], sd[DIM];
-#pragma unroll
-                        for (int c = 0; c < DIM; ++c) { gd[c] = T(0); sd[c] = T(0); }
-                        for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
-                            const T iv = invb[o * NO + lane];
-                            if (DIM == 2) {
-                                const T t0 = hv[1][m1] * iv, t1 = hv[0][m0] * iv;
-                                gd[0] += h1[0][m0] * t0;
-                                sd[0] += h2u[0][m0] * t0;
-                                gd[1] += h1[1][m1] * t1;
-                                sd[1] += h2u[1][m1] * t1;
-                            } else {
-                                const T t0 = hv[1][m1] * hv[DIM - 1][m2] * iv;
-                                const T t1 = hv[0][m0] * hv[DIM - 1][m2] * iv;
-                                const T t2 = hv[0][m0] * hv[1][m1] * iv;
-                                gd[0] += h1[0][m0] * t0;
-                                sd[0] += h2u[0][m0] * t0;
-                                gd[1] += h1[1][m1] * t1;
-                                sd[1] += h2u[1][m1] * t1;
-                                gd[DIM - 1] += h1[DIM - 1][m2] * t2;
-                                sd[DIM - 1] += h2u[DIM - 1][m2] * t2;
-                            }
-                        });
-#pragma unroll
-                        for (int c = 0; c < DIM; ++c) {
-                            dd[q * DIM + c] = gd[c];
-                            sdd[q * DIM + c] = sd[c];
-                        }
-                    }
-                }
-                // ---- Pade gradient vector, running sums and pair masks
-                if (flags & F_PADE) {
-#pragma unroll
-                    for (int jj = 0; jj < 2; ++jj) {
-                        const int j = lane + 32 * jj;
-                        if (j < N && j != p) {
-#pragma unroll
-                            for (int c = 0; c < DIM; ++c) gj[j * DIM + c] += gdel[jj][c];
-                            smask[j] |= (1ull << p);
-                        }
-                    }
-                    if (lane == (p & 31)) {
-#pragma unroll
-                        for (int c = 0; c < DIM; ++c) gj[p * DIM + c] = gp_new[c];
-                        smask[p] = ~0ull;
-                    }
-                    sc[SC_LAPJ] += (double)d_lap;
-                    sc[SC_BH2] += (double)d_bh2;
-                }
-                if (flags & F_COULOMB) sc[SC_VINT] += (double)d_vint;
-                __syncwarp();
-            }
-
-            // ---- local energy and parameter gradients (Sampler::sample)
-            if (it_step >= a.burn_in || a.rec_en) {
-                T ks = T(0);
-                for (int c = lane; c < D; c += 32) {
-                    const T xc = x[c];
-                    T G = T(0), lc = T(0);
-                    if (flags & F_GAUSS) G += -wa * xc;
-                    if (K > 0) {
-                        const T g = dd[c];
-                        G += g;
-                        lc += sdd[c] - g * g;
-                    }
-                    if (flags & F_PADE) G += gj[c];
-                    if (flags & F_HYDROGENLIKE) {
-                        const int q = c / DIM;
-                        T r2s = T(0);
-#pragma unroll
-                        for (int e2 = 0; e2 < DIM; ++e2) r2s += x[q * DIM + e2] * x[q * DIM + e2];
-                        G += -az * xc / vsqrt(r2s);
-                    }
-                    ks += G * G + lc;
-                }
-                const double lap = (double)warp_sum(ks) + sc[SC_LAPJ] * ((flags & F_PADE) ? 1.0 : 0.0) +
-                                   ((flags & F_GAUSS) ? -(double)wa * D : 0.0) +
-                                   ((flags & F_HYDROGENLIKE) ? -2.0 * (double)az * sc[SC_INVR] : 0.0);
-                const double ekin = -0.5 * lap;
-                const double vext = (flags & F_ATOM) ? -P.Z * sc[SC_INVR]
-                                                     : 0.5 * P.omega * P.omega * sc[SC_SUMX2];
-                const double vint = (flags & F_COULOMB) ? sc[SC_VINT] : 0.0;
-                const double el = ekin + vext + vint;
-                if (el != el) status |= ST_NAN_ENERGY;
-                if (a.rec_en && lane == 0) {
-                    double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
-                    o[0] = ekin;
-                    o[1] = vext;
-                    o[2] = vint;
-                }
-                if (it_step >= a.burn_in) {
-                    const bool win = it_step > a.win_lo && it_step < a.win_hi;
-                    double q = 0.0;
-                    const int i = lane;
-                    if (i < 9) {
-                        q = i == 0 ? el : i == 1 ? el * el : i == 2 ? ekin : i == 3 ? ekin * ekin
-                          : i == 4 ? vext : i == 5 ? vext * vext : i == 6 ? vint : i == 7 ? vint * vint
-                          : (accept ? 1.0 : 0.0);
-                    } else if (win && i < 9 + 2 * P.ep) {
-                        const int j = (i - 9) % P.ep;
-                        double g = 0.0;
-                        if (j == P.idx_alpha) g = -0.5 * P.omega * sc[SC_SUMX2];
-                        else if (j == P.idx_gamma) g = ((flags & Q_PADE_DGAMMA) ? -0.5 : -1.0) * sc[SC_BH2];
-                        else if (j == P.idx_alpha_h) g = -P.Z * sc[SC_SUMR];
-                        q = (i - 9 < P.ep) ? g : g * el;
-                    }
-                    if (lane < P.nacc) kadd(acc_s, acc_c, q);
-                }
-            }
-            if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
-        }
-
-        // ---- write the walker back
-        __syncwarp();
-        {
-            const int nv = L.rec * (int)sizeof(T) / 16;
-            const uint4 *s4 = reinterpret_cast<const uint4 *>(sm);
-            uint4 *d4 = reinterpret_cast<uint4 *>(g_rec);
-            for (int i = lane; i < nv; i += 32) d4[i] = s4[i];
-        }
-        for (int j = lane; j < N; j += 32) P.mask[(size_t)w * N + j] = smask[j];
-        if (lane == 0) {
-#pragma unroll
-            for (int i = 0; i < NSCAL; ++i) P.scal[(size_t)w * NSCAL + i] = sc[i];
-            P.counter[w] = ctr;
-        }
-        if (lane < P.nacc) {
-            P.acc[((size_t)w * P.nacc + lane) * 2] = acc_s;
-            P.acc[((size_t)w * P.nacc + lane) * 2 + 1] = acc_c;
-        }
-        status = __reduce_or_sync(FULL, status);
-        if (lane == 0 && status) P.status[w] |= status;
-        __syncwarp();
-    }
-}
+namespace vmc {
 
 // ------------------------------------------------------------------ FP64 rebuild
 
@@ -842,30 +429,6 @@ __global__ void initial_positions_kernel(Layout L, int W, void *state, unsigned 
     reinterpret_cast<T *>(state)[(size_t)w * L.rec + L.off_x + c] = T(val);
 }
 
-// Deterministic compensated reduction of the per-walker accumulators:
-// one block, thread group per accumulator, fixed summation order.
-__global__ void reduce_acc_kernel(const double *acc, int W, int nacc, double *out)
-{
-    const int a = blockIdx.x;  // accumulator index
-    double s = 0.0, c = 0.0;
-    for (int w = threadIdx.x; w < W; w += blockDim.x) {
-        kadd(s, c, acc[((size_t)w * nacc + a) * 2]);
-        kadd(s, c, acc[((size_t)w * nacc + a) * 2 + 1]);
-    }
-    __shared__ double ss[256], cc[256];
-    ss[threadIdx.x] = s;
-    cc[threadIdx.x] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double S = 0.0, C = 0.0;
-        for (int t = 0; t < (int)blockDim.x; ++t) {
-            kadd(S, C, ss[t]);
-            kadd(S, C, cc[t]);
-        }
-        out[a] = S + C;
-    }
-}
-
 // FMA throughput calibration: FMA_CHAINS independent register chains per thread.
 constexpr int FMA_CHAINS = 8;
 template <typename R>
@@ -881,6 +444,62 @@ __global__ void fma_peak_kernel(R *out, int iters, R m)
 #pragma unroll
     for (int i = 0; i < FMA_CHAINS; ++i) s += v[i];
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// ------------------------------------------------------------------ dispatch
+
+struct KernelSet {
+    const void *sweep = nullptr, *rebuild = nullptr, *eval = nullptr, *initpos = nullptr;
+};
+
+template <typename T, int DIM, int K, int FX>
+KernelSet make_set()
+{
+    KernelSet s;
+    s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX>);
+    s.rebuild = reinterpret_cast<const void *>(&rebuild_kernel<T, DIM, K>);
+    s.eval = reinterpret_cast<const void *>(&eval_kernel<T, DIM, K>);
+    s.initpos = reinterpret_cast<const void *>(&initial_positions_kernel<T>);
+    return s;
+}
+
+template <typename T, int K>
+bool select_2d(int flags, KernelSet &out)
+{
+    if (K > 0 && flags == FX_DOT_COMPAT) { out = make_set<T, 2, K, (K > 0 ? FX_DOT_COMPAT : 0)>(); return true; }
+    if (K > 0 && flags == FX_DOT_CORRECTED) { out = make_set<T, 2, K, (K > 0 ? FX_DOT_CORRECTED : 0)>(); return true; }
+    out = make_set<T, 2, K, 0>();
+    return true;
+}
+
+// Kernel set for (dimension, Hermite shells, flags) in precision T.
+template <typename T>
+bool select_kernels(int dim, int K, int flags, KernelSet &out)
+{
+    if (dim == 2) {
+        switch (K) {
+        case 0: return select_2d<T, 0>(flags, out);
+        case 1: return select_2d<T, 1>(flags, out);
+        case 2: return select_2d<T, 2>(flags, out);
+        case 3: return select_2d<T, 3>(flags, out);
+        case 4: return select_2d<T, 4>(flags, out);
+        case 5: return select_2d<T, 5>(flags, out);
+        case 6: return select_2d<T, 6>(flags, out);
+        case 7: return select_2d<T, 7>(flags, out);
+        default: return false;
+        }
+    }
+    if (dim == 3) {
+        switch (K) {
+        case 0: out = make_set<T, 3, 0, 0>(); return true;
+        case 1: out = make_set<T, 3, 1, 0>(); return true;
+        case 2: out = make_set<T, 3, 2, 0>(); return true;
+        case 3: out = make_set<T, 3, 3, 0>(); return true;
+        case 4: out = make_set<T, 3, 4, 0>(); return true;
+        default: return false;
+        }
+    }
+    return false;
 }
 
 }  // namespace vmc

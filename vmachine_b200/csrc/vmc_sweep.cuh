@@ -1,0 +1,666 @@
+// Metropolis sweep kernel: one warp per walker, WPB walkers per CTA.
+//
+// Per step (System::runMetropolisCycles body, src/system.cpp:149-163):
+//   1. draw (k, displacement, uniform) from the walker's Philox stream (or a replay
+//      stream); propose x_k' (brute force: bruteforce.cpp:34; importance sampling
+//      with the drift 2 grad ln Psi: importancesampling.cpp:49-60);
+//   2. |Psi'|^2/|Psi|^2 per element without touching the state:
+//      Slater  R = phi(r_p') . inv[:, p]   (lanes over inverse columns)
+//      Pade    sum over partners of beta (h' - h)   (lanes over partners)
+//   3. accept: Sherman-Morrison rank-1 update of the moved particle's spin block,
+//      refresh of that block's d ln det / d^2 det / det vectors, Pade gradient
+//      vector and running pair sums (Laplacian, beta h^2, Coulomb);
+//   4. sample E_L = T + V_ext + V_int and dlnPsi/dtheta every step after burn-in
+//      into per-lane Neumaier-compensated FP64 accumulators (sampler.cpp:52-90).
+// Nothing is snapshotted: a rejected move leaves the state untouched.
+//
+// Orbital sums are factorised over Hermite degrees: phi_o(r) = prod_c h_{m_c(o)}(x_c),
+// so phi(r) . v = sum_{m0} h_{m0}(x) sum_{m1} h_{m1}(y) v_o and the derivative
+// vectors contract per-degree partial sums with h' and h''.
+//
+// Template FX: 0 = element flags read at run time (any supported system); a
+// non-zero flag set compiles the flags in (the quantum-dot paths).
+//
+// Shared memory per warp: the walker record (see Layout), the Pade pair mask
+// (N x u64) and the FP64 running scalars (NSCAL doubles).
+#pragma once
+#include <type_traits>
+
+namespace vmc {
+
+template <typename T> struct Fast;
+template <> struct Fast<float> {
+    static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+    static __device__ __forceinline__ float exp(float x) { return __expf(x); }
+};
+template <> struct Fast<double> {
+    static __device__ __forceinline__ double rsqrt(double x) { return ::rsqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+    static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+};
+
+// phi(r) . v, where v(o) returns the column entry of orbital o (shared memory or a
+// lane's registers).
+template <typename T, int DIM, int K, typename V>
+__device__ __forceinline__ T orbital_dot(const T (&hv)[DIM][K], V &&v)
+{
+    T part[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) part[m] = T(0);
+    for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
+        T f = hv[1][m1];
+        if (DIM == 3) f *= hv[DIM - 1][m2];
+        part[m0] += f * v(o);
+    });
+    T s = T(0);
+#pragma unroll
+    for (int m = 0; m < K; ++m) s += hv[0][m] * part[m];
+    return s;
+}
+
+// d_c phi(r) . v and d_c^2 phi(r) . v for every dimension c.
+template <typename T, int DIM, int K, typename V>
+__device__ __forceinline__ void orbital_derivs(const T (&hv)[DIM][K], V &&vf, T (&gd)[DIM],
+                                               T (&sd)[DIM])
+{
+    T part[DIM][K];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c)
+#pragma unroll
+        for (int m = 0; m < K; ++m) part[c][m] = T(0);
+    for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
+        const T v = vf(o);
+        if (DIM == 2) {
+            part[0][m0] += hv[1][m1] * v;
+            part[1][m1] += hv[0][m0] * v;
+        } else {
+            part[0][m0] += (hv[1][m1] * hv[DIM - 1][m2]) * v;
+            part[1][m1] += (hv[0][m0] * hv[DIM - 1][m2]) * v;
+            part[DIM - 1][m2] += (hv[0][m0] * hv[1][m1]) * v;
+        }
+    });
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+        T g = T(0), s2 = T(0);
+#pragma unroll
+        for (int m = 1; m < K; ++m) g += hC<T>(m) * hv[c][m - 1] * part[c][m];
+#pragma unroll
+        for (int m = 2; m < K; ++m) s2 += hE<T>(m) * hv[c][m - 2] * part[c][m];
+        gd[c] = g;
+        sd[c] = s2;
+    }
+}
+
+// Coordinates of particle j (2D: one 8- or 16-byte load, no bank conflicts).
+template <typename T, int DIM>
+__device__ __forceinline__ void load_coords(const T *x, int j, T (&out)[DIM])
+{
+    if constexpr (DIM == 2) {
+        using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+        const V v = reinterpret_cast<const V *>(x)[j];
+        out[0] = v.x;
+        out[1] = v.y;
+    } else {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) out[c] = x[j * DIM + c];
+    }
+}
+
+template <typename T, int DIM>
+__device__ __forceinline__ void store_coords(T *x, int j, const T (&in)[DIM])
+{
+    if constexpr (DIM == 2) {
+        using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+        V v;
+        v.x = in[0];
+        v.y = in[1];
+        reinterpret_cast<V *>(x)[j] = v;
+    } else {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) x[j * DIM + c] = in[c];
+    }
+}
+
+// d ln Psi / d x_k at the proposed point for the corrected Fokker-Planck Green's
+// ratio (compat off): Slater part (d_a phi(r_p') . inv[:, p]) / R.  Out of line so
+// its registers stay off the common path; compiled out of the compat kernels.
+template <typename T, int DIM, int K>
+__device__ __noinline__ T slater_grad_new(const T *invb, const T *xpn, int adim, int pl, T R)
+{
+    T hv[DIM][K];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
+    T gd[DIM], sd[DIM];
+    constexpr int NO = Shells<DIM, K>::n;
+    orbital_derivs<T, DIM, K>(hv, [&](int o) { return invb[o * NO + pl]; }, gd, sd);
+    T g = gd[0];
+#pragma unroll
+    for (int c = 1; c < DIM; ++c)
+        if (c == adim) g = gd[c];
+    return g / R;
+}
+
+// Reduce-scatter of 8 per-lane values over the warp (xor butterfly that halves the
+// value set at each stage): returns, in lane L, the warp total of value L >> 2.
+// 9 shuffles instead of 40 for eight all-reduces.
+template <typename R>
+__device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
+{
+    const bool h4 = lane & 16;
+    R w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const R mine = h4 ? v[4 + i] : v[i];
+        const R other = h4 ? v[i] : v[4 + i];
+        w[i] = mine + __shfl_xor_sync(FULL, other, 16);
+    }
+    const bool h3 = lane & 8;
+    R u[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const R mine = h3 ? w[2 + i] : w[i];
+        const R other = h3 ? w[i] : w[2 + i];
+        u[i] = mine + __shfl_xor_sync(FULL, other, 8);
+    }
+    const bool h2 = lane & 4;
+    R t = (h2 ? u[1] : u[0]) + __shfl_xor_sync(FULL, h2 ? u[0] : u[1], 4);
+    t += __shfl_xor_sync(FULL, t, 2);
+    t += __shfl_xor_sync(FULL, t, 1);
+    return t;
+}
+
+// Register-resident inverse: each lane would keep its inverse columns (one per
+// spin block) in registers, since the S_j dot, the Sherman-Morrison update and the
+// derivative refresh all read column `lane`.  Measured with ptxas at N = 56: the
+// two 28-entry columns plus the step's working set need more than 200 registers
+// per thread and spill, so the inverse stays in shared memory for every shape.
+template <typename T, int K>
+struct InvInRegisters {
+    static constexpr bool value = false;
+};
+
+template <typename T, int DIM, int K, int FX>
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
+    sweep_kernel(const SweepArgs a)
+{
+    using F = Fast<T>;
+    constexpr int NO = K > 0 ? Shells<DIM, K>::n : 0;
+    constexpr int NK = 2 * NO;                  // particles when the Slater fixes N
+    constexpr int DK = NK * DIM;                // coordinates when the Slater fixes N
+    constexpr bool REGINV = InvInRegisters<T, K>::value;
+    constexpr int NOR = REGINV ? NO : 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Params &P = a.P;
+    const Layout L = P.L;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    T *sm = reinterpret_cast<T *>(smem_raw + (size_t)wib * a.smem_per_warp);
+    const int N = K > 0 ? NK : P.N;
+    const int D = K > 0 ? DK : L.D;
+    const int sm_elems = REGINV ? L.off_inv : L.rec;  // record part staged in shared memory
+    unsigned long long *smask = reinterpret_cast<unsigned long long *>(sm + sm_elems);
+    T creg[2][NOR];
+    double *ssc = reinterpret_cast<double *>(smask + N);
+    T *x = sm + L.off_x, *fc = sm + L.off_fc, *dd = sm + L.off_dd, *sdd = sm + L.off_sdd;
+    T *gj = sm + L.off_gj, *inv = sm + L.off_inv;
+    const int flags = FX ? FX : P.flags;
+    const bool is = flags & F_IS;
+
+    // accumulator slot of this lane: 0..7 energy moments, 8 accepts, then the
+    // parameter gradients (kind 1 alpha, 2 gamma, 3 hydrogen-like alpha) and
+    // the same times E_L.
+    int pkind = 0;
+    bool times_e = false;
+    if (lane >= 9 && lane < P.nacc) {
+        int j = lane - 9;
+        times_e = j >= P.ep;
+        if (times_e) j -= P.ep;
+        pkind = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : j == P.idx_alpha_h ? 3 : 0;
+    }
+
+    for (int w = blockIdx.x * a.wpb + wib; w < P.W; w += gridDim.x * a.wpb) {
+        T *g_rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
+        copy_in(sm, g_rec, sm_elems, lane);
+        if constexpr (REGINV) {
+#pragma unroll
+            for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+                for (int o = 0; o < NO; ++o)
+                    creg[bb][o] = lane < NO ? g_rec[L.off_inv + (bb * NO + o) * NO + lane] : T(0);
+        }
+        for (int j = lane; j < N; j += 32) smask[j] = P.mask[(size_t)w * N + j];
+        if (lane < NSCAL) ssc[lane] = P.scal[(size_t)w * NSCAL + lane];
+        double acc_s = 0.0, acc_c = 0.0;
+        if (lane < P.nacc) {
+            acc_s = P.acc[((size_t)w * P.nacc + lane) * 2];
+            acc_c = P.acc[((size_t)w * P.nacc + lane) * 2 + 1];
+        }
+        unsigned long long ctr = P.counter[w];
+        unsigned status = 0;
+        int rng_k = 0;        // this lane's step of the current 32-step random block
+        T rng_z = T(0);
+        unsigned rng_u = 0u;
+        __syncwarp();
+
+        const bool use_philox = !a.probe_k && !a.replay;
+        for (int s0 = 0; s0 < a.steps; s0 += 32) {
+          if (use_philox) {
+            // Lane-parallel Philox: lane i draws the numbers of step counter ctr + i
+            // (the same per-step stream as a serial draw); each step of this block
+            // takes its triple from lane (step - s0) by shuffle.
+            const unsigned long long c = ctr + (unsigned long long)lane;
+            const uint4 v = philox(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)w, 0u),
+                                   make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
+            rng_k = (int)__umulhi(v.x, (unsigned)D);
+            if (is) {
+                if (sizeof(T) == 8) {
+                    const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
+                    rng_z = T(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2));
+                } else {
+                    const float u1 = ((float)v.y + 1.0f) * 2.3283064e-10f;
+                    const float u2 = (float)v.z * 2.3283064e-10f;
+                    rng_z = T(sqrtf(-2.0f * __logf(u1)) * __cosf(6.2831853f * u2));
+                }
+            } else {
+                rng_z = T(v.y * TWO_M32);
+            }
+            rng_u = v.w;
+          }
+          const int s_end = min(s0 + 32, a.steps);
+          for (int s = s0; s < s_end; ++s) {
+            const int it_step = a.step_offset + s;
+            const T wa = T(P.omega * P.alpha);
+            // ---- 1. random numbers and the proposal
+            int k;
+            T r1;
+            double r2;
+            if (a.probe_k) {
+                k = a.probe_k[w];
+                r1 = T(0);
+                r2 = 0.0;
+            } else if (a.replay) {
+                const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
+                k = (int)floor(q[0] * D);
+                r1 = T(q[1]);
+                r2 = q[2];
+            } else {
+                const int slot = s - s0;
+                ++ctr;
+                k = __shfl_sync(FULL, rng_k, slot);
+                r1 = __shfl_sync(FULL, rng_z, slot);
+                r2 = __shfl_sync(FULL, rng_u, slot) * TWO_M32;
+            }
+            const int p = k / DIM, adim = k - p * DIM;
+            const T xo = x[k];
+            T Gk = T(0);
+            if (flags & F_GAUSS) Gk += -wa * xo;
+            if (K > 0) Gk += dd[k];
+            if (flags & F_PADE) Gk += gj[k];
+            T rpo = T(0);
+            if (flags & (F_HYDROGENLIKE | F_ATOM)) {
+                T r2s = T(0);
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) r2s += x[p * DIM + c] * x[p * DIM + c];
+                rpo = r2s * F::rsqrt(r2s);
+                if (flags & F_HYDROGENLIKE) Gk += -T(P.alpha_h * P.Z) * xo / rpo;
+            }
+            T dx, Fn = T(0);
+            if (a.probe_k) {
+                dx = T(a.probe_x[w]) - xo;
+            } else if (is) {
+                Fn = T(2) * Gk;
+                dx = T(0.5 * P.step) * Fn + r1 * T(sqrt(P.step));
+            } else {
+                dx = T(10) * (r1 - T(0.5)) * T(P.step);
+            }
+            const T xn = a.probe_k ? T(a.probe_x[w]) : xo + dx;
+            T xpn[DIM];
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) xpn[c] = (c == adim) ? xn : x[p * DIM + c];
+
+            // ---- 2a. Slater: S_j = phi(r_p') . inv[:, j] for lane j, R = S_pl
+            T Sj = T(0), R = T(1);
+            int b = 0, pl = 0;
+            if constexpr (K > 0) {
+                b = p / NO;
+                pl = p - b * NO;
+                T hv[DIM][K];
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
+                if constexpr (REGINV) {
+                    if (b == 0) Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return creg[0][o]; });
+                    else Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return creg[1][o]; });
+                } else if (lane < NO) {
+                    const T *col = inv + b * NO * NO + lane;
+                    Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return col[o * NO]; });
+                }
+                R = __shfl_sync(FULL, Sj, pl);
+            }
+
+            // ---- 2b. pair terms of the moved particle (Pade, Coulomb)
+            constexpr int NJ = K > 0 ? (NK + 31) / 32 : 2;
+            T sum_ratio = T(0), d_lap = T(0), d_bh2 = T(0), d_vint = T(0), pair_total = T(0);
+            T gp_new[DIM], gdel[NJ][DIM];
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+                gp_new[c] = T(0);
+#pragma unroll
+                for (int jj = 0; jj < NJ; ++jj) gdel[jj][c] = T(0);
+            }
+            if (flags & (F_PADE | F_COULOMB)) {
+                const unsigned long long mp = smask[p];
+                const T gam = T(P.gamma), gamp = T(P.gamma_prev);
+#pragma unroll
+                for (int jj = 0; jj < NJ; ++jj) {
+                    const int j = lane + 32 * jj;
+                    if (j < N && j != p) {
+                        T dxo[DIM], dxn[DIM], r2o = T(0), r2n = T(0), xjv[DIM];
+                        load_coords<T, DIM>(x, j, xjv);
+#pragma unroll
+                        for (int c = 0; c < DIM; ++c) {
+                            const T xj = xjv[c];
+                            dxo[c] = ((c == adim) ? xo : xpn[c]) - xj;
+                            dxn[c] = xpn[c] - xj;
+                            r2o += dxo[c] * dxo[c];
+                            r2n += dxn[c] * dxn[c];
+                        }
+                        const T iro = F::rsqrt(r2o), irn = F::rsqrt(r2n);
+                        if (flags & F_PADE) {
+                            const T ro = r2o * iro, rn = r2n * irn;
+                            const T beta = same_spin(p, j, N) ? T(P.beta_same) : T(P.beta_anti);
+                            const T gpair = ((flags & Q_PADE_STALE) && !((mp >> j) & 1ull)) ? gamp : gam;
+                            const T fo1 = F::rcp(T(1) + gpair * ro), fo = beta * fo1 * fo1, ho = ro * fo1;
+                            const T fn1 = F::rcp(T(1) + gam * rn), fn = beta * fn1 * fn1, hn = rn * fn1;
+                            if (!(flags & Q_PADE_RATIO) || j > p) sum_ratio += beta * (hn - ho);
+                            const T fni = fn * irn, foi = fo * iro;
+#pragma unroll
+                            for (int c = 0; c < DIM; ++c) {
+                                const T tn = fni * dxn[c];
+                                gp_new[c] += tn;
+                                gdel[jj][c] = foi * dxo[c] - tn;  // particle j sees -(x_p - x_j)
+                            }
+                            d_lap += T(2) * (fni * (T(DIM) - (T(1) + T(2) * gam * hn)) -
+                                             foi * (T(DIM) - (T(1) + T(2) * gam * ho)));
+                            d_bh2 += beta * (hn * hn - ho * ho);
+                        }
+                        if (flags & F_COULOMB) d_vint += irn - iro;
+                    }
+                }
+                // one reduce-scatter for all pair sums: lane L ends with the total of
+                // value L >> 2 (0 ratio exponent, 1 Laplacian, 2 beta h^2, 3 Coulomb,
+                // 4.. the moved particle's new Pade gradient)
+                T vals[8] = {sum_ratio, d_lap, d_bh2, d_vint, T(0), T(0), T(0), T(0)};
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) vals[4 + c] = gp_new[c];
+                pair_total = warp_reduce_scatter8(vals, lane);
+                sum_ratio = __shfl_sync(FULL, pair_total, 0);
+            }
+
+            // ---- 2c. element ratios, multiplied in configuration order
+            T rpn = T(0);
+            if (flags & (F_HYDROGENLIKE | F_ATOM)) {
+                T r2s = T(0);
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) r2s += xpn[c] * xpn[c];
+                rpn = r2s * F::rsqrt(r2s);
+            }
+            const T rat_g = (flags & F_GAUSS) ? F::exp(wa * (xo * xo - xn * xn)) : T(1);
+            const T rat_p = (flags & F_PADE) ? F::exp(T(2) * sum_ratio) : T(1);
+            const T rat_h = (flags & F_HYDROGENLIKE) ? F::exp(T(2 * P.alpha_h * P.Z) * (rpo - rpn)) : T(1);
+            double prob = 1.0;
+            if (FX && !a.probe_k) {
+                // compiled-in dot: Slater x Gaussian x Pade (order only affects rounding)
+                prob = (double)(R * R) * (double)rat_g * (double)rat_p;
+            } else {
+                for (int e = 0; e < P.n_elem; ++e) {
+                    const int kind = P.elem_kind[e];
+                    const T r = kind == 0 ? rat_g : kind == 1 ? R * R : kind == 2 ? rat_p : kind == 6 ? rat_h : T(1);
+                    prob *= (double)r;
+                    if (a.probe_k && lane == 0) a.probe_ratio[(size_t)w * P.n_elem + e] = (double)r;
+                }
+            }
+
+            // ---- 2d. accept / reject
+            bool accept = true;
+            if (!a.probe_k) {
+                double wgt = prob;
+                if (is) {
+                    if (flags & Q_IS_GREEN) {
+                        // importancesampling.cpp:43-47: exp(0.5 (F_old(k) - F_new(k)) dx) + 1
+                        const T ex = F::exp(T(0.5) * (fc[k] - Fn) * dx);
+                        wgt = ((double)ex + 1.0) * prob;
+                    } else {
+                        T gy = T(0);
+                        if (flags & F_GAUSS) gy += -wa * xn;
+                        if (flags & F_PADE) gy += __shfl_sync(FULL, pair_total, 16 + 4 * adim);
+                        if (flags & F_HYDROGENLIKE) gy += -T(P.alpha_h * P.Z) * xn / rpn;
+                        if constexpr (REGINV) {
+                            T hvn[DIM][K];
+#pragma unroll
+                            for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hvn[c]);
+                            T gd[DIM], sd[DIM];
+                            if (b == 0) orbital_derivs<T, DIM, K>(hvn, [&](int o) { return creg[0][o]; }, gd, sd);
+                            else orbital_derivs<T, DIM, K>(hvn, [&](int o) { return creg[1][o]; }, gd, sd);
+                            T g = gd[0];
+#pragma unroll
+                            for (int c = 1; c < DIM; ++c)
+                                if (c == adim) g = gd[c];
+                            gy += __shfl_sync(FULL, g, pl) / R;
+                        } else if constexpr (K > 0) {
+                            gy += slater_grad_new<T, DIM, K>(inv + b * NO * NO, xpn, adim, pl, R);
+                        }
+                        const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
+                        wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
+                    }
+                }
+                if (wgt != wgt) status |= ST_BAD_RATIO;
+                accept = !(wgt < r2);
+            }
+
+            if (accept) {
+                // ---- 3. state update
+                __syncwarp();
+                if (lane == 0) {
+                    x[k] = xn;
+                    if (is) fc[k] = Fn;
+                    ssc[SC_SUMX2] += (double)xn * (double)xn - (double)xo * (double)xo;
+                    if (flags & (F_HYDROGENLIKE | F_ATOM)) {
+                        ssc[SC_INVR] += 1.0 / (double)rpn - 1.0 / (double)rpo;
+                        ssc[SC_SUMR] += (double)rpn - (double)rpo;
+                    }
+                }
+                // owners of the reduced pair sums apply them: value v (lanes 4v..4v+3)
+                // 1, 2 -> SC_LAPJ, SC_BH2 (= v); 3 -> SC_VINT (= v); 4 + c -> gj of p
+                if ((flags & (F_PADE | F_COULOMB)) && (lane & 3) == 0 && lane >= 4 && lane < 16 + 4 * DIM) {
+                    const int v = lane >> 2;
+                    if (v < 4) {
+                        if ((v == 3) ? (flags & F_COULOMB) : (flags & F_PADE)) ssc[v] += (double)pair_total;
+                    } else if (flags & F_PADE) {
+                        gj[p * DIM + v - 4] = pair_total;
+                    }
+                }
+                if constexpr (K > 0) {
+                    // Sherman-Morrison (slaterdeterminant.cpp:165-175)
+                    T *invb = inv + b * NO * NO;
+                    const T rinv = F::rcp(R);  // an accepted move has |R| well above underflow
+                    const T coef = Sj * rinv;
+                    if constexpr (REGINV) {
+                        auto update = [&](T (&cr)[NOR]) {
+#pragma unroll
+                            for (int o = 0; o < NO; ++o) {
+                                const T c = __shfl_sync(FULL, cr[o], pl);  // inv[o][pl]
+                                cr[o] = (lane == pl) ? c * rinv : cr[o] - coef * c;
+                            }
+                        };
+                        if (b == 0) update(creg[0]);
+                        else update(creg[1]);
+                    } else {
+                        // lanes >= NO read a valid entry and store nothing (a predicated
+                        // store, no branch per row)
+                        const int lc = lane < NO ? lane : 0;
+                        const T colp = invb[lc * NO + pl];
+                        __syncwarp();
+#pragma unroll
+                        for (int o = 0; o < NO; ++o) {
+                            const T c = __shfl_sync(FULL, colp, o);
+                            const T v = invb[o * NO + lc];
+                            const T nv = (lane == pl) ? c * rinv : v - coef * c;
+                            if (lane < NO) invb[o * NO + lane] = nv;
+                        }
+                    }
+                    __syncwarp();
+                    // d ln det / dx and (d^2 det / dx^2) / det of the block
+                    // (slaterdeterminant.cpp:155-163), lanes over the block's particles
+                    if (lane < NO) {
+                        const int q = b * NO + lane;
+                        T xq[DIM];
+                        load_coords<T, DIM>(x, q, xq);
+                        T hv[DIM][K];
+#pragma unroll
+                        for (int c = 0; c < DIM; ++c) hermite_values<K>(xq[c], hv[c]);
+                        T gd[DIM], sd[DIM];
+                        if constexpr (REGINV) {
+                            if (b == 0) orbital_derivs<T, DIM, K>(hv, [&](int o) { return creg[0][o]; }, gd, sd);
+                            else orbital_derivs<T, DIM, K>(hv, [&](int o) { return creg[1][o]; }, gd, sd);
+                        } else {
+                            const T *col = invb + lane;
+                            orbital_derivs<T, DIM, K>(hv, [&](int o) { return col[o * NO]; }, gd, sd);
+                        }
+                        store_coords<T, DIM>(dd, q, gd);
+                        store_coords<T, DIM>(sdd, q, sd);
+                    }
+                }
+                if (flags & F_PADE) {
+#pragma unroll
+                    for (int jj = 0; jj < NJ; ++jj) {
+                        const int j = lane + 32 * jj;
+                        if (j < N && j != p) {
+                            T gv[DIM];
+                            load_coords<T, DIM>(gj, j, gv);
+#pragma unroll
+                            for (int c = 0; c < DIM; ++c) gv[c] += gdel[jj][c];
+                            store_coords<T, DIM>(gj, j, gv);
+                            smask[j] |= (1ull << p);
+                        }
+                    }
+                    if (lane == (p & 31)) smask[p] = ~0ull;
+                }
+                __syncwarp();
+            }
+
+            // ---- 4. local energy and parameter gradients (Sampler::sample)
+            if (it_step >= a.burn_in || a.rec_en) {
+                // per coordinate: (sum_e grad_e)^2 + Slater's d2/det - (d ln det)^2; the
+                // Slater-fixed shapes read VW consecutive coordinates per lane
+                constexpr int VW = sizeof(T) == 4 ? 4 : 2;
+                constexpr bool VEC = K > 0 && DK % VW == 0;
+                constexpr int NV = VEC ? DK / VW : 1;
+                T ks = T(0);
+                auto coord_term = [&](int c, T xc, T g_s, T s_s, T g_j) {
+                    T G = T(0), lc = T(0);
+                    if (flags & F_GAUSS) G += -wa * xc;
+                    if (K > 0) {
+                        G += g_s;
+                        lc += s_s - g_s * g_s;
+                    }
+                    if (flags & F_PADE) G += g_j;
+                    if (flags & F_HYDROGENLIKE) {
+                        const int q = c / DIM;
+                        T r2s = T(0);
+#pragma unroll
+                        for (int e2 = 0; e2 < DIM; ++e2) r2s += x[q * DIM + e2] * x[q * DIM + e2];
+                        G += -T(P.alpha_h * P.Z) * xc * F::rsqrt(r2s);
+                    }
+                    ks += G * G + lc;
+                };
+                if constexpr (VEC) {
+                    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+#pragma unroll
+                    for (int i = 0; i < (NV + 31) / 32; ++i) {
+                        const int vi = lane + 32 * i;
+                        if (vi < NV) {
+                            const V vx = reinterpret_cast<const V *>(x)[vi];
+                            const V vd = reinterpret_cast<const V *>(dd)[vi];
+                            const V vs = reinterpret_cast<const V *>(sdd)[vi];
+                            const V vj = reinterpret_cast<const V *>(gj)[vi];
+                            const T *ax = reinterpret_cast<const T *>(&vx), *ad = reinterpret_cast<const T *>(&vd);
+                            const T *as = reinterpret_cast<const T *>(&vs), *aj = reinterpret_cast<const T *>(&vj);
+#pragma unroll
+                            for (int e = 0; e < VW; ++e) coord_term(vi * VW + e, ax[e], ad[e], as[e], aj[e]);
+                        }
+                    }
+                } else {
+                    constexpr int NC = K > 0 ? (DK + 31) / 32 : 6;
+#pragma unroll
+                    for (int i = 0; i < NC; ++i) {
+                        const int c = lane + 32 * i;
+                        if (c < D)
+                            coord_term(c, x[c], K > 0 ? dd[c] : T(0), K > 0 ? sdd[c] : T(0),
+                                       (flags & F_PADE) ? gj[c] : T(0));
+                    }
+                }
+                ks = warp_sum(ks);
+                double lap = (double)ks;
+                if (flags & F_PADE) lap += ssc[SC_LAPJ];
+                if (flags & F_GAUSS) lap -= P.omega * P.alpha * D;
+                if (flags & F_HYDROGENLIKE) lap -= 2.0 * P.alpha_h * P.Z * ssc[SC_INVR];
+                const double ekin = -0.5 * lap;
+                const double vext = (flags & F_ATOM) ? -P.Z * ssc[SC_INVR]
+                                                     : 0.5 * P.omega * P.omega * ssc[SC_SUMX2];
+                const double vint = (flags & F_COULOMB) ? ssc[SC_VINT] : 0.0;
+                const double el = ekin + vext + vint;
+                if (el != el) status |= ST_NAN_ENERGY;
+                if (a.rec_en && lane == 0) {
+                    double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
+                    o[0] = ekin;
+                    o[1] = vext;
+                    o[2] = vint;
+                }
+                if (it_step >= a.burn_in) {
+                    // branch-free slot selection; lanes past the accumulators add zero
+                    const int g2 = (lane >> 1) & 3;
+                    const double base = g2 == 0 ? el : g2 == 1 ? ekin : g2 == 2 ? vext : vint;
+                    const double qe = (lane & 1) ? base * base : base;
+                    const bool win = it_step > a.win_lo && it_step < a.win_hi;
+                    const double g = pkind == 1 ? -0.5 * P.omega * ssc[SC_SUMX2]
+                                   : pkind == 2 ? ((flags & Q_PADE_DGAMMA) ? -0.5 : -1.0) * ssc[SC_BH2]
+                                   : pkind == 3 ? -P.Z * ssc[SC_SUMR] : 0.0;
+                    const double qp = win ? (times_e ? g * el : g) : 0.0;
+                    const double q = lane < 8 ? qe : lane == 8 ? (accept ? 1.0 : 0.0) : qp;
+                    kadd(acc_s, acc_c, q);
+                }
+            }
+            if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
+          }
+        }
+
+        // ---- write the walker back
+        __syncwarp();
+        {
+            const int nv = sm_elems * (int)sizeof(T) / 16;
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(sm);
+            uint4 *d4 = reinterpret_cast<uint4 *>(g_rec);
+            for (int i = lane; i < nv; i += 32) d4[i] = s4[i];
+        }
+        if constexpr (REGINV) {
+            if (lane < NO) {
+#pragma unroll
+                for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+                    for (int o = 0; o < NO; ++o) g_rec[L.off_inv + (bb * NO + o) * NO + lane] = creg[bb][o];
+            }
+        }
+        for (int j = lane; j < N; j += 32) P.mask[(size_t)w * N + j] = smask[j];
+        if (lane < NSCAL) P.scal[(size_t)w * NSCAL + lane] = ssc[lane];
+        if (lane == 0) P.counter[w] = ctr;
+        if (lane < P.nacc) {
+            P.acc[((size_t)w * P.nacc + lane) * 2] = acc_s;
+            P.acc[((size_t)w * P.nacc + lane) * 2 + 1] = acc_c;
+        }
+        status = __reduce_or_sync(FULL, status);
+        if (lane == 0 && status) P.status[w] |= status;
+        __syncwarp();
+    }
+}
+
+}  // namespace vmc

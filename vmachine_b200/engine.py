@@ -52,7 +52,7 @@ EXPORTS = ["vmc_abi_version", "vmc_create", "vmc_destroy", "vmc_get_info", "vmc_
            "vmc_set_parameters", "vmc_get_parameters", "vmc_init_walkers", "vmc_get_positions",
            "vmc_sample", "vmc_run_iteration", "vmc_get_walker_energies", "vmc_eval",
            "vmc_probe_move", "vmc_replay", "vmc_set_replay", "vmc_get_status",
-           "vmc_run_simulation", "vmc_stopwatch", "vmc_measure_fma_peak"]
+           "vmc_run_simulation", "vmc_stopwatch", "vmc_measure_fma_peak", "vmc_apply_sums"]
 
 
 def library():
@@ -76,6 +76,7 @@ def library():
     L.vmc_get_positions.argtypes = [vp, vp]
     L.vmc_sample.argtypes = [vp, ip, ip, ip, ctypes.POINTER(Sums), vp, vp]
     L.vmc_run_iteration.argtypes = [vp, ip, ctypes.POINTER(Averages)]
+    L.vmc_apply_sums.argtypes = [vp, ctypes.POINTER(Sums), vp, vp, ctypes.POINTER(Averages)]
     L.vmc_get_walker_energies.argtypes = [vp, vp]
     L.vmc_eval.argtypes = [vp, vp, vp, vp, vp]
     L.vmc_probe_move.argtypes = [vp, vp, vp, vp]
@@ -167,6 +168,15 @@ class Engine:
                                          _p(g), _p(ge)))
         return s, g, ge
 
+    def apply_sums(self, sums, grad_sum, egrad_sum):
+        """Averages + optimiser step from (possibly all-reduced) totals."""
+        a = Averages()
+        g = np.ascontiguousarray(grad_sum, np.float64).reshape(self.E, self.P)
+        ge = np.ascontiguousarray(egrad_sum, np.float64).reshape(self.E, self.P)
+        self._check(library().vmc_apply_sums(self._h, ctypes.byref(sums), _p(g), _p(ge),
+                                             ctypes.byref(a)))
+        return a
+
     def run_iteration(self, iteration):
         a = Averages()
         self._check(library().vmc_run_iteration(self._h, iteration, ctypes.byref(a)))
@@ -224,6 +234,12 @@ class Engine:
         ms = ctypes.c_double()
         self._check(library().vmc_stopwatch(self._h, 1, ctypes.byref(ms)))
         return ms.value
+
+    def refresh_interval(self):
+        """Current FP64 rebuild cadence in steps (autotuned for `refreshInterval: auto`)."""
+        info = Info()
+        self._check(library().vmc_get_info(self._h, ctypes.byref(info)))
+        return info.refresh_interval
 
     def status(self):
         out = np.zeros(self.W, np.uint32)
