@@ -37,8 +37,8 @@ N_PART, OMEGA, DT = 56, 0.28, 0.005
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "vmachine_ref")
 
 
-def workload_text(walkers, steps_per_walker, precision, seed):
-    return "\n".join([
+def workload_text(walkers, steps_per_walker, precision, seed, refresh="auto"):
+    return "\n".join([f"refreshInterval: {refresh}",
         f"numParticles: {N_PART}", "numDimensions: 2", "hamiltonian: harmonicOscillator",
         f"omega: {OMEGA}", "interactionStyle: coulomb",
         "waveFunctionElement: slaterDeterminant", "waveFunctionElement: gaussian",
@@ -240,7 +240,7 @@ def run_engine_arm(args):
     from vmachine_b200 import distributed as vd
     W, spw = args.walkers, args.steps_per_walker
     seed = 1000 + rank
-    text = workload_text(W, spw, "mixed", seed)
+    text = workload_text(W, spw, "mixed", seed, args.refresh_interval)
     eng = Engine(text, device=local)
     eng.init_walkers(None, seed=seed)
     burn = eng.info.burn_in
@@ -248,17 +248,18 @@ def run_engine_arm(args):
     for it in range(args.warmup):
         vd.run_iteration(eng, it)
     barrier(pg, local)
-    sweep_s, launches, sig = 0.0, 0.0, []
+    sweep_s, launches, sig, energies = 0.0, 0.0, [], []
     with ClockSampler(local) as clk:
         eng.stopwatch_start()
         for it in range(args.steps):
             a = vd.run_iteration(eng, args.warmup + it)  # all-reduce of the sums when N > 1
             sig.append(a.walker_std_error)
+            energies.append((a.energy, a.walker_std_error))
         ms = eng.stopwatch_stop()
     # per-launch sweep timing of one more iteration (same work, not in the timed region)
     sums, _, _ = eng.sample(args.warmup + args.steps, spw + burn, burn)
     sweep_s, launches = sums.sweep_seconds, sums.sweep_launches
-    max_drift = sums.max_drift
+    max_drift, q99_drift = sums.max_drift, sums.q99_drift
     refresh_now = eng.refresh_interval()
     ms = max_over_ranks(pg, local, ms)
     total_moves = moves_per_step * args.steps * world
@@ -287,17 +288,23 @@ def run_engine_arm(args):
     # FP64 engine on the same workload (same walkers, fewer steps per iteration)
     fp64 = None
     if not args.no_fp64:
-        eng64 = Engine(workload_text(W, args.fp64_steps_per_walker, "fp64", seed), device=local)
+        # same walkers, seeds and schedule as the mixed arm: energies comparable
+        eng64 = Engine(workload_text(W, spw, "fp64", seed), device=local)
         eng64.init_walkers(None, seed=seed)
-        vd.run_iteration(eng64, 0)
+        for it in range(args.warmup):
+            vd.run_iteration(eng64, it)
         barrier(pg, local)
         eng64.stopwatch_start()
-        a64 = vd.run_iteration(eng64, 1)
-        ms64 = max_over_ranks(pg, local, eng64.stopwatch_stop())
-        mv64 = W * (args.fp64_steps_per_walker + eng64.info.burn_in) * world
-        fp64 = {"value": mv64 / (ms64 * 1e-3), "ms_per_step": ms64,
-                "steps_per_walker": args.fp64_steps_per_walker, "energy": a64.energy,
-                "sigma_e_walkers": a64.walker_std_error}
+        e64 = []
+        for it in range(args.fp64_steps):
+            a64 = vd.run_iteration(eng64, args.warmup + it)
+            e64.append((a64.energy, a64.walker_std_error))
+        ms64 = max_over_ranks(pg, local, eng64.stopwatch_stop()) / args.fp64_steps
+        mv64 = W * (spw + eng64.info.burn_in) * world
+        fp64 = {"value": mv64 / (ms64 * 1e-3), "ms_per_step": ms64, "steps": args.fp64_steps,
+                "energy": e64[-1][0], "sigma_e_walkers": e64[-1][1],
+                "mixed_energy_same_iteration": energies[args.fp64_steps - 1][0],
+                "mixed_sigma_same_iteration": energies[args.fp64_steps - 1][1]}
         eng64.close()
 
     if rank != 0:
@@ -319,7 +326,7 @@ def run_engine_arm(args):
                                f"dt={DT}, E_L + dlnPsi every move, ADAM",
                    "walkers_per_gpu": W, "steps_per_walker": spw, "burn_in": burn,
                    "precision": "mixed", "refresh_interval": refresh_now,
-                   "max_inverse_drift": max_drift,
+                   "inverse_drift": {"max": max_drift, "q99": q99_drift},
                    "walkers_per_block": eng.info.walkers_per_block,
                    "l2": "walker state %.0f MB per GPU > 126 MB L2, streamed every launch"
                          % (W * (eng.info.n_coords * 5 * 4 + 2 * 28 * 28 * 4 + 56 * 8 + 64) / 1e6)},
@@ -361,7 +368,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--walkers", type=int, default=16384)
     ap.add_argument("--steps-per-walker", type=int, default=20000)
-    ap.add_argument("--fp64-steps-per-walker", type=int, default=4000)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--refresh-interval", default="auto")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-steps", type=int, default=60000)
     ap.add_argument("--no-e2e", action="store_true")

@@ -80,6 +80,7 @@ typedef struct {
     double sweep_seconds; /* device time of the sweep kernel launches alone            */
     double sweep_launches;/* number of sweep kernel launches                           */
     double max_drift;     /* mixed precision: largest |inverse - FP64 rebuild| / |inverse| seen */
+    double q99_drift;     /* its 99th percentile over walkers (drives refreshInterval: auto) */
     uint32_t status;      /* OR of walker status bits (1 NaN energy, 2 bad ratio, 4 singular) */
 } vmc_sums;
 

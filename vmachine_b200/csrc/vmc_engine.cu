@@ -248,7 +248,7 @@ int run_rebuild(vmc_engine *e, int mode, double *drift)
     a.mode = mode;
     a.drift = drift;
     a.wpb = 4;
-    a.smem_per_warp = std::max(16, round_up(2 * e->n_orb * e->n_orb * 8, 16));
+    a.smem_per_warp = std::max(16, round_up(e->n_orb * e->n_orb * 8, 16));
     const size_t smem = (size_t)a.wpb * a.smem_per_warp;
     CUDA_TRY(cudaFuncSetAttribute(e->ks.rebuild, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (e->W + a.wpb - 1) / a.wpb;
@@ -671,12 +671,20 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         CUDA_TRY(cudaEventElapsedTime(&t, e->sweep_events[2 * i], e->sweep_events[2 * i + 1]));
         sweep_ms += t;
     }
+    double q99_drift = 0.0;
     for (double d : drift) max_drift = std::max(max_drift, d);
+    if (!drift.empty()) {
+        const size_t i99 = (size_t)(0.99 * (drift.size() - 1));
+        std::nth_element(drift.begin(), drift.begin() + i99, drift.end());
+        q99_drift = drift[i99];
+    }
     if (e->refresh_auto && n_refresh) {
-        // FP64 re-inversion cadence against the measured drift of the FP32
-        // Sherman-Morrison inverse: halve past the tolerance, double well below it
-        if (max_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
-        else if (max_drift < e->drift_tol / 16) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
+        // FP64 re-inversion cadence against the drift of the FP32 Sherman-Morrison
+        // inverse: the 99th percentile over walkers (the maximum is set by the few
+        // walkers sitting near a node of the determinant) halves the interval past
+        // the tolerance and doubles it well below
+        if (q99_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
+        else if (q99_drift < e->drift_tol / 16) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
     }
     vmc_sums s{};
     s.energy = sums[0];
@@ -694,6 +702,7 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
     s.sweep_seconds = sweep_ms * 1e-3;
     s.sweep_launches = n_launch;
     s.max_drift = max_drift;
+    s.q99_drift = q99_drift;
     for (unsigned v : st) s.status |= v;
     e->last = s;
     e->last_samples_per_walker = steps - burn_in;

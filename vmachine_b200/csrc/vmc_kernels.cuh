@@ -10,8 +10,9 @@
 //   dd[D]     d ln det / dx_k  (SlaterDeterminant::m_determinantDerivative)
 //   sdd[D]    (d^2 det / dx_k^2) / det (m_determinantSecondDerivative)
 //   gj[D]     d J / dx_k of the Pade factor, J = sum_{i<j} beta r/(1 + gamma r)
-//   inv[2][n][n]  inverse Slater blocks, inv[b][o][i] = A_b^{-1}(o, i) for orbital o,
-//                 particle i of spin block b (m_slaterMatrixInverse, n x N)
+//   inv[2][n][S]  inverse Slater blocks stored by particle: row i of block b holds
+//                 A_b^{-1}(o, i) for the orbitals o (the reference's
+//                 m_slaterMatrixInverse, n x N, column b*n + i), row stride S
 //
 // plus FP64 per-walker scalars (running sums, see SC_*), a 64-bit per-particle mask
 // of Pade pairs computed with the current gamma, and the Philox step counter.
@@ -35,9 +36,21 @@ enum : int {
 struct Layout {
     int N, D, n;  // particles, coordinates, orbitals per spin block (0: no Slater)
     int off_x, off_fc, off_dd, off_sdd, off_gj, off_inv, rec;  // in elements of T
+    int inv_stride;  // row stride S of the inverse blocks
 };
 
 __host__ __device__ inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Row stride of an inverse block: a multiple of the 16-byte vector width VE (4
+// floats or 2 doubles) with an odd number of vectors, so that the 8 lanes of one
+// 128-bit shared-memory phase start on distinct 4-bank groups (no conflicts).
+__host__ __device__ constexpr int inv_row_stride(int n, int elem_bytes)
+{
+    const int ve = 16 / elem_bytes;
+    int s = (n + ve - 1) / ve * ve;
+    if (s > 0 && ((s / ve) & 1) == 0) s += ve;
+    return s;
+}
 
 __host__ __device__ inline Layout make_layout(int N, int dim, int n, int elem_bytes)
 {
@@ -53,7 +66,8 @@ __host__ __device__ inline Layout make_layout(int N, int dim, int n, int elem_by
     L.off_sdd = L.off_dd + Dp;
     L.off_gj = L.off_sdd + Dp;
     L.off_inv = L.off_gj + Dp;
-    L.rec = round_up(L.off_inv + 2 * n * n, a);
+    L.inv_stride = inv_row_stride(n, elem_bytes);
+    L.rec = round_up(L.off_inv + 2 * n * L.inv_stride, a);
     return L;
 }
 
@@ -140,7 +154,6 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
     const Layout L = P.L;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double *A = reinterpret_cast<double *>(smem_raw + (size_t)wib * a.smem_per_warp);
-    double *B = A + NO * NO;
     const int N = P.N, D = L.D, flags = P.flags;
     const double wa = P.omega * P.alpha, az = P.alpha_h * P.Z;
 
@@ -172,9 +185,15 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
                         if (DIM == 3) phi *= hv[DIM - 1][m2];
                         A[lane * NO + o] = phi;
                     });
-                    for (int o = 0; o < NO; ++o) B[lane * NO + o] = (o == lane) ? 1.0 : 0.0;
                 }
                 __syncwarp();
+                // In-place Gauss-Jordan inversion with partial (row) pivoting: column c
+                // of the working array becomes column c of the inverse; the row swaps
+                // are undone as column swaps at the end.  Elimination factors are read
+                // once per column and broadcast by shuffle.
+                int perm_mine = lane;  // lane c records the pivot row of column c
+                double pivprod = 1.0;  // |product of pivots| as mantissa x 2^pivexp
+                int pivexp = 0;
                 for (int c = 0; c < NO; ++c) {
                     double v = (lane >= c && lane < NO) ? fabs(A[lane * NO + c]) : -1.0;
                     int idx = lane;
@@ -186,39 +205,56 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
                     }
                     const int pr = idx;
                     if (!(v > 0.0)) status |= ST_SINGULAR;
-                    __syncwarp();
+                    if (lane == c) perm_mine = pr;
                     if (pr != c && lane < NO) {
-                        double t = A[c * NO + lane]; A[c * NO + lane] = A[pr * NO + lane]; A[pr * NO + lane] = t;
-                        t = B[c * NO + lane]; B[c * NO + lane] = B[pr * NO + lane]; B[pr * NO + lane] = t;
+                        const double t = A[c * NO + lane];
+                        A[c * NO + lane] = A[pr * NO + lane];
+                        A[pr * NO + lane] = t;
                     }
                     __syncwarp();
                     const double piv = A[c * NO + c];
-                    logdet += log(fabs(piv));
-                    const double ip = 1.0 / piv;
-                    __syncwarp();
-                    if (lane < NO) { A[c * NO + lane] *= ip; B[c * NO + lane] *= ip; }
-                    __syncwarp();
-                    for (int r = 0; r < NO; ++r) {
-                        if (r == c) continue;
-                        const double f = A[r * NO + c];
-                        __syncwarp();
-                        if (lane < NO && f != 0.0) {
-                            A[r * NO + lane] -= f * A[c * NO + lane];
-                            B[r * NO + lane] -= f * B[c * NO + lane];
-                        }
-                        __syncwarp();
+                    {
+                        int ex;
+                        pivprod = frexp(pivprod * fabs(piv), &ex);
+                        pivexp += ex;
                     }
+                    const double ip = 1.0 / piv;
+                    // pivot row (lanes over columns) and elimination factors (lanes over rows)
+                    const int lc = lane < NO ? lane : 0;
+                    const double rowc = ((lane == c) ? 1.0 : A[c * NO + lc]) * ip;
+                    const double fr = (lane != c && lane < NO) ? A[lc * NO + c] : 0.0;
+                    __syncwarp();
+                    if (lane < NO) A[c * NO + lane] = rowc;
+                    for (int r = 0; r < NO; ++r) {
+                        const double f = __shfl_sync(FULL, fr, r);
+                        if (r != c && lane < NO) {
+                            const double a0 = (lane == c) ? 0.0 : A[r * NO + lane];
+                            A[r * NO + lane] = a0 - f * rowc;
+                        }
+                    }
+                    __syncwarp();
                 }
-                // B[o][i] = A^{-1}(o, i): store, measure drift of the carried inverse
-                T *invb = inv + b * NO * NO;
+                logdet += log(pivprod) + pivexp * 0.6931471805599453;  // ln 2
+                // undo the row interchanges as column interchanges, last first
+                for (int c = NO - 1; c >= 0; --c) {
+                    const int pr = __shfl_sync(FULL, perm_mine, c);
+                    if (pr != c && lane < NO) {
+                        const double t = A[lane * NO + c];
+                        A[lane * NO + c] = A[lane * NO + pr];
+                        A[lane * NO + pr] = t;
+                    }
+                    __syncwarp();
+                }
+                // A now holds A^{-1}: A[o][i] = A^{-1}(o, i); store as row i, measure drift
+                T *row = inv + (size_t)(b * NO + (lane < NO ? lane : 0)) * L.inv_stride;
                 if (lane < NO) {
                     for (int o = 0; o < NO; ++o) {
-                        const double nv = B[o * NO + lane];
+                        const double nv = A[o * NO + lane];
                         if (a.mode == RB_REFRESH) {
-                            drift_num = fmax(drift_num, fabs((double)invb[o * NO + lane] - nv));
+                            drift_num = fmax(drift_num, fabs((double)row[o] - nv));
                             drift_den = fmax(drift_den, fabs(nv));
                         }
-                        invb[o * NO + lane] = T(nv);
+                        row[o] = T(nv);
                     }
                     // derivative vectors with the FP64 inverse
                     const int q = b * NO + lane;
@@ -233,7 +269,7 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
                     for (int c = 0; c < DIM; ++c) { gd[c] = 0.0; sd[c] = 0.0; }
                     for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
                         const int mm[3] = {m0, m1, m2};
-                        const double iv = B[o * NO + lane];
+                        const double iv = A[o * NO + lane];
 #pragma unroll
                         for (int c = 0; c < DIM; ++c) {
                             double t = iv;
@@ -272,7 +308,7 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
                 double dxv[DIM], r2 = 0.0;
 #pragma unroll
                 for (int c = 0; c < DIM; ++c) { dxv[c] = xi[c] - (double)x[j * DIM + c]; r2 += dxv[c] * dxv[c]; }
-                const double r = sqrt(r2), ir = 1.0 / r;
+                const double ir = rsqrt(r2), r = r2 * ir;
                 if (flags & F_PADE) {
                     const double beta = same_spin(i, j, N) ? P.beta_same : P.beta_anti;
                     const double gp = ((flags & Q_PADE_STALE) && !((mi >> j) & 1ull)) ? P.gamma_prev : P.gamma;

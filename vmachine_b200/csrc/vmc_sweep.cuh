@@ -5,7 +5,7 @@
 //      stream); propose x_k' (brute force: bruteforce.cpp:34; importance sampling
 //      with the drift 2 grad ln Psi: importancesampling.cpp:49-60);
 //   2. |Psi'|^2/|Psi|^2 per element without touching the state:
-//      Slater  R = phi(r_p') . inv[:, p]   (lanes over inverse columns)
+//      Slater  R = phi(r_p') . inv[:, p]   (lane j reads row j of the transposed inverse)
 //      Pade    sum over partners of beta (h' - h)   (lanes over partners)
 //   3. accept: Sherman-Morrison rank-1 update of the moved particle's spin block,
 //      refresh of that block's d ln det / d^2 det / det vectors, Pade gradient
@@ -59,6 +59,40 @@ __device__ __forceinline__ T orbital_dot(const T (&hv)[DIM][K], V &&v)
     return s;
 }
 
+// Per-degree partial sums of the derivative vectors: orbital o = (m0, m1, m2) with
+// inverse entry v adds, for each dimension c, prod_{c' != c} h_{m_c'} * v to
+// part[c][m_c].
+template <typename T, int DIM, int K>
+__device__ __forceinline__ void accumulate_orbital(const T (&hv)[DIM][K], T (&part)[DIM][K], T v,
+                                                   int m0, int m1, int m2)
+{
+    if (DIM == 2) {
+        part[0][m0] += hv[1][m1] * v;
+        part[1][m1] += hv[0][m0] * v;
+    } else {
+        part[0][m0] += (hv[1][m1] * hv[DIM - 1][m2]) * v;
+        part[1][m1] += (hv[0][m0] * hv[DIM - 1][m2]) * v;
+        part[DIM - 1][m2] += (hv[0][m0] * hv[1][m1]) * v;
+    }
+}
+
+// d_c phi . v = sum_m h'_m(x_c) part[c][m],  d_c^2 phi . v = sum_m h''_m(x_c) part[c][m]
+template <typename T, int DIM, int K>
+__device__ __forceinline__ void contract_orbitals(const T (&hv)[DIM][K], const T (&part)[DIM][K],
+                                                  T (&gd)[DIM], T (&sd)[DIM])
+{
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+        T g = T(0), s2 = T(0);
+#pragma unroll
+        for (int m = 1; m < K; ++m) g += hC<T>(m) * hv[c][m - 1] * part[c][m];
+#pragma unroll
+        for (int m = 2; m < K; ++m) s2 += hE<T>(m) * hv[c][m - 2] * part[c][m];
+        gd[c] = g;
+        sd[c] = s2;
+    }
+}
+
 // d_c phi(r) . v and d_c^2 phi(r) . v for every dimension c.
 template <typename T, int DIM, int K, typename V>
 __device__ __forceinline__ void orbital_derivs(const T (&hv)[DIM][K], V &&vf, T (&gd)[DIM],
@@ -70,25 +104,31 @@ __device__ __forceinline__ void orbital_derivs(const T (&hv)[DIM][K], V &&vf, T 
 #pragma unroll
         for (int m = 0; m < K; ++m) part[c][m] = T(0);
     for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
-        const T v = vf(o);
-        if (DIM == 2) {
-            part[0][m0] += hv[1][m1] * v;
-            part[1][m1] += hv[0][m0] * v;
-        } else {
-            part[0][m0] += (hv[1][m1] * hv[DIM - 1][m2]) * v;
-            part[1][m1] += (hv[0][m0] * hv[DIM - 1][m2]) * v;
-            part[DIM - 1][m2] += (hv[0][m0] * hv[1][m1]) * v;
-        }
+        accumulate_orbital<T, DIM, K>(hv, part, vf(o), m0, m1, m2);
     });
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-        T g = T(0), s2 = T(0);
-#pragma unroll
-        for (int m = 1; m < K; ++m) g += hC<T>(m) * hv[c][m - 1] * part[c][m];
-#pragma unroll
-        for (int m = 2; m < K; ++m) s2 += hE<T>(m) * hv[c][m - 2] * part[c][m];
-        gd[c] = g;
-        sd[c] = s2;
+    contract_orbitals<T, DIM, K>(hv, part, gd, sd);
+}
+
+// 16-byte shared-memory vector of 4 floats or 2 doubles
+template <typename T>
+__device__ __forceinline__ void vload(const T *p, T *out)
+{
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    } else {
+        const double2 v = *reinterpret_cast<const double2 *>(p);
+        out[0] = v.x; out[1] = v.y;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void vstore(T *p, const T *in)
+{
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4 *>(p) = make_float4(in[0], in[1], in[2], in[3]);
+    } else {
+        *reinterpret_cast<double2 *>(p) = make_double2(in[0], in[1]);
     }
 }
 
@@ -126,14 +166,13 @@ __device__ __forceinline__ void store_coords(T *x, int j, const T (&in)[DIM])
 // ratio (compat off): Slater part (d_a phi(r_p') . inv[:, p]) / R.  Out of line so
 // its registers stay off the common path; compiled out of the compat kernels.
 template <typename T, int DIM, int K>
-__device__ __noinline__ T slater_grad_new(const T *invb, const T *xpn, int adim, int pl, T R)
+__device__ __noinline__ T slater_grad_new(const T *row_p, const T *xpn, int adim, T R)
 {
     T hv[DIM][K];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
     T gd[DIM], sd[DIM];
-    constexpr int NO = Shells<DIM, K>::n;
-    orbital_derivs<T, DIM, K>(hv, [&](int o) { return invb[o * NO + pl]; }, gd, sd);
+    orbital_derivs<T, DIM, K>(hv, [&](int o) { return row_p[o]; }, gd, sd);
     T g = gd[0];
 #pragma unroll
     for (int c = 1; c < DIM; ++c)
@@ -170,15 +209,9 @@ __device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
     return t;
 }
 
-// Register-resident inverse: each lane would keep its inverse columns (one per
-// spin block) in registers, since the S_j dot, the Sherman-Morrison update and the
-// derivative refresh all read column `lane`.  Measured with ptxas at N = 56: the
-// two 28-entry columns plus the step's working set need more than 200 registers
-// per thread and spill, so the inverse stays in shared memory for every shape.
-template <typename T, int K>
-struct InvInRegisters {
-    static constexpr bool value = false;
-};
+// A register-resident inverse (each lane keeping its two rows in registers) was
+// measured with ptxas at N = 56: the two 28-entry rows plus the step's working set
+// need more than 200 registers per thread and spill, so rows stay in shared memory.
 
 template <typename T, int DIM, int K, int FX>
 __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
@@ -188,8 +221,9 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
     constexpr int NO = K > 0 ? Shells<DIM, K>::n : 0;
     constexpr int NK = 2 * NO;                  // particles when the Slater fixes N
     constexpr int DK = NK * DIM;                // coordinates when the Slater fixes N
-    constexpr bool REGINV = InvInRegisters<T, K>::value;
-    constexpr int NOR = REGINV ? NO : 1;
+    constexpr int VE = 16 / (int)sizeof(T);                     // entries per 16-byte vector
+    constexpr int IS = K > 0 ? inv_row_stride(NO, sizeof(T)) : 0; // inverse row stride
+    constexpr int NQ = (NO + VE - 1) / VE;                        // vectors per inverse row
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params &P = a.P;
     const Layout L = P.L;
@@ -197,9 +231,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
     T *sm = reinterpret_cast<T *>(smem_raw + (size_t)wib * a.smem_per_warp);
     const int N = K > 0 ? NK : P.N;
     const int D = K > 0 ? DK : L.D;
-    const int sm_elems = REGINV ? L.off_inv : L.rec;  // record part staged in shared memory
-    unsigned long long *smask = reinterpret_cast<unsigned long long *>(sm + sm_elems);
-    T creg[2][NOR];
+    unsigned long long *smask = reinterpret_cast<unsigned long long *>(sm + L.rec);
     double *ssc = reinterpret_cast<double *>(smask + N);
     T *x = sm + L.off_x, *fc = sm + L.off_fc, *dd = sm + L.off_dd, *sdd = sm + L.off_sdd;
     T *gj = sm + L.off_gj, *inv = sm + L.off_inv;
@@ -220,14 +252,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
 
     for (int w = blockIdx.x * a.wpb + wib; w < P.W; w += gridDim.x * a.wpb) {
         T *g_rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
-        copy_in(sm, g_rec, sm_elems, lane);
-        if constexpr (REGINV) {
-#pragma unroll
-            for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-                for (int o = 0; o < NO; ++o)
-                    creg[bb][o] = lane < NO ? g_rec[L.off_inv + (bb * NO + o) * NO + lane] : T(0);
-        }
+        copy_in(sm, g_rec, L.rec, lane);
         for (int j = lane; j < N; j += 32) smask[j] = P.mask[(size_t)w * N + j];
         if (lane < NSCAL) ssc[lane] = P.scal[(size_t)w * NSCAL + lane];
         double acc_s = 0.0, acc_c = 0.0;
@@ -327,12 +352,13 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                 T hv[DIM][K];
 #pragma unroll
                 for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
-                if constexpr (REGINV) {
-                    if (b == 0) Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return creg[0][o]; });
-                    else Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return creg[1][o]; });
-                } else if (lane < NO) {
-                    const T *col = inv + b * NO * NO + lane;
-                    Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return col[o * NO]; });
+                if (lane < NO) {
+                    // this lane's row (column `lane` of A^{-1}), 16-byte vector loads
+                    T rv[NQ * VE];
+                    const T *row = inv + (b * NO + lane) * IS;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) vload<T>(row + q * VE, rv + q * VE);
+                    Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return rv[o]; });
                 }
                 R = __shfl_sync(FULL, Sj, pl);
             }
@@ -434,21 +460,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                         if (flags & F_GAUSS) gy += -wa * xn;
                         if (flags & F_PADE) gy += __shfl_sync(FULL, pair_total, 16 + 4 * adim);
                         if (flags & F_HYDROGENLIKE) gy += -T(P.alpha_h * P.Z) * xn / rpn;
-                        if constexpr (REGINV) {
-                            T hvn[DIM][K];
-#pragma unroll
-                            for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hvn[c]);
-                            T gd[DIM], sd[DIM];
-                            if (b == 0) orbital_derivs<T, DIM, K>(hvn, [&](int o) { return creg[0][o]; }, gd, sd);
-                            else orbital_derivs<T, DIM, K>(hvn, [&](int o) { return creg[1][o]; }, gd, sd);
-                            T g = gd[0];
-#pragma unroll
-                            for (int c = 1; c < DIM; ++c)
-                                if (c == adim) g = gd[c];
-                            gy += __shfl_sync(FULL, g, pl) / R;
-                        } else if constexpr (K > 0) {
-                            gy += slater_grad_new<T, DIM, K>(inv + b * NO * NO, xpn, adim, pl, R);
-                        }
+                        if constexpr (K > 0) gy += slater_grad_new<T, DIM, K>(inv + (b * NO + pl) * IS, xpn, adim, R);
                         const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
                         wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
                     }
@@ -480,54 +492,46 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                     }
                 }
                 if constexpr (K > 0) {
-                    // Sherman-Morrison (slaterdeterminant.cpp:165-175)
-                    T *invb = inv + b * NO * NO;
+                    // Sherman-Morrison (slaterdeterminant.cpp:165-175) on the rows of
+                    // block b, fused with the refresh of the block's derivative vectors
+                    // (slaterdeterminant.cpp:155-163): lane j updates row j and feeds
+                    // the new entries straight into particle j's d ln det sums.
                     const T rinv = F::rcp(R);  // an accepted move has |R| well above underflow
                     const T coef = Sj * rinv;
-                    if constexpr (REGINV) {
-                        auto update = [&](T (&cr)[NOR]) {
-#pragma unroll
-                            for (int o = 0; o < NO; ++o) {
-                                const T c = __shfl_sync(FULL, cr[o], pl);  // inv[o][pl]
-                                cr[o] = (lane == pl) ? c * rinv : cr[o] - coef * c;
-                            }
-                        };
-                        if (b == 0) update(creg[0]);
-                        else update(creg[1]);
-                    } else {
-                        // lanes >= NO read a valid entry and store nothing (a predicated
-                        // store, no branch per row)
-                        const int lc = lane < NO ? lane : 0;
-                        const T colp = invb[lc * NO + pl];
-                        __syncwarp();
-#pragma unroll
-                        for (int o = 0; o < NO; ++o) {
-                            const T c = __shfl_sync(FULL, colp, o);
-                            const T v = invb[o * NO + lc];
-                            const T nv = (lane == pl) ? c * rinv : v - coef * c;
-                            if (lane < NO) invb[o * NO + lane] = nv;
-                        }
-                    }
-                    __syncwarp();
-                    // d ln det / dx and (d^2 det / dx^2) / det of the block
-                    // (slaterdeterminant.cpp:155-163), lanes over the block's particles
-                    if (lane < NO) {
-                        const int q = b * NO + lane;
+                    __syncwarp();  // x[k] written by lane 0
+                    const int lr = lane < NO ? lane : pl;   // lanes >= NO shadow row pl, store nothing
+                    T *row_j = inv + (b * NO + lr) * IS;
+                    const T *row_p = inv + (b * NO + pl) * IS;
+                    T hv[DIM][K];
+                    {
                         T xq[DIM];
-                        load_coords<T, DIM>(x, q, xq);
-                        T hv[DIM][K];
+                        load_coords<T, DIM>(x, b * NO + lr, xq);
 #pragma unroll
                         for (int c = 0; c < DIM; ++c) hermite_values<K>(xq[c], hv[c]);
+                    }
+                    T part[DIM][K];
+#pragma unroll
+                    for (int c = 0; c < DIM; ++c)
+#pragma unroll
+                        for (int m = 0; m < K; ++m) part[c][m] = T(0);
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) {
+                        T cv[VE], vv[VE];
+                        vload<T>(row_p + q * VE, cv);   // old row of the moved particle
+                        vload<T>(row_j + q * VE, vv);
+                        __syncwarp();                   // row p read by all before it changes
+#pragma unroll
+                        for (int e = 0; e < VE; ++e) vv[e] = (lane == pl) ? cv[e] * rinv : vv[e] - coef * cv[e];
+                        if (lane < NO) vstore<T>(row_j + q * VE, vv);
+                        for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
+                            if (o / VE == q) accumulate_orbital<T, DIM, K>(hv, part, vv[o % VE], m0, m1, m2);
+                        });
+                    }
+                    if (lane < NO) {
                         T gd[DIM], sd[DIM];
-                        if constexpr (REGINV) {
-                            if (b == 0) orbital_derivs<T, DIM, K>(hv, [&](int o) { return creg[0][o]; }, gd, sd);
-                            else orbital_derivs<T, DIM, K>(hv, [&](int o) { return creg[1][o]; }, gd, sd);
-                        } else {
-                            const T *col = invb + lane;
-                            orbital_derivs<T, DIM, K>(hv, [&](int o) { return col[o * NO]; }, gd, sd);
-                        }
-                        store_coords<T, DIM>(dd, q, gd);
-                        store_coords<T, DIM>(sdd, q, sd);
+                        contract_orbitals<T, DIM, K>(hv, part, gd, sd);
+                        store_coords<T, DIM>(dd, b * NO + lane, gd);
+                        store_coords<T, DIM>(sdd, b * NO + lane, sd);
                     }
                 }
                 if (flags & F_PADE) {
@@ -637,18 +641,10 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
         // ---- write the walker back
         __syncwarp();
         {
-            const int nv = sm_elems * (int)sizeof(T) / 16;
+            const int nv = L.rec * (int)sizeof(T) / 16;
             const uint4 *s4 = reinterpret_cast<const uint4 *>(sm);
             uint4 *d4 = reinterpret_cast<uint4 *>(g_rec);
             for (int i = lane; i < nv; i += 32) d4[i] = s4[i];
-        }
-        if constexpr (REGINV) {
-            if (lane < NO) {
-#pragma unroll
-                for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-                    for (int o = 0; o < NO; ++o) g_rec[L.off_inv + (bb * NO + o) * NO + lane] = creg[bb][o];
-            }
         }
         for (int j = lane; j < N; j += 32) P.mask[(size_t)w * N + j] = smask[j];
         if (lane < NSCAL) P.scal[(size_t)w * NSCAL + lane] = ssc[lane];

@@ -38,7 +38,7 @@ class Sums(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "energy", "energy2", "kinetic", "kinetic2", "external", "external2", "interaction",
         "interaction2", "accepts", "n_samples", "n_window", "seconds", "sweep_seconds",
-        "sweep_launches", "max_drift")] + [
+        "sweep_launches", "max_drift", "q99_drift")] + [
         ("status", ctypes.c_uint32)]
 
 
