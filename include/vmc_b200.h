@@ -185,6 +185,40 @@ int vmc_stopwatch(vmc_engine *e, int mode, double *ms);
  * roofline denominator of the CUDA-core-bound sweep kernel. */
 int vmc_measure_fma_peak(int device, int precision, double *tflops);
 
+/* ---- Allocation-free evaluation (no counterpart in the reference) ----
+ *
+ * Kinetic, external and interaction energy ({T, V_ext, V_int}, as vmc_eval's
+ * `energies`) of n_walkers walkers at caller-given positions, in FP64, without
+ * creating an engine and without allocating device memory.  For callers that
+ * cannot allocate at that moment: a process whose device memory is held by
+ * another framework's pool, a loop that must not stall other streams (freeing
+ * device memory synchronises the device), code running while a stream is being
+ * captured into a graph.
+ *
+ * input_in_text: the system as for vmc_create (numWalkers and precision are
+ *   ignored); theta: host, n_elements x p_max row-major, the shape
+ *   vmc_get_info reports; positions: device memory of the current device,
+ *   n_walkers x (numParticles x numDimensions) doubles; energies: device memory
+ *   of the current device, n_walkers x 3 doubles; stream: cudaStream_t (NULL =
+ *   the default stream).  The work is enqueued on `stream` and the call returns
+ *   without waiting: energies are valid once that work completes.  A walker
+ *   whose Slater block is singular at its positions gets NaN energies.
+ *
+ * Every intermediate lives in one fixed device array of
+ * VMC_NOALLOC_SCRATCH_BYTES per device (reserved when the library's module
+ * loads); a walker count whose intermediates do not fit is rejected with
+ * VMC_E_ARG and a message giving the largest count that fits (1,584 walkers
+ * at 56 particles in 2D, 27,503 at 6).  All
+ * calls share that array: calls whose GPU work overlaps (different streams or
+ * host threads without ordering) race and corrupt each other's results, so
+ * serialise them, e.g. on one stream.  The first call on each device looks up
+ * the array's address and uploads the kernels' coefficient table with
+ * synchronous copies: make it before any stream capture. */
+#define VMC_NOALLOC_SCRATCH_BYTES (32u << 20)
+int vmc_local_energies_noalloc(const char *input_in_text, const double *theta, int n_elements,
+                               int p_max, const double *positions, int n_walkers,
+                               double *energies, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,7 @@ __global__ void reduce_acc_kernel(const double *acc, int W, int nacc, double *ou
         out[a] = S + C;
     }
 }
+int set_last_error(int code, const char *msg);
 }  // namespace vmc
 
 namespace {
@@ -54,6 +55,13 @@ int fail(int code, const std::string &msg)
     g_last_error = msg;
     return code;
 }
+
+}  // namespace
+
+// Error channel for entry points defined in other files (vmc_noalloc.cu).
+int vmc::set_last_error(int code, const char *msg) { return fail(code, msg); }
+
+namespace {
 
 #define CUDA_TRY(expr)                                                                   \
     do {                                                                                 \
