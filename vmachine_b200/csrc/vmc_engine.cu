@@ -256,7 +256,7 @@ int run_rebuild(vmc_engine *e, int mode, double *drift)
     a.mode = mode;
     a.drift = drift;
     a.wpb = 4;
-    a.smem_per_warp = std::max(16, round_up(e->n_orb * e->n_orb * 8, 16));
+    a.smem_per_warp = rebuild_smem_per_warp(e->N, e->dim, e->n_orb);
     const size_t smem = (size_t)a.wpb * a.smem_per_warp;
     CUDA_TRY(cudaFuncSetAttribute(e->ks.rebuild, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (e->W + a.wpb - 1) / a.wpb;

@@ -71,6 +71,14 @@ __host__ __device__ inline Layout make_layout(int N, int dim, int n, int elem_by
     return L;
 }
 
+// Shared memory per warp of the rebuild kernel: the pivot row, M (odd row stride)
+// and the pivot rows of the Slater phase, or the positions of the pair phase.
+__host__ __device__ inline int rebuild_smem_per_warp(int N, int dim, int n)
+{
+    const int slater = n > 0 ? ((n + 1) & ~1) * 8 + n * (n | 1) * 8 + n * 4 : 0;
+    return round_up(slater > N * dim * 8 ? slater : N * dim * 8, 16);
+}
+
 constexpr int MAX_ELEM = 8;
 constexpr int MAX_N = 64;
 
@@ -146,7 +154,7 @@ struct RebuildArgs {
 // the Pade gradient vector and pair sums, Coulomb, radial sums and, at
 // initialisation, the importance-sampling force cache.
 template <typename T, int DIM, int K>
-__global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
+__global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
 {
     constexpr int NO = K > 0 ? Shells<DIM, K>::n : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -173,111 +181,125 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
         double logdet = 0.0, drift_num = 0.0, drift_den = 0.0;
 
         if constexpr (K > 0) {
+            // Per block, lane r < NO holds row r of the Slater block, a[o] = phi_o(r_r),
+            // in registers.  Gauss-Jordan with implicit partial pivoting: column c
+            // takes the unused row with the largest |a_rc| (a 32-bit magnitude key
+            // reduced by redux.sync; the lowest lane wins ties), the pivot row goes
+            // through shared memory, and every row is updated in place.  Rows are never
+            // interchanged, so the result M satisfies M[p_c][o] = A^{-1}[c][p_o], with
+            // p_c the pivot row of column c.
+            constexpr int MS = NO | 1;  // odd row stride of M: conflict-free 8-byte access
+            double *buf = A;                                       // pivot row, NO (+1) doubles
+            double *Msm = A + ((NO + 1) & ~1);                      // NO x MS
+            int *prow_of = reinterpret_cast<int *>(Msm + NO * MS);  // p_c, NO ints
+            constexpr int VE = 16 / (int)sizeof(T);
+            constexpr int S = inv_row_stride(NO, (int)sizeof(T));
+            const bool mine = lane < NO;
             for (int b = 0; b < 2; ++b) {
-                // A[i][o] = phi_o(r_i), i in block b
-                if (lane < NO) {
-                    const int q = b * NO + lane;
+                double av[NO];
+                const int q = b * NO + (mine ? lane : 0);
+                {
                     double hv[DIM][K];
 #pragma unroll
                     for (int c = 0; c < DIM; ++c) hermite_values<K>((double)x[q * DIM + c], hv[c]);
                     for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
                         double phi = hv[0][m0] * hv[1][m1];
                         if (DIM == 3) phi *= hv[DIM - 1][m2];
-                        A[lane * NO + o] = phi;
+                        av[o] = mine ? phi : 0.0;
                     });
                 }
-                __syncwarp();
-                // In-place Gauss-Jordan inversion with partial (row) pivoting: column c
-                // of the working array becomes column c of the inverse; the row swaps
-                // are undone as column swaps at the end.  Elimination factors are read
-                // once per column and broadcast by shuffle.
-                int perm_mine = lane;  // lane c records the pivot row of column c
+                bool used = !mine;
+                int col_mine = 0;
                 double pivprod = 1.0;  // |product of pivots| as mantissa x 2^pivexp
                 int pivexp = 0;
-                for (int c = 0; c < NO; ++c) {
-                    double v = (lane >= c && lane < NO) ? fabs(A[lane * NO + c]) : -1.0;
-                    int idx = lane;
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        const double v2 = __shfl_xor_sync(FULL, v, o);
-                        const int i2 = __shfl_xor_sync(FULL, idx, o);
-                        if (v2 > v || (v2 == v && i2 < idx)) { v = v2; idx = i2; }
+                for (int c = 0; c < NO; ++c) {
+                    const unsigned key =
+                        used ? 0u : ((__float_as_uint((float)fabs(av[c])) >> 1) | 0x80000000u);
+                    const unsigned kmax = __reduce_max_sync(FULL, key);
+                    const int p = __ffs(__ballot_sync(FULL, key == kmax)) - 1;  // an unused row < NO
+                    if (lane == p) {
+                        used = true;
+                        col_mine = c;
+                        prow_of[c] = p;
+#pragma unroll
+                        for (int o = 0; o < NO; ++o) buf[o] = (o == c) ? 1.0 : av[o];
                     }
-                    const int pr = idx;
-                    if (!(v > 0.0)) status |= ST_SINGULAR;
-                    if (lane == c) perm_mine = pr;
-                    if (pr != c && lane < NO) {
-                        const double t = A[c * NO + lane];
-                        A[c * NO + lane] = A[pr * NO + lane];
-                        A[pr * NO + lane] = t;
-                    }
-                    __syncwarp();
-                    const double piv = A[c * NO + c];
-                    {
-                        int ex;
-                        pivprod = frexp(pivprod * fabs(piv), &ex);
-                        pivexp += ex;
-                    }
-                    const double ip = 1.0 / piv;
-                    // pivot row (lanes over columns) and elimination factors (lanes over rows)
-                    const int lc = lane < NO ? lane : 0;
-                    const double rowc = ((lane == c) ? 1.0 : A[c * NO + lc]) * ip;
-                    const double fr = (lane != c && lane < NO) ? A[lc * NO + c] : 0.0;
-                    __syncwarp();
-                    if (lane < NO) A[c * NO + lane] = rowc;
-                    for (int r = 0; r < NO; ++r) {
-                        const double f = __shfl_sync(FULL, fr, r);
-                        if (r != c && lane < NO) {
-                            const double a0 = (lane == c) ? 0.0 : A[r * NO + lane];
-                            A[r * NO + lane] = a0 - f * rowc;
+                    const double piv = __shfl_sync(FULL, av[c], p);
+                    if (!(fabs(piv) > 0.0)) status |= ST_SINGULAR;
+                    pivprod *= fabs(piv);
+                    if (c % 6 == 5 || c == NO - 1) {
+                        // renormalise: move the binary exponent into pivexp (normal numbers;
+                        // a zero product already carries ST_SINGULAR)
+                        const long long bits = __double_as_longlong(pivprod);
+                        const int e = (int)((bits >> 52) & 0x7ff);
+                        if (e != 0 && e != 0x7ff) {
+                            pivexp += e - 1023;
+                            pivprod = __longlong_as_double((bits & ~(0x7ffll << 52)) | (1023ll << 52));
                         }
                     }
+                    const double ip = 1.0 / piv;
+                    __syncwarp();
+                    // rows r != p: a_r -= (a_rc / piv) * a_p, with a_rc <- -a_rc / piv;
+                    // row p: a_p <- a_p / piv, with a_pc <- 1 / piv
+                    const double f = (lane == p) ? 1.0 - ip : av[c] * ip;
+                    av[c] = 0.0;
+#pragma unroll
+                    for (int o = 0; o + 1 < NO; o += 2) {
+                        const double2 bv = *reinterpret_cast<const double2 *>(buf + o);
+                        av[o] = fma(-f, bv.x, av[o]);
+                        av[o + 1] = fma(-f, bv.y, av[o + 1]);
+                    }
+                    if (NO & 1) av[NO - 1] = fma(-f, buf[NO - 1], av[NO - 1]);
+                    if (lane == p) av[c] = ip;
                     __syncwarp();
                 }
                 logdet += log(pivprod) + pivexp * 0.6931471805599453;  // ln 2
-                // undo the row interchanges as column interchanges, last first
-                for (int c = NO - 1; c >= 0; --c) {
-                    const int pr = __shfl_sync(FULL, perm_mine, c);
-                    if (pr != c && lane < NO) {
-                        const double t = A[lane * NO + c];
-                        A[lane * NO + c] = A[lane * NO + pr];
-                        A[lane * NO + pr] = t;
-                    }
-                    __syncwarp();
-                }
-                // A now holds A^{-1}: A[o][i] = A^{-1}(o, i); store as row i, measure drift
-                T *row = inv + (size_t)(b * NO + (lane < NO ? lane : 0)) * L.inv_stride;
-                if (lane < NO) {
-                    for (int o = 0; o < NO; ++o) {
-                        const double nv = A[o * NO + lane];
-                        if (a.mode == RB_REFRESH) {
-                            drift_num = fmax(drift_num, fabs((double)row[o] - nv));
-                            drift_den = fmax(drift_den, fabs(nv));
-                        }
-                        row[o] = T(nv);
-                    }
-                    // derivative vectors with the FP64 inverse
-                    const int q = b * NO + lane;
-                    double hv[DIM][K], h1[DIM][K], h2u[DIM][K];
+                if (mine)
 #pragma unroll
-                    for (int c = 0; c < DIM; ++c) {
-                        hermite_values<K>((double)x[q * DIM + c], hv[c]);
-                        hermite_derivs<K>(hv[c], h1[c], h2u[c]);
+                    for (int o = 0; o < NO; ++o) Msm[lane * MS + o] = av[o];
+                __syncwarp();
+                if (mine) {
+                    // row i of the stored inverse holds A^{-1}(c, i) = M[p_c][col(i)], c = 0..NO-1
+                    const double *mcol = Msm + col_mine;
+                    T *row = inv + (size_t)q * L.inv_stride;
+#pragma unroll
+                    for (int v = 0; v < S / VE; ++v) {
+                        T ov[VE], nv[VE];
+                        if (a.mode == RB_REFRESH) vload<T>(row + v * VE, ov);
+#pragma unroll
+                        for (int e2 = 0; e2 < VE; ++e2) {
+                            const int o = v * VE + e2;
+                            const double val = o < NO ? mcol[prow_of[o < NO ? o : 0] * MS] : 0.0;
+                            if (a.mode == RB_REFRESH && o < NO) {
+                                drift_num = fmax(drift_num, fabs((double)ov[e2] - val));
+                                drift_den = fmax(drift_den, fabs(val));
+                            }
+                            nv[e2] = T(val);
+                        }
+                        vstore<T>(row + v * VE, nv);
                     }
+                    // derivative vectors of particle q with the FP64 inverse row
+                    double hv[DIM][K];
+#pragma unroll
+                    for (int c = 0; c < DIM; ++c) hermite_values<K>((double)x[q * DIM + c], hv[c]);
                     double gd[DIM], sd[DIM];
 #pragma unroll
                     for (int c = 0; c < DIM; ++c) { gd[c] = 0.0; sd[c] = 0.0; }
                     for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
                         const int mm[3] = {m0, m1, m2};
-                        const double iv = A[o * NO + lane];
+                        const double iv = mcol[prow_of[o] * MS];
 #pragma unroll
                         for (int c = 0; c < DIM; ++c) {
                             double t = iv;
 #pragma unroll
                             for (int e2 = 0; e2 < DIM; ++e2)
                                 if (e2 != c) t *= hv[e2][mm[e2]];
-                            gd[c] += h1[c][mm[c]] * t;
-                            sd[c] += h2u[c][mm[c]] * t;
+                            const int m = mm[c];
+                            const double d1 = m >= 1 ? hC<double>(m) * hv[c][m >= 1 ? m - 1 : 0] : 0.0;
+                            const double d2 = m >= 2 ? hE<double>(m) * hv[c][m >= 2 ? m - 2 : 0] : 0.0;
+                            gd[c] += d1 * t;
+                            sd[c] += d2 * t;
                         }
                     });
 #pragma unroll
@@ -290,12 +312,17 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
             }
         }
 
+        // positions in shared memory for the pair loop (the Slater scratch is free again)
+        double *xs = A;
+        for (int c = lane; c < D; c += 32) xs[c] = (double)x[c];
+        __syncwarp();
+
         // pair sums: lanes over particles i; pairs j > i counted once
         double lapj = 0.0, bh2 = 0.0, vint = 0.0, invr = 0.0, sumr = 0.0;
         for (int i = lane; i < N; i += 32) {
             double xi[DIM], r2s = 0.0;
 #pragma unroll
-            for (int c = 0; c < DIM; ++c) { xi[c] = (double)x[i * DIM + c]; r2s += xi[c] * xi[c]; }
+            for (int c = 0; c < DIM; ++c) { xi[c] = xs[i * DIM + c]; r2s += xi[c] * xi[c]; }
             const double ri = sqrt(r2s);
             invr += 1.0 / ri;
             sumr += ri;
@@ -307,7 +334,7 @@ __global__ void __launch_bounds__(128) rebuild_kernel(const RebuildArgs a)
                 if (j == i) continue;
                 double dxv[DIM], r2 = 0.0;
 #pragma unroll
-                for (int c = 0; c < DIM; ++c) { dxv[c] = xi[c] - (double)x[j * DIM + c]; r2 += dxv[c] * dxv[c]; }
+                for (int c = 0; c < DIM; ++c) { dxv[c] = xi[c] - xs[j * DIM + c]; r2 += dxv[c] * dxv[c]; }
                 const double ir = rsqrt(r2), r = r2 * ir;
                 if (flags & F_PADE) {
                     const double beta = same_spin(i, j, N) ? P.beta_same : P.beta_anti;

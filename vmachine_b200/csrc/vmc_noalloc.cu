@@ -298,8 +298,8 @@ extern "C" int vmc_local_energies_noalloc(const char *input_in_text, const doubl
     ra.mode = RB_INIT;
     ra.drift = nullptr;
     ra.wpb = 4;
-    ra.smem_per_warp = std::max(16, round_up(s.n_orb * s.n_orb * 8, 16));
-    const size_t rb_smem = (size_t)ra.wpb * ra.smem_per_warp;  // <= 4 x 28 x 28 x 8 B: below the 48 KB default
+    ra.smem_per_warp = rebuild_smem_per_warp(s.c.N, s.c.dim, s.n_orb);
+    const size_t rb_smem = (size_t)ra.wpb * ra.smem_per_warp;  // <= 4 x 6.9 KB (28 orbitals): below the 48 KB default
     void *rb_args[1] = {&ra};
     ce = cudaLaunchKernel(ks.rebuild, dim3((n_walkers + ra.wpb - 1) / ra.wpb), dim3(32 * ra.wpb), rb_args,
                           rb_smem, st);
