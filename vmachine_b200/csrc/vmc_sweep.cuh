@@ -40,6 +40,21 @@ template <> struct Fast<double> {
     static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
 };
 
+// Two values of T in one register pair: FP32 pairs issue one packed sm_100
+// instruction (FFMA2 / FMUL2 / FADD2) for both, FP64 pairs stay two instructions.
+template <typename T> using Two = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+__device__ __forceinline__ float2 two(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 two(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c)
+{
+    return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 mul2(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
 // phi(r) . v, where v(o) returns the column entry of orbital o (shared memory or a
 // lane's registers).
 template <typename T, int DIM, int K, typename V>
@@ -376,40 +391,47 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
             if (flags & (F_PADE | F_COULOMB)) {
                 const unsigned long long mp = smask[p];
                 const T gam = T(P.gamma), gamp = T(P.gamma_prev);
+                // old and new position of the moved particle side by side: every pair
+                // quantity below is a (before, after) pair computed by packed instructions
+                Two<T> xon[DIM];
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) xon[c] = two((c == adim) ? xo : xpn[c], xpn[c]);
+                const Two<T> lap_c = two(T(DIM - 1), T(DIM - 1)), m2gam = two(T(-2) * gam, T(-2) * gam);
 #pragma unroll
                 for (int jj = 0; jj < NJ; ++jj) {
                     const int j = lane + 32 * jj;
                     if (j < N && j != p) {
-                        T dxo[DIM], dxn[DIM], r2o = T(0), r2n = T(0), xjv[DIM];
+                        T xjv[DIM];
                         load_coords<T, DIM>(x, j, xjv);
+                        Two<T> dv[DIM], r2 = two(T(0), T(0));
 #pragma unroll
                         for (int c = 0; c < DIM; ++c) {
-                            const T xj = xjv[c];
-                            dxo[c] = ((c == adim) ? xo : xpn[c]) - xj;
-                            dxn[c] = xpn[c] - xj;
-                            r2o += dxo[c] * dxo[c];
-                            r2n += dxn[c] * dxn[c];
+                            dv[c] = add2(xon[c], two(-xjv[c], -xjv[c]));
+                            r2 = fma2(dv[c], dv[c], r2);
                         }
-                        const T iro = F::rsqrt(r2o), irn = F::rsqrt(r2n);
+                        const Two<T> ir = two(F::rsqrt(r2.x), F::rsqrt(r2.y));
                         if (flags & F_PADE) {
-                            const T ro = r2o * iro, rn = r2n * irn;
+                            const Two<T> r = mul2(r2, ir);
                             const T beta = same_spin(p, j, N) ? T(P.beta_same) : T(P.beta_anti);
                             const T gpair = ((flags & Q_PADE_STALE) && !((mp >> j) & 1ull)) ? gamp : gam;
-                            const T fo1 = F::rcp(T(1) + gpair * ro), fo = beta * fo1 * fo1, ho = ro * fo1;
-                            const T fn1 = F::rcp(T(1) + gam * rn), fn = beta * fn1 * fn1, hn = rn * fn1;
-                            if (!(flags & Q_PADE_RATIO) || j > p) sum_ratio += beta * (hn - ho);
-                            const T fni = fn * irn, foi = fo * iro;
+                            const Two<T> den = fma2(two(gpair, gam), r, two(T(1), T(1)));
+                            const Two<T> f1 = two(F::rcp(den.x), F::rcp(den.y));
+                            const Two<T> h = mul2(r, f1);                              // r / (1 + g r)
+                            const Two<T> fi = mul2(mul2(f1, f1), mul2(two(beta, beta), ir));  // beta f1^2 / r
+                            if (!(flags & Q_PADE_RATIO) || j > p) sum_ratio += beta * (h.y - h.x);
 #pragma unroll
                             for (int c = 0; c < DIM; ++c) {
-                                const T tn = fni * dxn[c];
-                                gp_new[c] += tn;
-                                gdel[jj][c] = foi * dxo[c] - tn;  // particle j sees -(x_p - x_j)
+                                const Two<T> t = mul2(fi, dv[c]);
+                                gp_new[c] += t.y;
+                                gdel[jj][c] = t.x - t.y;  // particle j sees -(x_p - x_j)
                             }
-                            d_lap += T(2) * (fni * (T(DIM) - (T(1) + T(2) * gam * hn)) -
-                                             foi * (T(DIM) - (T(1) + T(2) * gam * ho)));
-                            d_bh2 += beta * (hn * hn - ho * ho);
+                            // 2 f (DIM - (1 + 2 gamma h)) / r, new minus old
+                            const Two<T> lq = mul2(fi, fma2(m2gam, h, lap_c));
+                            d_lap += T(2) * (lq.y - lq.x);
+                            const Two<T> hh = mul2(h, h);
+                            d_bh2 += beta * (hh.y - hh.x);
                         }
-                        if (flags & F_COULOMB) d_vint += irn - iro;
+                        if (flags & F_COULOMB) d_vint += ir.y - ir.x;
                     }
                 }
                 // one reduce-scatter for all pair sums: lane L ends with the total of
@@ -465,8 +487,12 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                         wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
                     }
                 }
+                // the reference rejects when weight < u (bruteforce.cpp:44,
+                // importancesampling.cpp:72); a NaN weight (an FP32 overflow of a proposal
+                // thrown far out by the drift near a node) is flagged and rejected here
+                // instead of accepted
                 if (wgt != wgt) status |= ST_BAD_RATIO;
-                accept = !(wgt < r2);
+                accept = wgt >= r2;
             }
 
             if (accept) {
@@ -497,7 +523,10 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                     // (slaterdeterminant.cpp:155-163): lane j updates row j and feeds
                     // the new entries straight into particle j's d ln det sums.
                     const T rinv = F::rcp(R);  // an accepted move has |R| well above underflow
-                    const T coef = Sj * rinv;
+                    // row j -= (S_j / R) row p for j != p; row p *= 1 / R, written as
+                    // row p += (1 / R - 1) row p (exact when 1 / R lies in [0.5, 2]):
+                    // one fused multiply-add per entry on every lane
+                    const T tl = (lane == pl) ? rinv - T(1) : -(Sj * rinv);
                     __syncwarp();  // x[k] written by lane 0
                     const int lr = lane < NO ? lane : pl;   // lanes >= NO shadow row pl, store nothing
                     T *row_j = inv + (b * NO + lr) * IS;
@@ -521,7 +550,11 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                         vload<T>(row_j + q * VE, vv);
                         __syncwarp();                   // row p read by all before it changes
 #pragma unroll
-                        for (int e = 0; e < VE; ++e) vv[e] = (lane == pl) ? cv[e] * rinv : vv[e] - coef * cv[e];
+                        for (int e = 0; e < VE; e += 2) {
+                            const Two<T> nv = fma2(two(cv[e], cv[e + 1]), two(tl, tl), two(vv[e], vv[e + 1]));
+                            vv[e] = nv.x;
+                            vv[e + 1] = nv.y;
+                        }
                         if (lane < NO) vstore<T>(row_j + q * VE, vv);
                         for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
                             if (o / VE == q) accumulate_orbital<T, DIM, K>(hv, part, vv[o % VE], m0, m1, m2);
@@ -589,8 +622,23 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                             const V vj = reinterpret_cast<const V *>(gj)[vi];
                             const T *ax = reinterpret_cast<const T *>(&vx), *ad = reinterpret_cast<const T *>(&vd);
                             const T *as = reinterpret_cast<const T *>(&vs), *aj = reinterpret_cast<const T *>(&vj);
+                            if (!(flags & F_HYDROGENLIKE)) {
+                                // G^2 + s - g^2 = (G - g)(G + g) + s with G - g the
+                                // Gaussian + Pade part: coordinates two at a time
+                                Two<T> k2 = two(T(0), T(0));
 #pragma unroll
-                            for (int e = 0; e < VW; ++e) coord_term(vi * VW + e, ax[e], ad[e], as[e], aj[e]);
+                                for (int e = 0; e < VW; e += 2) {
+                                    Two<T> A = two(T(0), T(0));
+                                    if (flags & F_GAUSS) A = mul2(two(-wa, -wa), two(ax[e], ax[e + 1]));
+                                    if (flags & F_PADE) A = add2(A, two(aj[e], aj[e + 1]));
+                                    const Two<T> B = fma2(two(T(2), T(2)), two(ad[e], ad[e + 1]), A);
+                                    k2 = fma2(A, B, add2(k2, two(as[e], as[e + 1])));
+                                }
+                                ks += k2.x + k2.y;
+                            } else {
+#pragma unroll
+                                for (int e = 0; e < VW; ++e) coord_term(vi * VW + e, ax[e], ad[e], as[e], aj[e]);
+                            }
                         }
                     }
                 } else {
