@@ -269,9 +269,10 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
     a.wpb = e->wpb;
     a.smem_per_warp = sweep_smem_per_warp(e);
     const size_t smem = (size_t)a.wpb * a.smem_per_warp;
-    CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const void *fn = (!a.probe_k && !a.replay && !a.rec_en && !a.rec_acc) ? e->ks.sweep_plain : e->ks.sweep;
+    CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (e->W + a.wpb - 1) / a.wpb;
-    return launch(e->ks.sweep, grid, 32 * a.wpb, smem, e->stream, &a);
+    return launch(fn, grid, 32 * a.wpb, smem, e->stream, &a);
 }
 
 int choose_wpb(vmc_engine *e)
@@ -282,15 +283,15 @@ int choose_wpb(vmc_engine *e)
     }
     const int per_warp = sweep_smem_per_warp(e);
     cudaFuncAttributes fa;
-    CUDA_TRY(cudaFuncGetAttributes(&fa, e->ks.sweep));
+    CUDA_TRY(cudaFuncGetAttributes(&fa, e->ks.sweep_plain));
     int best = 1, best_warps = -1;
     for (int wpb : {8, 4, 2, 1}) {
         if (32 * wpb > fa.maxThreadsPerBlock) continue;
         const size_t smem = (size_t)wpb * per_warp;
         if (smem > 227 * 1024) continue;
-        CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int blocks = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, e->ks.sweep, 32 * wpb, smem));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, e->ks.sweep_plain, 32 * wpb, smem));
         if (blocks * wpb > best_warps) {
             best_warps = blocks * wpb;
             best = wpb;
@@ -690,9 +691,10 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         // FP64 re-inversion cadence against the drift of the FP32 Sherman-Morrison
         // inverse: the 99th percentile over walkers (the maximum is set by the few
         // walkers sitting near a node of the determinant) halves the interval past
-        // the tolerance and doubles it well below
+        // the tolerance and doubles it below 1/2.5 of it (drift grows about in
+        // proportion to the interval, so a doubling stays under the tolerance)
         if (q99_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
-        else if (q99_drift < e->drift_tol / 16) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
+        else if (q99_drift < e->drift_tol / 2.5) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
     }
     vmc_sums s{};
     s.energy = sums[0];

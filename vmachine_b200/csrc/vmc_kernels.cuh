@@ -513,13 +513,16 @@ __global__ void fma_peak_kernel(R *out, int iters, R m)
 
 struct KernelSet {
     const void *sweep = nullptr, *rebuild = nullptr, *eval = nullptr, *initpos = nullptr;
+    const void *sweep_plain = nullptr;  // production sweep: no probe, replay or recording
 };
 
 template <typename T, int DIM, int K, int FX>
 KernelSet make_set()
 {
     KernelSet s;
-    s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX>);
+    s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, false>);
+    if constexpr (FX != 0) s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
+    else s.sweep_plain = s.sweep;
     s.rebuild = reinterpret_cast<const void *>(&rebuild_kernel<T, DIM, K>);
     s.eval = reinterpret_cast<const void *>(&eval_kernel<T, DIM, K>);
     s.initpos = reinterpret_cast<const void *>(&initial_positions_kernel<T>);

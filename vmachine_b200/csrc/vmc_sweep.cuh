@@ -228,10 +228,16 @@ __device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
 // measured with ptxas at N = 56: the two 28-entry rows plus the step's working set
 // need more than 200 registers per thread and spill, so rows stay in shared memory.
 
-template <typename T, int DIM, int K, int FX>
+template <typename T, int DIM, int K, int FX, bool PL>
 __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
     sweep_kernel(const SweepArgs a)
 {
+    // PL: the production form (Philox numbers, no probe, no recording), with the
+    // branches of the test and replay modes compiled out
+    const int *const probe_k = PL ? nullptr : a.probe_k;
+    const double *const replay = PL ? nullptr : a.replay;
+    double *const rec_en = PL ? nullptr : a.rec_en;
+    unsigned char *const rec_acc = PL ? nullptr : a.rec_acc;
     using F = Fast<T>;
     constexpr int NO = K > 0 ? Shells<DIM, K>::n : 0;
     constexpr int NK = 2 * NO;                  // particles when the Slater fixes N
@@ -282,7 +288,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
         unsigned rng_u = 0u;
         __syncwarp();
 
-        const bool use_philox = !a.probe_k && !a.replay;
+        const bool use_philox = !probe_k && !replay;
         for (int s0 = 0; s0 < a.steps; s0 += 32) {
           if (use_philox) {
             // Lane-parallel Philox: lane i draws the numbers of step counter ctr + i
@@ -314,12 +320,12 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
             int k;
             T r1;
             double r2;
-            if (a.probe_k) {
-                k = a.probe_k[w];
+            if (probe_k) {
+                k = probe_k[w];
                 r1 = T(0);
                 r2 = 0.0;
-            } else if (a.replay) {
-                const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
+            } else if (replay) {
+                const double *q = replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
                 k = (int)floor(q[0] * D);
                 r1 = T(q[1]);
                 r2 = q[2];
@@ -345,7 +351,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                 if (flags & F_HYDROGENLIKE) Gk += -T(P.alpha_h * P.Z) * xo / rpo;
             }
             T dx, Fn = T(0);
-            if (a.probe_k) {
+            if (probe_k) {
                 dx = T(a.probe_x[w]) - xo;
             } else if (is) {
                 Fn = T(2) * Gk;
@@ -353,7 +359,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
             } else {
                 dx = T(10) * (r1 - T(0.5)) * T(P.step);
             }
-            const T xn = a.probe_k ? T(a.probe_x[w]) : xo + dx;
+            const T xn = probe_k ? T(a.probe_x[w]) : xo + dx;
             T xpn[DIM];
 #pragma unroll
             for (int c = 0; c < DIM; ++c) xpn[c] = (c == adim) ? xn : x[p * DIM + c];
@@ -456,7 +462,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
             const T rat_p = (flags & F_PADE) ? F::exp(T(2) * sum_ratio) : T(1);
             const T rat_h = (flags & F_HYDROGENLIKE) ? F::exp(T(2 * P.alpha_h * P.Z) * (rpo - rpn)) : T(1);
             double prob = 1.0;
-            if (FX && !a.probe_k) {
+            if (FX && !probe_k) {
                 // compiled-in dot: Slater x Gaussian x Pade (order only affects rounding)
                 prob = (double)(R * R) * (double)rat_g * (double)rat_p;
             } else {
@@ -464,13 +470,13 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                     const int kind = P.elem_kind[e];
                     const T r = kind == 0 ? rat_g : kind == 1 ? R * R : kind == 2 ? rat_p : kind == 6 ? rat_h : T(1);
                     prob *= (double)r;
-                    if (a.probe_k && lane == 0) a.probe_ratio[(size_t)w * P.n_elem + e] = (double)r;
+                    if (probe_k && lane == 0) a.probe_ratio[(size_t)w * P.n_elem + e] = (double)r;
                 }
             }
 
             // ---- 2d. accept / reject
             bool accept = true;
-            if (!a.probe_k) {
+            if (!probe_k) {
                 double wgt = prob;
                 if (is) {
                     if (flags & Q_IS_GREEN) {
@@ -586,7 +592,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
             }
 
             // ---- 4. local energy and parameter gradients (Sampler::sample)
-            if (it_step >= a.burn_in || a.rec_en) {
+            if (it_step >= a.burn_in || rec_en) {
                 // per coordinate: (sum_e grad_e)^2 + Slater's d2/det - (d ln det)^2; the
                 // Slater-fixed shapes read VW consecutive coordinates per lane
                 constexpr int VW = sizeof(T) == 4 ? 4 : 2;
@@ -662,8 +668,8 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                 const double vint = (flags & F_COULOMB) ? ssc[SC_VINT] : 0.0;
                 const double el = ekin + vext + vint;
                 if (el != el) status |= ST_NAN_ENERGY;
-                if (a.rec_en && lane == 0) {
-                    double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
+                if (rec_en && lane == 0) {
+                    double *o = rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
                     o[0] = ekin;
                     o[1] = vext;
                     o[2] = vint;
@@ -682,7 +688,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                     kadd(acc_s, acc_c, q);
                 }
             }
-            if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
+            if (rec_acc && lane == 0) rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
           }
         }
 
