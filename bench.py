@@ -49,6 +49,19 @@ def workload_text(walkers, steps_per_walker, precision, seed, refresh="auto"):
     ]) + "\n"
 
 
+def sweep_traffic():
+    """DRAM bytes (read + write) of one sweep launch, from the committed ncu summary."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        "sweep_kernel_f32_n56_dot.md")
+    try:
+        for line in open(path):
+            if "dram_bytes_per_launch:" in line:
+                return int(line.split("dram_bytes_per_launch:")[1].split("|")[0].strip())
+    except OSError:
+        pass
+    return None
+
+
 def flops_per_step(N, d=2):
     """Algorithmic flops of one accepted move plus one E_L / dlnPsi sample in the
     engine's incremental, degree-factorised scheme (FMA = 2, MUL/ADD = 1,
@@ -335,7 +348,11 @@ def run_engine_arm(args):
         "gpu_launches": int(args.steps * (2 * launches + 1)),
         "roofline": {"bound": "fp32-pipe", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                     "traffic": None,
+                     "traffic": sweep_traffic(),
+                     "traffic_note": "dram read + write bytes of one sweep launch from the ncu "
+                                     "capture in profiles/sweep_kernel_f32_n56_dot.md (448 steps; "
+                                     "the walker state is streamed once per launch whatever its "
+                                     "length, so the figure holds for these launches)",
                      "peak_source": "vmc_measure_fma_peak (FP32 FMA loop, this GPU, this run); "
                                     "MEASURED_PEAKS.json has no FP32 pipe figure",
                      "flops_per_move": fl, "kernel": "sweep_kernel<float,2,7>",

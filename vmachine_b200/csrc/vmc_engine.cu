@@ -987,26 +987,32 @@ int vmc_measure_fma_peak(int device, int precision, double *tflops)
     CUDA_TRY(cudaSetDevice(device));
     int sms = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    const int threads = 256, blocks = sms * 8, iters = precision == VMC_PRECISION_MIXED ? 4096 : 1024;
+    // about 2 ms per launch, best of the launches after the first; FP32 takes the
+    // better of scalar FFMA and packed FFMA2 chains
+    const int threads = 256, blocks = sms * 8, iters = precision == VMC_PRECISION_MIXED ? 32768 : 8192;
     float *out = nullptr;
     CUDA_TRY(cudaMalloc(&out, (size_t)blocks * threads * sizeof(double)));
     cudaEvent_t a, b;
     CUDA_TRY(cudaEventCreate(&a));
     CUDA_TRY(cudaEventCreate(&b));
     double best = 0.0;
-    for (int rep = 0; rep < 4; ++rep) {
-        CUDA_TRY(cudaEventRecord(a));
-        if (precision == VMC_PRECISION_MIXED)
-            fma_peak_kernel<float><<<blocks, threads>>>(reinterpret_cast<float *>(out), iters, 1.0f + 1e-7f);
-        else
-            fma_peak_kernel<double><<<blocks, threads>>>(reinterpret_cast<double *>(out), iters, 1.0 + 1e-15);
-        CUDA_TRY(cudaEventRecord(b));
-        CUDA_TRY(cudaEventSynchronize(b));
-        float ms = 0.f;
-        CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
-        const double flops = 2.0 * FMA_CHAINS * (double)iters * blocks * threads;
-        if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
-    }
+    const int variants = precision == VMC_PRECISION_MIXED ? 2 : 1;
+    for (int var = 0; var < variants; ++var)
+        for (int rep = 0; rep < 4; ++rep) {
+            CUDA_TRY(cudaEventRecord(a));
+            if (precision != VMC_PRECISION_MIXED)
+                fma_peak_kernel<double><<<blocks, threads>>>(reinterpret_cast<double *>(out), iters, 1.0 + 1e-15);
+            else if (var == 0)
+                fma_peak_kernel<float><<<blocks, threads>>>(reinterpret_cast<float *>(out), iters, 1.0f + 1e-7f);
+            else
+                fma2_peak_kernel<<<blocks, threads>>>(reinterpret_cast<float *>(out), iters / 2, 1.0f + 1e-7f);
+            CUDA_TRY(cudaEventRecord(b));
+            CUDA_TRY(cudaEventSynchronize(b));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+            const double flops = 2.0 * FMA_CHAINS * (double)iters * blocks * threads;
+            if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+        }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaFree(out);

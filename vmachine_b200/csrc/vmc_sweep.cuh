@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
                 r1 = T(q[1]);
                 r2 = q[2];
             } else {
-                const int slot = s - s0;
+                const int slot = (s - s0) & 31;  // s - s0 < 32 (the mask frees a register)
                 ++ctr;
                 k = __shfl_sync(FULL, rng_k, slot);
                 r1 = __shfl_sync(FULL, rng_z, slot);
