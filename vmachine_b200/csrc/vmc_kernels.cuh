@@ -509,22 +509,6 @@ __global__ void fma_peak_kernel(R *out, int iters, R m)
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-// The same with packed FP32 pairs (FFMA2): 2 FMAs per instruction.
-__global__ void fma2_peak_kernel(float *out, int iters, float m)
-{
-    float2 v[FMA_CHAINS];
-    const float2 mm = make_float2(m, m);
-#pragma unroll
-    for (int i = 0; i < FMA_CHAINS; ++i) v[i] = make_float2(threadIdx.x + i, threadIdx.x - i);
-    for (int it = 0; it < iters; ++it)
-#pragma unroll
-        for (int i = 0; i < FMA_CHAINS; ++i) v[i] = __ffma2_rn(v[i], mm, mm);
-    float s = 0.f;
-#pragma unroll
-    for (int i = 0; i < FMA_CHAINS; ++i) s += v[i].x + v[i].y;
-    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
-}
-
 // ------------------------------------------------------------------ dispatch
 
 struct KernelSet {
