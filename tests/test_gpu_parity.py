@@ -12,8 +12,8 @@ import os
 import numpy as np
 import pytest
 
-from oracle_bind import (GAUSSIAN, HYDROGENLIKE, PADE, SLATER, Oracle, SystemSpec, load_cases,
-                         spec_from_case)
+from oracle_bind import (GAUSSIAN, HYDROGENLIKE, PADE, RBMGAUSSIAN, RBMPRODUCT, SIMPLEJASTROW, SLATER,
+                         Oracle, SystemSpec, load_cases, spec_from_case)
 
 pytestmark = pytest.mark.gpu
 
@@ -22,7 +22,7 @@ GOLD = os.path.join(HERE, "golden")
 EVAL = load_cases(os.path.join(GOLD, "eval_fixed.npz"))
 CHAINS = load_cases(os.path.join(GOLD, "chains.npz"))
 ITERS = load_cases(os.path.join(GOLD, "iterations.npz"))
-ENGINE_ELEMENTS = {GAUSSIAN, SLATER, PADE, HYDROGENLIKE}
+ENGINE_ELEMENTS = {GAUSSIAN, SLATER, PADE, HYDROGENLIKE, SIMPLEJASTROW, RBMGAUSSIAN, RBMPRODUCT}
 
 
 def supported(c):

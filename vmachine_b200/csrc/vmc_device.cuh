@@ -26,6 +26,12 @@ enum : int {
     Q_PADE_STALE = 1 << 8,   // Pade pairs keep the previous gamma until their particle moves
     F_HYDROGENLIKE = 1 << 9, // exp(-alpha Z sum r_i)
     F_IS = 1 << 10,          // importance sampling (else brute force)
+    // general path only
+    F_SIMPLEJ = 1 << 11,     // SimpleJastrow
+    F_RBMG = 1 << 12,        // RBMGaussian
+    F_RBMP = 1 << 13,        // RBMProduct
+    Q_SJ_RATIO = 1 << 14,    // SimpleJastrow ratio over partners j > moved particle only
+    Q_RBM_SORT = 1 << 15,    // RBMProduct hidden units see the sorted coordinates
 };
 
 // Flag sets with a compiled-in sweep: the 2D quantum dot, Slater x Gaussian x Pade

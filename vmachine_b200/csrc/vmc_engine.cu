@@ -15,6 +15,7 @@
 
 #include "vmc_b200.h"
 #include "vmc_config.hpp"
+#include "vmc_general.hpp"
 #include "vmc_kernels.cuh"
 
 using namespace vmc;
@@ -135,6 +136,7 @@ int hermite_init_device(int device)
     }
     CUDA_TRY(upload_hermite_f32(h));
     CUDA_TRY(upload_hermite_f64(h));
+    CUDA_TRY(upload_hermite_gen(h));
     if (device < 64) done[device] = true;
     return VMC_OK;
 }
@@ -155,6 +157,10 @@ struct vmc_engine {
     size_t elem_bytes = 8;
     Layout L{};
     KernelSet ks;
+    // general path (SimpleJastrow, RBM, hydrogen orbitals): FP64 kernels of vmc_general.cu
+    bool general = false;
+    GenParams gen{};
+    double *d_theta = nullptr;  // E x p_max on the device (general path)
     std::vector<double> theta;
     double gamma_prev = 0.0;
     bool have_walkers = false;
@@ -193,6 +199,7 @@ void free_engine(vmc_engine *e)
     cudaFree(e->d_counter);
     cudaFree(e->d_status);
     cudaFree(e->d_replay);
+    cudaFree(e->d_theta);
     for (cudaEvent_t ev : e->sweep_events) cudaEventDestroy(ev);
     if (e->sw0) cudaEventDestroy(e->sw0);
     if (e->sw1) cudaEventDestroy(e->sw1);
@@ -270,6 +277,11 @@ int sweep_smem_per_warp(const vmc_engine *e)
 
 int run_rebuild(vmc_engine *e, int mode, double *drift)
 {
+    if (e->general) {
+        CUDA_TRY(gen_launch_state(make_params(e), e->gen, mode == RB_INIT ? GEN_INIT : GEN_STATE, nullptr,
+                                  nullptr, nullptr, nullptr, e->stream));
+        return VMC_OK;
+    }
     RebuildArgs a{};
     a.P = make_params(e);
     a.mode = mode;
@@ -285,6 +297,10 @@ int run_rebuild(vmc_engine *e, int mode, double *drift)
 int run_sweep(vmc_engine *e, SweepArgs &a)
 {
     a.P = make_params(e);
+    if (e->general) {
+        CUDA_TRY(gen_launch_sweep(a, e->gen, e->stream));
+        return VMC_OK;
+    }
     a.wpb = e->wpb;
     a.smem_per_warp = sweep_smem_per_warp(e);
     const size_t smem = (size_t)a.wpb * a.smem_per_warp;
@@ -296,6 +312,10 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
 
 int choose_wpb(vmc_engine *e)
 {
+    if (e->general) {
+        e->wpb = 4;  // the general kernels' fixed warps per CTA
+        return VMC_OK;
+    }
     if (e->cfg.walkers_per_block > 0) {
         e->wpb = e->cfg.walkers_per_block;
         return VMC_OK;
@@ -374,6 +394,14 @@ int initial_weights(vmc_engine *e)
     return VMC_OK;
 }
 
+int upload_theta(vmc_engine *e)
+{
+    if (!e->general) return VMC_OK;  // the quantum-dot kernels take their scalars by value
+    CUDA_TRY(cudaMemcpyAsync(e->d_theta, e->theta.data(), e->theta.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, e->stream));
+    return VMC_OK;
+}
+
 int refresh_all(vmc_engine *e)
 {
     if (!e->have_walkers) return VMC_OK;
@@ -422,29 +450,40 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     if (c.N < 2 || c.N > MAX_N) return reject("numParticles must be in [2, 64]");
     int flags = 0;
     int K = 0;
+    // SimpleJastrow, the RBM elements and hydrogen orbitals run on the general path
+    bool general = false;
+    for (int el : c.elements)
+        general |= el == E_SIMPLEJASTROW || el == E_RBMGAUSSIAN || el == E_RBMPRODUCT ||
+                   (el == E_SLATER && c.basis == "hydrogenOrbital");
     for (int el : c.elements) {
         switch (el) {
         case E_GAUSSIAN: flags |= F_GAUSS; break;
         case E_PADE: flags |= F_PADE; break;
         case E_HYDROGENLIKE: flags |= F_HYDROGENLIKE; break;
+        case E_SIMPLEJASTROW: flags |= F_SIMPLEJ; break;
+        case E_RBMGAUSSIAN: flags |= F_RBMG; break;
+        case E_RBMPRODUCT: flags |= F_RBMP; break;
         case E_SLATER:
-            if (c.basis != "hermite") return reject("Slater determinant needs basis: hermite on this engine");
-            K = closed_shells_2d(c.N, c.dim);
-            if (K < 0) return reject("open shell: numParticles is not a closed shell");
-            if ((c.dim == 2 && K > 7) || (c.dim == 3 && K > 4)) return reject("too many shells");
+            if (c.basis != "hermite" && c.basis != "hydrogenOrbital")
+                return reject("Slater determinant needs basis: hermite or hydrogenOrbital");
+            if (!general) {
+                K = closed_shells_2d(c.N, c.dim);
+                if (K < 0) return reject("open shell: numParticles is not a closed shell");
+                if ((c.dim == 2 && K > 7) || (c.dim == 3 && K > 4)) return reject("too many shells");
+            }
             flags |= F_SLATER;
             break;
         default: return reject("wave function element not implemented on the engine");
         }
     }
-    if (std::count(c.elements.begin(), c.elements.end(), (int)E_PADE) > 1 ||
-        std::count(c.elements.begin(), c.elements.end(), (int)E_GAUSSIAN) > 1 ||
-        std::count(c.elements.begin(), c.elements.end(), (int)E_SLATER) > 1)
-        return reject("repeated element");
+    for (int el : {E_PADE, E_GAUSSIAN, E_SLATER, E_SIMPLEJASTROW, E_RBMGAUSSIAN, E_RBMPRODUCT})
+        if (std::count(c.elements.begin(), c.elements.end(), (int)el) > 1) return reject("repeated element");
     if (c.coulomb) flags |= F_COULOMB;
     if (c.hamiltonian == "atomicNucleus") flags |= F_ATOM;
-    if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
+    if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE | Q_SJ_RATIO;
+    if (c.compat && c.sorting) flags |= Q_RBM_SORT;
     if (c.sampling != "bruteForce") flags |= F_IS;
+    e->general = general;
     e->flags = flags;
     e->K = K;
     e->compat = c.compat;
@@ -461,7 +500,15 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     for (int el : c.elements) e->Pmax = std::max(e->Pmax, element_parameters(c, el));
     e->EP = e->E * e->Pmax;
     e->nacc = 9 + 2 * e->EP;
-    if (e->nacc > 32) return reject("more than 11 parameters per walker is not supported");
+    if (!general && e->nacc > 32) return reject("more than 11 parameters per walker is not supported");
+    if (general) {
+        if (e->precision == VMC_PRECISION_MIXED)
+            return reject("mixed precision covers Gaussian, Hermite Slater, Pade and hydrogen-like "
+                          "systems; this system runs with precision: fp64");
+        const std::string why = gen_configure(c, e->E, e->Pmax, e->gen);
+        if (!why.empty()) return reject(why);
+        e->n_orb = e->gen.n;
+    }
     // userinput.cpp:60-81 with walkers in place of ranks: numSteps is the total
     // over walkers; each walker burns in its own share times the fraction.
     e->steps_per_walker = (int)(c.num_steps / e->W);
@@ -470,7 +517,13 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     e->batches = c.optimization == "adam" ? 10 : 1;  // adam.h:15, gradientdescent.h:13
     e->elem_bytes = e->precision == VMC_PRECISION_MIXED ? 4 : 8;
     e->L = make_layout(e->N, e->dim, e->n_orb, (int)e->elem_bytes);
-    if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) return reject("no kernel for this shape");
+    if (general) {  // positions first in the general record (vmc_general.hpp)
+        e->L.off_x = 0;
+        e->L.rec = e->gen.rec;
+        if (!select_set(VMC_PRECISION_FP64, e->dim, 0, 0, e->ks)) return reject("no kernel for this shape");
+    } else if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) {
+        return reject("no kernel for this shape");
+    }
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
                           : (e->precision == VMC_PRECISION_MIXED ? 4 * e->D : 0);
     e->refresh_auto = c.refresh_interval < 0 && e->precision == VMC_PRECISION_MIXED;
@@ -494,6 +547,10 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
             CUDA_TRY(cudaMalloc(&e->d_mask, W * e->N * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_counter, W * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_status, W * sizeof(unsigned)));
+            if (e->general) {
+                CUDA_TRY(cudaMalloc(&e->d_theta, std::max<size_t>(1, (size_t)e->EP) * sizeof(double)));
+                e->gen.theta = e->d_theta;
+            }
             CUDA_TRY(cudaMemsetAsync(e->d_state, 0, W * e->L.rec * e->elem_bytes, e->stream));
             CUDA_TRY(cudaMemsetAsync(e->d_scal, 0, W * NSCAL * sizeof(double), e->stream));
             CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc * 2 * sizeof(double), e->stream));
@@ -506,7 +563,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         free_engine(e);
         return rc;
     }
-    if ((rc = initial_weights(e))) {
+    if ((rc = initial_weights(e)) || (rc = upload_theta(e))) {
         free_engine(e);
         return rc;
     }
@@ -559,7 +616,8 @@ int vmc_set_parameters(vmc_engine *e, const double *theta, int n_elements, int p
     } else {
         e->gamma_prev = make_params(e).gamma;
     }
-    return refresh_all(e);
+    int rc = upload_theta(e);
+    return rc ? rc : refresh_all(e);
 }
 
 int vmc_get_parameters(const vmc_engine *e, double *theta, int n_elements, int p_max)
@@ -862,7 +920,13 @@ int vmc_eval(vmc_engine *e, double *grad, double *lap, double *pgrad, double *en
     a.lap = d + ng;
     a.pgrad = d + ng + nl;
     a.energies = d + ng + nl + np;
-    int rc = launch(e->ks.eval, (e->W + 3) / 4, 128, 0, e->stream, &a);
+    int rc = VMC_OK;
+    if (e->general) {
+        const cudaError_t ge = gen_launch_state(a.P, e->gen, GEN_STATE, a.grad, a.lap, a.pgrad, a.energies, e->stream);
+        if (ge != cudaSuccess) rc = fail(VMC_E_CUDA, cudaGetErrorString(ge));
+    } else {
+        rc = launch(e->ks.eval, (e->W + 3) / 4, 128, 0, e->stream, &a);
+    }
     if (rc) { cudaFree(d); return rc; }
     std::vector<double> h(ng + nl + np + ne);
     cudaError_t ce = cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream);

@@ -1,0 +1,831 @@
+// General walker path: every wave-function element of the reference on one FP64
+// warp-per-walker kernel family, for the systems the quantum-dot sweep does not
+// take: SimpleJastrow (simplejastrow.cpp), RBMGaussian (rbmgaussian.cpp),
+// RBMProduct (rbmproduct.cpp), and Slater determinants of hydrogen orbitals
+// (hydrogenorbital.cpp) or Hermite functions next to those elements.
+//
+// One warp owns one walker; its record lives in HBM (small systems: it stays in
+// L1/L2) and holds the positions, the importance-sampling force cache, the total
+// gradient of ln|Psi| at the current positions, the local-energy parts and the
+// parameter gradients at the current positions, and the transposed inverse of
+// each Slater block.  A proposal computes each element's |Psi'|^2/|Psi|^2 without
+// touching the record; an accepted move applies the Sherman-Morrison update to
+// the moved particle's block and re-evaluates the walker (gradients, Laplacians,
+// energies, parameter gradients) from its new positions, so rejected steps sample
+// the stored values.  Every parameter gradient is accumulated (nothing caps the
+// parameter count): lanes stride over the accumulators in HBM.
+//
+// Elements, Hamiltonians, samplers and the reference's quirks follow the CPU
+// restatement in oracle/vmc_oracle.c function for function (eval_impl,
+// ratio_impl, vmo_run).
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "vmc_general.hpp"
+
+namespace vmc {
+
+namespace {
+
+constexpr int GEN_WPB = 4;     // walkers (warps) per CTA
+constexpr int GEN_SCR = 256;   // shared doubles per warp
+// shared scratch of a warp: orbital values at the proposal | moved row | RBM visible
+// (sorted) | RBM hidden p_j = 1/(1+e^v) | RBM hidden e^v/(1+e^v)
+constexpr int SCR_PHI = 0, SCR_ROW = 32, SCR_XS = 64, SCR_PN = 128, SCR_NN = 192;
+
+__device__ __forceinline__ double gen_dist(const double *x, int dim, int i, int j)
+{
+    double s = 0.0;
+    for (int c = 0; c < dim; ++c) {
+        const double t = x[i * dim + c] - x[j * dim + c];
+        s += t * t;
+    }
+    return sqrt(s);
+}
+
+__device__ __forceinline__ double gen_radius(const double *x, int dim, int i)
+{
+    double s = 0.0;
+    for (int c = 0; c < dim; ++c) s += x[i * dim + c] * x[i * dim + c];
+    return sqrt(s);
+}
+
+// h_m(x), h_m'(x), h_m''(x) of the normalised Hermite functions by the recurrence
+// h_{j+1} = A_j x h_j - B_j h_{j-1}; h_m' = C_m h_{m-1}, h_m'' = E_m h_{m-2}.
+__device__ __forceinline__ void herm3(int m, double x, double &h, double &h1, double &h2)
+{
+    double hm2 = 0.0, hm1 = 0.0, hc = 1.0;
+    for (int j = 0; j < m; ++j) {
+        const double nx = hA<double>(j) * x * hc - hB<double>(j) * hm1;
+        hm2 = hm1;
+        hm1 = hc;
+        hc = nx;
+    }
+    h = hc;
+    h1 = m >= 1 ? hC<double>(m) * hm1 : 0.0;
+    h2 = m >= 2 ? hE<double>(m) * hm2 : 0.0;
+}
+
+// Value, d/dx_c and d^2/dx_c^2 (c = 0..dim-1) of orbital o at point r.
+// Hermite: prod_c h_{m_c}(x_c) (basis.cpp:81-116, argument unscaled, hermite.h:8).
+// Hydrogen (3D, hydrogenorbital.cpp:108-394 with alpha = 1, k = Z): a polynomial
+// angular factor A (1 or one coordinate) times a radial factor
+// R(r) = f(r) exp(-k r / n); derivatives by the chain rule:
+//   d_i phi   = (d_i A) R + A R' x_i / r
+//   d_i^2 phi = 2 (d_i A) R' x_i / r + A (R'' x_i^2 / r^2 + R' (1/r - x_i^2 / r^3))
+__device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const double *r, double &v,
+                            double *d1, double *d2)
+{
+    if (g.basis == BASIS_HERMITE) {
+        double h[3], h1[3], h2[3];
+        for (int c = 0; c < dim; ++c) herm3(g.orb[o][c], r[c], h[c], h1[c], h2[c]);
+        v = 1.0;
+        for (int c = 0; c < dim; ++c) v *= h[c];
+        for (int c = 0; c < dim; ++c) {
+            double rest = 1.0;
+            for (int c2 = 0; c2 < dim; ++c2)
+                if (c2 != c) rest *= h[c2];
+            d1[c] = h1[c] * rest;
+            d2[c] = h2[c] * rest;
+        }
+        return;
+    }
+    const int nq = g.orb[o][0], l = g.orb[o][1], m = (int)g.orb[o][2] - 1;
+    const double k = Z;
+    const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    double f = 1.0, fp = 0.0, fpp = 0.0;
+    if (nq == 2 && l == 0) { f = 2.0 - k * rr; fp = -k; }
+    if (nq == 3 && l == 0) { f = 2.0 * k * k * rr * rr - 18.0 * k * rr + 27.0; fp = 4.0 * k * k * rr - 18.0 * k; fpp = 4.0 * k * k; }
+    if (nq == 3 && l == 1) { f = k * rr - 6.0; fp = k; }
+    const double a = k / nq, ex = exp(-a * rr);
+    const double R = f * ex, R1 = (fp - a * f) * ex, R2 = (fpp - 2.0 * a * fp + a * a * f) * ex;
+    const int ca = l == 1 ? (m == 1 ? 0 : m == -1 ? 1 : 2) : -1;  // m = 1: x, -1: y, 0: z
+    const double A = ca >= 0 ? r[ca] : 1.0;
+    v = A * R;
+    for (int c = 0; c < 3; ++c) {
+        const double xc = r[c], u = xc / rr, dA = (c == ca) ? 1.0 : 0.0;
+        d1[c] = dA * R + A * R1 * u;
+        d2[c] = 2.0 * dA * R1 * u + A * (R2 * u * u + R1 * (1.0 / rr - u * u / rr));
+    }
+}
+
+// RBMProduct visible vector: the coordinates, sorted ascending under the
+// reference's in-place sort (wavefunction.cpp:40-55; stable, as the oracle's
+// insertion sort), with coordinate k replaced by xk_new when k >= 0.
+__device__ void rbm_visible(const double *x, int D, int k, double xk_new, bool sort, double *xs, int lane)
+{
+    for (int i = lane; i < D; i += 32) {
+        const double xi = i == k ? xk_new : x[i];
+        int rank = i;
+        if (sort) {
+            rank = 0;
+            for (int j = 0; j < D; ++j) {
+                const double xj = j == k ? xk_new : x[j];
+                rank += (xj < xi) || (xj == xi && j < i);
+            }
+        }
+        xs[rank] = xi;
+    }
+    __syncwarp();
+}
+
+// hidden activations: v_j = b_j + sum_i W_ij xs_i / sigma^2 (rbmproduct.cpp:191-197),
+// p_j = 1 / (e^v + 1), n_j = e^v p_j into the scratch
+__device__ void rbm_hidden(const double *th, int D, int H, double s2, const double *xs, double *pn,
+                           double *nn, int lane)
+{
+    for (int j = lane; j < H; j += 32) {
+        double acc = 0.0;
+        for (int i = 0; i < D; ++i) acc += th[H + i + D * j] * xs[i];
+        const double v = th[j] + acc / s2, e = exp(v);
+        pn[j] = 1.0 / (e + 1.0);
+        nn[j] = e * pn[j];
+    }
+    __syncwarp();
+}
+
+// Pade-Jastrow gamma of pair (i, j): the previous gamma while the pair is stale
+__device__ __forceinline__ double pade_gamma(const Params &P, const unsigned long long *mask, int i, int j,
+                                             double gam)
+{
+    return ((P.flags & Q_PADE_STALE) && !((mask[i] >> j) & 1ull)) ? P.gamma_prev : gam;
+}
+
+__device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
+{
+    return same_spin(i, j, P.N) ? P.beta_same : P.beta_anti;
+}
+
+// Evaluate the walker at its positions (eval_impl): per-element gradient,
+// Laplacian and parameter gradient, the local-energy parts.  Writes the total
+// gradient, energies and parameter gradients into the record and, when given,
+// the per-element outputs of one walker (grad E x D, lap E, pgrad E x p_max,
+// energies 3).
+__device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, double *rec,
+                             const unsigned long long *mask, double *scr, int lane, double *o_grad,
+                             double *o_lap, double *o_pg, double *o_en)
+{
+    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
+    const double *x = rec;
+    double *G = rec + g.off_g, *pg = rec + g.off_pg;
+    const double *inv = rec + g.off_inv;
+    for (int k = lane; k < D; k += 32) G[k] = 0.0;
+    for (int j = lane; j < g.EP; j += 32) pg[j] = 0.0;
+    __syncwarp();
+    double lap_total = 0.0;
+    for (int e = 0; e < E; ++e) {
+        const double *th = g.theta + (size_t)e * PM;
+        double *pge = pg + (size_t)e * PM;
+        double lap_l = 0.0, lap_u = 0.0;  // lane partial, uniform part
+        double *oge = o_grad ? o_grad + (size_t)e * D : nullptr;
+        switch (P.elem_kind[e]) {
+        case 0: {  // Gaussian (gaussian.cpp:62-78)
+            const double wa = P.omega * th[0];
+            double x2 = 0.0;
+            for (int k = lane; k < D; k += 32) {
+                const double gk = -wa * x[k];
+                G[k] += gk;
+                if (oge) oge[k] = gk;
+                x2 += x[k] * x[k];
+            }
+            x2 = warp_sum(x2);
+            lap_u = -wa * D;
+            if (lane == 0) pge[0] = -0.5 * P.omega * x2;
+            break;
+        }
+        case 1: {  // Slater determinant (slaterdeterminant.cpp:155-191)
+            const int n = g.n;
+            for (int q = lane; q < N; q += 32) {
+                const int b = q / n, il = q - b * n;
+                const double *row = inv + (size_t)(b * n + il) * n;
+                double dd[3] = {0.0, 0.0, 0.0}, sdd[3] = {0.0, 0.0, 0.0};
+                for (int o = 0; o < n; ++o) {
+                    double v, d1[3], d2[3];
+                    gen_orbital(g, dim, P.Z, o, x + q * dim, v, d1, d2);
+                    for (int c = 0; c < dim; ++c) {
+                        dd[c] += d1[c] * row[o];
+                        sdd[c] += d2[c] * row[o];
+                    }
+                }
+                for (int c = 0; c < dim; ++c) {
+                    G[q * dim + c] += dd[c];
+                    if (oge) oge[q * dim + c] = dd[c];
+                    lap_l += sdd[c] - dd[c] * dd[c];
+                }
+            }
+            break;
+        }
+        case 2: {  // Pade-Jastrow (padejastrow.cpp:75-116)
+            const double gam = th[0];
+            double dg = 0.0;
+            for (int i = lane; i < N; i += 32) {
+                double gi[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < N; ++j) {
+                    if (j == i) continue;
+                    const int lo = min(i, j), hi = max(i, j);
+                    const double r = gen_dist(x, dim, i, j), beta = pade_beta_of(P, i, j);
+                    const double gp = pade_gamma(P, mask, lo, hi, gam);
+                    const double f1 = 1.0 / (1.0 + gp * r), f = beta * f1 * f1, h = r * f1;
+                    double c2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        const double cc = (x[i * dim + c] - x[j * dim + c]) / r;
+                        gi[c] += f * cc;
+                        c2 += 2.0 * f * (1.0 - (1.0 + 2.0 * gam * h) * cc * cc) / r;
+                    }
+                    if (j > i) {
+                        lap_l += c2;
+                        dg += beta * h * h;
+                    }
+                }
+                for (int c = 0; c < dim; ++c) {
+                    G[i * dim + c] += gi[c];
+                    if (oge) oge[i * dim + c] = gi[c];
+                }
+            }
+            dg = warp_sum(dg);
+            if (lane == 0) pge[0] = (P.flags & Q_PADE_DGAMMA) ? -0.5 * dg : -dg;
+            break;
+        }
+        case 3: {  // SimpleJastrow (simplejastrow.cpp:67-111)
+            for (int i = lane; i < N; i += 32) {
+                double gi[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < N; ++j) {
+                    if (j == i) continue;
+                    const int lo = min(i, j), hi = max(i, j);
+                    const double r = gen_dist(x, dim, i, j), beta = th[lo + N * hi];
+                    double c2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        const double cc = (x[i * dim + c] - x[j * dim + c]) / r;
+                        gi[c] += beta * cc;
+                        c2 += 2.0 * beta * (1.0 - cc * cc) / r;
+                    }
+                    if (j > i) {
+                        lap_l += c2;
+                        pge[i + N * j] = r;
+                    }
+                }
+                for (int c = 0; c < dim; ++c) {
+                    G[i * dim + c] += gi[c];
+                    if (oge) oge[i * dim + c] = gi[c];
+                }
+            }
+            break;
+        }
+        case 4: {  // RBMGaussian (rbmgaussian.cpp:67-87)
+            const double s2 = g.sigma * g.sigma;
+            for (int k = lane; k < D; k += 32) {
+                const double t = (x[k] - th[k]) / s2;
+                G[k] += -t;
+                if (oge) oge[k] = -t;
+                pge[k] = t;
+            }
+            lap_u = -D / s2;
+            break;
+        }
+        case 5: {  // RBMProduct (rbmproduct.cpp:167-189)
+            const int H = g.hidden;
+            const double s2 = 100.0 * g.sigma * g.sigma, s4 = s2 * s2;
+            double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
+            rbm_visible(x, D, -1, 0.0, P.flags & Q_RBM_SORT, xs, lane);
+            rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
+            for (int k = lane; k < D; k += 32) {
+                double acc = 0.0, acc2 = 0.0;
+                for (int j = 0; j < H; ++j) {
+                    const double w = th[H + k + D * j];
+                    acc += w * nn[j];
+                    acc2 += w * w * pn[j] * nn[j];
+                }
+                G[k] += acc / s2;
+                if (oge) oge[k] = acc / s2;
+                lap_l += acc2 / s4;
+            }
+            for (int t = lane; t < H * (D + 1); t += 32) {
+                if (t < H) pge[t] = nn[t];
+                else {
+                    const int j = (t - H) / D, i = (t - H) - j * D;
+                    pge[H + i + D * j] = xs[i] * nn[j];
+                }
+            }
+            break;
+        }
+        case 6: {  // HydrogenLike (hydrogenlike.cpp:268-286)
+            const double az = th[0] * P.Z;
+            double rs = 0.0;
+            for (int i = lane; i < N; i += 32) {
+                const double r = gen_radius(x, dim, i);
+                rs += r;
+                for (int c = 0; c < dim; ++c) {
+                    const double gk = -az * x[i * dim + c] / r;
+                    G[i * dim + c] += gk;
+                    if (oge) oge[i * dim + c] = gk;
+                }
+                lap_l -= 2.0 / r;
+            }
+            rs = warp_sum(rs);
+            lap_l *= az;
+            if (lane == 0) pge[0] = -P.Z * rs;
+            break;
+        }
+        default: break;
+        }
+        __syncwarp();
+        const double lap_e = warp_sum(lap_l) + lap_u;
+        lap_total += lap_e;
+        if (o_lap && lane == 0) o_lap[e] = lap_e;
+    }
+    // System::getKineticEnergy (elementoperation.cpp:95-109) and the potentials
+    double g2 = 0.0, vx = 0.0, vi = 0.0;
+    for (int k = lane; k < D; k += 32) g2 += G[k] * G[k];
+    if (P.flags & F_ATOM) {
+        for (int i = lane; i < N; i += 32) vx += 1.0 / gen_radius(x, dim, i);
+    } else {
+        for (int k = lane; k < D; k += 32) vx += x[k] * x[k];
+    }
+    if (P.flags & F_COULOMB)
+        for (int i = lane; i < N; i += 32)
+            for (int j = i + 1; j < N; ++j) vi += 1.0 / gen_dist(x, dim, i, j);
+    g2 = warp_sum(g2);
+    vx = warp_sum(vx);
+    vi = warp_sum(vi);
+    const double ekin = -0.5 * (lap_total + g2);
+    const double vext = (P.flags & F_ATOM) ? -P.Z * vx : 0.5 * P.omega * P.omega * vx;
+    double *en = rec + g.off_en;
+    if (lane == 0) {
+        en[0] = ekin;
+        en[1] = vext;
+        en[2] = vi;
+    }
+    if (o_pg)
+        for (int j = lane; j < g.EP; j += 32) o_pg[j] = pg[j];
+    if (o_en && lane == 0) {
+        o_en[0] = ekin;
+        o_en[1] = vext;
+        o_en[2] = vi;
+    }
+    __syncwarp();
+}
+
+// Element ratios |Psi(y)|^2 / |Psi(x)|^2 for coordinate k moved to xn (ratio_impl)
+// and, when grad_y is given, d ln Psi / d y_k at the proposal (the corrected
+// Fokker-Planck Green's ratio).  Orbital values at the proposal go to the scratch
+// (the Sherman-Morrison update reuses them).  Returns the product in element order.
+__device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const double *rec,
+                             const unsigned long long *mask, double *scr, int lane, int k, double xn,
+                             double *ratios, double *grad_y, double &R_out)
+{
+    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
+    const double *x = rec;
+    const int p = k / dim, adim = k - p * dim;
+    double yp[3];
+    for (int c = 0; c < dim; ++c) yp[c] = c == adim ? xn : x[p * dim + c];
+    const double xo = x[k];
+    double prob = 1.0, gy = 0.0;
+    R_out = 1.0;
+    for (int e = 0; e < E; ++e) {
+        const double *th = g.theta + (size_t)e * PM;
+        double r = 1.0;
+        switch (P.elem_kind[e]) {
+        case 0:  // gaussian.cpp:23-28
+            r = exp(P.omega * th[0] * (xo * xo - xn * xn));
+            gy += -P.omega * th[0] * xn;
+            break;
+        case 1: {  // slaterdeterminant.cpp:150-153, 177-180
+            const int n = g.n, b = p / n, pl = p - b * n;
+            double s = 0.0, sg = 0.0;
+            if (lane < n) {
+                double v, d1[3], d2[3];
+                gen_orbital(g, dim, P.Z, lane, yp, v, d1, d2);
+                scr[SCR_PHI + lane] = v;
+                const double iv = rec[g.off_inv + (size_t)(b * n + pl) * n + lane];
+                s = v * iv;
+                sg = d1[adim] * iv;
+            }
+            const double R = warp_sum(s);
+            R_out = R;
+            r = R * R;
+            if (grad_y) gy += warp_sum(sg) / R;
+            __syncwarp();
+            break;
+        }
+        case 2: {  // padejastrow.cpp:211-218
+            const double gam = th[0];
+            const int j0 = (P.flags & Q_PADE_RATIO) ? p + 1 : 0;
+            double acc = 0.0, gyl = 0.0;
+            for (int j = lane; j < N; j += 32) {
+                if (j == p) continue;
+                const int lo = min(p, j), hi = max(p, j);
+                double rn2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[j * dim + c];
+                    rn2 += t * t;
+                }
+                const double ro = gen_dist(x, dim, p, j), rn = sqrt(rn2), beta = pade_beta_of(P, p, j);
+                const double gp = pade_gamma(P, mask, lo, hi, gam);
+                if (j >= j0) acc += beta * (rn / (1.0 + gam * rn) - ro / (1.0 + gp * ro));
+                const double f1 = 1.0 / (1.0 + gam * rn);
+                gyl += beta * f1 * f1 * (yp[adim] - x[j * dim + adim]) / rn;
+            }
+            acc = warp_sum(acc);
+            r = exp(2.0 * acc);
+            if (grad_y) gy += warp_sum(gyl);
+            break;
+        }
+        case 3: {  // simplejastrow.cpp:145-156
+            const int j0 = (P.flags & Q_SJ_RATIO) ? p + 1 : 0;
+            double acc = 0.0, gyl = 0.0;
+            for (int j = lane; j < N; j += 32) {
+                if (j == p) continue;
+                const int lo = min(p, j), hi = max(p, j);
+                double rn2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[j * dim + c];
+                    rn2 += t * t;
+                }
+                const double rn = sqrt(rn2), beta = th[lo + N * hi];
+                if (j >= j0) acc += beta * (rn - gen_dist(x, dim, p, j));
+                gyl += beta * (yp[adim] - x[j * dim + adim]) / rn;
+            }
+            acc = warp_sum(acc);
+            r = exp(2.0 * acc);
+            if (grad_y) gy += warp_sum(gyl);
+            break;
+        }
+        case 4: {  // rbmgaussian.cpp:34-46
+            const double s2 = g.sigma * g.sigma, a = xo - th[k], bn = xn - th[k];
+            r = exp((a * a - bn * bn) / (2.0 * s2));
+            gy += -bn / s2;
+            break;
+        }
+        case 5: {  // rbmproduct.cpp:199-203
+            const int H = g.hidden;
+            const double s2 = 100.0 * g.sigma * g.sigma;
+            double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
+            const bool sort = P.flags & Q_RBM_SORT;
+            rbm_visible(x, D, -1, 0.0, sort, xs, lane);
+            rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
+            double po[2] = {1.0, 1.0};
+            for (int t = 0; t < 2; ++t) {
+                const int j = lane + 32 * t;
+                if (j < H) po[t] = pn[j];
+            }
+            __syncwarp();
+            rbm_visible(x, D, k, xn, sort, xs, lane);
+            rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
+            double prod = 1.0, gyl = 0.0;
+            for (int t = 0; t < 2; ++t) {
+                const int j = lane + 32 * t;
+                if (j < H) {
+                    prod *= po[t] / pn[j];
+                    gyl += th[H + k + D * j] * nn[j];
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) prod *= __shfl_xor_sync(FULL, prod, o);
+            r = prod * prod;
+            if (grad_y) gy += warp_sum(gyl) / s2;
+            __syncwarp();
+            break;
+        }
+        case 6: {  // hydrogenlike.cpp:231-242
+            double rn2 = 0.0;
+            for (int c = 0; c < dim; ++c) rn2 += yp[c] * yp[c];
+            const double rn = sqrt(rn2);
+            r = exp(2.0 * P.Z * th[0] * (gen_radius(x, dim, p) - rn));
+            gy += -th[0] * P.Z * xn / rn;
+            break;
+        }
+        default: break;
+        }
+        if (ratios) ratios[e] = r;
+        prob *= r;  // elementoperation.cpp:80-87
+    }
+    if (grad_y) *grad_y = gy;
+    return prob;
+}
+
+// Transposed inverse of both Slater blocks by Gauss-Jordan elimination with
+// partial pivoting on [A | I] in shared memory (n <= 32); row i of block b holds
+// A^{-1}(o, i) over orbitals o.  Returns the warp's singular flag.
+__device__ unsigned gen_invert(const Params &P, const GenParams &g, int dim, double *rec, double *M,
+                               int lane)
+{
+    const int n = g.n, w2 = 2 * n;
+    unsigned status = 0;
+    for (int b = 0; b < 2; ++b) {
+        for (int i = 0; i < n; ++i)
+            for (int c = lane; c < w2; c += 32) M[i * w2 + c] = c >= n ? (c - n == i ? 1.0 : 0.0) : 0.0;
+        __syncwarp();
+        if (lane < n)
+            for (int i = 0; i < n; ++i) {
+                double v, d1[3], d2[3];
+                gen_orbital(g, dim, P.Z, lane, rec + (b * n + i) * dim, v, d1, d2);
+                M[i * w2 + lane] = v;  // A[i][o] = phi_o(r_i)
+            }
+        __syncwarp();
+        for (int c = 0; c < n; ++c) {
+            double v = (lane >= c && lane < n) ? fabs(M[lane * w2 + c]) : -1.0;
+            int idx = lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v2 = __shfl_xor_sync(FULL, v, o);
+                const int i2 = __shfl_xor_sync(FULL, idx, o);
+                if (v2 > v || (v2 == v && i2 < idx)) { v = v2; idx = i2; }
+            }
+            if (!(v > 0.0)) status |= ST_SINGULAR;
+            const int pr = idx < n ? idx : c;
+            if (pr != c)
+                for (int col = lane; col < w2; col += 32) {
+                    const double t = M[c * w2 + col];
+                    M[c * w2 + col] = M[pr * w2 + col];
+                    M[pr * w2 + col] = t;
+                }
+            __syncwarp();
+            const double ip = 1.0 / M[c * w2 + c];
+            __syncwarp();
+            for (int col = lane; col < w2; col += 32) M[c * w2 + col] *= ip;
+            __syncwarp();
+            for (int r = 0; r < n; ++r) {
+                if (r == c) continue;
+                const double f = M[r * w2 + c];
+                __syncwarp();
+                for (int col = lane; col < w2; col += 32) M[r * w2 + col] -= f * M[c * w2 + col];
+                __syncwarp();
+            }
+        }
+        // A^{-1}(o, i) = M[o][n + i]
+        for (int i = 0; i < n; ++i)
+            for (int o = lane; o < n; o += 32) rec[g.off_inv + (size_t)(b * n + i) * n + o] = M[o * w2 + n + i];
+        __syncwarp();
+    }
+    return status;
+}
+
+__global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P, const GenParams g, int mode,
+                                                                double *o_grad, double *o_lap, double *o_pg,
+                                                                double *o_en)
+{
+    extern __shared__ __align__(16) double gsm[];
+    __shared__ double scratch[GEN_WPB][GEN_SCR];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int w = blockIdx.x * GEN_WPB + wib;
+    if (w >= P.W) return;
+    const int dim = g.D / P.N;
+    double *rec = reinterpret_cast<double *>(P.state) + (size_t)w * g.rec;
+    unsigned long long *mask = P.mask + (size_t)w * P.N;
+    unsigned status = 0;
+    if (mode == GEN_INIT) {
+        for (int j = lane; j < P.N; j += 32) mask[j] = ~0ull;
+        if (P.flags & F_SLATER) status = gen_invert(P, g, dim, rec, gsm + (size_t)wib * g.n * 2 * g.n, lane);
+        __syncwarp();
+    }
+    const size_t E = P.n_elem;
+    gen_evaluate(P, g, dim, rec, mask, scratch[wib], lane, o_grad ? o_grad + (size_t)w * E * g.D : nullptr,
+                 o_lap ? o_lap + (size_t)w * E : nullptr, o_pg ? o_pg + (size_t)w * g.EP : nullptr,
+                 o_en ? o_en + (size_t)w * 3 : nullptr);
+    if (mode == GEN_INIT && P.sampling == SAMPLER_IS)  // ImportanceSampling::initialize: F = 2 grad
+        for (int k = lane; k < g.D; k += 32) rec[g.off_fc + k] = 2.0 * rec[g.off_g + k];
+    status = __reduce_or_sync(FULL, status);
+    if (lane == 0 && status) P.status[w] |= status;
+}
+
+__global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs a, const GenParams g)
+{
+    __shared__ double scratch[GEN_WPB][GEN_SCR];
+    const Params &P = a.P;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int w = blockIdx.x * GEN_WPB + wib;
+    if (w >= P.W) return;
+    const int N = P.N, D = g.D, dim = D / N;
+    double *rec = reinterpret_cast<double *>(P.state) + (size_t)w * g.rec;
+    double *x = rec, *fc = rec + g.off_fc;
+    unsigned long long *mask = P.mask + (size_t)w * N;
+    double *scr = scratch[wib];
+    double *acc = P.acc + (size_t)w * P.nacc * 2;
+    unsigned long long ctr = P.counter[w];
+    unsigned status = 0;
+    const bool is = P.sampling == SAMPLER_IS;
+    const double dt = P.step, sqdt = sqrt(P.step);
+
+    for (int s = 0; s < a.steps; ++s) {
+        const int it_step = a.step_offset + s;
+        // ---- random numbers (vmo_step_randoms) or the caller's
+        int k;
+        double r1, r2;
+        if (a.probe_k) {
+            k = a.probe_k[w];
+            r1 = 0.0;
+            r2 = 0.0;
+        } else if (a.replay) {
+            const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
+            k = (int)floor(q[0] * D);
+            r1 = q[1];
+            r2 = q[2];
+        } else {
+            const uint4 v = philox(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)w, 0u),
+                                   make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
+            ++ctr;
+            k = (int)__umulhi(v.x, (unsigned)D);
+            if (is) {
+                const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
+                r1 = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+            } else {
+                r1 = v.y * TWO_M32;
+            }
+            r2 = v.w * TWO_M32;
+        }
+        // ---- proposal (importancesampling.cpp:49-60, bruteforce.cpp:34)
+        const double xo = x[k];
+        double dx, fn = 0.0;
+        if (a.probe_k) {
+            dx = a.probe_x[w] - xo;
+        } else if (is) {
+            fn = 2.0 * rec[g.off_g + k];
+            dx = 0.5 * dt * fn + r1 * sqdt;
+        } else {
+            dx = 10.0 * (r1 - 0.5) * P.step;
+        }
+        const double xn = a.probe_k ? a.probe_x[w] : xo + dx;
+        const bool corrected = is && !(P.flags & Q_IS_GREEN) && !a.probe_k;
+        double gy = 0.0, R = 1.0;
+        double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
+        const double prob = gen_ratios(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
+                                       corrected ? &gy : nullptr, R);
+        bool accept = true;
+        if (!a.probe_k) {
+            double wgt = prob;
+            if (is) {
+                if (P.flags & Q_IS_GREEN) {
+                    wgt = (exp(0.5 * (fc[k] - fn) * dx) + 1.0) * prob;  // importancesampling.cpp:43-47
+                } else {
+                    const double fy = 2.0 * gy;
+                    wgt = prob * exp(0.5 * (fn + fy) * (0.25 * dt * (fn - fy) - dx));
+                }
+            }
+            // the reference rejects when weight < u (importancesampling.cpp:72,
+            // bruteforce.cpp:44); a NaN weight is flagged and rejected
+            if (wgt != wgt) status |= ST_BAD_RATIO;
+            accept = wgt >= r2;
+        }
+        if (accept) {
+            const int p = k / dim;
+            if (P.flags & F_SLATER) {
+                // Sherman-Morrison on the moved particle's block (slaterdeterminant.cpp:165-175)
+                const int n = g.n, b = p / n, pl = p - b * n;
+                double *rows = rec + g.off_inv + (size_t)b * n * n;
+                for (int o = lane; o < n; o += 32) scr[SCR_ROW + o] = rows[(size_t)pl * n + o];
+                __syncwarp();
+                if (lane < n) {
+                    double *row = rows + (size_t)lane * n;
+                    double S = 0.0;
+                    for (int o = 0; o < n; ++o) S += scr[SCR_PHI + o] * row[o];
+                    const double c = S / R;
+                    for (int o = 0; o < n; ++o)
+                        row[o] = lane == pl ? scr[SCR_ROW + o] / R : row[o] - c * scr[SCR_ROW + o];
+                }
+                __syncwarp();
+            }
+            if (lane == 0) {
+                x[k] = xn;
+                if (is) fc[k] = fn;
+            }
+            if (P.flags & Q_PADE_STALE) {  // the moved particle's pairs take the current gamma
+                for (int j = lane; j < N; j += 32)
+                    if (j != p) mask[j] |= 1ull << p;
+                if (lane == 0) mask[p] = ~0ull;
+            }
+            __syncwarp();
+            gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr);
+        }
+        if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
+        const double *en = rec + g.off_en;
+        if (a.rec_en && lane == 0) {
+            double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
+            o[0] = en[0];
+            o[1] = en[1];
+            o[2] = en[2];
+        }
+        if (it_step >= a.burn_in) {  // Sampler::sample (sampler.cpp:52-90)
+            const double el = en[0] + en[1] + en[2];
+            if (el != el) status |= ST_NAN_ENERGY;
+            const bool win = it_step > a.win_lo && it_step < a.win_hi;
+            const int top = win ? P.nacc : 9;
+            const double *pg = rec + g.off_pg;
+            for (int t = lane; t < top; t += 32) {
+                double q;
+                if (t < 8) {
+                    const double base = t < 2 ? el : en[(t >> 1) - 1];
+                    q = (t & 1) ? base * base : base;
+                } else if (t == 8) {
+                    q = accept ? 1.0 : 0.0;
+                } else {
+                    const int j = t - 9;
+                    q = j < g.EP ? pg[j] : el * pg[j - g.EP];
+                }
+                double s1 = acc[2 * t], c1 = acc[2 * t + 1];
+                kadd(s1, c1, q);
+                acc[2 * t] = s1;
+                acc[2 * t + 1] = c1;
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        P.counter[w] = ctr;
+        if (status) P.status[w] |= status;
+    }
+}
+
+}  // namespace
+
+cudaError_t upload_hermite_gen(const HermiteCoef &h) { return cudaMemcpyToSymbol(c_herm, &h, sizeof(h)); }
+
+std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
+{
+    g = GenParams{};
+    const int N = c.N, dim = c.dim, D = N * dim;
+    g.D = D;
+    g.p_max = p_max;
+    g.EP = E * p_max;
+    g.hidden = c.hidden;
+    g.sigma = c.sigma;
+    g.basis = c.basis == "hydrogenOrbital" ? BASIS_HYDROGEN : BASIS_HERMITE;
+    const bool slater = std::count(c.elements.begin(), c.elements.end(), (int)E_SLATER) > 0;
+    g.n = slater ? N / 2 : 0;
+    if (slater) {
+        if (N % 2) return "Slater determinant needs an even particle count";
+        if (g.n > 32) return "more than 32 orbitals per spin block";
+        if (g.basis == BASIS_HERMITE) {
+            int o = 0;
+            for (int s = 0; o < g.n; ++s) {  // shells in the reference's order (basis.cpp:81-116)
+                if (dim == 2) {
+                    for (int j = 0; j <= s && o < g.n; ++j, ++o) {
+                        g.orb[o][0] = (unsigned char)(s - j);
+                        g.orb[o][1] = (unsigned char)j;
+                        g.orb[o][2] = 0;
+                    }
+                } else {
+                    for (int j = 0; j <= s && o < g.n; ++j)
+                        for (int l = 0; l <= s - j && o < g.n; ++l, ++o) {
+                            g.orb[o][0] = (unsigned char)(s - j - l);
+                            g.orb[o][1] = (unsigned char)j;
+                            g.orb[o][2] = (unsigned char)l;
+                        }
+                }
+                if (s > 12) return "too many Hermite shells";
+            }
+            // closed shells only (basis.cpp:62-79)
+            int count = 0, s = 0;
+            while (count < g.n) {
+                count += dim == 2 ? s + 1 : (s + 1) * (s + 2) / 2;
+                ++s;
+            }
+            if (count != g.n) return "open shell: numParticles is not a closed shell";
+        } else {
+            if (dim != 3) return "hydrogen orbitals are three-dimensional (hydrogenorbital.cpp:17)";
+            // closed-shell atoms He, Be, Ne, Mg, Ar (hydrogenorbital.cpp:28-58) with
+            // orbitals (n, l, m) in the reference's order (generateLOS), l <= 1
+            if (N != 2 && N != 4 && N != 10 && N != 12 && N != 18)
+                return "hydrogen orbitals: numParticles must be 2, 4, 10, 12 or 18 on this engine";
+            int o = 0;
+            for (int nq = 1; nq <= 3 && o < g.n; ++nq)
+                for (int l = 0; l < nq && o < g.n; ++l)
+                    for (int m = -l; m <= l && o < g.n; ++m, ++o) {
+                        g.orb[o][0] = (unsigned char)nq;
+                        g.orb[o][1] = (unsigned char)l;
+                        g.orb[o][2] = (unsigned char)(m + 1);
+                    }
+        }
+    }
+    const bool rbmp = std::count(c.elements.begin(), c.elements.end(), (int)E_RBMPRODUCT) > 0;
+    if (rbmp && (D > GEN_SCR / 4 || c.hidden > 64)) return "RBMProduct: at most 64 coordinates and 64 hidden units";
+    // record layout (doubles): x | fc | grad | energies (4) | pgrad (E p_max) | inverse (2 n n)
+    g.off_fc = D;
+    g.off_g = 2 * D;
+    g.off_en = 3 * D;
+    g.off_pg = 3 * D + 4;
+    g.off_inv = round_up(g.off_pg + g.EP, 2);
+    g.rec = round_up(g.off_inv + 2 * g.n * g.n, 2);
+    return "";
+}
+
+int gen_smem_per_warp(const GenParams &g) { return g.n * 2 * g.n * 8; }
+
+cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, double *o_grad, double *o_lap,
+                             double *o_pg, double *o_en, cudaStream_t st)
+{
+    const size_t smem = mode == GEN_INIT ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0;
+    cudaError_t e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    gen_state_kernel<<<(P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(P, g, mode, o_grad, o_lap, o_pg,
+                                                                                o_en);
+    return cudaGetLastError();
+}
+
+cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st)
+{
+    gen_sweep_kernel<<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, 0, st>>>(a, g);
+    return cudaGetLastError();
+}
+
+}  // namespace vmc

@@ -1,0 +1,34 @@
+// General walker path (vmc_general.cu): FP64 kernels for every wave-function
+// element, used when a system has SimpleJastrow, RBM or hydrogen-orbital parts.
+#pragma once
+#include <string>
+
+#include "vmc_config.hpp"
+#include "vmc_kernels.cuh"
+
+namespace vmc {
+
+enum : int { BASIS_HERMITE = 1, BASIS_HYDROGEN = 2 };
+enum : int { GEN_INIT = 0, GEN_STATE = 1 };
+
+// Record layout (offsets in doubles), element data and orbital table of the
+// general path; passed by value to its kernels.
+struct GenParams {
+    int D, n, EP, p_max;        // coordinates, orbitals per block, E x p_max, p_max
+    int off_fc, off_g, off_en, off_pg, off_inv, rec;
+    int basis, hidden;          // BASIS_*, RBMProduct hidden units
+    double sigma;               // RBM width
+    const double *theta;        // E x p_max parameters on the device
+    unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
+};
+
+// "" when the general path takes the configuration (fills g except theta), else why not.
+std::string gen_configure(const Config &c, int n_elements, int p_max, GenParams &g);
+// Initialise (invert the Slater blocks, evaluate, force cache) or re-evaluate every
+// walker; with output pointers, also the per-element values of vmc_eval.
+cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, double *o_grad, double *o_lap,
+                             double *o_pg, double *o_en, cudaStream_t st);
+cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st);
+cudaError_t upload_hermite_gen(const HermiteCoef &h);
+
+}  // namespace vmc
