@@ -69,13 +69,55 @@ static void hermite_table(double x, int mmax, double *h, double *h1, double *h2)
 
 /* phi_k(r) and derivatives along dim a (hermite.cpp:35-72: product over dims). */
 typedef struct {
-    int n, d, mmax;
-    int q[MAXORB][3];
+    int n, d, mmax, basis, horb3;
+    double Z;
+    int q[MAXORB][3]; /* Hermite degrees, or hydrogen (n, l, m) */
 } orbset;
+
+/* Hydrogen orbitals of hydrogenorbital.cpp:108-394 (alpha fixed at 1, k = Z),
+ * n <= 3 and l <= 1: phi = A(r) f(r) exp(-k r / n) with A = 1 (s) or one
+ * coordinate (p: m = 1 -> x, -1 -> y, 0 -> z) and f = 1 (1s, 2p), 2 - k r (2s),
+ * 2 k^2 r^2 - 18 k r + 27 (3s), k r - 6 (3p).  With R = f exp(-k r / n):
+ *   d_a phi   = (d_a A) R + A R' x_a / r
+ *   d_a^2 phi = 2 (d_a A) R' x_a / r + A (R'' x_a^2 / r^2 + R' (1 / r - x_a^2 / r^3)). */
+static void hydrogen_eval(const orbset *o, const double *r, double *phi, double *dphi, double *d2phi)
+{
+    double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), k = o->Z;
+    for (int q = 0; q < o->n; q++) {
+        int nq = o->q[q][0], l = o->q[q][1], m = o->q[q][2];
+        double f = 1.0, fp = 0.0, fpp = 0.0;
+        if (nq == 2 && l == 0) { f = 2.0 - k * rr; fp = -k; }
+        if (nq == 3 && l == 0) { f = 2.0 * k * k * rr * rr - 18.0 * k * rr + 27.0; fp = 4.0 * k * k * rr - 18.0 * k; fpp = 4.0 * k * k; }
+        if (nq == 3 && l == 1) { f = k * rr - 6.0; fp = k; }
+        double a = k / nq, ex = exp(-a * rr);
+        double R = f * ex, R1 = (fp - a * f) * ex, R2 = (fpp - 2.0 * a * fp + a * a * f) * ex;
+        int ca = l == 1 ? (m == 1 ? 0 : m == -1 ? 1 : 2) : -1;
+        double A = ca >= 0 ? r[ca] : 1.0;
+        if (phi) phi[q] = A * R;
+        for (int c = 0; c < 3; c++) {
+            double u = r[c] / rr, dA = c == ca ? 1.0 : 0.0;
+            if (dphi) dphi[c * o->n + q] = dA * R + A * R1 * u;
+            double d2 = 2.0 * dA * R1 * u + A * (R2 * u * u + R1 * (1.0 / rr - u * u / rr));
+            if (nq == 3 && o->horb3) {
+                /* the reference's n = 3 "second derivatives" (hydrogenorbital.cpp:351-364),
+                 * which are not d^2/dx_c^2: reproduced under the quirk */
+                double kr = k * rr, pre = k * ex / (81.0 * rr * rr * rr);
+                d2 = l == 0 ? pre * (rr * rr * (2.0 * kr * (5.0 - 3.0 * kr) - 27.0) +
+                                     r[c] * r[c] * (kr * (2.0 * kr * (kr - 18.0) + 9.0) + 27.0))
+                            : pre * A * (kr - 18.0) * (kr - 6.0) / rr;
+            }
+            if (d2phi) d2phi[c * o->n + q] = d2;
+        }
+    }
+}
 
 static void orb_eval(const orbset *o, const double *r, double *phi, double *dphi /*d x n*/,
                      double *d2phi /*d x n*/)
 {
+    if (o->basis == VMO_BASIS_HYDROGEN) {
+        hydrogen_eval(o, r, phi, dphi, d2phi);
+        return;
+    }
     double h[3][MAXDEG], h1[3][MAXDEG], h2[3][MAXDEG];
     for (int a = 0; a < o->d; a++) hermite_table(r[a], o->mmax, h[a], h1[a], h2[a]);
     for (int k = 0; k < o->n; k++) {
@@ -95,6 +137,24 @@ static void orb_eval(const orbset *o, const double *r, double *phi, double *dphi
 static int orb_setup(const vmo_system *s, orbset *o)
 {
     o->d = s->d;
+    o->basis = s->basis;
+    o->Z = s->Z;
+    o->horb3 = (s->quirks & VMO_Q_HORB3) != 0;
+    if (s->basis == VMO_BASIS_HYDROGEN) {
+        /* closed-shell atoms (hydrogenorbital.cpp:28-58); orbitals (n, l, m) in the
+         * order of generateLOS (hydrogenorbital.cpp:60-76), l <= 1 here */
+        if (s->d != 3 || (s->N != 2 && s->N != 4 && s->N != 10 && s->N != 12 && s->N != 18)) return -1;
+        int cnt = 0;
+        for (int nq = 1; nq <= 3 && cnt < s->N / 2; nq++)
+            for (int l = 0; l < nq && l <= 1 && cnt < s->N / 2; l++)
+                for (int m = -l; m <= l && cnt < s->N / 2; m++) {
+                    o->q[cnt][0] = nq; o->q[cnt][1] = l; o->q[cnt][2] = m;
+                    cnt++;
+                }
+        o->n = cnt;
+        o->mmax = 0;
+        return 0;
+    }
     int n = hermite_orbitals(s->N, s->d, o->q);
     if (n < 0 || n > MAXORB) return -1;
     o->n = n;

@@ -41,7 +41,8 @@ enum {
     VMO_Q_SJ_RATIO = 4,       /* SimpleJastrow ratio over j > moved particle only (simplejastrow.cpp:148) */
     VMO_Q_IS_GREEN = 8,       /* IS Green's ratio as in importancesampling.cpp:43-47,58          */
     VMO_Q_RBM_SORT = 16,      /* RBMProduct hidden units see sorted coordinates (wavefunction.cpp:40-55) */
-    VMO_Q_ALL = 31,
+    VMO_Q_HORB3 = 32,         /* n = 3 hydrogen-orbital second derivatives as hydrogenorbital.cpp:351-364 */
+    VMO_Q_ALL = 63,
 };
 
 #define VMO_MAX_ELEM 8

@@ -5,7 +5,8 @@ oracle/Makefile (`make ref`) compiles from the reference's own C++ sources.  The
 fixtures it writes are committed, so the tests that use them need neither the
 reference nor its build.
 
-    python tests/golden/make_golden.py      # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py            # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py hydrogen   # only hydrogen_orbitals.npz
 
 Every input is seeded synthetic data: walker positions ~ N(0, 1/sqrt(omega)),
 replayed uniforms/normals from numpy's PCG64 with fixed seeds.
@@ -28,7 +29,7 @@ def spec_fields(spec):
                 coulomb=int(spec.coulomb), sampling=spec.sampling, step=spec.step,
                 hidden=spec.hidden, atom=int(spec.atom), sorting=int(spec.sorting),
                 optimization=spec.optimization, learning_rate=spec.learning_rate,
-                num_steps=spec.num_steps, config=spec.input_in())
+                num_steps=spec.num_steps, basis=spec.basis, config=spec.input_in())
 
 
 EVAL_CASES = [
@@ -84,6 +85,25 @@ ITER_CASES = [
 ]
 
 
+# Slater determinants of hydrogen orbitals (hydrogenorbital.cpp): He, Be, Ne, Mg, Ar.
+# Written to their own file with their own seed, so the fixtures above stay as they are.
+H_ORB = dict(d=3, atom=True, basis="hydrogenOrbital")
+HYDROGEN_EVAL = [
+    ("he_horb_pade", SystemSpec(N=2, Z=2, elements=(S, P), **H_ORB), 1.0, [[0], [0.4]]),
+    ("be_horb_pade", SystemSpec(N=4, Z=4, elements=(S, P), **H_ORB), 1.0, [[0], [0.35]]),
+    ("ne_horb_pade", SystemSpec(N=10, Z=10, elements=(S, P), **H_ORB), 0.6, [[0], [0.3]]),
+    ("ne_horb_noint", SystemSpec(N=10, Z=10, elements=(S,), coulomb=False, **H_ORB), 0.6, None),
+    ("mg_horb_pade", SystemSpec(N=12, Z=12, elements=(S, P), **H_ORB), 0.8, [[0], [0.3]]),
+    ("ar_horb_pade", SystemSpec(N=18, Z=18, elements=(S, P), **H_ORB), 0.8, [[0], [0.25]]),
+]
+HYDROGEN_CHAINS = [
+    ("he_horb_pade_is", SystemSpec(N=2, Z=2, elements=(S, P), step=0.05, **H_ORB), 300),
+    ("ne_horb_pade_is", SystemSpec(N=10, Z=10, elements=(S, P), step=0.01, **H_ORB), 300),
+    ("ne_horb_pade_bf", SystemSpec(N=10, Z=10, elements=(S, P), sampling="bruteForce", step=0.02,
+                                   **H_ORB), 300),
+]
+
+
 def theta_for(spec, how, rng):
     E = len(spec.elements)
     Pm = spec.p_max
@@ -97,9 +117,9 @@ def theta_for(spec, how, rng):
     return th
 
 
-def make_eval(rng):
+def make_eval(rng, cases=EVAL_CASES):
     out = {}
-    for name, spec, scale, how in EVAL_CASES:
+    for name, spec, scale, how in cases:
         theta = theta_for(spec, how, rng)
         rec = {k: [] for k in ("pos", "grad", "lap", "pgrad", "energies", "k", "xnew", "ratios",
                                "grad2", "lap2", "pgrad2", "energies2")}
@@ -132,9 +152,9 @@ def make_stream(spec, steps, rng):
     return st
 
 
-def make_chains(rng):
+def make_chains(rng, cases=CHAIN_CASES):
     out = {}
-    for name, spec, steps in CHAIN_CASES:
+    for name, spec, steps in cases:
         scale = 1.0 / np.sqrt(spec.omega) if not spec.atom else 1.0
         pos = rng.normal(0.0, scale, spec.D)
         stream = make_stream(spec, steps, rng)
@@ -199,7 +219,18 @@ def make_blocking(rng):
     return out
 
 
+def make_hydrogen():
+    rng = np.random.default_rng(20261204)
+    out = make_eval(rng, HYDROGEN_EVAL)
+    out.update({f"chain_{k}": v for k, v in make_chains(rng, HYDROGEN_CHAINS).items()})
+    np.savez_compressed(os.path.join(HERE, "hydrogen_orbitals.npz"), **out)
+
+
 def main():
+    if sys.argv[1:] == ["hydrogen"]:
+        make_hydrogen()
+        return
+    make_hydrogen()
     rng = np.random.default_rng(20261203)
     np.savez_compressed(os.path.join(HERE, "eval_fixed.npz"), **make_eval(rng))
     np.savez_compressed(os.path.join(HERE, "chains.npz"), **make_chains(rng))

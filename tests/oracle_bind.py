@@ -24,8 +24,8 @@ ELEMENT_KEYS = {
     SIMPLEJASTROW: "simpleJastrow", RBMGAUSSIAN: "RBMGaussian", RBMPRODUCT: "RBMProduct",
     HYDROGENLIKE: "hydrogenLike",
 }
-Q_PADE_RATIO, Q_PADE_DGAMMA, Q_SJ_RATIO, Q_IS_GREEN, Q_RBM_SORT = 1, 2, 4, 8, 16
-Q_ALL = 31
+Q_PADE_RATIO, Q_PADE_DGAMMA, Q_SJ_RATIO, Q_IS_GREEN, Q_RBM_SORT, Q_HORB3 = 1, 2, 4, 8, 16, 32
+Q_ALL = 63
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -323,4 +323,5 @@ def spec_from_case(c):
         sampling=str(c["spec_sampling"]), step=float(c["spec_step"]), hidden=int(c["spec_hidden"]),
         atom=bool(c["spec_atom"]), sorting=bool(c["spec_sorting"]),
         optimization=str(c["spec_optimization"]), learning_rate=float(c["spec_learning_rate"]),
-        num_steps=int(c["spec_num_steps"]))
+        num_steps=int(c["spec_num_steps"]),
+        basis=str(c["spec_basis"]) if "spec_basis" in c else "hermite")

@@ -240,7 +240,7 @@ Params make_params(const vmc_engine *e)
     P.gamma = 0.0;
     P.alpha_h = 0.0;
     P.idx_alpha = P.idx_gamma = P.idx_alpha_h = -1;
-    for (int i = 0; i < e->E; ++i) {
+    for (int i = 0; i < e->E && e->Pmax > 0; ++i) {  // no parameters: nothing to read
         const double t0 = e->theta[(size_t)i * e->Pmax];
         switch (e->cfg.elements[i]) {
         case E_GAUSSIAN: P.alpha = t0; P.idx_alpha = i * e->Pmax; break;

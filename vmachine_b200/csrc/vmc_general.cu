@@ -107,6 +107,14 @@ __device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const 
         const double xc = r[c], u = xc / rr, dA = (c == ca) ? 1.0 : 0.0;
         d1[c] = dA * R + A * R1 * u;
         d2[c] = 2.0 * dA * R1 * u + A * (R2 * u * u + R1 * (1.0 / rr - u * u / rr));
+        if (nq == 3 && g.horb3) {
+            // compat: the reference's n = 3 "second derivatives" (hydrogenorbital.cpp:351-364),
+            // which are not d^2/dx_c^2
+            const double kr = k * rr, pre = k * ex / (81.0 * rr * rr * rr);
+            d2[c] = l == 0 ? pre * (rr * rr * (2.0 * kr * (5.0 - 3.0 * kr) - 27.0) +
+                                    xc * xc * (kr * (2.0 * kr * (kr - 18.0) + 9.0) + 27.0))
+                           : pre * A * (kr - 18.0) * (kr - 6.0) / rr;
+        }
     }
 }
 
@@ -750,6 +758,7 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     g.hidden = c.hidden;
     g.sigma = c.sigma;
     g.basis = c.basis == "hydrogenOrbital" ? BASIS_HYDROGEN : BASIS_HERMITE;
+    g.horb3 = c.compat ? 1 : 0;
     const bool slater = std::count(c.elements.begin(), c.elements.end(), (int)E_SLATER) > 0;
     g.n = slater ? N / 2 : 0;
     if (slater) {

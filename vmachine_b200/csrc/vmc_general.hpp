@@ -17,6 +17,7 @@ struct GenParams {
     int D, n, EP, p_max;        // coordinates, orbitals per block, E x p_max, p_max
     int off_fc, off_g, off_en, off_pg, off_inv, rec;
     int basis, hidden;          // BASIS_*, RBMProduct hidden units
+    int horb3;                  // n = 3 hydrogen orbitals with the reference's second derivatives
     double sigma;               // RBM width
     const double *theta;        // E x p_max parameters on the device
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)

@@ -267,7 +267,7 @@ extern "C" int vmc_local_energies_noalloc(const char *input_in_text, const doubl
     P.Z = s.c.Z;
     P.step = s.c.step_length;
     P.idx_alpha = P.idx_gamma = P.idx_alpha_h = -1;
-    for (int i = 0; i < s.E; ++i) {
+    for (int i = 0; i < s.E && s.Pmax > 0; ++i) {  // no parameters: nothing to read
         const double t0 = theta[(size_t)i * s.Pmax];
         switch (s.c.elements[i]) {
         case E_GAUSSIAN: P.alpha = t0; P.idx_alpha = i * s.Pmax; break;
