@@ -341,6 +341,7 @@ def run_engine_arm(args):
                    "precision": "mixed", "refresh_interval": refresh_now,
                    "inverse_drift": {"max": max_drift, "q99": q99_drift},
                    "walkers_per_block": eng.info.walkers_per_block,
+                   "kernel": ["runtime-flags", "compiled-in dot flags", "general"][eng.info.kernel_variant],
                    "l2": "walker state %.0f MB per GPU > 126 MB L2, streamed every launch"
                          % (W * (eng.info.n_coords * 5 * 4 + 2 * 28 * 28 * 4 + 56 * 8 + 64) / 1e6)},
         "el_samples_per_s": value * spw / (spw + burn),

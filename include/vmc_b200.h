@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define VMC_ABI_VERSION 1
+#define VMC_ABI_VERSION 2
 
 enum {
     VMC_OK = 0,
@@ -57,7 +57,12 @@ typedef struct {
     int n_accumulators;                         /* 9 + 2 * n_elements * p_max          */
     int walkers_per_block, refresh_interval;
     int element_kind[8];                        /* VMC_ELEM_* in configuration order    */
+    int kernel_variant;                         /* VMC_KERNEL_* of the sweep            */
 } vmc_info;
+
+/* Sweep implementations: element flags read at run time, the quantum-dot flag
+ * set compiled in, or the general FP64 path (SimpleJastrow, RBM, hydrogen orbitals). */
+enum { VMC_KERNEL_RUNTIME_FLAGS = 0, VMC_KERNEL_DOT = 1, VMC_KERNEL_GENERAL = 2 };
 
 enum {
     VMC_ELEM_GAUSSIAN = 0,

@@ -28,7 +28,8 @@ def test_library_exports_every_declared_symbol():
     for name in declared_functions():
         assert hasattr(lib, name), name
     assert set(EXPORTS) <= set(declared_functions())
-    assert lib.vmc_abi_version() == 1
+    version = int(re.search(r"#define VMC_ABI_VERSION (\d+)", open(HEADER).read()).group(1))
+    assert lib.vmc_abi_version() == version
 
 
 @pytest.mark.parametrize("text,code", [

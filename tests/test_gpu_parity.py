@@ -185,3 +185,21 @@ def test_mixed_precision_tracks_fp64(n):
         el64 = e64[w, :upto].sum(-1)
         el32 = e32[w, :upto].sum(-1)
         assert np.max(np.abs(el32 - el64) / np.abs(el64)) < 1e-4
+
+
+def test_kernel_selection():
+    """Quantum dots run the compiled-in flag set in both compat modes and both
+    precisions; systems without a Slater determinant read flags at run time;
+    SimpleJastrow / RBM / hydrogen orbitals take the general path."""
+    from vmachine_b200 import Engine
+    from vmachine_b200.engine import KERNEL_DOT, KERNEL_GENERAL, KERNEL_RUNTIME_FLAGS
+    dot = SystemSpec(N=56, omega=0.28, elements=(SLATER, GAUSSIAN, PADE), num_steps=64 * 100)
+    for compat in (1, 0):
+        for precision in (0, 1):
+            with Engine(dot.input_in(), walkers=64, precision=precision, compat=compat) as eng:
+                assert eng.info.kernel_variant == KERNEL_DOT, (compat, precision)
+    with Engine(SystemSpec(N=2, elements=(GAUSSIAN, PADE)).input_in(), walkers=4) as eng:
+        assert eng.info.kernel_variant == KERNEL_RUNTIME_FLAGS
+    sj = SystemSpec(N=6, elements=(SLATER, GAUSSIAN, SIMPLEJASTROW), sorting=True)
+    with Engine(sj.input_in(), walkers=4) as eng:
+        assert eng.info.kernel_variant == KERNEL_GENERAL

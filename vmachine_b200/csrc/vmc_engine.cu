@@ -480,8 +480,11 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         if (std::count(c.elements.begin(), c.elements.end(), (int)el) > 1) return reject("repeated element");
     if (c.coulomb) flags |= F_COULOMB;
     if (c.hamiltonian == "atomicNucleus") flags |= F_ATOM;
-    if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE | Q_SJ_RATIO;
-    if (c.compat && c.sorting) flags |= Q_RBM_SORT;
+    if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
+    // quirk bits of the general-path elements only where those elements are present,
+    // so a quantum dot keeps its compiled-in flag set
+    if (c.compat && (flags & F_SIMPLEJ)) flags |= Q_SJ_RATIO;
+    if (c.compat && c.sorting && (flags & F_RBMP)) flags |= Q_RBM_SORT;
     if (c.sampling != "bruteForce") flags |= F_IS;
     e->general = general;
     e->flags = flags;
@@ -598,6 +601,9 @@ int vmc_get_info(const vmc_engine *e, vmc_info *o)
     o->walkers_per_block = e->wpb;
     o->refresh_interval = e->refresh_interval;
     for (int i = 0; i < e->E && i < 8; ++i) o->element_kind[i] = e->cfg.elements[i];
+    o->kernel_variant = e->general ? VMC_KERNEL_GENERAL
+                        : (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED) && e->K > 0
+                            ? VMC_KERNEL_DOT : VMC_KERNEL_RUNTIME_FLAGS;
     return VMC_OK;
 }
 
