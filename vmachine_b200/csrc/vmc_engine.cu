@@ -173,6 +173,7 @@ struct vmc_engine {
     double *d_scal = nullptr, *d_acc = nullptr, *d_out = nullptr, *d_drift = nullptr;
     unsigned long long *d_mask = nullptr, *d_counter = nullptr;
     unsigned *d_status = nullptr;
+    double *d_pos = nullptr;  // W x D positions staged for the host link
     std::vector<cudaEvent_t> sweep_events;  // per-launch timing of the sweep kernel
     cudaEvent_t sw0 = nullptr, sw1 = nullptr;  // vmc_stopwatch
     // optional replayed random stream consumed by vmc_sample (W x replay_len x 3)
@@ -200,6 +201,7 @@ void free_engine(vmc_engine *e)
     cudaFree(e->d_status);
     cudaFree(e->d_replay);
     cudaFree(e->d_theta);
+    cudaFree(e->d_pos);
     for (cudaEvent_t ev : e->sweep_events) cudaEventDestroy(ev);
     if (e->sw0) cudaEventDestroy(e->sw0);
     if (e->sw1) cudaEventDestroy(e->sw1);
@@ -550,6 +552,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
             CUDA_TRY(cudaMalloc(&e->d_mask, W * e->N * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_counter, W * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_status, W * sizeof(unsigned)));
+            CUDA_TRY(cudaMalloc(&e->d_pos, W * e->D * sizeof(double)));
             if (e->general) {
                 CUDA_TRY(cudaMalloc(&e->d_theta, std::max<size_t>(1, (size_t)e->EP) * sizeof(double)));
                 e->gen.theta = e->d_theta;
@@ -641,15 +644,16 @@ int vmc_init_walkers(vmc_engine *e, const double *pos, uint64_t seed)
     e->seed = seed;
     const size_t W = e->W;
     if (pos) {
-        std::vector<char> host(W * e->L.rec * e->elem_bytes, 0);
-        for (size_t w = 0; w < W; ++w)
-            for (int c = 0; c < e->D; ++c) {
-                const double v = pos[w * e->D + c];
-                char *dst = host.data() + (w * e->L.rec + e->L.off_x + c) * e->elem_bytes;
-                if (e->elem_bytes == 8) std::memcpy(dst, &v, 8);
-                else { const float f = (float)v; std::memcpy(dst, &f, 4); }
-            }
-        CUDA_TRY(cudaMemcpyAsync(e->d_state, host.data(), host.size(), cudaMemcpyHostToDevice, e->stream));
+        // positions only over the host link; the records are cleared and filled on the device
+        const size_t n = W * e->D;
+        CUDA_TRY(cudaMemsetAsync(e->d_state, 0, W * e->L.rec * e->elem_bytes, e->stream));
+        CUDA_TRY(cudaMemcpyAsync(e->d_pos, pos, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        Layout L = e->L;
+        int Wi = e->W;
+        const double *dp = e->d_pos;
+        void *st = e->d_state;
+        void *args[] = {&L, &Wi, &dp, &st};
+        CUDA_TRY(cudaLaunchKernel(e->ks.scatter, dim3((unsigned)((n + 255) / 256)), dim3(256), args, 0, e->stream));
     } else {
         const bool normal = e->cfg.initial_state == "randomNormal";
         const double sd = 1.0 / e->cfg.omega;  // randomnormal.cpp:19
@@ -682,16 +686,16 @@ int vmc_get_positions(const vmc_engine *e, double *pos)
 {
     if (!e || !pos) return fail(VMC_E_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(e->device));
-    const size_t W = e->W;
-    std::vector<char> host(W * e->L.rec * e->elem_bytes);
-    CUDA_TRY(cudaMemcpyAsync(host.data(), e->d_state, host.size(), cudaMemcpyDeviceToHost, e->stream));
+    // gathered on the device: only the positions cross the host link
+    const size_t n = (size_t)e->W * e->D;
+    Layout L = e->L;
+    int Wi = e->W;
+    const void *st = e->d_state;
+    double *dp = e->d_pos;
+    void *args[] = {&L, &Wi, &st, &dp};
+    CUDA_TRY(cudaLaunchKernel(e->ks.gather, dim3((unsigned)((n + 255) / 256)), dim3(256), args, 0, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(pos, e->d_pos, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
-    for (size_t w = 0; w < W; ++w)
-        for (int c = 0; c < e->D; ++c) {
-            const char *src = host.data() + (w * e->L.rec + e->L.off_x + c) * e->elem_bytes;
-            if (e->elem_bytes == 8) std::memcpy(&pos[w * e->D + c], src, 8);
-            else { float f; std::memcpy(&f, src, 4); pos[w * e->D + c] = f; }
-        }
     return VMC_OK;
 }
 

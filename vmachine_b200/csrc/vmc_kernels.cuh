@@ -492,6 +492,26 @@ __global__ void initial_positions_kernel(Layout L, int W, void *state, unsigned 
     reinterpret_cast<T *>(state)[(size_t)w * L.rec + L.off_x + c] = T(val);
 }
 
+// Caller positions (W x D doubles, device) into the walker records, and back:
+// only the positions cross the host link, the rest of the record stays on the device.
+template <typename T>
+__global__ void scatter_positions_kernel(Layout L, int W, const double *__restrict__ pos, void *state)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)W * L.D) return;
+    const size_t w = i / L.D, c = i - w * L.D;
+    reinterpret_cast<T *>(state)[w * L.rec + L.off_x + c] = T(pos[i]);
+}
+
+template <typename T>
+__global__ void gather_positions_kernel(Layout L, int W, const void *state, double *__restrict__ pos)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)W * L.D) return;
+    const size_t w = i / L.D, c = i - w * L.D;
+    pos[i] = (double)reinterpret_cast<const T *>(state)[w * L.rec + L.off_x + c];
+}
+
 // FMA throughput calibration: FMA_CHAINS independent register chains per thread.
 constexpr int FMA_CHAINS = 8;
 template <typename R>
@@ -514,6 +534,7 @@ __global__ void fma_peak_kernel(R *out, int iters, R m)
 struct KernelSet {
     const void *sweep = nullptr, *rebuild = nullptr, *eval = nullptr, *initpos = nullptr;
     const void *sweep_plain = nullptr;  // production sweep: no probe, replay or recording
+    const void *scatter = nullptr, *gather = nullptr;  // positions in and out of the records
 };
 
 template <typename T, int DIM, int K, int FX>
@@ -526,6 +547,8 @@ KernelSet make_set()
     s.rebuild = reinterpret_cast<const void *>(&rebuild_kernel<T, DIM, K>);
     s.eval = reinterpret_cast<const void *>(&eval_kernel<T, DIM, K>);
     s.initpos = reinterpret_cast<const void *>(&initial_positions_kernel<T>);
+    s.scatter = reinterpret_cast<const void *>(&scatter_positions_kernel<T>);
+    s.gather = reinterpret_cast<const void *>(&gather_positions_kernel<T>);
     return s;
 }
 
