@@ -54,7 +54,7 @@ typedef struct {
     int n_walkers, precision, sampling;         /* sampling: 0 importance, 1 brute force */
     int steps_per_walker, burn_in, batches;     /* per-iteration schedule              */
     int n_iterations, compat;
-    int n_accumulators;                         /* 9 + 2 * n_elements * p_max          */
+    int n_accumulators;                         /* per walker: 9 + 2 x accumulated parameters */
     int walkers_per_block, refresh_interval;
     int element_kind[8];                        /* VMC_ELEM_* in configuration order    */
     int kernel_variant;                         /* VMC_KERNEL_* of the sweep            */

@@ -1,0 +1,100 @@
+"""The learned MLP Jastrow on the GPU (through the C ABI) against the FP64 oracle
+(oracle/mlp_jastrow.py, itself checked by finite differences).
+
+The engine evaluates the networks in FP32 with bfloat16 weights, so the bar is
+relative (max-abs over an array, relative to its max-abs): 2e-5 for J-derived
+gradients, Laplacians, energies and ratios, 1e-4 for dJ/dtheta (sums over pairs
+of FP32 products).  The Slater and Gaussian parts come from the C oracle at 1e-11.
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp_jastrow as mj
+from oracle_bind import GAUSSIAN, SLATER, Oracle, SystemSpec
+
+pytestmark = pytest.mark.gpu
+
+
+def config(N, omega=1.0, sampling="importanceSampling", steps=1000, extra=()):
+    lines = [f"numParticles: {N}", "numDimensions: 2", "hamiltonian: harmonicOscillator",
+             f"omega: {omega!r}", "interactionStyle: coulomb",
+             "waveFunctionElement: slaterDeterminant", "waveFunctionElement: gaussian",
+             "waveFunctionElement: mlpJastrow", "basis: hermite", f"sampling: {sampling}",
+             "stepLength: 0.05", "optimization: adam", "learningRate: 0.01", f"numSteps: {steps}"]
+    return "\n".join(list(lines) + list(extra)) + "\n"
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def theta_for(seed, alpha=0.93):
+    rng = np.random.default_rng(seed)
+    t = np.zeros((3, mj.n_params()))
+    t[1, 0] = alpha
+    t[2] = rng.normal(0.0, 0.3, mj.n_params())
+    return t
+
+
+def oracle_parts(N, theta, pos):
+    spec = SystemSpec(N=N, elements=(SLATER, GAUSSIAN))
+    g, lap, pg, en = Oracle().eval(spec, theta[:2, :1], pos)
+    J, gJ, lJ = mj.jastrow(theta[2], pos, N, 2)
+    return g, lap, en, J, gJ, lJ
+
+
+@pytest.mark.parametrize("N", [2, 6, 12])
+def test_fixed_positions(N):
+    from vmachine_b200 import Engine
+    theta = theta_for(N)
+    rng = np.random.default_rng(100 + N)
+    W = 3
+    pos = rng.normal(0.0, 1.0, (W, 2 * N))
+    with Engine(config(N), walkers=W, precision=0) as eng:
+        eng.set_parameters(theta)
+        eng.init_walkers(pos)
+        g, lap, pg, en = eng.eval()
+        for w in range(W):
+            gs, ls, ens, J, gJ, lJ = oracle_parts(N, theta, pos[w])
+            assert rel(g[w, 2], gJ) < 2e-5
+            assert abs(lap[w, 2] - lJ) < 2e-5 * max(1.0, abs(lJ))
+            assert rel(g[w, :2], gs) < 1e-11
+            kin = -0.5 * (ls.sum() + lJ + ((gs.sum(0) + gJ) ** 2).sum())
+            assert abs(en[w, 0] - kin) < 2e-5 * max(1.0, abs(kin))
+            assert rel(en[w, 1:], ens[1:]) < 1e-11
+            assert rel(pg[w, 2], mj.param_gradient(theta[2], pos[w], N, 2)) < 1e-4
+        # a forced move: the MLP ratio is exp(2 (J(y) - J(x)))
+        k = rng.integers(0, 2 * N, W)
+        xn = pos[np.arange(W), k] + rng.normal(0.0, 0.3, W)
+        r = eng.probe_move(k, xn)
+        g2, lap2, pg2, en2 = eng.eval()
+        for w in range(W):
+            y = pos[w].copy()
+            y[k[w]] = xn[w]
+            want = np.exp(2.0 * (mj.jastrow_value(theta[2], y, N, 2) -
+                                 mj.jastrow_value(theta[2], pos[w], N, 2)))
+            assert abs(r[w, 2] - want) < 2e-5 * want
+            gs, ls, ens, J, gJ, lJ = oracle_parts(N, theta, y)
+            assert rel(g2[w, 2], gJ) < 2e-5
+            kin = -0.5 * (ls.sum() + lJ + ((gs.sum(0) + gJ) ** 2).sum())
+            assert abs(en2[w, 0] - kin) < 2e-5 * max(1.0, abs(kin))
+
+
+def test_sampled_gradient_sums():
+    """One iteration: the MLP rows of the gradient sums come from the window's
+    snapshots, scaled to the window's sample count; dJ/db3 is the pair count, so its
+    sum is pairs x walkers x sampled window steps."""
+    from vmachine_b200 import Engine
+    N, W = 6, 64
+    with Engine(config(N, steps=W * 600), walkers=W, precision=0) as eng:
+        eng.set_parameters(theta_for(5))
+        eng.init_walkers(None, seed=3)
+        info = eng.info
+        sums, g, ge = eng.sample(0, info.steps_per_walker + info.burn_in, info.burn_in)
+        assert np.all(np.isfinite(g)) and np.all(np.isfinite(ge))
+        assert np.abs(g[2]).max() > 0 and np.abs(ge[2]).max() > 0
+        bs = info.steps_per_walker // info.batches
+        lo, hi = max(1, info.burn_in), min(bs - 1, info.steps_per_walker + info.burn_in - 1)
+        n_win = hi - lo + 1
+        assert abs(g[2, 4416] - N * (N - 1) / 2 * W * n_win) < 1e-9 * g[2, 4416]

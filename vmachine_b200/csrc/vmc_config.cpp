@@ -46,6 +46,7 @@ const char *element_label(int e)
     case E_RBMGAUSSIAN: return "RBM-Gaussian";
     case E_RBMPRODUCT: return "RBM-product";
     case E_HYDROGENLIKE: return "hydrogenlike";
+    case E_MLP: return "MLP-Jastrow";
     default: return "other";
     }
 }
@@ -118,6 +119,7 @@ int element_parameters(const Config &cfg, int e)
     case E_SIMPLEJASTROW: return cfg.N * cfg.N;
     case E_RBMGAUSSIAN: return D;
     case E_RBMPRODUCT: return cfg.hidden * D + cfg.hidden;
+    case E_MLP: return MLP_PARAMS;
     default: return 1;
     }
 }
@@ -269,6 +271,7 @@ std::string parse_config(const std::string &text, Config &c)
                 else if (v0 == "RBMProduct") c.elements.push_back(E_RBMPRODUCT);
                 else if (v0 == "hydrogenLike") c.elements.push_back(E_HYDROGENLIKE);
                 else if (v0 == "hardCoreJastrow") c.elements.push_back(E_OTHER);
+                else if (v0 == "mlpJastrow") c.elements.push_back(E_MLP);  // engine element
                 else return err("Wave function element '" + v0 + "' does not exist!");
             } else if (key == "interactionStyle") {
                 if (v0 == "noInteraction") c.coulomb = false;

@@ -7,7 +7,14 @@
 namespace vmc {
 
 enum Element { E_GAUSSIAN = 0, E_SLATER = 1, E_PADE = 2, E_SIMPLEJASTROW = 3,
-               E_RBMGAUSSIAN = 4, E_RBMPRODUCT = 5, E_HYDROGENLIKE = 6, E_OTHER = 99 };
+               E_RBMGAUSSIAN = 4, E_RBMPRODUCT = 5, E_HYDROGENLIKE = 6,
+               E_MLP = 7,  // learned MLP Jastrow (no counterpart in the reference)
+               E_OTHER = 99 };
+
+// MLP Jastrow shape: pair network 2 -> 64 -> 64 -> 1, one-body network 1 -> 32 -> 32 -> 1
+constexpr int MLP_H = 64, MLP_G = 32;
+constexpr int MLP_PARAMS = MLP_H * 2 + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1 +
+                           MLP_G + MLP_G + MLP_G * MLP_G + MLP_G + MLP_G + 1;  // 5570
 
 struct Config {
     // system

@@ -32,6 +32,7 @@ enum : int {
     F_RBMP = 1 << 13,        // RBMProduct
     Q_SJ_RATIO = 1 << 14,    // SimpleJastrow ratio over partners j > moved particle only
     Q_RBM_SORT = 1 << 15,    // RBMProduct hidden units see the sorted coordinates
+    F_MLP = 1 << 16,         // learned MLP Jastrow
 };
 
 // Flag sets with a compiled-in sweep: the 2D quantum dot, Slater x Gaussian x Pade

@@ -149,6 +149,11 @@ struct vmc_engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int W = 0, N = 0, dim = 0, D = 0, n_orb = 0, K = 0, E = 0, Pmax = 0, EP = 0, nacc = 0;
+    // accumulators per walker on the device: nacc on the quantum-dot path; on the
+    // general path 9 + 2 x the active parameters (act, no padding, no MLP row)
+    int nacc_dev = 0;
+    std::vector<int> act;
+    int *d_act = nullptr;
     int precision = 0, compat = 1, flags = 0, sampling = 0;
     int steps_per_walker = 0, burn_in = 0, batches = 1;
     int wpb = 0, refresh_interval = 0, sweep_chunk = 2048;
@@ -161,6 +166,12 @@ struct vmc_engine {
     bool general = false;
     GenParams gen{};
     double *d_theta = nullptr;  // E x p_max on the device (general path)
+    // MLP Jastrow: bf16-rounded weights, parameter-gradient snapshots and sums
+    int mlp_e = -1;                // element index, or -1
+    float *d_mlpw = nullptr;
+    float *d_snap_x = nullptr;
+    double *d_snap_e = nullptr, *d_mlp_out = nullptr;
+    size_t snap_cap = 0;           // snapshots the buffers hold
     std::vector<double> theta;
     double gamma_prev = 0.0;
     bool have_walkers = false;
@@ -201,6 +212,11 @@ void free_engine(vmc_engine *e)
     cudaFree(e->d_status);
     cudaFree(e->d_replay);
     cudaFree(e->d_theta);
+    cudaFree(e->d_act);
+    cudaFree(e->d_mlpw);
+    cudaFree(e->d_snap_x);
+    cudaFree(e->d_snap_e);
+    cudaFree(e->d_mlp_out);
     cudaFree(e->d_pos);
     for (cudaEvent_t ev : e->sweep_events) cudaEventDestroy(ev);
     if (e->sw0) cudaEventDestroy(e->sw0);
@@ -231,7 +247,7 @@ Params make_params(const vmc_engine *e)
     P.N = e->N;
     P.n_elem = e->E;
     P.ep = e->EP;
-    P.nacc = e->nacc;
+    P.nacc = e->nacc_dev;
     for (int i = 0; i < e->E && i < MAX_ELEM; ++i) P.elem_kind[i] = e->cfg.elements[i];
     P.flags = e->flags;
     P.sampling = e->sampling;
@@ -393,6 +409,24 @@ int initial_weights(vmc_engine *e)
             for (int j = 0; j < e->Pmax; ++j) e->theta[(size_t)i * e->Pmax + j] = rows[i][j];
         }
     }
+    if (e->mlp_e >= 0 && method != "fromfile") {
+        // MLP Jastrow: Xavier-uniform hidden layers, zero biases and output layers, so
+        // the factor starts as its cusp term alone (host Philox, stream tag 3)
+        double *t = e->theta.data() + (size_t)e->mlp_e * e->Pmax;
+        std::fill(t, t + e->Pmax, 0.0);
+        auto u3 = [&](uint32_t i) {
+            const uint4 v = host_philox(make_uint4(i, 0u, 0u, 3u), make_uint2((uint32_t)s, (uint32_t)(s >> 32)));
+            return v.x * 2.3283064365386963e-10;
+        };
+        auto fill = [&](int off, int n, int fan_in, int fan_out) {
+            const double lim = std::sqrt(6.0 / (fan_in + fan_out));
+            for (int i = 0; i < n; ++i) t[off + i] = -lim + 2 * lim * u3((uint32_t)(off + i));
+        };
+        fill(MW_W1, MLP_H * 2, 2, MLP_H);
+        fill(MW_W2, MLP_H * MLP_H, MLP_H, MLP_H);
+        fill(MW_V1, MLP_G, 1, MLP_G);
+        fill(MW_V2, MLP_G * MLP_G, MLP_G, MLP_G);
+    }
     return VMC_OK;
 }
 
@@ -401,6 +435,19 @@ int upload_theta(vmc_engine *e)
     if (!e->general) return VMC_OK;  // the quantum-dot kernels take their scalars by value
     CUDA_TRY(cudaMemcpyAsync(e->d_theta, e->theta.data(), e->theta.size() * sizeof(double),
                              cudaMemcpyHostToDevice, e->stream));
+    if (e->mlp_e >= 0) {
+        // the networks run with their weights rounded to bfloat16 (nearest even)
+        std::vector<float> w(MLP_PARAMS);
+        for (int i = 0; i < MLP_PARAMS; ++i) {
+            const float f = (float)e->theta[(size_t)e->mlp_e * e->Pmax + i];
+            uint32_t b;
+            std::memcpy(&b, &f, 4);
+            b = ((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16) << 16;
+            std::memcpy(&w[i], &b, 4);
+        }
+        CUDA_TRY(cudaMemcpyAsync(e->d_mlpw, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));  // w is a local buffer
+    }
     return VMC_OK;
 }
 
@@ -455,7 +502,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     // SimpleJastrow, the RBM elements and hydrogen orbitals run on the general path
     bool general = false;
     for (int el : c.elements)
-        general |= el == E_SIMPLEJASTROW || el == E_RBMGAUSSIAN || el == E_RBMPRODUCT ||
+        general |= el == E_SIMPLEJASTROW || el == E_RBMGAUSSIAN || el == E_RBMPRODUCT || el == E_MLP ||
                    (el == E_SLATER && c.basis == "hydrogenOrbital");
     for (int el : c.elements) {
         switch (el) {
@@ -465,6 +512,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         case E_SIMPLEJASTROW: flags |= F_SIMPLEJ; break;
         case E_RBMGAUSSIAN: flags |= F_RBMG; break;
         case E_RBMPRODUCT: flags |= F_RBMP; break;
+        case E_MLP: flags |= F_MLP; break;
         case E_SLATER:
             if (c.basis != "hermite" && c.basis != "hydrogenOrbital")
                 return reject("Slater determinant needs basis: hermite or hydrogenOrbital");
@@ -478,7 +526,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         default: return reject("wave function element not implemented on the engine");
         }
     }
-    for (int el : {E_PADE, E_GAUSSIAN, E_SLATER, E_SIMPLEJASTROW, E_RBMGAUSSIAN, E_RBMPRODUCT})
+    for (int el : {E_PADE, E_GAUSSIAN, E_SLATER, E_SIMPLEJASTROW, E_RBMGAUSSIAN, E_RBMPRODUCT, E_MLP})
         if (std::count(c.elements.begin(), c.elements.end(), (int)el) > 1) return reject("repeated element");
     if (c.coulomb) flags |= F_COULOMB;
     if (c.hamiltonian == "atomicNucleus") flags |= F_ATOM;
@@ -506,6 +554,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     e->EP = e->E * e->Pmax;
     e->nacc = 9 + 2 * e->EP;
     if (!general && e->nacc > 32) return reject("more than 11 parameters per walker is not supported");
+    e->nacc_dev = e->nacc;
     if (general) {
         if (e->precision == VMC_PRECISION_MIXED)
             return reject("mixed precision covers Gaussian, Hermite Slater, Pade and hydrogen-like "
@@ -513,6 +562,13 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         const std::string why = gen_configure(c, e->E, e->Pmax, e->gen);
         if (!why.empty()) return reject(why);
         e->n_orb = e->gen.n;
+        e->nacc_dev = 0;  // set below from the active parameters
+        for (int i = 0; i < e->E; ++i)
+            if (c.elements[i] == E_MLP) e->mlp_e = i;
+        for (int i = 0; i < e->E; ++i)
+            if (i != e->mlp_e)
+                for (int q = 0; q < element_parameters(c, c.elements[i]); ++q) e->act.push_back(i * e->Pmax + q);
+        e->nacc_dev = 9 + 2 * (int)e->act.size();
     }
     // userinput.cpp:60-81 with walkers in place of ranks: numSteps is the total
     // over walkers; each walker burns in its own share times the fraction.
@@ -546,8 +602,8 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
             const size_t W = e->W;
             CUDA_TRY(cudaMalloc(&e->d_state, W * e->L.rec * e->elem_bytes));
             CUDA_TRY(cudaMalloc(&e->d_scal, W * NSCAL * sizeof(double)));
-            CUDA_TRY(cudaMalloc(&e->d_acc, W * e->nacc * 2 * sizeof(double)));
-            CUDA_TRY(cudaMalloc(&e->d_out, 64 * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_acc, W * e->nacc_dev * 2 * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_out, std::max(64, e->nacc_dev) * sizeof(double)));
             CUDA_TRY(cudaMalloc(&e->d_drift, W * sizeof(double)));
             CUDA_TRY(cudaMalloc(&e->d_mask, W * e->N * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_counter, W * sizeof(unsigned long long)));
@@ -556,10 +612,20 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
             if (e->general) {
                 CUDA_TRY(cudaMalloc(&e->d_theta, std::max<size_t>(1, (size_t)e->EP) * sizeof(double)));
                 e->gen.theta = e->d_theta;
+                CUDA_TRY(cudaMalloc(&e->d_act, std::max<size_t>(1, e->act.size()) * sizeof(int)));
+                if (!e->act.empty())
+                    CUDA_TRY(cudaMemcpy(e->d_act, e->act.data(), e->act.size() * sizeof(int), cudaMemcpyHostToDevice));
+                e->gen.act = e->d_act;
+                e->gen.n_act = (int)e->act.size();
+            }
+            if (e->mlp_e >= 0) {
+                CUDA_TRY(cudaMalloc(&e->d_mlpw, MLP_PARAMS * sizeof(float)));
+                CUDA_TRY(cudaMalloc(&e->d_mlp_out, 2 * MLP_PARAMS * sizeof(double)));
+                e->gen.mlp = e->d_mlpw;
             }
             CUDA_TRY(cudaMemsetAsync(e->d_state, 0, W * e->L.rec * e->elem_bytes, e->stream));
             CUDA_TRY(cudaMemsetAsync(e->d_scal, 0, W * NSCAL * sizeof(double), e->stream));
-            CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc * 2 * sizeof(double), e->stream));
+            CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc_dev * 2 * sizeof(double), e->stream));
             CUDA_TRY(cudaMemsetAsync(e->d_drift, 0, W * sizeof(double), e->stream));
             CUDA_TRY(cudaMemsetAsync(e->d_mask, 0xff, W * e->N * sizeof(unsigned long long), e->stream));
             CUDA_TRY(cudaMemsetAsync(e->d_counter, 0, W * sizeof(unsigned long long), e->stream));
@@ -600,7 +666,7 @@ int vmc_get_info(const vmc_engine *e, vmc_info *o)
     o->batches = e->batches;
     o->n_iterations = e->cfg.iterations;
     o->compat = e->compat;
-    o->n_accumulators = e->nacc;
+    o->n_accumulators = e->nacc_dev;
     o->walkers_per_block = e->wpb;
     o->refresh_interval = e->refresh_interval;
     for (int i = 0; i < e->E && i < 8; ++i) o->element_kind[i] = e->cfg.elements[i];
@@ -707,7 +773,7 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
     if (steps < 1 || burn_in < 0 || burn_in >= steps) return fail(VMC_E_ARG, "bad step counts");
     CUDA_TRY(cudaSetDevice(e->device));
     const size_t W = e->W;
-    CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc * 2 * sizeof(double), e->stream));
+    CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc_dev * 2 * sizeof(double), e->stream));
     const int bs = (steps - burn_in) / e->batches;
     const int m = iteration % e->batches;
     double max_drift = 0.0;
@@ -721,15 +787,45 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         CUDA_TRY(cudaEventCreate(&ev));
         e->sweep_events.push_back(ev);
     }
+    // MLP Jastrow parameter gradient: snapshots every D steps of the gradient window
+    // (steps win_lo < s < win_hi, sampled ones s >= burn_in); slot = (s - win_lo) / D - first
+    const int win_lo = bs * m, win_hi = bs * (m + 1);
+    int snap_interval = 0, snap_first = 0, n_slots = 0, n_win = 0;
+    if (e->mlp_e >= 0) {
+        snap_interval = e->D;
+        const int lo = std::max(win_lo + 1, burn_in), hi = std::min(win_hi - 1, steps - 1);
+        n_win = std::max(0, hi - lo + 1);
+        snap_first = std::max(1, (lo - win_lo + snap_interval - 1) / snap_interval);
+        const int last = hi >= win_lo ? (hi - win_lo) / snap_interval : 0;
+        n_slots = std::max(0, last - snap_first + 1);
+        const size_t need = W * (size_t)n_slots;
+        if (need > e->snap_cap) {
+            cudaFree(e->d_snap_x);
+            cudaFree(e->d_snap_e);
+            e->d_snap_x = nullptr;
+            e->d_snap_e = nullptr;
+            e->snap_cap = 0;
+            CUDA_TRY(cudaMalloc(&e->d_snap_x, need * e->D * sizeof(float)));
+            CUDA_TRY(cudaMalloc(&e->d_snap_e, need * sizeof(double)));
+            e->snap_cap = need;
+        }
+    }
     int n_refresh = 0, li = 0;
     for (int off = 0; off < steps; off += chunk, ++li) {
         SweepArgs a{};
         a.steps = std::min(chunk, steps - off);
         a.step_offset = off;
         a.burn_in = burn_in;
-        a.win_lo = bs * m;
-        a.win_hi = bs * (m + 1);
+        a.win_lo = win_lo;
+        a.win_hi = win_hi;
         a.seed = e->seed;
+        if (n_slots > 0) {
+            a.snap_x = e->d_snap_x;
+            a.snap_e = e->d_snap_e;
+            a.snap_stride = n_slots;
+            a.snap_interval = snap_interval;
+            a.snap_first = snap_first;
+        }
         if (e->d_replay) {
             if (e->replay_pos + steps > e->replay_len) return fail(VMC_E_ARG, "replay stream exhausted");
             a.replay = e->d_replay;
@@ -746,12 +842,22 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
             ++n_refresh;
         }
     }
+    if (n_slots > 0) {
+        CUDA_TRY(cudaMemsetAsync(e->d_mlp_out, 0, 2 * MLP_PARAMS * sizeof(double), e->stream));
+        CUDA_TRY(mlp_launch_grad(e->gen, e->N, e->dim, e->d_snap_x, e->d_snap_e, (long long)W * n_slots,
+                                 e->d_mlp_out, e->stream));
+    }
     CUDA_TRY(cudaEventRecord(e->ev1, e->stream));
     if (e->d_replay) e->replay_pos += steps;
-    reduce_acc_kernel<<<e->nacc, 256, 0, e->stream>>>(e->d_acc, e->W, e->nacc, e->d_out);
+    reduce_acc_kernel<<<e->nacc_dev, 256, 0, e->stream>>>(e->d_acc, e->W, e->nacc_dev, e->d_out);
     CUDA_TRY(cudaGetLastError());
-    std::vector<double> sums(e->nacc);
-    CUDA_TRY(cudaMemcpyAsync(sums.data(), e->d_out, e->nacc * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    std::vector<double> sums(e->nacc, 0.0), dev_sums(e->nacc_dev);
+    CUDA_TRY(cudaMemcpyAsync(dev_sums.data(), e->d_out, e->nacc_dev * sizeof(double), cudaMemcpyDeviceToHost,
+                             e->stream));
+    std::vector<double> mlp_sums(n_slots > 0 ? 2 * MLP_PARAMS : 0);
+    if (n_slots > 0)
+        CUDA_TRY(cudaMemcpyAsync(mlp_sums.data(), e->d_mlp_out, mlp_sums.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, e->stream));
     std::vector<unsigned> st(W);
     CUDA_TRY(cudaMemcpyAsync(st.data(), e->d_status, W * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
     if (n_refresh) {
@@ -759,6 +865,16 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         CUDA_TRY(cudaMemcpyAsync(drift.data(), e->d_drift, W * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (e->general) {  // active parameters back to their (element, parameter) slots
+        std::copy(dev_sums.begin(), dev_sums.begin() + 9, sums.begin());
+        const size_t na = e->act.size();
+        for (size_t c = 0; c < na; ++c) {
+            sums[9 + e->act[c]] = dev_sums[9 + c];
+            sums[9 + e->EP + e->act[c]] = dev_sums[9 + na + c];
+        }
+    } else {
+        sums = dev_sums;
+    }
     float ms = 0.f;
     CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
     double sweep_ms = 0.0;
@@ -815,6 +931,16 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         e->last_walker_std_error = std::sqrt(v2 / (e->W - 1) / e->W);
     }
     if (out) *out = s;
+    if (n_slots > 0) {
+        // the MLP row: snapshot sums scaled to the window's sample count (one snapshot
+        // stands for n_win / n_slots sampled steps of its walker)
+        const double scale = (double)n_win / n_slots;
+        const size_t o = 9 + (size_t)e->mlp_e * e->Pmax;
+        for (int i = 0; i < MLP_PARAMS; ++i) {
+            sums[o + i] = scale * mlp_sums[i];
+            sums[o + e->EP + i] = scale * mlp_sums[MLP_PARAMS + i];
+        }
+    }
     if (grad_sum) std::copy(sums.begin() + 9, sums.begin() + 9 + e->EP, grad_sum);
     if (egrad_sum) std::copy(sums.begin() + 9 + e->EP, sums.begin() + 9 + 2 * e->EP, egrad_sum);
     return VMC_OK;
@@ -825,7 +951,7 @@ int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy)
     if (!e || !mean_energy) return fail(VMC_E_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(e->device));
     std::vector<double> col((size_t)e->W * 2);
-    CUDA_TRY(cudaMemcpy2DAsync(col.data(), 2 * sizeof(double), e->d_acc, e->nacc * 2 * sizeof(double),
+    CUDA_TRY(cudaMemcpy2DAsync(col.data(), 2 * sizeof(double), e->d_acc, e->nacc_dev * 2 * sizeof(double),
                                2 * sizeof(double), e->W, cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     const double n = std::max(1.0, e->last_samples_per_walker);
@@ -947,6 +1073,31 @@ int vmc_eval(vmc_engine *e, double *grad, double *lap, double *pgrad, double *en
     std::copy(h.begin() + ng, h.begin() + ng + nl, lap);
     std::copy(h.begin() + ng + nl, h.begin() + ng + nl + np, pgrad);
     std::copy(h.begin() + ng + nl + np, h.end(), energies);
+    if (e->mlp_e >= 0) {
+        // MLP row: the production backward kernel, one walker's positions at a time
+        std::vector<double> pos(W * e->D);
+        int prc = vmc_get_positions(e, pos.data());
+        if (prc) return prc;
+        std::vector<float> xf(pos.begin(), pos.end());
+        float *dx = nullptr;
+        double *dout = nullptr;
+        CUDA_TRY(cudaMalloc(&dx, xf.size() * sizeof(float)));
+        CUDA_TRY(cudaMalloc(&dout, W * 2 * MLP_PARAMS * sizeof(double)));
+        cudaError_t ge = cudaMemcpyAsync(dx, xf.data(), xf.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream);
+        if (ge == cudaSuccess) ge = cudaMemsetAsync(dout, 0, W * 2 * MLP_PARAMS * sizeof(double), e->stream);
+        for (size_t w = 0; w < W && ge == cudaSuccess; ++w)
+            ge = mlp_launch_grad(e->gen, e->N, e->dim, dx + w * e->D, nullptr, 1, dout + w * 2 * MLP_PARAMS, e->stream);
+        std::vector<double> g(W * 2 * MLP_PARAMS);
+        if (ge == cudaSuccess)
+            ge = cudaMemcpyAsync(g.data(), dout, g.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+        if (ge == cudaSuccess) ge = cudaStreamSynchronize(e->stream);
+        cudaFree(dx);
+        cudaFree(dout);
+        if (ge != cudaSuccess) return fail(VMC_E_CUDA, cudaGetErrorString(ge));
+        for (size_t w = 0; w < W; ++w)
+            std::copy(g.begin() + w * 2 * MLP_PARAMS, g.begin() + w * 2 * MLP_PARAMS + MLP_PARAMS,
+                      pgrad + (w * e->E + e->mlp_e) * e->Pmax);
+    }
     return VMC_OK;
 }
 

@@ -165,6 +165,117 @@ __device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
     return same_spin(i, j, P.N) ? P.beta_same : P.beta_anti;
 }
 
+// ------------------------------------------------------------ MLP Jastrow
+// J = sum_{i<j} u(r_ij, s_ij) + sum_i chi(r_i) with
+//   u(r, s) = a_s r / (1 + r) + w3 . tanh(W2 tanh(W1 [r, s] + b1) + b2) + b3   (2 -> 64 -> 64 -> 1)
+//   chi(r)  = v3 . tanh(V2 tanh(V1 r + c1) + c2) + c3                        (1 -> 32 -> 32 -> 1)
+// evaluated in FP32 with the weights rounded to bfloat16; a_s is the Pade cusp
+// coefficient (s = 1 same spin).  Radial derivatives by forward-mode
+// differentiation: h' = (1 - h^2) z', h'' = (1 - h^2)(z'' - 2 h z'^2).
+// Shared-memory weight block of a CTA: the packed row, W2 transposed ([k][m]) and
+// V2 transposed, so that lanes over output units read consecutive words.
+constexpr int MLP_SMEM_FLOATS = MLP_PARAMS + 2 + MLP_H * MLP_H + MLP_G * MLP_G;  // 10692
+constexpr int MW_W2T = MLP_PARAMS + 2, MW_V2T = MW_W2T + MLP_H * MLP_H;
+constexpr int MLP_SMEM_DOUBLES = (MLP_SMEM_FLOATS + 3) / 4 * 2;  // 16-byte multiple
+
+__device__ __forceinline__ float mlp_tanh(float x)
+{
+    x = fminf(fmaxf(x, -9.0f), 9.0f);  // tanh(9) = 1 in FP32
+    return 1.0f - __fdividef(2.0f, __expf(2.0f * x) + 1.0f);
+}
+
+// Cooperative copy of the weights into shared memory (all threads of the CTA).
+__device__ void mlp_stage(const float *__restrict__ src, float *w)
+{
+    for (int i = threadIdx.x; i < MLP_PARAMS; i += blockDim.x) w[i] = src[i];
+    for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
+        const int k = i / MLP_H, m = i - k * MLP_H;
+        w[MW_W2T + i] = src[MW_W2 + m * MLP_H + k];
+    }
+    for (int i = threadIdx.x; i < MLP_G * MLP_G; i += blockDim.x) {
+        const int k = i / MLP_G, m = i - k * MLP_G;
+        w[MW_V2T + i] = src[MW_V2 + m * MLP_G + k];
+    }
+}
+
+__device__ __forceinline__ float mlp_cusp(int dim, bool same)
+{
+    return same ? (dim == 2 ? 1.0f / 3 : 0.25f) : (dim == 2 ? 1.0f : 0.5f);
+}
+
+// u, du/dr, d2u/dr2 of the pair network for one pair (one lane).
+__device__ void mlp_pair(const float *w, float r, float s, float a, float &u, float &du, float &ddu)
+{
+    float uo = w[MW_B3], duo = 0.0f, dduo = 0.0f;
+    for (int half = 0; half < 2; ++half) {
+        float z[32], dz[32], ddz[32];
+#pragma unroll
+        for (int m = 0; m < 32; ++m) {
+            z[m] = w[MW_B2 + half * 32 + m];
+            dz[m] = 0.0f;
+            ddz[m] = 0.0f;
+        }
+        for (int k = 0; k < MLP_H; ++k) {
+            const float w1r = w[MW_W1 + 2 * k], w1s = w[MW_W1 + 2 * k + 1];
+            const float h = mlp_tanh(fmaf(w1r, r, fmaf(w1s, s, w[MW_B1 + k])));
+            const float d = (1.0f - h * h) * w1r, dd = -2.0f * h * d * w1r;
+            const float4 *col = reinterpret_cast<const float4 *>(w + MW_W2T + k * MLP_H + half * 32);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 v = col[q];
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    z[4 * q + e] = fmaf(vv[e], h, z[4 * q + e]);
+                    dz[4 * q + e] = fmaf(vv[e], d, dz[4 * q + e]);
+                    ddz[4 * q + e] = fmaf(vv[e], dd, ddz[4 * q + e]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 32; ++m) {
+            const float h2 = mlp_tanh(z[m]), g2 = 1.0f - h2 * h2, w3 = w[MW_W3 + half * 32 + m];
+            uo = fmaf(w3, h2, uo);
+            duo = fmaf(w3, g2 * dz[m], duo);
+            dduo = fmaf(w3, g2 * (ddz[m] - 2.0f * h2 * dz[m] * dz[m]), dduo);
+        }
+    }
+    const float q = 1.0f / (1.0f + r);
+    u = uo + a * r * q;
+    du = duo + a * q * q;
+    ddu = dduo - 2.0f * a * q * q * q;
+}
+
+// chi, dchi/dr, d2chi/dr2 of the one-body network at r: warp-cooperative, lane m
+// is hidden unit m of the second layer; every lane returns the totals.
+__device__ void mlp_body(const float *w, float r, int lane, float &c, float &dc, float &ddc)
+{
+    float z = w[MW_C2 + lane], dz = 0.0f, ddz = 0.0f;
+    for (int k = 0; k < MLP_G; ++k) {
+        const float v1 = w[MW_V1 + k];
+        const float h = mlp_tanh(fmaf(v1, r, w[MW_C1 + k]));
+        const float d = (1.0f - h * h) * v1, dd = -2.0f * h * d * v1, vv = w[MW_V2T + k * MLP_G + lane];
+        z = fmaf(vv, h, z);
+        dz = fmaf(vv, d, dz);
+        ddz = fmaf(vv, dd, ddz);
+    }
+    const float h2 = mlp_tanh(z), g2 = 1.0f - h2 * h2, v3 = w[MW_V3 + lane];
+    c = warp_sum(v3 * h2) + w[MW_C3];
+    dc = warp_sum(v3 * g2 * dz);
+    ddc = warp_sum(v3 * g2 * (ddz - 2.0f * h2 * dz * dz));
+}
+
+// pair index q < N(N-1)/2 -> (i, j), i < j, row-major over i
+__device__ __forceinline__ void pair_of(int q, int N, int &i, int &j)
+{
+    i = 0;
+    while (q >= N - 1 - i) {
+        q -= N - 1 - i;
+        ++i;
+    }
+    j = i + 1 + q;
+}
+
 // Evaluate the walker at its positions (eval_impl): per-element gradient,
 // Laplacian and parameter gradient, the local-energy parts.  Writes the total
 // gradient, energies and parameter gradients into the record and, when given,
@@ -172,7 +283,8 @@ __device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
 // energies 3).
 __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, double *rec,
                              const unsigned long long *mask, double *scr, int lane, double *o_grad,
-                             double *o_lap, double *o_pg, double *o_en)
+                             double *o_lap, double *o_pg, double *o_en, const float *mw = nullptr,
+                             bool full = true)
 {
     const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
     const double *x = rec;
@@ -317,6 +429,52 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             }
             break;
         }
+        case 7: {  // MLP Jastrow: caches of (u, u', u'') per pair and (chi, chi', chi'') per particle
+            double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
+            if (full) {  // from scratch (initialisation, parameter update, evaluation)
+                const int npair = N * (N - 1) / 2;
+                for (int q = lane; q < npair; q += 32) {
+                    int i, j;
+                    pair_of(q, N, i, j);
+                    const bool same = same_spin(i, j, N);
+                    float u, du, ddu;
+                    mlp_pair(mw, (float)gen_dist(x, dim, i, j), same ? 1.0f : 0.0f, mlp_cusp(dim, same), u, du, ddu);
+                    double *c3 = uc + (size_t)(i * N + j) * 3;
+                    c3[0] = u;
+                    c3[1] = du;
+                    c3[2] = ddu;
+                }
+                for (int i = 0; i < N; ++i) {
+                    float c, dc, ddc;
+                    mlp_body(mw, (float)gen_radius(x, dim, i), lane, c, dc, ddc);
+                    if (lane == 0) {
+                        oc[i * 3] = c;
+                        oc[i * 3 + 1] = dc;
+                        oc[i * 3 + 2] = ddc;
+                    }
+                }
+                __syncwarp();
+            }
+            for (int i = lane; i < N; i += 32) {
+                double gi[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < N; ++j) {
+                    if (j == i) continue;
+                    const int lo = min(i, j), hi = max(i, j);
+                    const double *c3 = uc + (size_t)(lo * N + hi) * 3;
+                    const double r = gen_dist(x, dim, i, j);
+                    for (int c = 0; c < dim; ++c) gi[c] += c3[1] * (x[i * dim + c] - x[j * dim + c]) / r;
+                    if (j > i) lap_l += 2.0 * (c3[2] + (dim - 1) * c3[1] / r);
+                }
+                const double ri = gen_radius(x, dim, i);
+                for (int c = 0; c < dim; ++c) gi[c] += oc[i * 3 + 1] * x[i * dim + c] / ri;
+                lap_l += oc[i * 3 + 2] + (dim - 1) * oc[i * 3 + 1] / ri;
+                for (int c = 0; c < dim; ++c) {
+                    G[i * dim + c] += gi[c];
+                    if (oge) oge[i * dim + c] = gi[c];
+                }
+            }
+            break;  // parameter gradients: mlp_grad_kernel, from snapshots
+        }
         case 6: {  // HydrogenLike (hydrogenlike.cpp:268-286)
             const double az = th[0] * P.Z;
             double rs = 0.0;
@@ -380,7 +538,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
 // (the Sherman-Morrison update reuses them).  Returns the product in element order.
 __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const double *rec,
                              const unsigned long long *mask, double *scr, int lane, int k, double xn,
-                             double *ratios, double *grad_y, double &R_out)
+                             double *ratios, double *grad_y, double &R_out, const float *mw = nullptr)
 {
     const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
     const double *x = rec;
@@ -495,6 +653,43 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
             __syncwarp();
             break;
         }
+        case 7: {  // MLP Jastrow: exp(2 (J(y) - J(x))); the new pair and one-body values
+                   // go to the scratch for an accepted move
+            const double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
+            double acc = 0.0, gyl = 0.0;
+            for (int j = lane; j < N; j += 32) {
+                if (j == p) continue;
+                double rn2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[j * dim + c];
+                    rn2 += t * t;
+                }
+                const double rn = sqrt(rn2);
+                const bool same = same_spin(p, j, N);
+                float u, du, ddu;
+                mlp_pair(mw, (float)rn, same ? 1.0f : 0.0f, mlp_cusp(dim, same), u, du, ddu);
+                scr[SCR_XS + j] = u;
+                scr[SCR_XS + 32 + j] = du;
+                scr[SCR_PN + j] = ddu;
+                acc += (double)u - uc[(size_t)(min(p, j) * N + max(p, j)) * 3];
+                gyl += du * (yp[adim] - x[j * dim + adim]) / rn;
+            }
+            double rp2 = 0.0;
+            for (int c = 0; c < dim; ++c) rp2 += yp[c] * yp[c];
+            const double rp = sqrt(rp2);
+            float cn, dcn, ddcn;
+            mlp_body(mw, (float)rp, lane, cn, dcn, ddcn);
+            if (lane == 0) {
+                scr[SCR_PN + 32] = cn;
+                scr[SCR_PN + 33] = dcn;
+                scr[SCR_PN + 34] = ddcn;
+            }
+            const double dj = warp_sum(acc) + ((double)cn - oc[p * 3]);
+            r = exp(2.0 * dj);
+            if (grad_y) gy += warp_sum(gyl) + dcn * yp[adim] / rp;
+            __syncwarp();
+            break;
+        }
         case 6: {  // hydrogenlike.cpp:231-242
             double rn2 = 0.0;
             for (int c = 0; c < dim; ++c) rn2 += yp[c] * yp[c];
@@ -577,6 +772,13 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
     __shared__ double scratch[GEN_WPB][GEN_SCR];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int w = blockIdx.x * GEN_WPB + wib;
+    // dynamic shared memory: MLP weights (when present), then the inversion matrices
+    float *mw = g.mlp ? reinterpret_cast<float *>(gsm) : nullptr;
+    double *inv_area = gsm + (g.mlp ? MLP_SMEM_DOUBLES : 0);
+    if (mw) {
+        mlp_stage(g.mlp, mw);
+        __syncthreads();
+    }
     if (w >= P.W) return;
     const int dim = g.D / P.N;
     double *rec = reinterpret_cast<double *>(P.state) + (size_t)w * g.rec;
@@ -584,13 +786,13 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
     unsigned status = 0;
     if (mode == GEN_INIT) {
         for (int j = lane; j < P.N; j += 32) mask[j] = ~0ull;
-        if (P.flags & F_SLATER) status = gen_invert(P, g, dim, rec, gsm + (size_t)wib * g.n * 2 * g.n, lane);
+        if (P.flags & F_SLATER) status = gen_invert(P, g, dim, rec, inv_area + (size_t)wib * g.n * 2 * g.n, lane);
         __syncwarp();
     }
     const size_t E = P.n_elem;
     gen_evaluate(P, g, dim, rec, mask, scratch[wib], lane, o_grad ? o_grad + (size_t)w * E * g.D : nullptr,
                  o_lap ? o_lap + (size_t)w * E : nullptr, o_pg ? o_pg + (size_t)w * g.EP : nullptr,
-                 o_en ? o_en + (size_t)w * 3 : nullptr);
+                 o_en ? o_en + (size_t)w * 3 : nullptr, mw, true);
     if (mode == GEN_INIT && P.sampling == SAMPLER_IS)  // ImportanceSampling::initialize: F = 2 grad
         for (int k = lane; k < g.D; k += 32) rec[g.off_fc + k] = 2.0 * rec[g.off_g + k];
     status = __reduce_or_sync(FULL, status);
@@ -599,10 +801,16 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
 
 __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs a, const GenParams g)
 {
+    extern __shared__ __align__(16) double gsm[];
     __shared__ double scratch[GEN_WPB][GEN_SCR];
     const Params &P = a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int w = blockIdx.x * GEN_WPB + wib;
+    float *mw = g.mlp ? reinterpret_cast<float *>(gsm) : nullptr;
+    if (mw) {
+        mlp_stage(g.mlp, mw);
+        __syncthreads();
+    }
     if (w >= P.W) return;
     const int N = P.N, D = g.D, dim = D / N;
     double *rec = reinterpret_cast<double *>(P.state) + (size_t)w * g.rec;
@@ -658,7 +866,7 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
         double gy = 0.0, R = 1.0;
         double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
         const double prob = gen_ratios(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
-                                       corrected ? &gy : nullptr, R);
+                                       corrected ? &gy : nullptr, R, mw);
         bool accept = true;
         if (!a.probe_k) {
             double wgt = prob;
@@ -697,13 +905,25 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
                 x[k] = xn;
                 if (is) fc[k] = fn;
             }
+            if (P.flags & F_MLP) {  // the moved particle's pair and one-body values from the proposal
+                double *uc = rec + g.off_uc;
+                for (int j = lane; j < N; j += 32)
+                    if (j != p) {
+                        double *c3 = uc + (size_t)(min(p, j) * N + max(p, j)) * 3;
+                        c3[0] = scr[SCR_XS + j];
+                        c3[1] = scr[SCR_XS + 32 + j];
+                        c3[2] = scr[SCR_PN + j];
+                    }
+                if (lane == 0)
+                    for (int t = 0; t < 3; ++t) rec[g.off_oc + p * 3 + t] = scr[SCR_PN + 32 + t];
+            }
             if (P.flags & Q_PADE_STALE) {  // the moved particle's pairs take the current gamma
                 for (int j = lane; j < N; j += 32)
                     if (j != p) mask[j] |= 1ull << p;
                 if (lane == 0) mask[p] = ~0ull;
             }
             __syncwarp();
-            gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr);
+            gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false);
         }
         if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
         const double *en = rec + g.off_en;
@@ -717,7 +937,16 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
             const double el = en[0] + en[1] + en[2];
             if (el != el) status |= ST_NAN_ENERGY;
             const bool win = it_step > a.win_lo && it_step < a.win_hi;
-            const int top = win ? P.nacc : 9;
+            if (win && a.snap_x && (it_step - a.win_lo) % a.snap_interval == 0) {
+                // MLP Jastrow parameter gradient: positions and E_L for mlp_grad_kernel
+                const int slot = (it_step - a.win_lo) / a.snap_interval - a.snap_first;
+                if (slot >= 0 && slot < a.snap_stride) {
+                    const size_t base = (size_t)w * a.snap_stride + slot;
+                    for (int t = lane; t < D; t += 32) a.snap_x[base * D + t] = (float)x[t];
+                    if (lane == 0) a.snap_e[base] = el;
+                }
+            }
+            const int top = win ? 9 + 2 * g.n_act : 9;  // == P.nacc inside the window
             const double *pg = rec + g.off_pg;
             for (int t = lane; t < top; t += 32) {
                 double q;
@@ -727,8 +956,8 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
                 } else if (t == 8) {
                     q = accept ? 1.0 : 0.0;
                 } else {
-                    const int j = t - 9;
-                    q = j < g.EP ? pg[j] : el * pg[j - g.EP];
+                    const int c = t - 9;
+                    q = c < g.n_act ? pg[g.act[c]] : el * pg[g.act[c - g.n_act]];
                 }
                 double s1 = acc[2 * t], c1 = acc[2 * t + 1];
                 kadd(s1, c1, q);
@@ -741,6 +970,224 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
     if (lane == 0) {
         P.counter[w] = ctr;
         if (status) P.status[w] |= status;
+    }
+}
+
+// dJ/dtheta of the MLP Jastrow for a set of position snapshots (backpropagation,
+// summed over pairs and particles), accumulated plain and weighted by each
+// snapshot's local energy.  One CTA of 256 threads per snapshot at a time; the
+// pair rows of a snapshot go through in tiles of 64:
+//   A: r, s and h1 = tanh(W1 [r, s] + b1) per row (warps over rows, lanes over units)
+//   B: z2 = W2 h1 + b2, h2 = tanh z2, delta2 = w3 (1 - h2^2)
+//   C: dJ/dW2 += delta2 (x) h1 over the rows (thread t: unit m = t / 4, 16 inputs)
+//   D: delta1 = (W2^T delta2)(1 - h1^2); dJ/dW1, dJ/db1
+// The one-body network (N rows) goes through one warp per particle with shared-
+// memory accumulation.  FP64 accumulators per thread, atomically added at the end.
+constexpr int MG_TILE = 64;
+constexpr int MG_BODY = MLP_G * MLP_G + 4 * MLP_G;  // one-body sums of a snapshot: V2, V1, c1, c2, v3
+constexpr int MG_SMEM_FLOATS = MLP_SMEM_FLOATS + 2 * MG_TILE * MLP_H + 2 * MG_TILE + 96 + MG_BODY;
+
+__global__ void __launch_bounds__(256) mlp_grad_kernel(const GenParams g, int N, int dim,
+                                                       const float *__restrict__ snap_x,
+                                                       const double *__restrict__ snap_e,
+                                                       long long n_snap, double *out)
+{
+    extern __shared__ __align__(16) float msm[];
+    float *w = msm;
+    float *h1s = w + MLP_SMEM_FLOATS;           // [MG_TILE][64]
+    float *d2s = h1s + MG_TILE * MLP_H;         // [MG_TILE][64]
+    float *rr = d2s + MG_TILE * MLP_H;          // [MG_TILE]
+    float *ss = rr + MG_TILE;                   // [MG_TILE]
+    float *xs = ss + MG_TILE;                   // positions, D <= 96
+    float *bv2 = xs + 96;                       // one-body sums: V2 [32][32], V1, c1, c2, v3 [32] each
+    float *bu = bv2 + MLP_G * MLP_G;
+    mlp_stage(g.mlp, w);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int D = N * dim, npair = N * (N - 1) / 2;
+    const int cm = t >> 2, ck = (t & 3) * 16;  // phase C ownership
+    double aW2[16], eW2[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) aW2[i] = eW2[i] = 0.0;
+    // lane-owned units k in {lane, lane + 32} (phases A, B, D), accumulated per warp
+    double aU[2][5], eU[2][5];  // [unit][b1, W1r, W1s, b2, w3]
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) aU[u][q] = eU[u][q] = 0.0;
+    double aV[4], eV[4], aB[4], eB[4];  // one-body: V2 entries 4t..4t+3; t < 32: V1/c1/c2/v3 of unit t
+#pragma unroll
+    for (int q = 0; q < 4; ++q) aV[q] = eV[q] = aB[q] = eB[q] = 0.0;
+    double n_rows = 0.0, e_rows = 0.0, n_body = 0.0, e_body = 0.0;
+    for (int i = t; i < MG_BODY; i += blockDim.x) bv2[i] = 0.0f;
+    __syncthreads();
+
+    for (long long sn = blockIdx.x; sn < n_snap; sn += gridDim.x) {
+        const double E = snap_e ? snap_e[sn] : 0.0;
+        for (int i = t; i < D; i += blockDim.x) xs[i] = snap_x[sn * D + i];
+        __syncthreads();
+        float sW2[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) sW2[i] = 0.0f;
+        float sU[2][5];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) sU[u][q] = 0.0f;
+        for (int base = 0; base < npair; base += MG_TILE) {
+            const int nrow = min(MG_TILE, npair - base);
+            // A
+            for (int row = warp; row < nrow; row += 8) {
+                int i, j;
+                pair_of(base + row, N, i, j);
+                float r2 = 0.0f;
+                for (int c = 0; c < dim; ++c) {
+                    const float d = xs[i * dim + c] - xs[j * dim + c];
+                    r2 += d * d;
+                }
+                const float r = sqrtf(r2), sv = same_spin(i, j, N) ? 1.0f : 0.0f;
+                if (lane == 0) {
+                    rr[row] = r;
+                    ss[row] = sv;
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int k = lane + 32 * u;
+                    h1s[row * MLP_H + k] = mlp_tanh(fmaf(w[MW_W1 + 2 * k], r, fmaf(w[MW_W1 + 2 * k + 1], sv, w[MW_B1 + k])));
+                }
+            }
+            __syncthreads();
+            // B
+            for (int row = warp; row < nrow; row += 8) {
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int m = lane + 32 * u;
+                    float z = w[MW_B2 + m];
+                    for (int k = 0; k < MLP_H; ++k) z = fmaf(w[MW_W2T + k * MLP_H + m], h1s[row * MLP_H + k], z);
+                    const float h2 = mlp_tanh(z), d2 = w[MW_W3 + m] * (1.0f - h2 * h2);
+                    d2s[row * MLP_H + m] = d2;
+                    sU[u][3] += d2;
+                    sU[u][4] += h2;
+                }
+            }
+            __syncthreads();
+            // C
+            for (int row = 0; row < nrow; ++row) {
+                const float dm = d2s[row * MLP_H + cm];
+                const float4 *hv = reinterpret_cast<const float4 *>(h1s + row * MLP_H + ck);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 v = hv[q];
+                    sW2[4 * q] = fmaf(dm, v.x, sW2[4 * q]);
+                    sW2[4 * q + 1] = fmaf(dm, v.y, sW2[4 * q + 1]);
+                    sW2[4 * q + 2] = fmaf(dm, v.z, sW2[4 * q + 2]);
+                    sW2[4 * q + 3] = fmaf(dm, v.w, sW2[4 * q + 3]);
+                }
+            }
+            // D
+            for (int row = warp; row < nrow; row += 8) {
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int k = lane + 32 * u;
+                    float acc = 0.0f;
+                    for (int m = 0; m < MLP_H; ++m) acc = fmaf(d2s[row * MLP_H + m], w[MW_W2 + m * MLP_H + k], acc);
+                    const float hk = h1s[row * MLP_H + k], d1 = acc * (1.0f - hk * hk);
+                    sU[u][0] += d1;
+                    sU[u][1] += d1 * rr[row];
+                    sU[u][2] += d1 * ss[row];
+                }
+            }
+            __syncthreads();
+        }
+        // one-body network: warp per particle, lane = hidden unit
+        for (int i = warp; i < N; i += 8) {
+            float r2 = 0.0f;
+            for (int c = 0; c < dim; ++c) r2 += xs[i * dim + c] * xs[i * dim + c];
+            const float r = sqrtf(r2);
+            const float h = mlp_tanh(fmaf(w[MW_V1 + lane], r, w[MW_C1 + lane]));
+            float z = w[MW_C2 + lane];
+            for (int k = 0; k < MLP_G; ++k) z = fmaf(w[MW_V2T + k * MLP_G + lane], __shfl_sync(FULL, h, k), z);
+            const float h2 = mlp_tanh(z), e2 = w[MW_V3 + lane] * (1.0f - h2 * h2);
+            // dJ/dV2[m][k] = e2_m h_k (lane m), dJ/dc2 = e2, dJ/dv3 = h2
+            for (int k = 0; k < MLP_G; ++k) atomicAdd(&bv2[lane * MLP_G + k], e2 * __shfl_sync(FULL, h, k));
+            float acc = 0.0f;  // backpropagated to the first layer: lane k
+            for (int m = 0; m < MLP_G; ++m) acc = fmaf(__shfl_sync(FULL, e2, m), w[MW_V2 + m * MLP_G + lane], acc);
+            const float e1 = acc * (1.0f - h * h);
+            atomicAdd(&bu[lane], e1 * r);               // V1
+            atomicAdd(&bu[MLP_G + lane], e1);           // c1
+            atomicAdd(&bu[2 * MLP_G + lane], e2);       // c2
+            atomicAdd(&bu[3 * MLP_G + lane], h2);       // v3
+        }
+        __syncthreads();
+        // fold the snapshot into the FP64 accumulators
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            aW2[i] += sW2[i];
+            eW2[i] += E * sW2[i];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                aU[u][q] += sU[u][q];
+                eU[u][q] += E * sU[u][q];
+            }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float v = bv2[4 * t + q];
+            aV[q] += v;
+            eV[q] += E * v;
+        }
+        if (t < MLP_G) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float b = bu[q * MLP_G + t];
+                aB[q] += b;
+                eB[q] += E * b;
+            }
+        }
+        n_rows += npair;
+        e_rows += E * npair;
+        n_body += N;
+        e_body += E * N;
+        __syncthreads();
+        for (int i = t; i < MG_BODY; i += blockDim.x) bv2[i] = 0.0f;
+        __syncthreads();
+    }
+    const int P = MLP_PARAMS;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        atomicAdd(&out[MW_W2 + cm * MLP_H + ck + i], aW2[i]);
+        atomicAdd(&out[P + MW_W2 + cm * MLP_H + ck + i], eW2[i]);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int k = lane + 32 * u;
+        const int idx[5] = {MW_B1 + k, MW_W1 + 2 * k, MW_W1 + 2 * k + 1, MW_B2 + k, MW_W3 + k};
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            atomicAdd(&out[idx[q]], aU[u][q]);
+            atomicAdd(&out[P + idx[q]], eU[u][q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int e = 4 * t + q;  // V2 entry (m, k) = (e / 32, e % 32)
+        atomicAdd(&out[MW_V2 + e], aV[q]);
+        atomicAdd(&out[P + MW_V2 + e], eV[q]);
+    }
+    if (t < MLP_G) {
+        const int idx[4] = {MW_V1 + t, MW_C1 + t, MW_C2 + t, MW_V3 + t};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            atomicAdd(&out[idx[q]], aB[q]);
+            atomicAdd(&out[P + idx[q]], eB[q]);
+        }
+    }
+    if (t == 0) {
+        atomicAdd(&out[MW_B3], n_rows);
+        atomicAdd(&out[P + MW_B3], e_rows);
+        atomicAdd(&out[MW_C3], n_body);
+        atomicAdd(&out[P + MW_C3], e_body);
     }
 }
 
@@ -814,7 +1261,11 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     g.off_en = 3 * D;
     g.off_pg = 3 * D + 4;
     g.off_inv = round_up(g.off_pg + g.EP, 2);
-    g.rec = round_up(g.off_inv + 2 * g.n * g.n, 2);
+    const bool mlp = std::count(c.elements.begin(), c.elements.end(), (int)E_MLP) > 0;
+    if (mlp && (N > 32 || dim * N > 96)) return "MLP Jastrow: at most 32 particles on this engine";
+    g.off_uc = g.off_inv + 2 * g.n * g.n;                 // MLP caches: N x N x 3, N x 3
+    g.off_oc = g.off_uc + (mlp ? N * N * 3 : 0);
+    g.rec = round_up(g.off_oc + (mlp ? N * 3 : 0), 2);
     return "";
 }
 
@@ -823,7 +1274,8 @@ int gen_smem_per_warp(const GenParams &g) { return g.n * 2 * g.n * 8; }
 cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, double *o_grad, double *o_lap,
                              double *o_pg, double *o_en, cudaStream_t st)
 {
-    const size_t smem = mode == GEN_INIT ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0;
+    const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) +
+                        (mode == GEN_INIT ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0);
     cudaError_t e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     gen_state_kernel<<<(P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(P, g, mode, o_grad, o_lap, o_pg,
@@ -833,7 +1285,29 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
 
 cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st)
 {
-    gen_sweep_kernel<<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, 0, st>>>(a, g);
+    const size_t smem = g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0;
+    cudaError_t e = cudaFuncSetAttribute(gen_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    gen_sweep_kernel<<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(a, g);
+    return cudaGetLastError();
+}
+
+}  // namespace vmc
+
+namespace vmc {
+
+cudaError_t mlp_launch_grad(const GenParams &g, int N, int dim, const float *snap_x, const double *snap_e,
+                            long long n_snap, double *out, cudaStream_t st)
+{
+    if (n_snap <= 0) return cudaSuccess;
+    const size_t smem = (size_t)MG_SMEM_FLOATS * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long grid = std::min<long long>(n_snap, (long long)sms);
+    mlp_grad_kernel<<<(unsigned)grid, 256, smem, st>>>(g, N, dim, snap_x, snap_e, n_snap, out);
     return cudaGetLastError();
 }
 

@@ -20,8 +20,21 @@ struct GenParams {
     int horb3;                  // n = 3 hydrogen orbitals with the reference's second derivatives
     double sigma;               // RBM width
     const double *theta;        // E x p_max parameters on the device
+    const float *mlp;           // MLP Jastrow weights rounded to bfloat16 (MLP_PARAMS), or null
+    int off_uc, off_oc;         // MLP caches: (u, u', u'') per pair i < j, (chi, chi', chi'') per particle
+    // parameters accumulated per walker (all but padding and the MLP row, whose
+    // gradient comes from snapshots): accumulator 9 + c holds parameter act[c]
+    const int *act;
+    int n_act;
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
 };
+
+// MLP Jastrow weight offsets (floats) in the packed parameter row
+enum : int {
+    MW_W1 = 0, MW_B1 = 128, MW_W2 = 192, MW_B2 = 4288, MW_W3 = 4352, MW_B3 = 4416,
+    MW_V1 = 4417, MW_C1 = 4449, MW_V2 = 4481, MW_C2 = 5505, MW_V3 = 5537, MW_C3 = 5569,
+};
+static_assert(MW_C3 + 1 == MLP_PARAMS, "MLP layout");
 
 // "" when the general path takes the configuration (fills g except theta), else why not.
 std::string gen_configure(const Config &c, int n_elements, int p_max, GenParams &g);
@@ -31,5 +44,10 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
                              double *o_pg, double *o_en, cudaStream_t st);
 cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st);
 cudaError_t upload_hermite_gen(const HermiteCoef &h);
+// dJ/dtheta of the MLP Jastrow summed over snapshots (positions n_snap x D floats,
+// local energies n_snap, or null = weights 0): out[0..P) += sum dJ/dtheta,
+// out[P..2P) += sum E dJ/dtheta (FP64 accumulators, zeroed by the caller).
+cudaError_t mlp_launch_grad(const GenParams &g, int N, int dim, const float *snap_x, const double *snap_e,
+                            long long n_snap, double *out, cudaStream_t st);
 
 }  // namespace vmc

@@ -113,6 +113,11 @@ struct SweepArgs {
     const double *probe_x;   // ... to probe_x[w], accepted; ratios to probe_ratio
     double *probe_ratio;     // W x n_elem
     int wpb, smem_per_warp;
+    // MLP Jastrow parameter-gradient snapshots (general path): positions and local
+    // energy every snap_interval steps inside the gradient window, snap_stride per walker
+    float *snap_x;
+    double *snap_e;
+    int snap_stride, snap_interval, snap_first;  // slot = (step - win_lo) / interval - first
 };
 
 // ------------------------------------------------------------------ helpers
