@@ -98,3 +98,36 @@ def test_sampled_gradient_sums():
         lo, hi = max(1, info.burn_in), min(bs - 1, info.steps_per_walker + info.burn_in - 1)
         n_win = hi - lo + 1
         assert abs(g[2, 4416] - N * (N - 1) / 2 * W * n_win) < 1e-9 * g[2, 4416]
+
+
+@pytest.mark.parametrize("compat,sampling", [(0, "importanceSampling"), (0, "bruteForce")])
+def test_zero_network_equals_pade(compat, sampling):
+    """With zero output layers the MLP factor is the cusp term a_s r / (1 + r), the
+    Pade-Jastrow at gamma = 1: on the same replayed stream both engines make the same
+    accept/reject decisions and record the same energies (the MLP path in FP32).
+    Corrected mode only: under compat the Pade ratio skips partners j < p, which the
+    MLP factor does not copy."""
+    from vmachine_b200 import Engine
+    N, W, steps = 6, 4, 400
+    rng = np.random.default_rng(9)
+    pos = rng.normal(0.0, 1.0, (W, 2 * N))
+    stream = np.stack([rng.random((W, steps)),
+                       rng.normal(size=(W, steps)) if sampling == "importanceSampling" else rng.random((W, steps)),
+                       rng.random((W, steps))], -1)
+    th = np.zeros((3, mj.n_params()))
+    th[1, 0] = 0.95
+    th[2] = mj.xavier(3)  # hidden layers random, output layers zero
+    pade = "\n".join(["numParticles: 6", "numDimensions: 2", "hamiltonian: harmonicOscillator",
+                      "omega: 1.0", "interactionStyle: coulomb", "waveFunctionElement: slaterDeterminant",
+                      "waveFunctionElement: gaussian", "waveFunctionElement: padeJastrow", "basis: hermite",
+                      f"sampling: {sampling}", "stepLength: 0.05", "numSteps: 1000"]) + "\n"
+    res = []
+    for text, theta in ((pade, np.array([[0.0], [0.95], [1.0]])),
+                        (config(N, sampling=sampling), th)):
+        with Engine(text, walkers=W, precision=0, compat=compat) as eng:
+            eng.set_parameters(theta)
+            eng.init_walkers(pos)
+            res.append(eng.replay(stream))
+    (a0, e0), (a1, e1) = res
+    assert np.array_equal(a0, a1)
+    assert rel(e1, e0) < 2e-5

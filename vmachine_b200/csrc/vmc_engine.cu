@@ -367,7 +367,12 @@ int initial_weights(vmc_engine *e)
     std::string method = c.initial_weights;
     double factor = c.weights_factor;
     bool xavier = false;
-    if (method == "automatize") {
+    if (method == "automatize" && e->mlp_e >= 0) {
+        // Slater / Gaussian next to the MLP Jastrow: the "VMC" rule (constant 1); the
+        // MLP row is set below
+        method = "constant";
+        factor = 1.0;
+    } else if (method == "automatize") {
         const std::string &t = c.trial_label;
         if (t == "VMC" || t == "BVMC") { method = "constant"; factor = 1.0; }
         else if (t == "RBM" || t == "RBMSJ" || t == "RBMPJ") { xavier = true; }
@@ -640,8 +645,11 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         return rc;
     }
     const size_t P = e->theta.size();
-    e->opt_m.assign(P, 1.0);  // adam.cpp:35-36 and gradientdescent.cpp/sgd.cpp: ones
-    e->opt_v.assign(P, 1.0);
+    // adam.cpp:35-36 and gradientdescent.cpp/sgd.cpp start their moments at ones;
+    // compat: corrected starts ADAM from zero
+    const double m0 = (e->compat || c.optimization != "adam") ? 1.0 : 0.0;
+    e->opt_m.assign(P, m0);
+    e->opt_v.assign(P, m0);
     e->gamma_prev = make_params(e).gamma;
     *out = e;
     return VMC_OK;
@@ -990,7 +998,9 @@ int vmc_apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum,
     e->opt_step += 1;
     const double eta = e->cfg.eta;
     if (e->cfg.optimization == "adam") {  // adam.cpp:22-37
-        const double b1 = 0.89, b2 = 0.999, eps = 1e-8;
+        // compat: reference beta1 = 0.89 with moments started at ones (adam.cpp:35-36,
+        // adam.h:72); corrected: the standard method (beta1 = 0.9, moments from zero)
+        const double b1 = e->compat ? 0.89 : 0.9, b2 = 0.999, eps = 1e-8;
         for (size_t i = 0; i < P; ++i) {
             e->opt_m[i] = b1 * e->opt_m[i] + (1 - b1) * grad[i];
             e->opt_v[i] = b2 * e->opt_v[i] + (1 - b2) * grad[i] * grad[i];
