@@ -51,7 +51,9 @@ def test_fixed_positions(N):
     rng = np.random.default_rng(100 + N)
     W = 3
     pos = rng.normal(0.0, 1.0, (W, 2 * N))
-    with Engine(config(N), walkers=W, precision=0) as eng:
+    # the FP32 network on the CUDA cores throughout (the probe move is a sweep step);
+    # the tensor-core sweep is held to this path in test_tensor_core_layer_tracks_fp32
+    with Engine(config(N, extra=["mlpTensorCores: false"]), walkers=W, precision=0) as eng:
         eng.set_parameters(theta)
         eng.init_walkers(pos)
         g, lap, pg, en = eng.eval()
@@ -131,3 +133,36 @@ def test_zero_network_equals_pade(compat, sampling):
     (a0, e0), (a1, e1) = res
     assert np.array_equal(a0, a1)
     assert rel(e1, e0) < 2e-5
+
+
+@pytest.mark.parametrize("N", [6, 20])
+def test_tensor_core_layer_tracks_fp32(N):
+    """The sweep's second layer on the tensor cores (bfloat16 operands, the values as a
+    high and a low part, FP32 accumulation) against the FP32 CUDA-core network on one
+    replayed stream: chains that agree for most of the run and energies within 1e-3
+    relative while they do."""
+    from vmachine_b200 import Engine
+    W, steps = 8, 300
+    omega = 1.0 if N == 6 else 0.5
+    rng = np.random.default_rng(N + 40)
+    pos = rng.normal(0.0, 1.0 / np.sqrt(omega), (W, 2 * N))
+    stream = np.stack([rng.random((W, steps)), rng.normal(size=(W, steps)), rng.random((W, steps))], -1)
+    theta = theta_for(N + 1)
+    theta[2] *= 0.5
+    res = {}
+    for tc in ("false", "true"):
+        with Engine(config(N, omega=omega, extra=[f"mlpTensorCores: {tc}"]), walkers=W, precision=0,
+                    compat=0) as eng:
+            eng.set_parameters(theta)
+            eng.init_walkers(pos)
+            res[tc] = eng.replay(stream)
+            assert not (eng.status() & 8).any()  # no tensor-core wait gave up
+    (a32, e32), (atc, etc) = res["false"], res["true"]
+    agree = 0
+    for w in range(W):
+        diff = np.nonzero(a32[w] != atc[w])[0]
+        upto = diff[0] if len(diff) else steps
+        agree += upto
+        el32, eltc = e32[w, :upto].sum(-1), etc[w, :upto].sum(-1)
+        assert np.max(np.abs(eltc - el32) / np.abs(el32)) < 1e-3
+    assert agree > 0.8 * W * steps

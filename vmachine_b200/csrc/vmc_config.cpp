@@ -292,6 +292,10 @@ std::string parse_config(const std::string &text, Config &c)
                 else return err("precision must be fp64 or mixed");
             } else if (key == "refreshInterval") {
                 c.refresh_interval = (v0 == "auto") ? -1 : std::stoi(v0);
+            } else if (key == "mlpTensorCores") {
+                if (v0 == "true") c.mlp_tc = true;
+                else if (v0 == "false") c.mlp_tc = false;
+                else return err("mlpTensorCores must be true or false");
             } else if (key == "compat") {
                 if (v0 == "reference") c.compat = 1;
                 else if (v0 == "corrected") c.compat = 0;

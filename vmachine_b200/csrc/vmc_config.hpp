@@ -57,6 +57,7 @@ struct Config {
     int precision = 0;           // 0 fp64, 1 mixed
     int refresh_interval = -1;   // -1 auto
     int compat = 1;              // 1 reference quirks, 0 corrected
+    bool mlp_tc = true;          // MLP Jastrow second layer on the tensor cores (mlpTensorCores)
     int walkers_per_block = 0;   // 0 auto
 };
 

@@ -48,6 +48,7 @@ enum : int {
     ST_NAN_ENERGY = 1,
     ST_BAD_RATIO = 2,
     ST_SINGULAR = 4,
+    ST_TC_TIMEOUT = 8,  // a tensor-core completion wait gave up (its results are not used)
 };
 
 // ------------------------------------------------------------------ RNG

@@ -22,6 +22,8 @@
 #include <cmath>
 #include <string>
 
+#include <cuda_bf16.h>
+
 #include "vmc_general.hpp"
 
 namespace vmc {
@@ -184,11 +186,13 @@ __device__ __forceinline__ float mlp_tanh(float x)
     return 1.0f - __fdividef(2.0f, __expf(2.0f * x) + 1.0f);
 }
 
-// Cooperative copy of the weights into shared memory (all threads of the CTA).
-__device__ void mlp_stage(const float *__restrict__ src, float *w)
+// Cooperative copy of the weights into shared memory (all threads of the CTA);
+// without w2t the W2-transposed region is left free (the tensor-core sweep uses it
+// as an operand tile).
+__device__ void mlp_stage(const float *__restrict__ src, float *w, bool w2t = true)
 {
     for (int i = threadIdx.x; i < MLP_PARAMS; i += blockDim.x) w[i] = src[i];
-    for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
+    for (int i = threadIdx.x; w2t && i < MLP_H * MLP_H; i += blockDim.x) {
         const int k = i / MLP_H, m = i - k * MLP_H;
         w[MW_W2T + i] = src[MW_W2 + m * MLP_H + k];
     }
@@ -291,7 +295,9 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
     double *G = rec + g.off_g, *pg = rec + g.off_pg;
     const double *inv = rec + g.off_inv;
     for (int k = lane; k < D; k += 32) G[k] = 0.0;
-    for (int j = lane; j < g.EP; j += 32) pg[j] = 0.0;
+    // only the accumulated parameters are ever written (padding and the MLP row stay
+    // zero from the record's initialisation): clear those
+    for (int c = lane; c < g.n_act; c += 32) pg[g.act[c]] = 0.0;
     __syncwarp();
     double lap_total = 0.0;
     for (int e = 0; e < E; ++e) {
@@ -455,19 +461,28 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
                 }
                 __syncwarp();
             }
+            // from the caches in FP32 (the network values are FP32 already)
             for (int i = lane; i < N; i += 32) {
-                double gi[3] = {0.0, 0.0, 0.0};
+                float gi[3] = {0.0f, 0.0f, 0.0f}, li = 0.0f, xi[3];
+                for (int c = 0; c < dim; ++c) xi[c] = (float)x[i * dim + c];
                 for (int j = 0; j < N; ++j) {
                     if (j == i) continue;
                     const int lo = min(i, j), hi = max(i, j);
                     const double *c3 = uc + (size_t)(lo * N + hi) * 3;
-                    const double r = gen_dist(x, dim, i, j);
-                    for (int c = 0; c < dim; ++c) gi[c] += c3[1] * (x[i * dim + c] - x[j * dim + c]) / r;
-                    if (j > i) lap_l += 2.0 * (c3[2] + (dim - 1) * c3[1] / r);
+                    float dv[3], r2 = 0.0f;
+                    for (int c = 0; c < dim; ++c) {
+                        dv[c] = xi[c] - (float)x[j * dim + c];
+                        r2 += dv[c] * dv[c];
+                    }
+                    const float ir = rsqrtf(r2), du = (float)c3[1];
+                    for (int c = 0; c < dim; ++c) gi[c] += du * dv[c] * ir;
+                    if (j > i) li += 2.0f * ((float)c3[2] + (dim - 1) * du * ir);
                 }
-                const double ri = gen_radius(x, dim, i);
-                for (int c = 0; c < dim; ++c) gi[c] += oc[i * 3 + 1] * x[i * dim + c] / ri;
-                lap_l += oc[i * 3 + 2] + (dim - 1) * oc[i * 3 + 1] / ri;
+                float r2i = 0.0f;
+                for (int c = 0; c < dim; ++c) r2i += xi[c] * xi[c];
+                const float iri = rsqrtf(r2i), dc = (float)oc[i * 3 + 1];
+                for (int c = 0; c < dim; ++c) gi[c] += dc * xi[c] * iri;
+                lap_l += (double)li + oc[i * 3 + 2] + (dim - 1) * dc * iri;
                 for (int c = 0; c < dim; ++c) {
                     G[i * dim + c] += gi[c];
                     if (oge) oge[i * dim + c] = gi[c];
@@ -510,7 +525,14 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
     }
     if (P.flags & F_COULOMB)
         for (int i = lane; i < N; i += 32)
-            for (int j = i + 1; j < N; ++j) vi += 1.0 / gen_dist(x, dim, i, j);
+            for (int j = i + 1; j < N; ++j) {
+                double r2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = x[i * dim + c] - x[j * dim + c];
+                    r2 += t * t;
+                }
+                vi += rsqrt(r2);
+            }
     g2 = warp_sum(g2);
     vx = warp_sum(vx);
     vi = warp_sum(vi);
@@ -538,7 +560,8 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
 // (the Sherman-Morrison update reuses them).  Returns the product in element order.
 __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const double *rec,
                              const unsigned long long *mask, double *scr, int lane, int k, double xn,
-                             double *ratios, double *grad_y, double &R_out, const float *mw = nullptr)
+                             double *ratios, double *grad_y, double &R_out, const float *mw = nullptr,
+                             const float *pre = nullptr)
 {
     const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
     const double *x = rec;
@@ -667,12 +690,18 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
                 const double rn = sqrt(rn2);
                 const bool same = same_spin(p, j, N);
                 float u, du, ddu;
-                mlp_pair(mw, (float)rn, same ? 1.0f : 0.0f, mlp_cusp(dim, same), u, du, ddu);
+                if (pre) {  // from the tensor-core pass of this step (lane j = partner j)
+                    u = pre[j];
+                    du = pre[32 + j];
+                    ddu = pre[64 + j];
+                } else {
+                    mlp_pair(mw, (float)rn, same ? 1.0f : 0.0f, mlp_cusp(dim, same), u, du, ddu);
+                }
                 scr[SCR_XS + j] = u;
                 scr[SCR_XS + 32 + j] = du;
                 scr[SCR_PN + j] = ddu;
                 acc += (double)u - uc[(size_t)(min(p, j) * N + max(p, j)) * 3];
-                gyl += du * (yp[adim] - x[j * dim + adim]) / rn;
+                gyl += du * (float)(yp[adim] - x[j * dim + adim]) * (float)(1.0 / rn);
             }
             double rp2 = 0.0;
             for (int c = 0; c < dim; ++c) rp2 += yp[c] * yp[c];
@@ -799,178 +828,418 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
     if (lane == 0 && status) P.status[w] |= status;
 }
 
+
+// ------------------------------------------------------------ MLP second layer on tcgen05
+// During a sweep the CTA's four walkers move in lockstep; the partners of the four
+// proposals fill one 128-row tile (warp w: rows 32 w .. 32 w + 31, lane = partner).
+// First layer and its radial derivatives (CUDA cores) go to three A tiles in
+// bfloat16 (the values as a high and a low bfloat16 part, about 16 significant
+// bits); z2 = W2 h1 and its two radial derivatives are M = 128, N = 64, K = 64
+// products on the 5th-generation tensor cores (kind::f16, BF16 in, FP32 accumulate
+// in tensor memory), issued by one thread; each lane then reads its row back
+// (tcgen05.ld) and finishes the third layer.
+// Shared-memory operands are K-major without swizzle: 8-row x 16-byte core
+// matrices, offset(row, k) = (row % 8) 16 + (row / 8) 1024 + (k / 8) 128 + (k % 8) 2,
+// so the two K chunks of a K = 16 step are 128 bytes apart (leading byte offset)
+// and 8-row groups 1024 bytes apart (stride byte offset).  Tensor memory holds D
+// for order o (value, d/dr, d2/dr2) in columns [64 o, 64 o + 64); lane = tile row.
+constexpr int TC_COLS = 256;  // TMEM columns per CTA (192 used); two CTAs per SM fit 512
+constexpr int TC_A_BYTES = 128 * MLP_H * 2, TC_B_BYTES = MLP_H * MLP_H * 2;
+constexpr int TC_SMEM = 3 * TC_A_BYTES + TC_B_BYTES + 1024;  // with alignment slack
+constexpr long TC_WAIT_LIMIT = 1L << 24;                     // bounded completion wait
+// kind::f16 instruction word: D F32 (bits 4-5), A and B BF16 (7-9, 10-12), both
+// K-major, N / 8 (17-22), M / 16 (24-28)
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+struct TcMlp {
+    unsigned char *a[4];  // A tiles: value (high bfloat16 part), d/dr, d2/dr2, value (low part)
+    uint32_t a_s[4], b_s; // their shared-window addresses, and B's
+    uint32_t bar;         // completion mbarrier
+    uint32_t tmem;        // TMEM base address (lane 0, first allocated column)
+    uint32_t phase;
+};
+
+__device__ __forceinline__ uint32_t tc_off(int row, int k)
+{
+    return (row & 7) * 16 + (row >> 3) * 1024 + (k >> 3) * 128 + (k & 7) * 2;
+}
+
+// shared-memory matrix descriptor: start address, LBO 128 B, SBO 1024 B, version 1,
+// base offset 0, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                   "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                   "=r"(v[14]), "=r"(v[15])
+                 : "r"(addr));
+}
+
+// Tiles after the weights, B = W2 ([out n][in k]; the weights are bfloat16 values
+// already), the mbarrier, and the TMEM allocation (warp 0).  The caller synchronises
+// the CTA and then calls tc_ready.
+__device__ void tc_setup(TcMlp &t, unsigned char *base, float *w, const float *__restrict__ src,
+                         unsigned long long *bar, uint32_t *slot, int wib)
+{
+    unsigned char *p = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(base) + 1023) & ~uintptr_t(1023));
+    for (int o = 0; o < 3; ++o) {
+        t.a[o] = p + o * TC_A_BYTES;
+        t.a_s[o] = (uint32_t)__cvta_generic_to_shared(t.a[o]);
+    }
+    t.a[3] = reinterpret_cast<unsigned char *>(w + MW_W2T);  // 16 KB, 16-byte aligned
+    t.a_s[3] = (uint32_t)__cvta_generic_to_shared(t.a[3]);
+    unsigned char *bt = p + 3 * TC_A_BYTES;
+    t.b_s = (uint32_t)__cvta_generic_to_shared(bt);
+    for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
+        const int n = i >> 6, k = i & 63;
+        *reinterpret_cast<__nv_bfloat16 *>(bt + tc_off(n, k)) = __float2bfloat16_rn(src[MW_W2 + n * MLP_H + k]);
+    }
+    t.bar = (uint32_t)__cvta_generic_to_shared(bar);
+    t.phase = 0;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t.bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (wib == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(slot)),
+                     "r"(TC_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_ready(TcMlp &t, const uint32_t *slot)
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    t.tmem = *slot;
+}
+
+// One step of the pair network's second layer for the whole CTA (every thread
+// calls it).  valid: this lane's row is a partner of its walker's proposal at
+// distance r, same-spin s, cusp coefficient a.  Writes u, du/dr, d2u/dr2 of the
+// row to pre[lane], pre[32 + lane], pre[64 + lane]; returns ST_TC_TIMEOUT when the
+// completion wait gave up.
+__device__ unsigned tc_pair_layer(TcMlp &t, const float *w, bool valid, float r, float s, float a, int lane,
+                                  int wib, float *pre)
+{
+    const int row = wib * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < 8; ++c) {  // 8 inputs of the second layer per 16-byte store
+        uint32_t hv[4], lv[4], dv[4], ddv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float h[2], d[2], dd[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int k = 8 * c + 2 * e + q;
+                const float w1r = w[MW_W1 + 2 * k], w1s = w[MW_W1 + 2 * k + 1];
+                const float hh = valid ? mlp_tanh(fmaf(w1r, r, fmaf(w1s, s, w[MW_B1 + k]))) : 0.0f;
+                h[q] = hh;
+                d[q] = valid ? (1.0f - hh * hh) * w1r : 0.0f;
+                dd[q] = -2.0f * hh * d[q] * w1r;
+            }
+            // value: high and low bfloat16 parts (about 16 significant bits together)
+            hv[e] = pack_bf16(h[0], h[1]);
+            const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&hv[e]);
+            lv[e] = pack_bf16(h[0] - __bfloat162float(hi.x), h[1] - __bfloat162float(hi.y));
+            dv[e] = pack_bf16(d[0], d[1]);
+            ddv[e] = pack_bf16(dd[0], dd[1]);
+        }
+        const uint32_t off = tc_off(row, 8 * c);
+        *reinterpret_cast<uint4 *>(t.a[0] + off) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<uint4 *>(t.a[1] + off) = make_uint4(dv[0], dv[1], dv[2], dv[3]);
+        *reinterpret_cast<uint4 *>(t.a[2] + off) = make_uint4(ddv[0], ddv[1], ddv[2], ddv[3]);
+        *reinterpret_cast<uint4 *>(t.a[3] + off) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+    }
+    // generic-proxy tile writes visible to the tensor cores; earlier TMEM reads done
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int o = 0; o < 4; ++o)  // value high, d/dr, d2/dr2, then value low into the value columns
+#pragma unroll
+            for (int st = 0; st < 4; ++st) {
+                const uint64_t ad = tc_desc(t.a_s[o] + st * 256), bd = tc_desc(t.b_s + st * 256);
+                const uint32_t dcol = t.tmem + 64 * (o == 3 ? 0 : o);
+                const uint32_t accumulate = (st > 0 || o == 3) ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                 dcol),
+                             "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+                             : "memory");
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(t.bar)
+                     : "memory");
+    }
+    uint32_t done = 0;
+    for (long it = 0; it < TC_WAIT_LIMIT && !done; ++it)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(t.bar), "r"(t.phase)
+                     : "memory");
+    t.phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float u = w[MW_B3], du = 0.0f, ddu = 0.0f;
+    const uint32_t lb = t.tmem + ((uint32_t)(wib * 32) << 16);
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+        uint32_t z[16], dz[16], ddz[16];
+        tmem_ld16(lb + 16 * c, z);
+        tmem_ld16(lb + 64 + 16 * c, dz);
+        tmem_ld16(lb + 128 + 16 * c, ddz);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            const int m = 16 * c + e;
+            const float zz = __uint_as_float(z[e]) + w[MW_B2 + m], d1 = __uint_as_float(dz[e]),
+                        d2 = __uint_as_float(ddz[e]);
+            const float h2 = mlp_tanh(zz), g2 = 1.0f - h2 * h2, w3 = w[MW_W3 + m];
+            u = fmaf(w3, h2, u);
+            du = fmaf(w3, g2 * d1, du);
+            ddu = fmaf(w3, g2 * (d2 - 2.0f * h2 * d1 * d1), ddu);
+        }
+    }
+    const float q = 1.0f / (1.0f + r);
+    pre[lane] = u + a * r * q;
+    pre[32 + lane] = du + a * q * q;
+    pre[64 + lane] = ddu - 2.0f * a * q * q * q;
+    __syncwarp();
+    return done ? 0u : (unsigned)ST_TC_TIMEOUT;
+}
+
+__device__ void tc_teardown(TcMlp &t, int wib)
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (wib == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(TC_COLS) : "memory");
+}
+
+template <bool TC>
 __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs a, const GenParams g)
 {
     extern __shared__ __align__(16) double gsm[];
     __shared__ double scratch[GEN_WPB][GEN_SCR];
+    __shared__ float pre[GEN_WPB][3 * 32];  // TC: u, du/dr, d2u/dr2 of each partner of the proposal
+    __shared__ __align__(8) unsigned long long tc_bar;
+    __shared__ uint32_t tc_slot;
     const Params &P = a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int w = blockIdx.x * GEN_WPB + wib;
     float *mw = g.mlp ? reinterpret_cast<float *>(gsm) : nullptr;
-    if (mw) {
-        mlp_stage(g.mlp, mw);
-        __syncthreads();
-    }
-    if (w >= P.W) return;
+    if (mw) mlp_stage(g.mlp, mw, !TC);
+    TcMlp tc{};
+    if (TC) tc_setup(tc, reinterpret_cast<unsigned char *>(gsm) + MLP_SMEM_DOUBLES * sizeof(double), mw, g.mlp,
+                     &tc_bar, &tc_slot, wib);
+    __syncthreads();
+    if (TC) tc_ready(tc, &tc_slot);
+    const bool active = w < P.W;
+    if (!TC && !active) return;
     const int N = P.N, D = g.D, dim = D / N;
-    double *rec = reinterpret_cast<double *>(P.state) + (size_t)w * g.rec;
+    const int ws = active ? w : 0;  // record pointers of a warp without a walker are never used
+    double *rec = reinterpret_cast<double *>(P.state) + (size_t)ws * g.rec;
     double *x = rec, *fc = rec + g.off_fc;
-    unsigned long long *mask = P.mask + (size_t)w * N;
+    unsigned long long *mask = P.mask + (size_t)ws * N;
     double *scr = scratch[wib];
-    double *acc = P.acc + (size_t)w * P.nacc * 2;
-    unsigned long long ctr = P.counter[w];
+    double *acc = P.acc + (size_t)ws * P.nacc * 2;
+    unsigned long long ctr = active ? P.counter[ws] : 0ull;
     unsigned status = 0;
     const bool is = P.sampling == SAMPLER_IS;
     const double dt = P.step, sqdt = sqrt(P.step);
 
     for (int s = 0; s < a.steps; ++s) {
         const int it_step = a.step_offset + s;
-        // ---- random numbers (vmo_step_randoms) or the caller's
-        int k;
-        double r1, r2;
-        if (a.probe_k) {
-            k = a.probe_k[w];
-            r1 = 0.0;
-            r2 = 0.0;
-        } else if (a.replay) {
-            const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
-            k = (int)floor(q[0] * D);
-            r1 = q[1];
-            r2 = q[2];
-        } else {
-            const uint4 v = philox(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)w, 0u),
-                                   make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
-            ++ctr;
-            k = (int)__umulhi(v.x, (unsigned)D);
-            if (is) {
-                const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
-                r1 = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+        int k = 0;
+        double r1 = 0.0, r2 = 0.0, xo = 0.0, dx = 0.0, fn = 0.0, xn = 0.0;
+        if (active) {
+            // ---- random numbers (vmo_step_randoms) or the caller's
+            k = 0;
+            r1 = r2 = 0.0;
+            if (a.probe_k) {
+                k = a.probe_k[w];
+                r1 = 0.0;
+                r2 = 0.0;
+            } else if (a.replay) {
+                const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
+                k = (int)floor(q[0] * D);
+                r1 = q[1];
+                r2 = q[2];
             } else {
-                r1 = v.y * TWO_M32;
-            }
-            r2 = v.w * TWO_M32;
-        }
-        // ---- proposal (importancesampling.cpp:49-60, bruteforce.cpp:34)
-        const double xo = x[k];
-        double dx, fn = 0.0;
-        if (a.probe_k) {
-            dx = a.probe_x[w] - xo;
-        } else if (is) {
-            fn = 2.0 * rec[g.off_g + k];
-            dx = 0.5 * dt * fn + r1 * sqdt;
-        } else {
-            dx = 10.0 * (r1 - 0.5) * P.step;
-        }
-        const double xn = a.probe_k ? a.probe_x[w] : xo + dx;
-        const bool corrected = is && !(P.flags & Q_IS_GREEN) && !a.probe_k;
-        double gy = 0.0, R = 1.0;
-        double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
-        const double prob = gen_ratios(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
-                                       corrected ? &gy : nullptr, R, mw);
-        bool accept = true;
-        if (!a.probe_k) {
-            double wgt = prob;
-            if (is) {
-                if (P.flags & Q_IS_GREEN) {
-                    wgt = (exp(0.5 * (fc[k] - fn) * dx) + 1.0) * prob;  // importancesampling.cpp:43-47
+                const uint4 v = philox(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)w, 0u),
+                                       make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
+                ++ctr;
+                k = (int)__umulhi(v.x, (unsigned)D);
+                if (is) {
+                    const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
+                    r1 = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
                 } else {
-                    const double fy = 2.0 * gy;
-                    wgt = prob * exp(0.5 * (fn + fy) * (0.25 * dt * (fn - fy) - dx));
+                    r1 = v.y * TWO_M32;
                 }
+                r2 = v.w * TWO_M32;
             }
-            // the reference rejects when weight < u (importancesampling.cpp:72,
-            // bruteforce.cpp:44); a NaN weight is flagged and rejected
-            if (wgt != wgt) status |= ST_BAD_RATIO;
-            accept = wgt >= r2;
+            // ---- proposal (importancesampling.cpp:49-60, bruteforce.cpp:34)
+            xo = x[k];
+            fn = 0.0;
+            if (a.probe_k) {
+                dx = a.probe_x[w] - xo;
+            } else if (is) {
+                fn = 2.0 * rec[g.off_g + k];
+                dx = 0.5 * dt * fn + r1 * sqdt;
+            } else {
+                dx = 10.0 * (r1 - 0.5) * P.step;
+            }
+            xn = a.probe_k ? a.probe_x[w] : xo + dx;
         }
-        if (accept) {
+        if (TC) {
+            // second layer of the pair network for the proposal's partners of all the
+            // CTA's walkers: one 128-row tile, tensor cores (value, d/dr, d2/dr2)
             const int p = k / dim;
-            if (P.flags & F_SLATER) {
-                // Sherman-Morrison on the moved particle's block (slaterdeterminant.cpp:165-175)
-                const int n = g.n, b = p / n, pl = p - b * n;
-                double *rows = rec + g.off_inv + (size_t)b * n * n;
-                for (int o = lane; o < n; o += 32) scr[SCR_ROW + o] = rows[(size_t)pl * n + o];
-                __syncwarp();
-                if (lane < n) {
-                    double *row = rows + (size_t)lane * n;
-                    double S = 0.0;
-                    for (int o = 0; o < n; ++o) S += scr[SCR_PHI + o] * row[o];
-                    const double c = S / R;
-                    for (int o = 0; o < n; ++o)
-                        row[o] = lane == pl ? scr[SCR_ROW + o] / R : row[o] - c * scr[SCR_ROW + o];
+            double yp[3] = {0.0, 0.0, 0.0};
+            for (int c = 0; c < dim; ++c) yp[c] = (active && c == k - p * dim) ? xn : (active ? x[p * dim + c] : 0.0);
+            float r = 0.0f, sv = 0.0f;
+            bool valid = active && lane < N && lane != p;
+            if (valid) {
+                double r2s = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[lane * dim + c];
+                    r2s += t * t;
+                }
+                r = (float)sqrt(r2s);
+                sv = same_spin(p, lane, N) ? 1.0f : 0.0f;
+            }
+            status |= tc_pair_layer(tc, mw, valid, r, sv, mlp_cusp(dim, sv > 0.5f), lane, wib, pre[wib]);
+        }
+        if (active) {
+            const bool corrected = is && !(P.flags & Q_IS_GREEN) && !a.probe_k;
+            double gy = 0.0, R = 1.0;
+            double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
+            const double prob = gen_ratios(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
+                                           corrected ? &gy : nullptr, R, mw, TC ? pre[wib] : nullptr);
+            bool accept = true;
+            if (!a.probe_k) {
+                double wgt = prob;
+                if (is) {
+                    if (P.flags & Q_IS_GREEN) {
+                        wgt = (exp(0.5 * (fc[k] - fn) * dx) + 1.0) * prob;  // importancesampling.cpp:43-47
+                    } else {
+                        const double fy = 2.0 * gy;
+                        wgt = prob * exp(0.5 * (fn + fy) * (0.25 * dt * (fn - fy) - dx));
+                    }
+                }
+                // the reference rejects when weight < u (importancesampling.cpp:72,
+                // bruteforce.cpp:44); a NaN weight is flagged and rejected
+                if (wgt != wgt) status |= ST_BAD_RATIO;
+                accept = wgt >= r2;
+            }
+            if (accept) {
+                const int p = k / dim;
+                if (P.flags & F_SLATER) {
+                    // Sherman-Morrison on the moved particle's block (slaterdeterminant.cpp:165-175)
+                    const int n = g.n, b = p / n, pl = p - b * n;
+                    double *rows = rec + g.off_inv + (size_t)b * n * n;
+                    for (int o = lane; o < n; o += 32) scr[SCR_ROW + o] = rows[(size_t)pl * n + o];
+                    __syncwarp();
+                    if (lane < n) {
+                        double *row = rows + (size_t)lane * n;
+                        double S = 0.0;
+                        for (int o = 0; o < n; ++o) S += scr[SCR_PHI + o] * row[o];
+                        const double c = S / R;
+                        for (int o = 0; o < n; ++o)
+                            row[o] = lane == pl ? scr[SCR_ROW + o] / R : row[o] - c * scr[SCR_ROW + o];
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0) {
+                    x[k] = xn;
+                    if (is) fc[k] = fn;
+                }
+                if (P.flags & F_MLP) {  // the moved particle's pair and one-body values from the proposal
+                    double *uc = rec + g.off_uc;
+                    for (int j = lane; j < N; j += 32)
+                        if (j != p) {
+                            double *c3 = uc + (size_t)(min(p, j) * N + max(p, j)) * 3;
+                            c3[0] = scr[SCR_XS + j];
+                            c3[1] = scr[SCR_XS + 32 + j];
+                            c3[2] = scr[SCR_PN + j];
+                        }
+                    if (lane == 0)
+                        for (int t = 0; t < 3; ++t) rec[g.off_oc + p * 3 + t] = scr[SCR_PN + 32 + t];
+                }
+                if (P.flags & Q_PADE_STALE) {  // the moved particle's pairs take the current gamma
+                    for (int j = lane; j < N; j += 32)
+                        if (j != p) mask[j] |= 1ull << p;
+                    if (lane == 0) mask[p] = ~0ull;
                 }
                 __syncwarp();
+                gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false);
             }
-            if (lane == 0) {
-                x[k] = xn;
-                if (is) fc[k] = fn;
+            if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
+            const double *en = rec + g.off_en;
+            if (a.rec_en && lane == 0) {
+                double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
+                o[0] = en[0];
+                o[1] = en[1];
+                o[2] = en[2];
             }
-            if (P.flags & F_MLP) {  // the moved particle's pair and one-body values from the proposal
-                double *uc = rec + g.off_uc;
-                for (int j = lane; j < N; j += 32)
-                    if (j != p) {
-                        double *c3 = uc + (size_t)(min(p, j) * N + max(p, j)) * 3;
-                        c3[0] = scr[SCR_XS + j];
-                        c3[1] = scr[SCR_XS + 32 + j];
-                        c3[2] = scr[SCR_PN + j];
+            if (it_step >= a.burn_in) {  // Sampler::sample (sampler.cpp:52-90)
+                const double el = en[0] + en[1] + en[2];
+                if (el != el) status |= ST_NAN_ENERGY;
+                const bool win = it_step > a.win_lo && it_step < a.win_hi;
+                if (win && a.snap_x && (it_step - a.win_lo) % a.snap_interval == 0) {
+                    // MLP Jastrow parameter gradient: positions and E_L for mlp_grad_kernel
+                    const int slot = (it_step - a.win_lo) / a.snap_interval - a.snap_first;
+                    if (slot >= 0 && slot < a.snap_stride) {
+                        const size_t base = (size_t)w * a.snap_stride + slot;
+                        for (int t = lane; t < D; t += 32) a.snap_x[base * D + t] = (float)x[t];
+                        if (lane == 0) a.snap_e[base] = el;
                     }
-                if (lane == 0)
-                    for (int t = 0; t < 3; ++t) rec[g.off_oc + p * 3 + t] = scr[SCR_PN + 32 + t];
-            }
-            if (P.flags & Q_PADE_STALE) {  // the moved particle's pairs take the current gamma
-                for (int j = lane; j < N; j += 32)
-                    if (j != p) mask[j] |= 1ull << p;
-                if (lane == 0) mask[p] = ~0ull;
+                }
+                const int top = win ? 9 + 2 * g.n_act : 9;  // == P.nacc inside the window
+                const double *pg = rec + g.off_pg;
+                for (int t = lane; t < top; t += 32) {
+                    double q;
+                    if (t < 8) {
+                        const double base = t < 2 ? el : en[(t >> 1) - 1];
+                        q = (t & 1) ? base * base : base;
+                    } else if (t == 8) {
+                        q = accept ? 1.0 : 0.0;
+                    } else {
+                        const int c = t - 9;
+                        q = c < g.n_act ? pg[g.act[c]] : el * pg[g.act[c - g.n_act]];
+                    }
+                    double s1 = acc[2 * t], c1 = acc[2 * t + 1];
+                    kadd(s1, c1, q);
+                    acc[2 * t] = s1;
+                    acc[2 * t + 1] = c1;
+                }
             }
             __syncwarp();
-            gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false);
         }
-        if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
-        const double *en = rec + g.off_en;
-        if (a.rec_en && lane == 0) {
-            double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
-            o[0] = en[0];
-            o[1] = en[1];
-            o[2] = en[2];
-        }
-        if (it_step >= a.burn_in) {  // Sampler::sample (sampler.cpp:52-90)
-            const double el = en[0] + en[1] + en[2];
-            if (el != el) status |= ST_NAN_ENERGY;
-            const bool win = it_step > a.win_lo && it_step < a.win_hi;
-            if (win && a.snap_x && (it_step - a.win_lo) % a.snap_interval == 0) {
-                // MLP Jastrow parameter gradient: positions and E_L for mlp_grad_kernel
-                const int slot = (it_step - a.win_lo) / a.snap_interval - a.snap_first;
-                if (slot >= 0 && slot < a.snap_stride) {
-                    const size_t base = (size_t)w * a.snap_stride + slot;
-                    for (int t = lane; t < D; t += 32) a.snap_x[base * D + t] = (float)x[t];
-                    if (lane == 0) a.snap_e[base] = el;
-                }
-            }
-            const int top = win ? 9 + 2 * g.n_act : 9;  // == P.nacc inside the window
-            const double *pg = rec + g.off_pg;
-            for (int t = lane; t < top; t += 32) {
-                double q;
-                if (t < 8) {
-                    const double base = t < 2 ? el : en[(t >> 1) - 1];
-                    q = (t & 1) ? base * base : base;
-                } else if (t == 8) {
-                    q = accept ? 1.0 : 0.0;
-                } else {
-                    const int c = t - 9;
-                    q = c < g.n_act ? pg[g.act[c]] : el * pg[g.act[c - g.n_act]];
-                }
-                double s1 = acc[2 * t], c1 = acc[2 * t + 1];
-                kadd(s1, c1, q);
-                acc[2 * t] = s1;
-                acc[2 * t + 1] = c1;
-            }
-        }
-        __syncwarp();
     }
-    if (lane == 0) {
+    if (active && lane == 0) {
         P.counter[w] = ctr;
         if (status) P.status[w] |= status;
     }
+    if (TC) tc_teardown(tc, wib);
 }
 
 // dJ/dtheta of the MLP Jastrow for a set of position snapshots (backpropagation,
@@ -1206,6 +1475,7 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     g.sigma = c.sigma;
     g.basis = c.basis == "hydrogenOrbital" ? BASIS_HYDROGEN : BASIS_HERMITE;
     g.horb3 = c.compat ? 1 : 0;
+    g.mlp_tc = c.mlp_tc ? 1 : 0;
     const bool slater = std::count(c.elements.begin(), c.elements.end(), (int)E_SLATER) > 0;
     g.n = slater ? N / 2 : 0;
     if (slater) {
@@ -1285,10 +1555,15 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
 
 cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st)
 {
-    const size_t smem = g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0;
-    cudaError_t e = cudaFuncSetAttribute(gen_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool tc = g.mlp && g.mlp_tc;
+    const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0);
+    const void *fn = tc ? (const void *)gen_sweep_kernel<true> : (const void *)gen_sweep_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    gen_sweep_kernel<<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(a, g);
+    if (tc)
+        gen_sweep_kernel<true><<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(a, g);
+    else
+        gen_sweep_kernel<false><<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(a, g);
     return cudaGetLastError();
 }
 

@@ -26,6 +26,7 @@ struct GenParams {
     // gradient comes from snapshots): accumulator 9 + c holds parameter act[c]
     const int *act;
     int n_act;
+    int mlp_tc;                 // MLP sweep with the second layer on the tensor cores
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
 };
 
