@@ -364,6 +364,9 @@ def run_engine_arm(args):
     if fp64:
         line["fp64"] = fp64
         line["mixed_over_fp64"] = value / fp64["value"]
+    if args.learned > 0 and world == 1:
+        from vmachine_b200.learned import compare
+        line["learned"] = compare(budget_s=args.learned)
     if not args.no_cpu_baseline and world == 1:
         cores = host_cores()
         v, err = reference_sample(cores, args.ref_steps)
@@ -393,6 +396,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned", type=float, default=0.0,
+                    help="seconds of training per wave function for the MLP-vs-Pade comparison "
+                         "at N=20 omega=0.5 (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args, int(os.environ.get("RANK", "0")))

@@ -1,0 +1,37 @@
+"""What the learned MLP Jastrow gains, trained on the GPU by the engine's own
+forward and backward kernels (N = 20, omega = 0.5 quantum dot).
+
+- Training lowers the energy of the MLP wave function far below its untrained
+  start (the network's output layers start at zero, so the untrained factor is the
+  cusp term alone, with alpha = 1).
+- At equal wall time the trained MLP is not worse than the Pade-Jastrow trained by
+  the same engine (the difference is printed; the longer run in
+  vmachine_b200.learned.compare measured the MLP 0.018 +- 0.009 lower).
+Energies are of the frozen wave functions, with error bars over walkers.
+"""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BUDGET_S = 40.0
+
+
+def test_trained_network_gains():
+    from vmachine_b200 import Engine
+    from vmachine_b200.learned import dot_config, evaluate, train
+    N, omega, W, steps = 20, 0.5, 2048, 800
+    mlp_text = dot_config(N, omega, "mlpJastrow", W, steps, 3e-4)
+    untrained = Engine(mlp_text)
+    untrained.init_walkers(None, seed=7)
+    e0, s0, _ = evaluate(untrained, 2000, burn_steps=1000)
+    untrained.close()
+    eng, hist = train(mlp_text, BUDGET_S)
+    e_mlp, s_mlp, _ = evaluate(eng, 2000)
+    eng.close()
+    pade, _ = train(dot_config(N, omega, "padeJastrow", W, steps, 0.01), BUDGET_S)
+    e_pade, s_pade, _ = evaluate(pade, 2000)
+    pade.close()
+    print(f"untrained {e0:.4f}+-{s0:.4f}  trained MLP {e_mlp:.4f}+-{s_mlp:.4f} ({len(hist)} iterations)  "
+          f"Pade {e_pade:.4f}+-{s_pade:.4f}")
+    assert e_mlp < e0 - 5 * (s0 + s_mlp)
+    assert e_mlp < e_pade + 3 * (s_mlp + s_pade)
