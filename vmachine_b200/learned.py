@@ -64,3 +64,47 @@ def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps
     out["gain"] = d
     out["gain_sigma"] = d / np.hypot(out["pade"]["error"], out["mlp"]["error"])
     return out
+
+
+def sweep_speed(walkers=8192, steps=100, N=20, omega=0.5, tensor_cores=True, iterations=2):
+    """Walker-moves per second of the MLP-Jastrow sweep (sampling and the backward
+    kernel included) over `iterations` optimisation iterations after one warm-up."""
+    text = dot_config(N, omega, "mlpJastrow", walkers, steps, 3e-4,
+                      extra=[f"mlpTensorCores: {'true' if tensor_cores else 'false'}"])
+    eng = Engine(text)
+    try:
+        eng.init_walkers(None, seed=1)
+        eng.run_iteration(0)
+        eng.stopwatch_start()
+        for it in range(iterations):
+            a = eng.run_iteration(1 + it)
+        ms = eng.stopwatch_stop()
+        moves = iterations * walkers * (eng.info.steps_per_walker + eng.info.burn_in)
+        return {"walkers": walkers, "steps_per_walker": steps, "tensor_cores": tensor_cores,
+                "ms_per_iteration": ms / iterations, "walker_moves_per_s": moves / (ms * 1e-3),
+                "energy": a.energy, "status": int(np.bitwise_or.reduce(eng.status()))}
+    finally:
+        eng.close()
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(prog="python -m vmachine_b200.learned")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    s = sub.add_parser("speed", help="sweep throughput of the MLP-Jastrow wave function")
+    s.add_argument("--walkers", type=int, default=8192)
+    s.add_argument("--steps", type=int, default=100)
+    s.add_argument("--cuda-cores", action="store_true", help="second layer on the CUDA cores")
+    c = sub.add_parser("compare", help="MLP against Pade at equal wall time")
+    c.add_argument("--budget", type=float, default=120.0)
+    c.add_argument("--walkers", type=int, default=4096)
+    a = ap.parse_args(argv)
+    if a.cmd == "speed":
+        print(json.dumps(sweep_speed(a.walkers, a.steps, tensor_cores=not a.cuda_cores)))
+    else:
+        print(json.dumps(compare(walkers=a.walkers, budget_s=a.budget)))
+
+
+if __name__ == "__main__":
+    main()
