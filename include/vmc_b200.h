@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define VMC_ABI_VERSION 2
+#define VMC_ABI_VERSION 3
 
 enum {
     VMC_OK = 0,
@@ -189,6 +189,122 @@ int vmc_stopwatch(vmc_engine *e, int mode, double *ms);
  * register-resident loop over all SMs; TFLOP/s counting an FMA as 2 flops.  The
  * roofline denominator of the CUDA-core-bound sweep kernel. */
 int vmc_measure_fma_peak(int device, int precision, double *tflops);
+
+/* ---- Blocking analysis (Sampler::doResampling, sampler.cpp:319-405, and the
+ * Blocker of include/block/blocker.cpp:10-71: automatic blocking, M. Jonsson,
+ * Phys. Rev. E 98, 043304 (2018)) ---- */
+typedef struct {
+    double mean;          /* Blocker::mean                                            */
+    double std_error;     /* Blocker::stdErr = sqrt(mse_mean)                         */
+    double mse_mean;      /* Blocker::mse_mean: variance of the mean at the chosen level */
+    double mse_std_error; /* Blocker::mse_stdErr = (2 nK - 1) mse_mean^2 / nK^2        */
+    long long n_k;        /* Blocker::nK: blocks at the chosen level                  */
+} vmc_block;
+
+typedef struct {
+    /* the walkers' series concatenated walker by walker (the reference's instant
+     * files appended over ranks, walkers in place of ranks); every field -1 unless
+     * n_walkers x samples_per_walker is a power of two (blocker.cpp:20-25) */
+    vmc_block energy, kinetic, external, interaction;
+    /* independent chains: mean of the walkers' means; mse_mean = sum over walkers of
+     * each walker's own blocked variance of its mean / W^2 (n_k = 0) */
+    vmc_block energy_walkers;
+    long long samples_per_walker; /* 2^d: the first 2^d sampled steps of each walker */
+} vmc_blocking_result;
+
+/* Blocker on a host series of n values; n not a power of two: every field -1 and
+ * n_k = 0 (the reference prints an error and sets -1). */
+int vmc_block_series(const double *x, long long n, vmc_block *out);
+/* `steps` moves per walker with the current parameters (no optimiser step; sums as
+ * vmc_sample with iteration 0), recording every walker's (T, V_ext, V_int) per step
+ * in device memory (W x steps x 24 bytes, released after), then blocking of E_L, T,
+ * V_ext and V_int on the device.  Consumes a replay stream set by vmc_set_replay. */
+int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out);
+
+/* ---- Checkpoint and resume ----
+ *
+ * Parameter files in the reference's text format (Sampler::printParametersToFile,
+ * sampler.cpp:507-515, read by FromFile, fromfile.cpp:30-79): one row per element,
+ * Eigen's default layout (common right-aligned width, one space between values).
+ * digits <= 0: 6 significant digits, the reference's files byte for byte; 17 keeps
+ * every bit.  vmc_run_simulation writes <path>weights_<it>.dat every checkpointFreq
+ * iterations when printParametersToFile is true (system.cpp:116-118). */
+/* The text of a parameter file for an n_elements x p_max matrix into buf (at most
+ * cap - 1 characters and a zero); returns its full length, or < 0 on error. */
+long long vmc_format_weights(const double *theta, int n_elements, int p_max, int digits, char *buf,
+                             long long cap);
+int vmc_write_weights(const vmc_engine *e, const char *path, int digits);
+/* FromFile::setupInitialWeights at any time: vmc_set_parameters from the file. */
+int vmc_read_weights(vmc_engine *e, const char *path);
+/* Walker state for an exact restart (no counterpart in the reference): the walkers'
+ * records, running sums, Pade masks, Philox counters and status words, the
+ * parameters, optimiser moments and step, and the refresh cadence, in a binary file.
+ * Loading needs an engine created from the same input.in (same particles, walkers,
+ * precision, elements); an engine resumed from a file continues exactly as the
+ * saving engine would have. */
+int vmc_save_state(const vmc_engine *e, const char *path);
+int vmc_load_state(vmc_engine *e, const char *path);
+
+/* ---- Multi-system batch (no counterpart in the reference) ----
+ *
+ * Many systems (quantum dots and atoms of different N, omega, Z), each with its
+ * own input.in text, walker pool, parameters and optimiser, iterated together:
+ * one persistent sweep kernel per round takes work items (a system's run of
+ * walkers) from a queue ordered by cost, so large and small systems share the
+ * GPU; every iteration is a captured CUDA graph (parameter upload, sweeps, FP64
+ * refreshes, reductions, result download) replayed with the current parameters.
+ * The CTA width (walkers per block) and work-item size are chosen by an
+ * autotuner that times one iteration per candidate (the first iterations run
+ * eagerly while it tunes).  Each system computes exactly what vmc_run_iteration
+ * computes for it alone (the same walker streams, reductions and optimiser step).
+ *
+ * Systems: 2D closed-shell quantum dots with Slater(Hermite) x Gaussian x Pade,
+ * Coulomb, importance sampling (all in the batch's precision and compat mode), and
+ * general-path systems in FP64 (hydrogen-orbital atoms, SimpleJastrow, RBM; not
+ * the MLP Jastrow).  Up to VMC_BATCH_MAX_SYSTEMS systems, at most 16 of them on the
+ * general path; one batch per device at a time (its system table is a device
+ * constant).  opt (may be NULL): device, compat and refresh_interval apply to
+ * every system, precision to the dots; walker counts come from each text. */
+#define VMC_BATCH_MAX_SYSTEMS 64
+typedef struct vmc_batch vmc_batch;
+
+typedef struct {
+    int n_systems, n_general;
+    long long n_walkers;        /* over all systems                                   */
+    int precision;              /* of the dots                                        */
+    int walkers_per_block;      /* chosen CTA width (warps), 0 while tuning            */
+    int walkers_per_item;       /* chosen work-item size                              */
+    int grid;                   /* persistent CTAs of the sweep                       */
+    int tuned;                  /* 1 once the autotuner (or vmc_batch_set_tile) chose   */
+    int graph_captures;         /* CUDA graphs captured so far                        */
+    int graph_replay;           /* 1 if the last iteration replayed a captured graph   */
+    int rounds;                 /* sweep launches of the last iteration               */
+    double seconds;             /* device time of the last iteration                  */
+    double sweep_seconds;       /* of its sweep launches                              */
+    double walker_moves;        /* walker-moves of the last iteration                 */
+} vmc_batch_info;
+
+typedef struct {
+    int walkers_per_block, walkers_per_item, grid;
+    double ns_per_walker_move;  /* sweep time per walker-move of its trial iteration, or < 0 */
+} vmc_batch_candidate;
+
+int vmc_batch_create(const char *const *input_texts, int n_systems, const vmc_options *opt, vmc_batch **out);
+void vmc_batch_destroy(vmc_batch *b);
+int vmc_batch_get_info(const vmc_batch *b, vmc_batch_info *out);
+/* The engine of system s (parameters, walkers, evaluation); owned by the batch. */
+int vmc_batch_system(vmc_batch *b, int s, vmc_engine **engine);
+/* vmc_init_walkers for every system; seeds: n_systems seeds, or NULL for each
+ * system's configured seed. */
+int vmc_batch_init_walkers(vmc_batch *b, const uint64_t *seeds);
+/* Fix the tile instead of tuning (walkers_per_block 1..8, walkers_per_item >= 1). */
+int vmc_batch_set_tile(vmc_batch *b, int walkers_per_block, int walkers_per_item);
+/* One optimisation iteration of every system; out: n_systems averages (may be
+ * NULL).  Each system's totals of the iteration: vmc_batch_last_sums. */
+int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *out);
+int vmc_batch_last_sums(const vmc_batch *b, vmc_sums *out /* n_systems */);
+/* The autotuner's candidates and their timings; returns how many (<= n written). */
+int vmc_batch_tuning(const vmc_batch *b, vmc_batch_candidate *out, int n);
 
 /* ---- Allocation-free evaluation (no counterpart in the reference) ----
  *

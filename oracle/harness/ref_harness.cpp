@@ -378,4 +378,24 @@ int vmref_blocking(const double *x, long n, double *out)
     return 0;
 }
 
+// The reference's parameter file text for an E x P row-major matrix
+// (Sampler::printParametersToFile, sampler.cpp:507-515: the matrix through Eigen's
+// default stream format, then endl).  Returns the length; writes at most cap - 1
+// characters and a terminating zero.
+long vmref_format_weights(const double *theta, int E, int P, char *buf, long cap)
+{
+    Eigen::MatrixXd m(E, P);
+    for (int i = 0; i < E; i++)
+        for (int j = 0; j < P; j++) m(i, j) = theta[i * P + j];
+    std::ostringstream os;
+    os << m << std::endl;
+    const std::string t = os.str();
+    if (cap > 0) {
+        const long n = std::min<long>((long)t.size(), cap - 1);
+        std::memcpy(buf, t.data(), n);
+        buf[n] = 0;
+    }
+    return (long)t.size();
+}
+
 }  // extern "C"

@@ -7,6 +7,7 @@ reference nor its build.
 
     python tests/golden/make_golden.py            # rewrites tests/golden/*.npz
     python tests/golden/make_golden.py hydrogen   # only hydrogen_orbitals.npz
+    python tests/golden/make_golden.py weights    # only weights_format.npz
 
 Every input is seeded synthetic data: walker positions ~ N(0, 1/sqrt(omega)),
 replayed uniforms/normals from numpy's PCG64 with fixed seeds.
@@ -219,6 +220,30 @@ def make_blocking(rng):
     return out
 
 
+def make_weights(rng):
+    """Parameter files as the reference writes them (Sampler::printParametersToFile:
+    the matrix through Eigen's default stream format, then endl)."""
+    import ctypes
+    from oracle_bind import REF_SO
+    lib = ctypes.CDLL(REF_SO)
+    lib.vmref_format_weights.restype = ctypes.c_long
+    lib.vmref_format_weights.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                         ctypes.c_long]
+    mats = [np.array([[0.0], [1.02029717], [0.35]]), np.array([[1.0], [0.5]]),
+            rng.normal(size=(2, 3)), rng.normal(scale=40.0, size=(3, 4)),
+            np.array([[1e-7, -123456.789, 0.0], [1.5e10, -2.5e-12, 7.0]]),
+            rng.normal(scale=0.3, size=(3, 36)), -np.abs(rng.normal(size=(4, 5))) * 1e-3]
+    out = {}
+    for i, m in enumerate(mats):
+        m = np.ascontiguousarray(m, np.float64)
+        buf = ctypes.create_string_buffer(1 << 16)
+        n = lib.vmref_format_weights(m.ctypes.data_as(ctypes.c_void_p), m.shape[0], m.shape[1], buf, len(buf))
+        assert 0 < n < len(buf)
+        out[f"matrix{i}/theta"] = m
+        out[f"matrix{i}/text"] = np.array(buf.value.decode())
+    return out
+
+
 def make_hydrogen():
     rng = np.random.default_rng(20261204)
     out = make_eval(rng, HYDROGEN_EVAL)
@@ -230,12 +255,17 @@ def main():
     if sys.argv[1:] == ["hydrogen"]:
         make_hydrogen()
         return
+    if sys.argv[1:] == ["weights"]:
+        np.savez_compressed(os.path.join(HERE, "weights_format.npz"),
+                            **make_weights(np.random.default_rng(20261205)))
+        return
     make_hydrogen()
     rng = np.random.default_rng(20261203)
     np.savez_compressed(os.path.join(HERE, "eval_fixed.npz"), **make_eval(rng))
     np.savez_compressed(os.path.join(HERE, "chains.npz"), **make_chains(rng))
     np.savez_compressed(os.path.join(HERE, "iterations.npz"), **make_iterations(rng))
     np.savez_compressed(os.path.join(HERE, "blocking.npz"), **make_blocking(rng))
+    np.savez_compressed(os.path.join(HERE, "weights_format.npz"), **make_weights(np.random.default_rng(20261205)))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

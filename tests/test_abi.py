@@ -13,7 +13,7 @@ HEADER = os.path.join(ROOT, "include", "vmc_b200.h")
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void|const char \*)\s*(vmc_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|long long|const char \*)\s*(vmc_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_entry_points():

@@ -13,10 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "vmc_b200.h"
-#include "vmc_config.hpp"
-#include "vmc_general.hpp"
-#include "vmc_kernels.cuh"
+#include "vmc_engine.hpp"
 
 using namespace vmc;
 
@@ -63,7 +60,6 @@ __global__ void reduce_acc_kernel(const double *acc, int W, int nacc, double *ou
         out[a] = S + C;
     }
 }
-int set_last_error(int code, const char *msg);
 }  // namespace vmc
 
 namespace {
@@ -123,17 +119,7 @@ int hermite_init_device(int device)
 {
     static bool done[64] = {false};
     if (device < 64 && done[device]) return VMC_OK;
-    HermiteCoef h;
-    for (int m = 0; m < HMAX; ++m) {
-        h.A[m] = std::sqrt(2.0 / (m + 1));
-        h.B[m] = std::sqrt((double)m / (m + 1));
-        h.C[m] = std::sqrt(2.0 * m);
-        h.E[m] = 2.0 * std::sqrt((double)m * (m - 1 > 0 ? m - 1 : 0));
-        h.Af[m] = (float)h.A[m];
-        h.Bf[m] = (float)h.B[m];
-        h.Cf[m] = (float)h.C[m];
-        h.Ef[m] = (float)h.E[m];
-    }
+    const HermiteCoef h = hermite_coefficients();
     CUDA_TRY(upload_hermite_f32(h));
     CUDA_TRY(upload_hermite_f64(h));
     CUDA_TRY(upload_hermite_gen(h));
@@ -142,59 +128,6 @@ int hermite_init_device(int device)
 }
 
 }  // namespace
-
-struct vmc_engine {
-    Config cfg;
-    int device = 0, num_sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int W = 0, N = 0, dim = 0, D = 0, n_orb = 0, K = 0, E = 0, Pmax = 0, EP = 0, nacc = 0;
-    // accumulators per walker on the device: nacc on the quantum-dot path; on the
-    // general path 9 + 2 x the active parameters (act, no padding, no MLP row)
-    int nacc_dev = 0;
-    std::vector<int> act;
-    int *d_act = nullptr;
-    int precision = 0, compat = 1, flags = 0, sampling = 0;
-    int steps_per_walker = 0, burn_in = 0, batches = 1;
-    int wpb = 0, refresh_interval = 0, sweep_chunk = 2048;
-    bool refresh_auto = false;          // refreshInterval: auto (mixed precision)
-    double drift_tol = 1e-4;            // inverse drift that halves the interval
-    size_t elem_bytes = 8;
-    Layout L{};
-    KernelSet ks;
-    // general path (SimpleJastrow, RBM, hydrogen orbitals): FP64 kernels of vmc_general.cu
-    bool general = false;
-    GenParams gen{};
-    double *d_theta = nullptr;  // E x p_max on the device (general path)
-    // MLP Jastrow: bf16-rounded weights, parameter-gradient snapshots and sums
-    int mlp_e = -1;                // element index, or -1
-    float *d_mlpw = nullptr;
-    float *d_snap_x = nullptr;
-    double *d_snap_e = nullptr, *d_mlp_out = nullptr;
-    size_t snap_cap = 0;           // snapshots the buffers hold
-    std::vector<double> theta;
-    double gamma_prev = 0.0;
-    bool have_walkers = false;
-    unsigned long long seed = 0;
-    // optimiser state (adam.cpp:12-37, gradientdescent.cpp/sgd.cpp)
-    std::vector<double> opt_m, opt_v;
-    int opt_step = 0;
-    // device buffers
-    void *d_state = nullptr;
-    double *d_scal = nullptr, *d_acc = nullptr, *d_out = nullptr, *d_drift = nullptr;
-    unsigned long long *d_mask = nullptr, *d_counter = nullptr;
-    unsigned *d_status = nullptr;
-    double *d_pos = nullptr;  // W x D positions staged for the host link
-    std::vector<cudaEvent_t> sweep_events;  // per-launch timing of the sweep kernel
-    cudaEvent_t sw0 = nullptr, sw1 = nullptr;  // vmc_stopwatch
-    // optional replayed random stream consumed by vmc_sample (W x replay_len x 3)
-    double *d_replay = nullptr;
-    int replay_len = 0, replay_pos = 0;
-    // last sampling pass
-    vmc_sums last{};
-    double last_samples_per_walker = 0.0;
-    double last_walker_std_error = 0.0;
-};
 
 namespace {
 
@@ -395,24 +328,10 @@ int initial_weights(vmc_engine *e)
     } else if (method == "randomuniform") {  // randomuniform.cpp (weights)
         for (size_t i = 0; i < e->theta.size(); ++i) e->theta[i] = factor * uniform((uint32_t)i);
     } else if (method == "fromfile") {  // fromfile.cpp:30-79
-        std::ifstream in(c.weights_file);
-        if (!in) return fail(VMC_E_CONFIG, "cannot open weights file '" + c.weights_file + "'");
-        std::vector<std::vector<double>> rows;
-        std::string line;
-        while (std::getline(in, line)) {
-            std::istringstream ls(line);
-            std::vector<double> r;
-            double v;
-            while (ls >> v) r.push_back(v);
-            if (!r.empty()) rows.push_back(r);
-        }
-        if ((int)rows.size() != e->E)
-            return fail(VMC_E_CONFIG, "weights file has " + std::to_string(rows.size()) + " rows, expected " + std::to_string(e->E));
-        for (int i = 0; i < e->E; ++i) {
-            if ((int)rows[i].size() != e->Pmax)
-                return fail(VMC_E_CONFIG, "weights file row " + std::to_string(i) + " has " + std::to_string(rows[i].size()) + " values, expected " + std::to_string(e->Pmax));
-            for (int j = 0; j < e->Pmax; ++j) e->theta[(size_t)i * e->Pmax + j] = rows[i][j];
-        }
+        std::vector<double> th;
+        const std::string why = read_weights_file(c.weights_file, e->E, e->Pmax, th);
+        if (!why.empty()) return fail(VMC_E_CONFIG, why);
+        e->theta = th;
     }
     if (e->mlp_e >= 0 && method != "fromfile") {
         // MLP Jastrow: Xavier-uniform hidden layers, zero biases and output layers, so
@@ -688,19 +607,7 @@ int vmc_set_parameters(vmc_engine *e, const double *theta, int n_elements, int p
 {
     if (!e || !theta) return fail(VMC_E_ARG, "null argument");
     if (n_elements != e->E || p_max != e->Pmax) return fail(VMC_E_ARG, "parameter shape mismatch");
-    const double old_gamma = make_params(e).gamma;
-    e->theta.assign(theta, theta + (size_t)e->E * e->Pmax);
-    CUDA_TRY(cudaSetDevice(e->device));
-    if (e->have_walkers && (e->flags & Q_PADE_STALE)) {
-        // Pade pairs keep the gamma they were computed with until one of their
-        // particles moves (padejastrow.cpp:65-68 only stores gamma)
-        e->gamma_prev = old_gamma;
-        CUDA_TRY(cudaMemsetAsync(e->d_mask, 0, (size_t)e->W * e->N * sizeof(unsigned long long), e->stream));
-    } else {
-        e->gamma_prev = make_params(e).gamma;
-    }
-    int rc = upload_theta(e);
-    return rc ? rc : refresh_all(e);
+    return set_parameters(e, theta, true);
 }
 
 int vmc_get_parameters(const vmc_engine *e, double *theta, int n_elements, int p_max)
@@ -784,7 +691,6 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
     CUDA_TRY(cudaMemsetAsync(e->d_acc, 0, W * e->nacc_dev * 2 * sizeof(double), e->stream));
     const int bs = (steps - burn_in) / e->batches;
     const int m = iteration % e->batches;
-    double max_drift = 0.0;
     std::vector<double> drift;
     CUDA_TRY(cudaMemsetAsync(e->d_drift, 0, W * sizeof(double), e->stream));
     CUDA_TRY(cudaEventRecord(e->ev0, e->stream));
@@ -834,6 +740,10 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
             a.snap_interval = snap_interval;
             a.snap_first = snap_first;
         }
+        if (e->d_rec) {
+            a.rec_en = e->d_rec;
+            a.rec_stride = e->rec_stride;
+        }
         if (e->d_replay) {
             if (e->replay_pos + steps > e->replay_len) return fail(VMC_E_ARG, "replay stream exhausted");
             a.replay = e->d_replay;
@@ -859,7 +769,7 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
     if (e->d_replay) e->replay_pos += steps;
     reduce_acc_kernel<<<e->nacc_dev, 256, 0, e->stream>>>(e->d_acc, e->W, e->nacc_dev, e->d_out);
     CUDA_TRY(cudaGetLastError());
-    std::vector<double> sums(e->nacc, 0.0), dev_sums(e->nacc_dev);
+    std::vector<double> dev_sums(e->nacc_dev);
     CUDA_TRY(cudaMemcpyAsync(dev_sums.data(), e->d_out, e->nacc_dev * sizeof(double), cudaMemcpyDeviceToHost,
                              e->stream));
     std::vector<double> mlp_sums(n_slots > 0 ? 2 * MLP_PARAMS : 0);
@@ -873,16 +783,6 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         CUDA_TRY(cudaMemcpyAsync(drift.data(), e->d_drift, W * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(e->stream));
-    if (e->general) {  // active parameters back to their (element, parameter) slots
-        std::copy(dev_sums.begin(), dev_sums.begin() + 9, sums.begin());
-        const size_t na = e->act.size();
-        for (size_t c = 0; c < na; ++c) {
-            sums[9 + e->act[c]] = dev_sums[9 + c];
-            sums[9 + e->EP + e->act[c]] = dev_sums[9 + na + c];
-        }
-    } else {
-        sums = dev_sums;
-    }
     float ms = 0.f;
     CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
     double sweep_ms = 0.0;
@@ -891,53 +791,14 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
         CUDA_TRY(cudaEventElapsedTime(&t, e->sweep_events[2 * i], e->sweep_events[2 * i + 1]));
         sweep_ms += t;
     }
-    double q99_drift = 0.0;
-    for (double d : drift) max_drift = std::max(max_drift, d);
-    if (!drift.empty()) {
-        const size_t i99 = (size_t)(0.99 * (drift.size() - 1));
-        std::nth_element(drift.begin(), drift.begin() + i99, drift.end());
-        q99_drift = drift[i99];
-    }
-    if (e->refresh_auto && n_refresh) {
-        // FP64 re-inversion cadence against the drift of the FP32 Sherman-Morrison
-        // inverse: the 99th percentile over walkers (the maximum is set by the few
-        // walkers sitting near a node of the determinant) halves the interval past
-        // the tolerance and doubles it below 1/2.5 of it (drift grows about in
-        // proportion to the interval, so a doubling stays under the tolerance)
-        if (q99_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
-        else if (q99_drift < e->drift_tol / 2.5) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
-    }
+    unsigned status = 0;
+    for (unsigned v : st) status |= v;
+    const SamplePass pass{steps, burn_in, bs, n_launch, n_refresh, dev_sums.data(), status,
+                          n_refresh ? &drift : nullptr, (double)ms, sweep_ms, -1.0};
     vmc_sums s{};
-    s.energy = sums[0];
-    s.energy2 = sums[1];
-    s.kinetic = sums[2];
-    s.kinetic2 = sums[3];
-    s.external = sums[4];
-    s.external2 = sums[5];
-    s.interaction = sums[6];
-    s.interaction2 = sums[7];
-    s.accepts = sums[8];
-    s.n_samples = (double)W * (steps - burn_in);
-    s.n_window = (double)W * bs;
-    s.seconds = ms * 1e-3;
-    s.sweep_seconds = sweep_ms * 1e-3;
-    s.sweep_launches = n_launch;
-    s.max_drift = max_drift;
-    s.q99_drift = q99_drift;
-    for (unsigned v : st) s.status |= v;
-    e->last = s;
-    e->last_samples_per_walker = steps - burn_in;
-    e->last_walker_std_error = 0.0;
-    if (e->W > 1) {  // independent chains: spread of the per-walker means
-        std::vector<double> we(e->W);
-        const int rc = vmc_get_walker_energies(e, we.data());
-        if (rc) return rc;
-        double mu = 0.0, v2 = 0.0;
-        for (double x : we) mu += x;
-        mu /= e->W;
-        for (double x : we) v2 += (x - mu) * (x - mu);
-        e->last_walker_std_error = std::sqrt(v2 / (e->W - 1) / e->W);
-    }
+    std::vector<double> sums;
+    const int frc = finish_sample(e, pass, &s, sums);
+    if (frc) return frc;
     if (out) *out = s;
     if (n_slots > 0) {
         // the MLP row: snapshot sums scaled to the window's sample count (one snapshot
@@ -970,57 +831,7 @@ int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy)
 int vmc_apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum,
                    const double *egrad_sum, vmc_averages *out)
 {
-    if (!e || !total || !grad_sum || !egrad_sum) return fail(VMC_E_ARG, "null argument");
-    const vmc_sums &s = *total;
-    if (!(s.n_samples > 0) || !(s.n_window > 0)) return fail(VMC_E_ARG, "empty totals");
-    // Sampler::computeAverages (sampler.cpp:194-226)
-    const double M = s.n_samples;
-    vmc_averages a{};
-    a.energy = s.energy / M;
-    a.kinetic = s.kinetic / M;
-    a.external = s.external / M;
-    a.interaction = s.interaction / M;
-    const double var = (s.energy2 / M - a.energy * a.energy) / M;
-    a.std_error = var > 0 ? std::sqrt(var) : 0.0;
-    a.acceptance = s.accepts / M;
-    a.walker_std_error = e->last_walker_std_error;
-    if (std::isnan(a.kinetic)) {
-        if (out) *out = a;
-        return fail(VMC_E_NAN, "Energy exploded, please decrease the learning rate");
-    }
-    // Optimization::getEnergyGradient (optimization.cpp:10-16)
-    const size_t P = e->theta.size();
-    std::vector<double> grad(P), delta(P);
-    for (size_t i = 0; i < P; ++i) {
-        const double dg = grad_sum[i] / s.n_window, dge = egrad_sum[i] / s.n_window;
-        grad[i] = 2.0 * (dge - a.energy * dg);
-    }
-    e->opt_step += 1;
-    const double eta = e->cfg.eta;
-    if (e->cfg.optimization == "adam") {  // adam.cpp:22-37
-        // compat: reference beta1 = 0.89 with moments started at ones (adam.cpp:35-36,
-        // adam.h:72); corrected: the standard method (beta1 = 0.9, moments from zero)
-        const double b1 = e->compat ? 0.89 : 0.9, b2 = 0.999, eps = 1e-8;
-        for (size_t i = 0; i < P; ++i) {
-            e->opt_m[i] = b1 * e->opt_m[i] + (1 - b1) * grad[i];
-            e->opt_v[i] = b2 * e->opt_v[i] + (1 - b2) * grad[i] * grad[i];
-            const double mh = e->opt_m[i] / (1 - std::pow(b1, e->opt_step));
-            const double vh = e->opt_v[i] / (1 - std::pow(b2, e->opt_step));
-            delta[i] = eta * mh / (std::sqrt(vh) + eps);
-        }
-    } else {  // gradientdescent.cpp:24-29, sgd.cpp:23-28
-        const double mono = 1.0 / std::pow((double)e->opt_step, e->cfg.opt_power);
-        for (size_t i = 0; i < P; ++i) {
-            e->opt_v[i] = e->cfg.opt_gamma * e->opt_v[i] + eta * grad[i] * mono;
-            delta[i] = e->opt_v[i];
-        }
-    }
-    std::vector<double> th(e->theta);
-    for (size_t i = 0; i < P; ++i) th[i] -= delta[i];  // system.cpp:114
-    const int rc = vmc_set_parameters(e, th.data(), e->E, e->Pmax);
-    if (rc) return rc;
-    if (out) *out = a;
-    return VMC_OK;
+    return apply_sums(e, total, grad_sum, egrad_sum, out, true);
 }
 
 int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out)
@@ -1046,6 +857,9 @@ int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)
         int rc = vmc_run_iteration(e, it, &a);
         if (history && it < n_history) history[it] = a;
         if (rc) return rc;
+        // checkpointing (system.cpp:116-118, sampler.cpp:507-515)
+        if (e->cfg.print_params && e->cfg.checkpoint_freq > 0 && it % e->cfg.checkpoint_freq == 0)
+            if ((rc = write_weights_file(e, e->cfg.path + "weights_" + std::to_string(it) + ".dat", 6))) return rc;
     }
     return VMC_OK;
 }
@@ -1275,3 +1089,172 @@ int vmc_measure_fma_peak(int device, int precision, double *tflops)
 }
 
 }  // extern "C"
+
+namespace vmc {
+
+HermiteCoef hermite_coefficients()
+{
+    HermiteCoef h;
+    for (int m = 0; m < HMAX; ++m) {
+        h.A[m] = std::sqrt(2.0 / (m + 1));
+        h.B[m] = std::sqrt((double)m / (m + 1));
+        h.C[m] = std::sqrt(2.0 * m);
+        h.E[m] = 2.0 * std::sqrt((double)m * (m - 1 > 0 ? m - 1 : 0));
+        h.Af[m] = (float)h.A[m];
+        h.Bf[m] = (float)h.B[m];
+        h.Cf[m] = (float)h.C[m];
+        h.Ef[m] = (float)h.E[m];
+    }
+    return h;
+}
+
+Params engine_params(const vmc_engine *e) { return make_params(e); }
+int upload_parameters(vmc_engine *e) { return upload_theta(e); }
+int engine_sweep_smem_per_warp(const vmc_engine *e) { return sweep_smem_per_warp(e); }
+int engine_rebuild_smem_per_warp(const vmc_engine *e) { return rebuild_smem_per_warp(e->N, e->dim, e->n_orb); }
+int engine_refresh(vmc_engine *e, double *drift) { return run_rebuild(e, RB_REFRESH, drift); }
+
+int set_parameters(vmc_engine *e, const double *theta, bool refresh)
+{
+    const double old_gamma = make_params(e).gamma;
+    e->theta.assign(theta, theta + (size_t)e->E * e->Pmax);
+    CUDA_TRY(cudaSetDevice(e->device));
+    if (e->have_walkers && (e->flags & Q_PADE_STALE)) {
+        // Pade pairs keep the gamma they were computed with until one of their
+        // particles moves (padejastrow.cpp:65-68 only stores gamma)
+        e->gamma_prev = old_gamma;
+        CUDA_TRY(cudaMemsetAsync(e->d_mask, 0, (size_t)e->W * e->N * sizeof(unsigned long long), e->stream));
+    } else {
+        e->gamma_prev = make_params(e).gamma;
+    }
+    int rc = upload_theta(e);
+    return rc ? rc : refresh ? refresh_all(e) : VMC_OK;
+}
+
+int apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum, const double *egrad_sum,
+               vmc_averages *out, bool refresh)
+{
+    if (!e || !total || !grad_sum || !egrad_sum) return fail(VMC_E_ARG, "null argument");
+    const vmc_sums &s = *total;
+    if (!(s.n_samples > 0) || !(s.n_window > 0)) return fail(VMC_E_ARG, "empty totals");
+    // Sampler::computeAverages (sampler.cpp:194-226)
+    const double M = s.n_samples;
+    vmc_averages a{};
+    a.energy = s.energy / M;
+    a.kinetic = s.kinetic / M;
+    a.external = s.external / M;
+    a.interaction = s.interaction / M;
+    const double var = (s.energy2 / M - a.energy * a.energy) / M;
+    a.std_error = var > 0 ? std::sqrt(var) : 0.0;
+    a.acceptance = s.accepts / M;
+    a.walker_std_error = e->last_walker_std_error;
+    if (std::isnan(a.kinetic)) {
+        if (out) *out = a;
+        return fail(VMC_E_NAN, "Energy exploded, please decrease the learning rate");
+    }
+    // Optimization::getEnergyGradient (optimization.cpp:10-16)
+    const size_t P = e->theta.size();
+    std::vector<double> grad(P), delta(P);
+    for (size_t i = 0; i < P; ++i) {
+        const double dg = grad_sum[i] / s.n_window, dge = egrad_sum[i] / s.n_window;
+        grad[i] = 2.0 * (dge - a.energy * dg);
+    }
+    e->opt_step += 1;
+    const double eta = e->cfg.eta;
+    if (e->cfg.optimization == "adam") {  // adam.cpp:22-37
+        // compat: reference beta1 = 0.89 with moments started at ones (adam.cpp:35-36,
+        // adam.h:72); corrected: the standard method (beta1 = 0.9, moments from zero)
+        const double b1 = e->compat ? 0.89 : 0.9, b2 = 0.999, eps = 1e-8;
+        for (size_t i = 0; i < P; ++i) {
+            e->opt_m[i] = b1 * e->opt_m[i] + (1 - b1) * grad[i];
+            e->opt_v[i] = b2 * e->opt_v[i] + (1 - b2) * grad[i] * grad[i];
+            const double mh = e->opt_m[i] / (1 - std::pow(b1, e->opt_step));
+            const double vh = e->opt_v[i] / (1 - std::pow(b2, e->opt_step));
+            delta[i] = eta * mh / (std::sqrt(vh) + eps);
+        }
+    } else {  // gradientdescent.cpp:24-29, sgd.cpp:23-28
+        const double mono = 1.0 / std::pow((double)e->opt_step, e->cfg.opt_power);
+        for (size_t i = 0; i < P; ++i) {
+            e->opt_v[i] = e->cfg.opt_gamma * e->opt_v[i] + eta * grad[i] * mono;
+            delta[i] = e->opt_v[i];
+        }
+    }
+    std::vector<double> th(e->theta);
+    for (size_t i = 0; i < P; ++i) th[i] -= delta[i];  // system.cpp:114
+    const int rc = set_parameters(e, th.data(), refresh);
+    if (rc) return rc;
+    if (out) *out = a;
+    return VMC_OK;
+}
+
+
+int finish_sample(vmc_engine *e, const SamplePass &p, vmc_sums *out, std::vector<double> &sums)
+{
+    const double *dev_sums = p.dev_sums;
+    sums.assign(e->nacc, 0.0);
+    if (e->general) {  // active parameters back to their (element, parameter) slots
+        std::copy(dev_sums, dev_sums + 9, sums.begin());
+        const size_t na = e->act.size();
+        for (size_t c = 0; c < na; ++c) {
+            sums[9 + e->act[c]] = dev_sums[9 + c];
+            sums[9 + e->EP + e->act[c]] = dev_sums[9 + na + c];
+        }
+    } else {
+        std::copy(dev_sums, dev_sums + e->nacc, sums.begin());
+    }
+    double max_drift = 0.0, q99_drift = 0.0;
+    if (p.drift && !p.drift->empty()) {
+        std::vector<double> &drift = *p.drift;
+        for (double d : drift) max_drift = std::max(max_drift, d);
+        const size_t i99 = (size_t)(0.99 * (drift.size() - 1));
+        std::nth_element(drift.begin(), drift.begin() + i99, drift.end());
+        q99_drift = drift[i99];
+    }
+    if (e->refresh_auto && p.n_refresh) {
+        // FP64 re-inversion cadence against the drift of the FP32 Sherman-Morrison
+        // inverse: the 99th percentile over walkers (the maximum is set by the few
+        // walkers sitting near a node of the determinant) halves the interval past
+        // the tolerance and doubles it below 1/2.5 of it (drift grows about in
+        // proportion to the interval, so a doubling stays under the tolerance)
+        if (q99_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
+        else if (q99_drift < e->drift_tol / 2.5) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
+    }
+    const double W = e->W;
+    vmc_sums s{};
+    s.energy = sums[0];
+    s.energy2 = sums[1];
+    s.kinetic = sums[2];
+    s.kinetic2 = sums[3];
+    s.external = sums[4];
+    s.external2 = sums[5];
+    s.interaction = sums[6];
+    s.interaction2 = sums[7];
+    s.accepts = sums[8];
+    s.n_samples = W * (p.steps - p.burn_in);
+    s.n_window = W * p.bs;
+    s.seconds = p.ms * 1e-3;
+    s.sweep_seconds = p.sweep_ms * 1e-3;
+    s.sweep_launches = p.n_launch;
+    s.max_drift = max_drift;
+    s.q99_drift = q99_drift;
+    s.status = p.status;
+    e->last = s;
+    e->last_samples_per_walker = p.steps - p.burn_in;
+    e->last_walker_std_error = 0.0;
+    if (p.walker_std_error >= 0.0) {
+        e->last_walker_std_error = p.walker_std_error;
+    } else if (e->W > 1) {  // independent chains: spread of the per-walker means
+        std::vector<double> we(e->W);
+        const int rc = vmc_get_walker_energies(e, we.data());
+        if (rc) return rc;
+        double mu = 0.0, v2 = 0.0;
+        for (double x : we) mu += x;
+        mu /= e->W;
+        for (double x : we) v2 += (x - mu) * (x - mu);
+        e->last_walker_std_error = std::sqrt(v2 / (e->W - 1) / e->W);
+    }
+    if (out) *out = s;
+    return VMC_OK;
+}
+
+}  // namespace vmc

@@ -1,0 +1,1204 @@
+// General walker path: every wave-function element of the reference on one FP64
+// warp-per-walker kernel family, for the systems the quantum-dot sweep does not
+// take: SimpleJastrow (simplejastrow.cpp), RBMGaussian (rbmgaussian.cpp),
+// RBMProduct (rbmproduct.cpp), and Slater determinants of hydrogen orbitals
+// (hydrogenorbital.cpp) or Hermite functions next to those elements.
+//
+// One warp owns one walker; its record lives in HBM (small systems: it stays in
+// L1/L2) and holds the positions, the importance-sampling force cache, the total
+// gradient of ln|Psi| at the current positions, the local-energy parts and the
+// parameter gradients at the current positions, and the transposed inverse of
+// each Slater block.  A proposal computes each element's |Psi'|^2/|Psi|^2 without
+// touching the record; an accepted move applies the Sherman-Morrison update to
+// the moved particle's block and re-evaluates the walker (gradients, Laplacians,
+// energies, parameter gradients) from its new positions, so rejected steps sample
+// the stored values.  Every parameter gradient is accumulated (nothing caps the
+// parameter count): lanes stride over the accumulators in HBM.
+//
+// Elements, Hamiltonians, samplers and the reference's quirks follow the CPU
+// restatement in oracle/vmc_oracle.c function for function (eval_impl,
+// ratio_impl, vmo_run).
+//
+// This header holds the path's device functions; vmc_general.cu has its kernels and
+// launchers, and the multi-system kernel (vmc_batch.cu) calls gen_sweep_walker.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include <cuda_bf16.h>
+
+#include "vmc_general.hpp"
+
+namespace vmc {
+
+namespace {
+
+
+constexpr int GEN_WPB = 4;     // walkers (warps) per CTA
+constexpr int GEN_SCR = 256;   // shared doubles per warp
+// shared scratch of a warp: orbital values at the proposal | moved row | RBM visible
+// (sorted) | RBM hidden p_j = 1/(1+e^v) | RBM hidden e^v/(1+e^v)
+constexpr int SCR_PHI = 0, SCR_ROW = 32, SCR_XS = 64, SCR_PN = 128, SCR_NN = 192;
+
+__device__ __forceinline__ double gen_dist(const double *x, int dim, int i, int j)
+{
+    double s = 0.0;
+    for (int c = 0; c < dim; ++c) {
+        const double t = x[i * dim + c] - x[j * dim + c];
+        s += t * t;
+    }
+    return sqrt(s);
+}
+
+__device__ __forceinline__ double gen_radius(const double *x, int dim, int i)
+{
+    double s = 0.0;
+    for (int c = 0; c < dim; ++c) s += x[i * dim + c] * x[i * dim + c];
+    return sqrt(s);
+}
+
+// h_m(x), h_m'(x), h_m''(x) of the normalised Hermite functions by the recurrence
+// h_{j+1} = A_j x h_j - B_j h_{j-1}; h_m' = C_m h_{m-1}, h_m'' = E_m h_{m-2}.
+__device__ __forceinline__ void herm3(int m, double x, double &h, double &h1, double &h2)
+{
+    double hm2 = 0.0, hm1 = 0.0, hc = 1.0;
+    for (int j = 0; j < m; ++j) {
+        const double nx = hA<double>(j) * x * hc - hB<double>(j) * hm1;
+        hm2 = hm1;
+        hm1 = hc;
+        hc = nx;
+    }
+    h = hc;
+    h1 = m >= 1 ? hC<double>(m) * hm1 : 0.0;
+    h2 = m >= 2 ? hE<double>(m) * hm2 : 0.0;
+}
+
+// Value, d/dx_c and d^2/dx_c^2 (c = 0..dim-1) of orbital o at point r.
+// Hermite: prod_c h_{m_c}(x_c) (basis.cpp:81-116, argument unscaled, hermite.h:8).
+// Hydrogen (3D, hydrogenorbital.cpp:108-394 with alpha = 1, k = Z): a polynomial
+// angular factor A (1 or one coordinate) times a radial factor
+// R(r) = f(r) exp(-k r / n); derivatives by the chain rule:
+//   d_i phi   = (d_i A) R + A R' x_i / r
+//   d_i^2 phi = 2 (d_i A) R' x_i / r + A (R'' x_i^2 / r^2 + R' (1/r - x_i^2 / r^3))
+__device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const double *r, double &v,
+                            double *d1, double *d2)
+{
+    if (g.basis == BASIS_HERMITE) {
+        double h[3], h1[3], h2[3];
+        for (int c = 0; c < dim; ++c) herm3(g.orb[o][c], r[c], h[c], h1[c], h2[c]);
+        v = 1.0;
+        for (int c = 0; c < dim; ++c) v *= h[c];
+        for (int c = 0; c < dim; ++c) {
+            double rest = 1.0;
+            for (int c2 = 0; c2 < dim; ++c2)
+                if (c2 != c) rest *= h[c2];
+            d1[c] = h1[c] * rest;
+            d2[c] = h2[c] * rest;
+        }
+        return;
+    }
+    const int nq = g.orb[o][0], l = g.orb[o][1], m = (int)g.orb[o][2] - 1;
+    const double k = Z;
+    const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    double f = 1.0, fp = 0.0, fpp = 0.0;
+    if (nq == 2 && l == 0) { f = 2.0 - k * rr; fp = -k; }
+    if (nq == 3 && l == 0) { f = 2.0 * k * k * rr * rr - 18.0 * k * rr + 27.0; fp = 4.0 * k * k * rr - 18.0 * k; fpp = 4.0 * k * k; }
+    if (nq == 3 && l == 1) { f = k * rr - 6.0; fp = k; }
+    const double a = k / nq, ex = exp(-a * rr);
+    const double R = f * ex, R1 = (fp - a * f) * ex, R2 = (fpp - 2.0 * a * fp + a * a * f) * ex;
+    const int ca = l == 1 ? (m == 1 ? 0 : m == -1 ? 1 : 2) : -1;  // m = 1: x, -1: y, 0: z
+    const double A = ca >= 0 ? r[ca] : 1.0;
+    v = A * R;
+    for (int c = 0; c < 3; ++c) {
+        const double xc = r[c], u = xc / rr, dA = (c == ca) ? 1.0 : 0.0;
+        d1[c] = dA * R + A * R1 * u;
+        d2[c] = 2.0 * dA * R1 * u + A * (R2 * u * u + R1 * (1.0 / rr - u * u / rr));
+        if (nq == 3 && g.horb3) {
+            // compat: the reference's n = 3 "second derivatives" (hydrogenorbital.cpp:351-364),
+            // which are not d^2/dx_c^2
+            const double kr = k * rr, pre = k * ex / (81.0 * rr * rr * rr);
+            d2[c] = l == 0 ? pre * (rr * rr * (2.0 * kr * (5.0 - 3.0 * kr) - 27.0) +
+                                    xc * xc * (kr * (2.0 * kr * (kr - 18.0) + 9.0) + 27.0))
+                           : pre * A * (kr - 18.0) * (kr - 6.0) / rr;
+        }
+    }
+}
+
+// RBMProduct visible vector: the coordinates, sorted ascending under the
+// reference's in-place sort (wavefunction.cpp:40-55; stable, as the oracle's
+// insertion sort), with coordinate k replaced by xk_new when k >= 0.
+__device__ void rbm_visible(const double *x, int D, int k, double xk_new, bool sort, double *xs, int lane)
+{
+    for (int i = lane; i < D; i += 32) {
+        const double xi = i == k ? xk_new : x[i];
+        int rank = i;
+        if (sort) {
+            rank = 0;
+            for (int j = 0; j < D; ++j) {
+                const double xj = j == k ? xk_new : x[j];
+                rank += (xj < xi) || (xj == xi && j < i);
+            }
+        }
+        xs[rank] = xi;
+    }
+    __syncwarp();
+}
+
+// hidden activations: v_j = b_j + sum_i W_ij xs_i / sigma^2 (rbmproduct.cpp:191-197),
+// p_j = 1 / (e^v + 1), n_j = e^v p_j into the scratch
+__device__ void rbm_hidden(const double *th, int D, int H, double s2, const double *xs, double *pn,
+                           double *nn, int lane)
+{
+    for (int j = lane; j < H; j += 32) {
+        double acc = 0.0;
+        for (int i = 0; i < D; ++i) acc += th[H + i + D * j] * xs[i];
+        const double v = th[j] + acc / s2, e = exp(v);
+        pn[j] = 1.0 / (e + 1.0);
+        nn[j] = e * pn[j];
+    }
+    __syncwarp();
+}
+
+// Pade-Jastrow gamma of pair (i, j): the previous gamma while the pair is stale
+__device__ __forceinline__ double pade_gamma(const Params &P, const unsigned long long *mask, int i, int j,
+                                             double gam)
+{
+    return ((P.flags & Q_PADE_STALE) && !((mask[i] >> j) & 1ull)) ? P.gamma_prev : gam;
+}
+
+__device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
+{
+    return same_spin(i, j, P.N) ? P.beta_same : P.beta_anti;
+}
+
+// ------------------------------------------------------------ MLP Jastrow
+// J = sum_{i<j} u(r_ij, s_ij) + sum_i chi(r_i) with
+//   u(r, s) = a_s r / (1 + r) + w3 . tanh(W2 tanh(W1 [r, s] + b1) + b2) + b3   (2 -> 64 -> 64 -> 1)
+//   chi(r)  = v3 . tanh(V2 tanh(V1 r + c1) + c2) + c3                        (1 -> 32 -> 32 -> 1)
+// evaluated in FP32 with the weights rounded to bfloat16; a_s is the Pade cusp
+// coefficient (s = 1 same spin).  Radial derivatives by forward-mode
+// differentiation: h' = (1 - h^2) z', h'' = (1 - h^2)(z'' - 2 h z'^2).
+// Shared-memory weight block of a CTA: the packed row, W2 transposed ([k][m]) and
+// V2 transposed, so that lanes over output units read consecutive words.
+constexpr int MLP_SMEM_FLOATS = MLP_PARAMS + 2 + MLP_H * MLP_H + MLP_G * MLP_G;  // 10692
+constexpr int MW_W2T = MLP_PARAMS + 2, MW_V2T = MW_W2T + MLP_H * MLP_H;
+constexpr int MLP_SMEM_DOUBLES = (MLP_SMEM_FLOATS + 3) / 4 * 2;  // 16-byte multiple
+
+__device__ __forceinline__ float mlp_tanh(float x)
+{
+    x = fminf(fmaxf(x, -9.0f), 9.0f);  // tanh(9) = 1 in FP32
+    return 1.0f - __fdividef(2.0f, __expf(2.0f * x) + 1.0f);
+}
+
+// Cooperative copy of the weights into shared memory (all threads of the CTA);
+// without w2t the W2-transposed region is left free (the tensor-core sweep uses it
+// as an operand tile).
+__device__ void mlp_stage(const float *__restrict__ src, float *w, bool w2t = true)
+{
+    for (int i = threadIdx.x; i < MLP_PARAMS; i += blockDim.x) w[i] = src[i];
+    for (int i = threadIdx.x; w2t && i < MLP_H * MLP_H; i += blockDim.x) {
+        const int k = i / MLP_H, m = i - k * MLP_H;
+        w[MW_W2T + i] = src[MW_W2 + m * MLP_H + k];
+    }
+    for (int i = threadIdx.x; i < MLP_G * MLP_G; i += blockDim.x) {
+        const int k = i / MLP_G, m = i - k * MLP_G;
+        w[MW_V2T + i] = src[MW_V2 + m * MLP_G + k];
+    }
+}
+
+__device__ __forceinline__ float mlp_cusp(int dim, bool same)
+{
+    return same ? (dim == 2 ? 1.0f / 3 : 0.25f) : (dim == 2 ? 1.0f : 0.5f);
+}
+
+// u, du/dr, d2u/dr2 of the pair network for one pair (one lane).
+__device__ void mlp_pair(const float *w, float r, float s, float a, float &u, float &du, float &ddu)
+{
+    float uo = w[MW_B3], duo = 0.0f, dduo = 0.0f;
+    for (int half = 0; half < 2; ++half) {
+        float z[32], dz[32], ddz[32];
+#pragma unroll
+        for (int m = 0; m < 32; ++m) {
+            z[m] = w[MW_B2 + half * 32 + m];
+            dz[m] = 0.0f;
+            ddz[m] = 0.0f;
+        }
+        for (int k = 0; k < MLP_H; ++k) {
+            const float w1r = w[MW_W1 + 2 * k], w1s = w[MW_W1 + 2 * k + 1];
+            const float h = mlp_tanh(fmaf(w1r, r, fmaf(w1s, s, w[MW_B1 + k])));
+            const float d = (1.0f - h * h) * w1r, dd = -2.0f * h * d * w1r;
+            const float4 *col = reinterpret_cast<const float4 *>(w + MW_W2T + k * MLP_H + half * 32);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 v = col[q];
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    z[4 * q + e] = fmaf(vv[e], h, z[4 * q + e]);
+                    dz[4 * q + e] = fmaf(vv[e], d, dz[4 * q + e]);
+                    ddz[4 * q + e] = fmaf(vv[e], dd, ddz[4 * q + e]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 32; ++m) {
+            const float h2 = mlp_tanh(z[m]), g2 = 1.0f - h2 * h2, w3 = w[MW_W3 + half * 32 + m];
+            uo = fmaf(w3, h2, uo);
+            duo = fmaf(w3, g2 * dz[m], duo);
+            dduo = fmaf(w3, g2 * (ddz[m] - 2.0f * h2 * dz[m] * dz[m]), dduo);
+        }
+    }
+    const float q = 1.0f / (1.0f + r);
+    u = uo + a * r * q;
+    du = duo + a * q * q;
+    ddu = dduo - 2.0f * a * q * q * q;
+}
+
+// chi, dchi/dr, d2chi/dr2 of the one-body network at r: warp-cooperative, lane m
+// is hidden unit m of the second layer; every lane returns the totals.
+__device__ void mlp_body(const float *w, float r, int lane, float &c, float &dc, float &ddc)
+{
+    float z = w[MW_C2 + lane], dz = 0.0f, ddz = 0.0f;
+    for (int k = 0; k < MLP_G; ++k) {
+        const float v1 = w[MW_V1 + k];
+        const float h = mlp_tanh(fmaf(v1, r, w[MW_C1 + k]));
+        const float d = (1.0f - h * h) * v1, dd = -2.0f * h * d * v1, vv = w[MW_V2T + k * MLP_G + lane];
+        z = fmaf(vv, h, z);
+        dz = fmaf(vv, d, dz);
+        ddz = fmaf(vv, dd, ddz);
+    }
+    const float h2 = mlp_tanh(z), g2 = 1.0f - h2 * h2, v3 = w[MW_V3 + lane];
+    c = warp_sum(v3 * h2) + w[MW_C3];
+    dc = warp_sum(v3 * g2 * dz);
+    ddc = warp_sum(v3 * g2 * (ddz - 2.0f * h2 * dz * dz));
+}
+
+// pair index q < N(N-1)/2 -> (i, j), i < j, row-major over i
+__device__ __forceinline__ void pair_of(int q, int N, int &i, int &j)
+{
+    i = 0;
+    while (q >= N - 1 - i) {
+        q -= N - 1 - i;
+        ++i;
+    }
+    j = i + 1 + q;
+}
+
+// Evaluate the walker at its positions (eval_impl): per-element gradient,
+// Laplacian and parameter gradient, the local-energy parts.  Writes the total
+// gradient, energies and parameter gradients into the record and, when given,
+// the per-element outputs of one walker (grad E x D, lap E, pgrad E x p_max,
+// energies 3).
+__device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, double *rec,
+                             const unsigned long long *mask, double *scr, int lane, double *o_grad,
+                             double *o_lap, double *o_pg, double *o_en, const float *mw = nullptr,
+                             bool full = true)
+{
+    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
+    const double *x = rec;
+    double *G = rec + g.off_g, *pg = rec + g.off_pg;
+    const double *inv = rec + g.off_inv;
+    for (int k = lane; k < D; k += 32) G[k] = 0.0;
+    // only the accumulated parameters are ever written (padding and the MLP row stay
+    // zero from the record's initialisation): clear those
+    for (int c = lane; c < g.n_act; c += 32) pg[g.act[c]] = 0.0;
+    __syncwarp();
+    double lap_total = 0.0;
+    for (int e = 0; e < E; ++e) {
+        const double *th = g.theta + (size_t)e * PM;
+        double *pge = pg + (size_t)e * PM;
+        double lap_l = 0.0, lap_u = 0.0;  // lane partial, uniform part
+        double *oge = o_grad ? o_grad + (size_t)e * D : nullptr;
+        switch (P.elem_kind[e]) {
+        case 0: {  // Gaussian (gaussian.cpp:62-78)
+            const double wa = P.omega * th[0];
+            double x2 = 0.0;
+            for (int k = lane; k < D; k += 32) {
+                const double gk = -wa * x[k];
+                G[k] += gk;
+                if (oge) oge[k] = gk;
+                x2 += x[k] * x[k];
+            }
+            x2 = warp_sum(x2);
+            lap_u = -wa * D;
+            if (lane == 0) pge[0] = -0.5 * P.omega * x2;
+            break;
+        }
+        case 1: {  // Slater determinant (slaterdeterminant.cpp:155-191)
+            const int n = g.n;
+            for (int q = lane; q < N; q += 32) {
+                const int b = q / n, il = q - b * n;
+                const double *row = inv + (size_t)(b * n + il) * n;
+                double dd[3] = {0.0, 0.0, 0.0}, sdd[3] = {0.0, 0.0, 0.0};
+                for (int o = 0; o < n; ++o) {
+                    double v, d1[3], d2[3];
+                    gen_orbital(g, dim, P.Z, o, x + q * dim, v, d1, d2);
+                    for (int c = 0; c < dim; ++c) {
+                        dd[c] += d1[c] * row[o];
+                        sdd[c] += d2[c] * row[o];
+                    }
+                }
+                for (int c = 0; c < dim; ++c) {
+                    G[q * dim + c] += dd[c];
+                    if (oge) oge[q * dim + c] = dd[c];
+                    lap_l += sdd[c] - dd[c] * dd[c];
+                }
+            }
+            break;
+        }
+        case 2: {  // Pade-Jastrow (padejastrow.cpp:75-116)
+            const double gam = th[0];
+            double dg = 0.0;
+            for (int i = lane; i < N; i += 32) {
+                double gi[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < N; ++j) {
+                    if (j == i) continue;
+                    const int lo = min(i, j), hi = max(i, j);
+                    const double r = gen_dist(x, dim, i, j), beta = pade_beta_of(P, i, j);
+                    const double gp = pade_gamma(P, mask, lo, hi, gam);
+                    const double f1 = 1.0 / (1.0 + gp * r), f = beta * f1 * f1, h = r * f1;
+                    double c2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        const double cc = (x[i * dim + c] - x[j * dim + c]) / r;
+                        gi[c] += f * cc;
+                        c2 += 2.0 * f * (1.0 - (1.0 + 2.0 * gam * h) * cc * cc) / r;
+                    }
+                    if (j > i) {
+                        lap_l += c2;
+                        dg += beta * h * h;
+                    }
+                }
+                for (int c = 0; c < dim; ++c) {
+                    G[i * dim + c] += gi[c];
+                    if (oge) oge[i * dim + c] = gi[c];
+                }
+            }
+            dg = warp_sum(dg);
+            if (lane == 0) pge[0] = (P.flags & Q_PADE_DGAMMA) ? -0.5 * dg : -dg;
+            break;
+        }
+        case 3: {  // SimpleJastrow (simplejastrow.cpp:67-111)
+            for (int i = lane; i < N; i += 32) {
+                double gi[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < N; ++j) {
+                    if (j == i) continue;
+                    const int lo = min(i, j), hi = max(i, j);
+                    const double r = gen_dist(x, dim, i, j), beta = th[lo + N * hi];
+                    double c2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        const double cc = (x[i * dim + c] - x[j * dim + c]) / r;
+                        gi[c] += beta * cc;
+                        c2 += 2.0 * beta * (1.0 - cc * cc) / r;
+                    }
+                    if (j > i) {
+                        lap_l += c2;
+                        pge[i + N * j] = r;
+                    }
+                }
+                for (int c = 0; c < dim; ++c) {
+                    G[i * dim + c] += gi[c];
+                    if (oge) oge[i * dim + c] = gi[c];
+                }
+            }
+            break;
+        }
+        case 4: {  // RBMGaussian (rbmgaussian.cpp:67-87)
+            const double s2 = g.sigma * g.sigma;
+            for (int k = lane; k < D; k += 32) {
+                const double t = (x[k] - th[k]) / s2;
+                G[k] += -t;
+                if (oge) oge[k] = -t;
+                pge[k] = t;
+            }
+            lap_u = -D / s2;
+            break;
+        }
+        case 5: {  // RBMProduct (rbmproduct.cpp:167-189)
+            const int H = g.hidden;
+            const double s2 = 100.0 * g.sigma * g.sigma, s4 = s2 * s2;
+            double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
+            rbm_visible(x, D, -1, 0.0, P.flags & Q_RBM_SORT, xs, lane);
+            rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
+            for (int k = lane; k < D; k += 32) {
+                double acc = 0.0, acc2 = 0.0;
+                for (int j = 0; j < H; ++j) {
+                    const double w = th[H + k + D * j];
+                    acc += w * nn[j];
+                    acc2 += w * w * pn[j] * nn[j];
+                }
+                G[k] += acc / s2;
+                if (oge) oge[k] = acc / s2;
+                lap_l += acc2 / s4;
+            }
+            for (int t = lane; t < H * (D + 1); t += 32) {
+                if (t < H) pge[t] = nn[t];
+                else {
+                    const int j = (t - H) / D, i = (t - H) - j * D;
+                    pge[H + i + D * j] = xs[i] * nn[j];
+                }
+            }
+            break;
+        }
+        case 7: {  // MLP Jastrow: caches of (u, u', u'') per pair and (chi, chi', chi'') per particle
+            double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
+            if (full) {  // from scratch (initialisation, parameter update, evaluation)
+                const int npair = N * (N - 1) / 2;
+                for (int q = lane; q < npair; q += 32) {
+                    int i, j;
+                    pair_of(q, N, i, j);
+                    const bool same = same_spin(i, j, N);
+                    float u, du, ddu;
+                    mlp_pair(mw, (float)gen_dist(x, dim, i, j), same ? 1.0f : 0.0f, mlp_cusp(dim, same), u, du, ddu);
+                    double *c3 = uc + (size_t)(i * N + j) * 3;
+                    c3[0] = u;
+                    c3[1] = du;
+                    c3[2] = ddu;
+                }
+                for (int i = 0; i < N; ++i) {
+                    float c, dc, ddc;
+                    mlp_body(mw, (float)gen_radius(x, dim, i), lane, c, dc, ddc);
+                    if (lane == 0) {
+                        oc[i * 3] = c;
+                        oc[i * 3 + 1] = dc;
+                        oc[i * 3 + 2] = ddc;
+                    }
+                }
+                __syncwarp();
+            }
+            // from the caches in FP32 (the network values are FP32 already)
+            for (int i = lane; i < N; i += 32) {
+                float gi[3] = {0.0f, 0.0f, 0.0f}, li = 0.0f, xi[3];
+                for (int c = 0; c < dim; ++c) xi[c] = (float)x[i * dim + c];
+                for (int j = 0; j < N; ++j) {
+                    if (j == i) continue;
+                    const int lo = min(i, j), hi = max(i, j);
+                    const double *c3 = uc + (size_t)(lo * N + hi) * 3;
+                    float dv[3], r2 = 0.0f;
+                    for (int c = 0; c < dim; ++c) {
+                        dv[c] = xi[c] - (float)x[j * dim + c];
+                        r2 += dv[c] * dv[c];
+                    }
+                    const float ir = rsqrtf(r2), du = (float)c3[1];
+                    for (int c = 0; c < dim; ++c) gi[c] += du * dv[c] * ir;
+                    if (j > i) li += 2.0f * ((float)c3[2] + (dim - 1) * du * ir);
+                }
+                float r2i = 0.0f;
+                for (int c = 0; c < dim; ++c) r2i += xi[c] * xi[c];
+                const float iri = rsqrtf(r2i), dc = (float)oc[i * 3 + 1];
+                for (int c = 0; c < dim; ++c) gi[c] += dc * xi[c] * iri;
+                lap_l += (double)li + oc[i * 3 + 2] + (dim - 1) * dc * iri;
+                for (int c = 0; c < dim; ++c) {
+                    G[i * dim + c] += gi[c];
+                    if (oge) oge[i * dim + c] = gi[c];
+                }
+            }
+            break;  // parameter gradients: mlp_grad_kernel, from snapshots
+        }
+        case 6: {  // HydrogenLike (hydrogenlike.cpp:268-286)
+            const double az = th[0] * P.Z;
+            double rs = 0.0;
+            for (int i = lane; i < N; i += 32) {
+                const double r = gen_radius(x, dim, i);
+                rs += r;
+                for (int c = 0; c < dim; ++c) {
+                    const double gk = -az * x[i * dim + c] / r;
+                    G[i * dim + c] += gk;
+                    if (oge) oge[i * dim + c] = gk;
+                }
+                lap_l -= 2.0 / r;
+            }
+            rs = warp_sum(rs);
+            lap_l *= az;
+            if (lane == 0) pge[0] = -P.Z * rs;
+            break;
+        }
+        default: break;
+        }
+        __syncwarp();
+        const double lap_e = warp_sum(lap_l) + lap_u;
+        lap_total += lap_e;
+        if (o_lap && lane == 0) o_lap[e] = lap_e;
+    }
+    // System::getKineticEnergy (elementoperation.cpp:95-109) and the potentials
+    double g2 = 0.0, vx = 0.0, vi = 0.0;
+    for (int k = lane; k < D; k += 32) g2 += G[k] * G[k];
+    if (P.flags & F_ATOM) {
+        for (int i = lane; i < N; i += 32) vx += 1.0 / gen_radius(x, dim, i);
+    } else {
+        for (int k = lane; k < D; k += 32) vx += x[k] * x[k];
+    }
+    if (P.flags & F_COULOMB)
+        for (int i = lane; i < N; i += 32)
+            for (int j = i + 1; j < N; ++j) {
+                double r2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = x[i * dim + c] - x[j * dim + c];
+                    r2 += t * t;
+                }
+                vi += rsqrt(r2);
+            }
+    g2 = warp_sum(g2);
+    vx = warp_sum(vx);
+    vi = warp_sum(vi);
+    const double ekin = -0.5 * (lap_total + g2);
+    const double vext = (P.flags & F_ATOM) ? -P.Z * vx : 0.5 * P.omega * P.omega * vx;
+    double *en = rec + g.off_en;
+    if (lane == 0) {
+        en[0] = ekin;
+        en[1] = vext;
+        en[2] = vi;
+    }
+    if (o_pg)
+        for (int j = lane; j < g.EP; j += 32) o_pg[j] = pg[j];
+    if (o_en && lane == 0) {
+        o_en[0] = ekin;
+        o_en[1] = vext;
+        o_en[2] = vi;
+    }
+    __syncwarp();
+}
+
+// Element ratios |Psi(y)|^2 / |Psi(x)|^2 for coordinate k moved to xn (ratio_impl)
+// and, when grad_y is given, d ln Psi / d y_k at the proposal (the corrected
+// Fokker-Planck Green's ratio).  Orbital values at the proposal go to the scratch
+// (the Sherman-Morrison update reuses them).  Returns the product in element order.
+__device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const double *rec,
+                             const unsigned long long *mask, double *scr, int lane, int k, double xn,
+                             double *ratios, double *grad_y, double &R_out, const float *mw = nullptr,
+                             const float *pre = nullptr)
+{
+    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
+    const double *x = rec;
+    const int p = k / dim, adim = k - p * dim;
+    double yp[3];
+    for (int c = 0; c < dim; ++c) yp[c] = c == adim ? xn : x[p * dim + c];
+    const double xo = x[k];
+    double prob = 1.0, gy = 0.0;
+    R_out = 1.0;
+    for (int e = 0; e < E; ++e) {
+        const double *th = g.theta + (size_t)e * PM;
+        double r = 1.0;
+        switch (P.elem_kind[e]) {
+        case 0:  // gaussian.cpp:23-28
+            r = exp(P.omega * th[0] * (xo * xo - xn * xn));
+            gy += -P.omega * th[0] * xn;
+            break;
+        case 1: {  // slaterdeterminant.cpp:150-153, 177-180
+            const int n = g.n, b = p / n, pl = p - b * n;
+            double s = 0.0, sg = 0.0;
+            if (lane < n) {
+                double v, d1[3], d2[3];
+                gen_orbital(g, dim, P.Z, lane, yp, v, d1, d2);
+                scr[SCR_PHI + lane] = v;
+                const double iv = rec[g.off_inv + (size_t)(b * n + pl) * n + lane];
+                s = v * iv;
+                sg = d1[adim] * iv;
+            }
+            const double R = warp_sum(s);
+            R_out = R;
+            r = R * R;
+            if (grad_y) gy += warp_sum(sg) / R;
+            __syncwarp();
+            break;
+        }
+        case 2: {  // padejastrow.cpp:211-218
+            const double gam = th[0];
+            const int j0 = (P.flags & Q_PADE_RATIO) ? p + 1 : 0;
+            double acc = 0.0, gyl = 0.0;
+            for (int j = lane; j < N; j += 32) {
+                if (j == p) continue;
+                const int lo = min(p, j), hi = max(p, j);
+                double rn2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[j * dim + c];
+                    rn2 += t * t;
+                }
+                const double ro = gen_dist(x, dim, p, j), rn = sqrt(rn2), beta = pade_beta_of(P, p, j);
+                const double gp = pade_gamma(P, mask, lo, hi, gam);
+                if (j >= j0) acc += beta * (rn / (1.0 + gam * rn) - ro / (1.0 + gp * ro));
+                const double f1 = 1.0 / (1.0 + gam * rn);
+                gyl += beta * f1 * f1 * (yp[adim] - x[j * dim + adim]) / rn;
+            }
+            acc = warp_sum(acc);
+            r = exp(2.0 * acc);
+            if (grad_y) gy += warp_sum(gyl);
+            break;
+        }
+        case 3: {  // simplejastrow.cpp:145-156
+            const int j0 = (P.flags & Q_SJ_RATIO) ? p + 1 : 0;
+            double acc = 0.0, gyl = 0.0;
+            for (int j = lane; j < N; j += 32) {
+                if (j == p) continue;
+                const int lo = min(p, j), hi = max(p, j);
+                double rn2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[j * dim + c];
+                    rn2 += t * t;
+                }
+                const double rn = sqrt(rn2), beta = th[lo + N * hi];
+                if (j >= j0) acc += beta * (rn - gen_dist(x, dim, p, j));
+                gyl += beta * (yp[adim] - x[j * dim + adim]) / rn;
+            }
+            acc = warp_sum(acc);
+            r = exp(2.0 * acc);
+            if (grad_y) gy += warp_sum(gyl);
+            break;
+        }
+        case 4: {  // rbmgaussian.cpp:34-46
+            const double s2 = g.sigma * g.sigma, a = xo - th[k], bn = xn - th[k];
+            r = exp((a * a - bn * bn) / (2.0 * s2));
+            gy += -bn / s2;
+            break;
+        }
+        case 5: {  // rbmproduct.cpp:199-203
+            const int H = g.hidden;
+            const double s2 = 100.0 * g.sigma * g.sigma;
+            double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
+            const bool sort = P.flags & Q_RBM_SORT;
+            rbm_visible(x, D, -1, 0.0, sort, xs, lane);
+            rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
+            double po[2] = {1.0, 1.0};
+            for (int t = 0; t < 2; ++t) {
+                const int j = lane + 32 * t;
+                if (j < H) po[t] = pn[j];
+            }
+            __syncwarp();
+            rbm_visible(x, D, k, xn, sort, xs, lane);
+            rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
+            double prod = 1.0, gyl = 0.0;
+            for (int t = 0; t < 2; ++t) {
+                const int j = lane + 32 * t;
+                if (j < H) {
+                    prod *= po[t] / pn[j];
+                    gyl += th[H + k + D * j] * nn[j];
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) prod *= __shfl_xor_sync(FULL, prod, o);
+            r = prod * prod;
+            if (grad_y) gy += warp_sum(gyl) / s2;
+            __syncwarp();
+            break;
+        }
+        case 7: {  // MLP Jastrow: exp(2 (J(y) - J(x))); the new pair and one-body values
+                   // go to the scratch for an accepted move
+            const double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
+            double acc = 0.0, gyl = 0.0;
+            for (int j = lane; j < N; j += 32) {
+                if (j == p) continue;
+                double rn2 = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[j * dim + c];
+                    rn2 += t * t;
+                }
+                const double rn = sqrt(rn2);
+                const bool same = same_spin(p, j, N);
+                float u, du, ddu;
+                if (pre) {  // from the tensor-core pass of this step (lane j = partner j)
+                    u = pre[j];
+                    du = pre[32 + j];
+                    ddu = pre[64 + j];
+                } else {
+                    mlp_pair(mw, (float)rn, same ? 1.0f : 0.0f, mlp_cusp(dim, same), u, du, ddu);
+                }
+                scr[SCR_XS + j] = u;
+                scr[SCR_XS + 32 + j] = du;
+                scr[SCR_PN + j] = ddu;
+                acc += (double)u - uc[(size_t)(min(p, j) * N + max(p, j)) * 3];
+                gyl += du * (float)(yp[adim] - x[j * dim + adim]) * (float)(1.0 / rn);
+            }
+            double rp2 = 0.0;
+            for (int c = 0; c < dim; ++c) rp2 += yp[c] * yp[c];
+            const double rp = sqrt(rp2);
+            float cn, dcn, ddcn;
+            mlp_body(mw, (float)rp, lane, cn, dcn, ddcn);
+            if (lane == 0) {
+                scr[SCR_PN + 32] = cn;
+                scr[SCR_PN + 33] = dcn;
+                scr[SCR_PN + 34] = ddcn;
+            }
+            const double dj = warp_sum(acc) + ((double)cn - oc[p * 3]);
+            r = exp(2.0 * dj);
+            if (grad_y) gy += warp_sum(gyl) + dcn * yp[adim] / rp;
+            __syncwarp();
+            break;
+        }
+        case 6: {  // hydrogenlike.cpp:231-242
+            double rn2 = 0.0;
+            for (int c = 0; c < dim; ++c) rn2 += yp[c] * yp[c];
+            const double rn = sqrt(rn2);
+            r = exp(2.0 * P.Z * th[0] * (gen_radius(x, dim, p) - rn));
+            gy += -th[0] * P.Z * xn / rn;
+            break;
+        }
+        default: break;
+        }
+        if (ratios) ratios[e] = r;
+        prob *= r;  // elementoperation.cpp:80-87
+    }
+    if (grad_y) *grad_y = gy;
+    return prob;
+}
+
+// Transposed inverse of both Slater blocks by Gauss-Jordan elimination with
+// partial pivoting on [A | I] in shared memory (n <= 32); row i of block b holds
+// A^{-1}(o, i) over orbitals o.  Returns the warp's singular flag.
+__device__ unsigned gen_invert(const Params &P, const GenParams &g, int dim, double *rec, double *M,
+                               int lane)
+{
+    const int n = g.n, w2 = 2 * n;
+    unsigned status = 0;
+    for (int b = 0; b < 2; ++b) {
+        for (int i = 0; i < n; ++i)
+            for (int c = lane; c < w2; c += 32) M[i * w2 + c] = c >= n ? (c - n == i ? 1.0 : 0.0) : 0.0;
+        __syncwarp();
+        if (lane < n)
+            for (int i = 0; i < n; ++i) {
+                double v, d1[3], d2[3];
+                gen_orbital(g, dim, P.Z, lane, rec + (b * n + i) * dim, v, d1, d2);
+                M[i * w2 + lane] = v;  // A[i][o] = phi_o(r_i)
+            }
+        __syncwarp();
+        for (int c = 0; c < n; ++c) {
+            double v = (lane >= c && lane < n) ? fabs(M[lane * w2 + c]) : -1.0;
+            int idx = lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v2 = __shfl_xor_sync(FULL, v, o);
+                const int i2 = __shfl_xor_sync(FULL, idx, o);
+                if (v2 > v || (v2 == v && i2 < idx)) { v = v2; idx = i2; }
+            }
+            if (!(v > 0.0)) status |= ST_SINGULAR;
+            const int pr = idx < n ? idx : c;
+            if (pr != c)
+                for (int col = lane; col < w2; col += 32) {
+                    const double t = M[c * w2 + col];
+                    M[c * w2 + col] = M[pr * w2 + col];
+                    M[pr * w2 + col] = t;
+                }
+            __syncwarp();
+            const double ip = 1.0 / M[c * w2 + c];
+            __syncwarp();
+            for (int col = lane; col < w2; col += 32) M[c * w2 + col] *= ip;
+            __syncwarp();
+            for (int r = 0; r < n; ++r) {
+                if (r == c) continue;
+                const double f = M[r * w2 + c];
+                __syncwarp();
+                for (int col = lane; col < w2; col += 32) M[r * w2 + col] -= f * M[c * w2 + col];
+                __syncwarp();
+            }
+        }
+        // A^{-1}(o, i) = M[o][n + i]
+        for (int i = 0; i < n; ++i)
+            for (int o = lane; o < n; o += 32) rec[g.off_inv + (size_t)(b * n + i) * n + o] = M[o * w2 + n + i];
+        __syncwarp();
+    }
+    return status;
+}
+
+// ------------------------------------------------------------ MLP second layer on tcgen05
+// During a sweep the CTA's four walkers move in lockstep; the partners of the four
+// proposals fill one 128-row tile (warp w: rows 32 w .. 32 w + 31, lane = partner).
+// First layer and its radial derivatives (CUDA cores) go to three A tiles in
+// bfloat16 (the values as a high and a low bfloat16 part, about 16 significant
+// bits); z2 = W2 h1 and its two radial derivatives are M = 128, N = 64, K = 64
+// products on the 5th-generation tensor cores (kind::f16, BF16 in, FP32 accumulate
+// in tensor memory), issued by one thread; each lane then reads its row back
+// (tcgen05.ld) and finishes the third layer.
+// Shared-memory operands are K-major without swizzle: 8-row x 16-byte core
+// matrices, offset(row, k) = (row % 8) 16 + (row / 8) 1024 + (k / 8) 128 + (k % 8) 2,
+// so the two K chunks of a K = 16 step are 128 bytes apart (leading byte offset)
+// and 8-row groups 1024 bytes apart (stride byte offset).  Tensor memory holds D
+// for order o (value, d/dr, d2/dr2) in columns [64 o, 64 o + 64); lane = tile row.
+constexpr int TC_COLS = 256;  // TMEM columns per CTA (192 used); two CTAs per SM fit 512
+constexpr int TC_A_BYTES = 128 * MLP_H * 2, TC_B_BYTES = MLP_H * MLP_H * 2;
+constexpr int TC_SMEM = 3 * TC_A_BYTES + TC_B_BYTES + 1024;  // with alignment slack
+constexpr long TC_WAIT_LIMIT = 1L << 24;                     // bounded completion wait
+// kind::f16 instruction word: D F32 (bits 4-5), A and B BF16 (7-9, 10-12), both
+// K-major, N / 8 (17-22), M / 16 (24-28)
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+struct TcMlp {
+    unsigned char *a[4];  // A tiles: value (high bfloat16 part), d/dr, d2/dr2, value (low part)
+    uint32_t a_s[4], b_s; // their shared-window addresses, and B's
+    uint32_t bar;         // completion mbarrier
+    uint32_t tmem;        // TMEM base address (lane 0, first allocated column)
+    uint32_t phase;
+};
+
+__device__ __forceinline__ uint32_t tc_off(int row, int k)
+{
+    return (row & 7) * 16 + (row >> 3) * 1024 + (k >> 3) * 128 + (k & 7) * 2;
+}
+
+// shared-memory matrix descriptor: start address, LBO 128 B, SBO 1024 B, version 1,
+// base offset 0, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                   "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                   "=r"(v[14]), "=r"(v[15])
+                 : "r"(addr));
+}
+
+// Tiles after the weights, B = W2 ([out n][in k]; the weights are bfloat16 values
+// already), the mbarrier, and the TMEM allocation (warp 0).  The caller synchronises
+// the CTA and then calls tc_ready.
+__device__ void tc_setup(TcMlp &t, unsigned char *base, float *w, const float *__restrict__ src,
+                         unsigned long long *bar, uint32_t *slot, int wib)
+{
+    unsigned char *p = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(base) + 1023) & ~uintptr_t(1023));
+    for (int o = 0; o < 3; ++o) {
+        t.a[o] = p + o * TC_A_BYTES;
+        t.a_s[o] = (uint32_t)__cvta_generic_to_shared(t.a[o]);
+    }
+    t.a[3] = reinterpret_cast<unsigned char *>(w + MW_W2T);  // 16 KB, 16-byte aligned
+    t.a_s[3] = (uint32_t)__cvta_generic_to_shared(t.a[3]);
+    unsigned char *bt = p + 3 * TC_A_BYTES;
+    t.b_s = (uint32_t)__cvta_generic_to_shared(bt);
+    for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
+        const int n = i >> 6, k = i & 63;
+        *reinterpret_cast<__nv_bfloat16 *>(bt + tc_off(n, k)) = __float2bfloat16_rn(src[MW_W2 + n * MLP_H + k]);
+    }
+    t.bar = (uint32_t)__cvta_generic_to_shared(bar);
+    t.phase = 0;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t.bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (wib == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(slot)),
+                     "r"(TC_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_ready(TcMlp &t, const uint32_t *slot)
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    t.tmem = *slot;
+}
+
+// One step of the pair network's second layer for the whole CTA (every thread
+// calls it).  valid: this lane's row is a partner of its walker's proposal at
+// distance r, same-spin s, cusp coefficient a.  Writes u, du/dr, d2u/dr2 of the
+// row to pre[lane], pre[32 + lane], pre[64 + lane]; returns ST_TC_TIMEOUT when the
+// completion wait gave up.
+__device__ unsigned tc_pair_layer(TcMlp &t, const float *w, bool valid, float r, float s, float a, int lane,
+                                  int wib, float *pre)
+{
+    const int row = wib * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < 8; ++c) {  // 8 inputs of the second layer per 16-byte store
+        uint32_t hv[4], lv[4], dv[4], ddv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float h[2], d[2], dd[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int k = 8 * c + 2 * e + q;
+                const float w1r = w[MW_W1 + 2 * k], w1s = w[MW_W1 + 2 * k + 1];
+                const float hh = valid ? mlp_tanh(fmaf(w1r, r, fmaf(w1s, s, w[MW_B1 + k]))) : 0.0f;
+                h[q] = hh;
+                d[q] = valid ? (1.0f - hh * hh) * w1r : 0.0f;
+                dd[q] = -2.0f * hh * d[q] * w1r;
+            }
+            // value: high and low bfloat16 parts (about 16 significant bits together)
+            hv[e] = pack_bf16(h[0], h[1]);
+            const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&hv[e]);
+            lv[e] = pack_bf16(h[0] - __bfloat162float(hi.x), h[1] - __bfloat162float(hi.y));
+            dv[e] = pack_bf16(d[0], d[1]);
+            ddv[e] = pack_bf16(dd[0], dd[1]);
+        }
+        const uint32_t off = tc_off(row, 8 * c);
+        *reinterpret_cast<uint4 *>(t.a[0] + off) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<uint4 *>(t.a[1] + off) = make_uint4(dv[0], dv[1], dv[2], dv[3]);
+        *reinterpret_cast<uint4 *>(t.a[2] + off) = make_uint4(ddv[0], ddv[1], ddv[2], ddv[3]);
+        *reinterpret_cast<uint4 *>(t.a[3] + off) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+    }
+    // generic-proxy tile writes visible to the tensor cores; earlier TMEM reads done
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int o = 0; o < 4; ++o)  // value high, d/dr, d2/dr2, then value low into the value columns
+#pragma unroll
+            for (int st = 0; st < 4; ++st) {
+                const uint64_t ad = tc_desc(t.a_s[o] + st * 256), bd = tc_desc(t.b_s + st * 256);
+                const uint32_t dcol = t.tmem + 64 * (o == 3 ? 0 : o);
+                const uint32_t accumulate = (st > 0 || o == 3) ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                 dcol),
+                             "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+                             : "memory");
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(t.bar)
+                     : "memory");
+    }
+    uint32_t done = 0;
+    for (long it = 0; it < TC_WAIT_LIMIT && !done; ++it)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(t.bar), "r"(t.phase)
+                     : "memory");
+    t.phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float u = w[MW_B3], du = 0.0f, ddu = 0.0f;
+    const uint32_t lb = t.tmem + ((uint32_t)(wib * 32) << 16);
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+        uint32_t z[16], dz[16], ddz[16];
+        tmem_ld16(lb + 16 * c, z);
+        tmem_ld16(lb + 64 + 16 * c, dz);
+        tmem_ld16(lb + 128 + 16 * c, ddz);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            const int m = 16 * c + e;
+            const float zz = __uint_as_float(z[e]) + w[MW_B2 + m], d1 = __uint_as_float(dz[e]),
+                        d2 = __uint_as_float(ddz[e]);
+            const float h2 = mlp_tanh(zz), g2 = 1.0f - h2 * h2, w3 = w[MW_W3 + m];
+            u = fmaf(w3, h2, u);
+            du = fmaf(w3, g2 * d1, du);
+            ddu = fmaf(w3, g2 * (d2 - 2.0f * h2 * d1 * d1), ddu);
+        }
+    }
+    const float q = 1.0f / (1.0f + r);
+    pre[lane] = u + a * r * q;
+    pre[32 + lane] = du + a * q * q;
+    pre[64 + lane] = ddu - 2.0f * a * q * q * q;
+    __syncwarp();
+    return done ? 0u : (unsigned)ST_TC_TIMEOUT;
+}
+
+__device__ void tc_teardown(TcMlp &t, int wib)
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (wib == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(TC_COLS) : "memory");
+}
+
+// Steps step_offset .. step_offset + steps - 1 of walker w by the calling warp.  scr: the warp's
+// GEN_SCR shared doubles; mw: the CTA's staged MLP weights or null; with TC the
+// CTA's four warps run in lockstep (inactive ones join the tensor-core steps).
+template <bool TC>
+__device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, int step_offset, const GenParams &g,
+                                                 int w, bool active, double *scr, float *mw, TcMlp &tc, float *pre_w)
+{
+    const Params &P = a.P;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+
+    const int N = P.N, D = g.D, dim = D / N;
+    const int ws = active ? w : 0;  // record pointers of a warp without a walker are never used
+    double *rec = reinterpret_cast<double *>(P.state) + (size_t)ws * g.rec;
+    double *x = rec, *fc = rec + g.off_fc;
+    unsigned long long *mask = P.mask + (size_t)ws * N;
+    double *acc = P.acc + (size_t)ws * P.nacc * 2;
+    unsigned long long ctr = active ? P.counter[ws] : 0ull;
+    unsigned status = 0;
+    const bool is = P.sampling == SAMPLER_IS;
+    const double dt = P.step, sqdt = sqrt(P.step);
+
+    for (int s = 0; s < steps; ++s) {
+        const int it_step = step_offset + s;
+        int k = 0;
+        double r1 = 0.0, r2 = 0.0, xo = 0.0, dx = 0.0, fn = 0.0, xn = 0.0;
+        if (active) {
+            // ---- random numbers (vmo_step_randoms) or the caller's
+            k = 0;
+            r1 = r2 = 0.0;
+            if (a.probe_k) {
+                k = a.probe_k[w];
+                r1 = 0.0;
+                r2 = 0.0;
+            } else if (a.replay) {
+                const double *q = a.replay + ((size_t)w * a.replay_stride + a.replay_offset + it_step) * 3;
+                k = (int)floor(q[0] * D);
+                r1 = q[1];
+                r2 = q[2];
+            } else {
+                const uint4 v = philox(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)w, 0u),
+                                       make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
+                ++ctr;
+                k = (int)__umulhi(v.x, (unsigned)D);
+                if (is) {
+                    const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
+                    r1 = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+                } else {
+                    r1 = v.y * TWO_M32;
+                }
+                r2 = v.w * TWO_M32;
+            }
+            // ---- proposal (importancesampling.cpp:49-60, bruteforce.cpp:34)
+            xo = x[k];
+            fn = 0.0;
+            if (a.probe_k) {
+                dx = a.probe_x[w] - xo;
+            } else if (is) {
+                fn = 2.0 * rec[g.off_g + k];
+                dx = 0.5 * dt * fn + r1 * sqdt;
+            } else {
+                dx = 10.0 * (r1 - 0.5) * P.step;
+            }
+            xn = a.probe_k ? a.probe_x[w] : xo + dx;
+        }
+        if (TC) {
+            // second layer of the pair network for the proposal's partners of all the
+            // CTA's walkers: one 128-row tile, tensor cores (value, d/dr, d2/dr2)
+            const int p = k / dim;
+            double yp[3] = {0.0, 0.0, 0.0};
+            for (int c = 0; c < dim; ++c) yp[c] = (active && c == k - p * dim) ? xn : (active ? x[p * dim + c] : 0.0);
+            float r = 0.0f, sv = 0.0f;
+            bool valid = active && lane < N && lane != p;
+            if (valid) {
+                double r2s = 0.0;
+                for (int c = 0; c < dim; ++c) {
+                    const double t = yp[c] - x[lane * dim + c];
+                    r2s += t * t;
+                }
+                r = (float)sqrt(r2s);
+                sv = same_spin(p, lane, N) ? 1.0f : 0.0f;
+            }
+            status |= tc_pair_layer(tc, mw, valid, r, sv, mlp_cusp(dim, sv > 0.5f), lane, wib, pre_w);
+        }
+        if (active) {
+            const bool corrected = is && !(P.flags & Q_IS_GREEN) && !a.probe_k;
+            double gy = 0.0, R = 1.0;
+            double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
+            const double prob = gen_ratios(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
+                                           corrected ? &gy : nullptr, R, mw, TC ? pre_w : nullptr);
+            bool accept = true;
+            if (!a.probe_k) {
+                double wgt = prob;
+                if (is) {
+                    if (P.flags & Q_IS_GREEN) {
+                        wgt = (exp(0.5 * (fc[k] - fn) * dx) + 1.0) * prob;  // importancesampling.cpp:43-47
+                    } else {
+                        const double fy = 2.0 * gy;
+                        wgt = prob * exp(0.5 * (fn + fy) * (0.25 * dt * (fn - fy) - dx));
+                    }
+                }
+                // the reference rejects when weight < u (importancesampling.cpp:72,
+                // bruteforce.cpp:44); a NaN weight is flagged and rejected
+                if (wgt != wgt) status |= ST_BAD_RATIO;
+                accept = wgt >= r2;
+            }
+            if (accept) {
+                const int p = k / dim;
+                if (P.flags & F_SLATER) {
+                    // Sherman-Morrison on the moved particle's block (slaterdeterminant.cpp:165-175)
+                    const int n = g.n, b = p / n, pl = p - b * n;
+                    double *rows = rec + g.off_inv + (size_t)b * n * n;
+                    for (int o = lane; o < n; o += 32) scr[SCR_ROW + o] = rows[(size_t)pl * n + o];
+                    __syncwarp();
+                    if (lane < n) {
+                        double *row = rows + (size_t)lane * n;
+                        double S = 0.0;
+                        for (int o = 0; o < n; ++o) S += scr[SCR_PHI + o] * row[o];
+                        const double c = S / R;
+                        for (int o = 0; o < n; ++o)
+                            row[o] = lane == pl ? scr[SCR_ROW + o] / R : row[o] - c * scr[SCR_ROW + o];
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0) {
+                    x[k] = xn;
+                    if (is) fc[k] = fn;
+                }
+                if (P.flags & F_MLP) {  // the moved particle's pair and one-body values from the proposal
+                    double *uc = rec + g.off_uc;
+                    for (int j = lane; j < N; j += 32)
+                        if (j != p) {
+                            double *c3 = uc + (size_t)(min(p, j) * N + max(p, j)) * 3;
+                            c3[0] = scr[SCR_XS + j];
+                            c3[1] = scr[SCR_XS + 32 + j];
+                            c3[2] = scr[SCR_PN + j];
+                        }
+                    if (lane == 0)
+                        for (int t = 0; t < 3; ++t) rec[g.off_oc + p * 3 + t] = scr[SCR_PN + 32 + t];
+                }
+                if (P.flags & Q_PADE_STALE) {  // the moved particle's pairs take the current gamma
+                    for (int j = lane; j < N; j += 32)
+                        if (j != p) mask[j] |= 1ull << p;
+                    if (lane == 0) mask[p] = ~0ull;
+                }
+                __syncwarp();
+                gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false);
+            }
+            if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
+            const double *en = rec + g.off_en;
+            if (a.rec_en && lane == 0) {
+                double *o = a.rec_en + ((size_t)w * a.rec_stride + it_step) * 3;
+                o[0] = en[0];
+                o[1] = en[1];
+                o[2] = en[2];
+            }
+            if (it_step >= a.burn_in) {  // Sampler::sample (sampler.cpp:52-90)
+                const double el = en[0] + en[1] + en[2];
+                if (el != el) status |= ST_NAN_ENERGY;
+                const bool win = it_step > a.win_lo && it_step < a.win_hi;
+                if (win && a.snap_x && (it_step - a.win_lo) % a.snap_interval == 0) {
+                    // MLP Jastrow parameter gradient: positions and E_L for mlp_grad_kernel
+                    const int slot = (it_step - a.win_lo) / a.snap_interval - a.snap_first;
+                    if (slot >= 0 && slot < a.snap_stride) {
+                        const size_t base = (size_t)w * a.snap_stride + slot;
+                        for (int t = lane; t < D; t += 32) a.snap_x[base * D + t] = (float)x[t];
+                        if (lane == 0) a.snap_e[base] = el;
+                    }
+                }
+                const int top = win ? 9 + 2 * g.n_act : 9;  // == P.nacc inside the window
+                const double *pg = rec + g.off_pg;
+                for (int t = lane; t < top; t += 32) {
+                    double q;
+                    if (t < 8) {
+                        const double base = t < 2 ? el : en[(t >> 1) - 1];
+                        q = (t & 1) ? base * base : base;
+                    } else if (t == 8) {
+                        q = accept ? 1.0 : 0.0;
+                    } else {
+                        const int c = t - 9;
+                        q = c < g.n_act ? pg[g.act[c]] : el * pg[g.act[c - g.n_act]];
+                    }
+                    double s1 = acc[2 * t], c1 = acc[2 * t + 1];
+                    kadd(s1, c1, q);
+                    acc[2 * t] = s1;
+                    acc[2 * t + 1] = c1;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (active && lane == 0) {
+        P.counter[w] = ctr;
+        if (status) P.status[w] |= status;
+    }
+}
+
+}  // namespace
+
+}  // namespace vmc

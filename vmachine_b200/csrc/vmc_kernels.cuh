@@ -158,25 +158,26 @@ struct RebuildArgs {
 // Slater blocks (Gauss-Jordan with partial pivoting), their derivative vectors,
 // the Pade gradient vector and pair sums, Coulomb, radial sums and, at
 // initialisation, the importance-sampling force cache.
+// Per warp (walkers w_first, w_first + w_stride, ... < w_end; shared slice at
+// warp_smem), called by the single-system kernel and the multi-system kernel.
 template <typename T, int DIM, int K>
-__global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
+__device__ __forceinline__ void rebuild_walkers(const Params &P, int mode, double *drift, unsigned char *warp_smem,
+                                                int w_first, int w_end, int w_stride)
 {
     constexpr int NO = K > 0 ? Shells<DIM, K>::n : 0;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Params &P = a.P;
     const Layout L = P.L;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *A = reinterpret_cast<double *>(smem_raw + (size_t)wib * a.smem_per_warp);
+    const int lane = threadIdx.x & 31;
+    double *A = reinterpret_cast<double *>(warp_smem);
     const int N = P.N, D = L.D, flags = P.flags;
     const double wa = P.omega * P.alpha, az = P.alpha_h * P.Z;
 
-    for (int w = blockIdx.x * a.wpb + wib; w < P.W; w += gridDim.x * a.wpb) {
+    for (int w = w_first; w < w_end; w += w_stride) {
         T *rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
         const T *x = rec + L.off_x;
         T *fc = rec + L.off_fc, *dd = rec + L.off_dd, *sdd = rec + L.off_sdd, *gj = rec + L.off_gj;
         T *inv = rec + L.off_inv;
         unsigned long long *mask = P.mask + (size_t)w * N;
-        if (a.mode == RB_INIT)
+        if (mode == RB_INIT)
             for (int j = lane; j < N; j += 32) mask[j] = ~0ull;
         __syncwarp();
         unsigned status = 0;
@@ -271,12 +272,12 @@ __global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
 #pragma unroll
                     for (int v = 0; v < S / VE; ++v) {
                         T ov[VE], nv[VE];
-                        if (a.mode == RB_REFRESH) vload<T>(row + v * VE, ov);
+                        if (mode == RB_REFRESH) vload<T>(row + v * VE, ov);
 #pragma unroll
                         for (int e2 = 0; e2 < VE; ++e2) {
                             const int o = v * VE + e2;
                             const double val = o < NO ? mcol[prow_of[o < NO ? o : 0] * MS] : 0.0;
-                            if (a.mode == RB_REFRESH && o < NO) {
+                            if (mode == RB_REFRESH && o < NO) {
                                 drift_num = fmax(drift_num, fabs((double)ov[e2] - val));
                                 drift_den = fmax(drift_den, fabs(val));
                             }
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
         invr = warp_sum(invr);
         sumr = warp_sum(sumr);
         __syncwarp();
-        if (a.mode == RB_INIT && P.sampling == SAMPLER_IS) {
+        if (mode == RB_INIT && P.sampling == SAMPLER_IS) {
             // ImportanceSampling::initialize: F = 2 * sum_e grad_e
             for (int c = lane; c < D; c += 32) {
                 double G = 0.0;
@@ -397,11 +398,20 @@ __global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
             sc[SC_INVR] = invr;
             sc[SC_LOGDET] = logdet;
             sc[SC_SUMR] = sumr;
-            if (a.drift) a.drift[w] = fmax(a.drift[w], drift_den > 0.0 ? drift_num / drift_den : 0.0);
+            if (drift) drift[w] = fmax(drift[w], drift_den > 0.0 ? drift_num / drift_den : 0.0);
             if (status) P.status[w] |= status;
         }
         __syncwarp();
     }
+}
+
+template <typename T, int DIM, int K>
+__global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5;
+    rebuild_walkers<T, DIM, K>(a.P, a.mode, a.drift, smem_raw + (size_t)wib * a.smem_per_warp,
+                               blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb);
 }
 
 // ------------------------------------------------------------------ evaluation

@@ -228,9 +228,14 @@ __device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
 // measured with ptxas at N = 56: the two 28-entry rows plus the step's working set
 // need more than 200 registers per thread and spill, so rows stay in shared memory.
 
+// The sweep of walkers w_first, w_first + w_stride, ... < w_end by the calling warp
+// (steps step_offset .. step_offset + steps - 1 of the iteration), whose slice of
+// shared memory starts at warp_smem.  The single-system kernel below
+// strides over its whole population; the multi-system kernel hands each warp the
+// walkers of one work item.
 template <typename T, int DIM, int K, int FX, bool PL>
-__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
-    sweep_kernel(const SweepArgs a)
+__device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int step_offset,
+                                              unsigned char *warp_smem, int w_first, int w_end, int w_stride)
 {
     // PL: the production form (Philox numbers, no probe, no recording), with the
     // branches of the test and replay modes compiled out
@@ -245,11 +250,10 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
     constexpr int VE = 16 / (int)sizeof(T);                     // entries per 16-byte vector
     constexpr int IS = K > 0 ? inv_row_stride(NO, sizeof(T)) : 0; // inverse row stride
     constexpr int NQ = (NO + VE - 1) / VE;                        // vectors per inverse row
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params &P = a.P;
     const Layout L = P.L;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    T *sm = reinterpret_cast<T *>(smem_raw + (size_t)wib * a.smem_per_warp);
+    const int lane = threadIdx.x & 31;
+    T *sm = reinterpret_cast<T *>(warp_smem);
     const int N = K > 0 ? NK : P.N;
     const int D = K > 0 ? DK : L.D;
     unsigned long long *smask = reinterpret_cast<unsigned long long *>(sm + L.rec);
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
         pkind = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : j == P.idx_alpha_h ? 3 : 0;
     }
 
-    for (int w = blockIdx.x * a.wpb + wib; w < P.W; w += gridDim.x * a.wpb) {
+    for (int w = w_first; w < w_end; w += w_stride) {
         T *g_rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
         copy_in(sm, g_rec, L.rec, lane);
         for (int j = lane; j < N; j += 32) smask[j] = P.mask[(size_t)w * N + j];
@@ -289,7 +293,7 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
         __syncwarp();
 
         const bool use_philox = !probe_k && !replay;
-        for (int s0 = 0; s0 < a.steps; s0 += 32) {
+        for (int s0 = 0; s0 < steps; s0 += 32) {
           if (use_philox) {
             // Lane-parallel Philox: lane i draws the numbers of step counter ctr + i
             // (the same per-step stream as a serial draw); each step of this block
@@ -312,9 +316,9 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
             }
             rng_u = v.w;
           }
-          const int s_end = min(s0 + 32, a.steps);
+          const int s_end = min(s0 + 32, steps);
           for (int s = s0; s < s_end; ++s) {
-            const int it_step = a.step_offset + s;
+            const int it_step = step_offset + s;
             const T wa = T(P.omega * P.alpha);
             // ---- 1. random numbers and the proposal
             int k;
@@ -711,6 +715,16 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
         if (lane == 0 && status) P.status[w] |= status;
         __syncwarp();
     }
+}
+
+template <typename T, int DIM, int K, int FX, bool PL>
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
+    sweep_kernel(const SweepArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5;
+    sweep_walkers<T, DIM, K, FX, PL>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
+                                     blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb);
 }
 
 }  // namespace vmc

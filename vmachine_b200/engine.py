@@ -50,11 +50,39 @@ class Averages(ctypes.Structure):
         "walker_std_error")]
 
 
+class Block(ctypes.Structure):
+    _fields_ = [("mean", ctypes.c_double), ("std_error", ctypes.c_double), ("mse_mean", ctypes.c_double),
+                ("mse_std_error", ctypes.c_double), ("n_k", ctypes.c_longlong)]
+
+
+class BlockingResult(ctypes.Structure):
+    _fields_ = [("energy", Block), ("kinetic", Block), ("external", Block), ("interaction", Block),
+                ("energy_walkers", Block), ("samples_per_walker", ctypes.c_longlong)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("n_systems", ctypes.c_int), ("n_general", ctypes.c_int), ("n_walkers", ctypes.c_longlong),
+                ("precision", ctypes.c_int), ("walkers_per_block", ctypes.c_int),
+                ("walkers_per_item", ctypes.c_int), ("grid", ctypes.c_int), ("tuned", ctypes.c_int),
+                ("graph_captures", ctypes.c_int), ("graph_replay", ctypes.c_int), ("rounds", ctypes.c_int),
+                ("seconds", ctypes.c_double), ("sweep_seconds", ctypes.c_double),
+                ("walker_moves", ctypes.c_double)]
+
+
+class BatchCandidate(ctypes.Structure):
+    _fields_ = [("walkers_per_block", ctypes.c_int), ("walkers_per_item", ctypes.c_int),
+                ("grid", ctypes.c_int), ("ns_per_walker_move", ctypes.c_double)]
+
+
 EXPORTS = ["vmc_abi_version", "vmc_create", "vmc_destroy", "vmc_get_info", "vmc_last_error",
            "vmc_set_parameters", "vmc_get_parameters", "vmc_init_walkers", "vmc_get_positions",
            "vmc_sample", "vmc_run_iteration", "vmc_get_walker_energies", "vmc_eval",
            "vmc_probe_move", "vmc_replay", "vmc_set_replay", "vmc_get_status",
-           "vmc_run_simulation", "vmc_stopwatch", "vmc_measure_fma_peak", "vmc_apply_sums"]
+           "vmc_run_simulation", "vmc_stopwatch", "vmc_measure_fma_peak", "vmc_apply_sums",
+           "vmc_batch_create", "vmc_batch_destroy", "vmc_batch_get_info", "vmc_batch_system",
+           "vmc_batch_init_walkers", "vmc_batch_set_tile", "vmc_batch_run_iteration",
+           "vmc_batch_last_sums", "vmc_batch_tuning", "vmc_block_series", "vmc_blocking",
+           "vmc_format_weights", "vmc_write_weights", "vmc_read_weights", "vmc_save_state", "vmc_load_state"]
 
 
 def library():
@@ -88,9 +116,27 @@ def library():
     L.vmc_run_simulation.argtypes = [vp, ctypes.POINTER(Averages), ip]
     L.vmc_stopwatch.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double)]
     L.vmc_measure_fma_peak.argtypes = [ip, ip, ctypes.POINTER(ctypes.c_double)]
+    L.vmc_format_weights.argtypes = [vp, ip, ip, ip, ctypes.c_char_p, ctypes.c_longlong]
+    L.vmc_write_weights.argtypes = [vp, ctypes.c_char_p, ip]
+    L.vmc_read_weights.argtypes = [vp, ctypes.c_char_p]
+    L.vmc_save_state.argtypes = [vp, ctypes.c_char_p]
+    L.vmc_load_state.argtypes = [vp, ctypes.c_char_p]
+    L.vmc_block_series.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(Block)]
+    L.vmc_blocking.argtypes = [vp, ip, ip, ctypes.POINTER(BlockingResult)]
+    L.vmc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ctypes.POINTER(Options), ctypes.POINTER(vp)]
+    L.vmc_batch_destroy.argtypes = [vp]
+    L.vmc_batch_destroy.restype = None
+    L.vmc_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
+    L.vmc_batch_system.argtypes = [vp, ip, ctypes.POINTER(vp)]
+    L.vmc_batch_init_walkers.argtypes = [vp, vp]
+    L.vmc_batch_set_tile.argtypes = [vp, ip, ip]
+    L.vmc_batch_run_iteration.argtypes = [vp, ip, vp]
+    L.vmc_batch_last_sums.argtypes = [vp, vp]
+    L.vmc_batch_tuning.argtypes = [vp, vp, ip]
     for name in EXPORTS:
-        if name not in ("vmc_destroy", "vmc_last_error"):
+        if name not in ("vmc_destroy", "vmc_last_error", "vmc_batch_destroy"):
             getattr(L, name).restype = ip
+    L.vmc_format_weights.restype = ctypes.c_longlong
     del dp
     _lib = L
     return L
@@ -243,10 +289,40 @@ class Engine:
         self._check(library().vmc_get_info(self._h, ctypes.byref(info)))
         return info.refresh_interval
 
+    # --- checkpoints
+    def write_weights(self, path, digits=0):
+        """Parameter file in the reference's format (digits <= 0: its 6 digits)."""
+        self._check(library().vmc_write_weights(self._h, os.fspath(path).encode(), int(digits)))
+
+    def read_weights(self, path):
+        self._check(library().vmc_read_weights(self._h, os.fspath(path).encode()))
+
+    def save_state(self, path):
+        """Walkers, parameters and optimiser state for an exact restart."""
+        self._check(library().vmc_save_state(self._h, os.fspath(path).encode()))
+
+    def load_state(self, path):
+        self._check(library().vmc_load_state(self._h, os.fspath(path).encode()))
+
+    def blocking(self, steps, burn_in=0):
+        """Sample `steps` moves per walker with the current parameters and block the
+        energy series on the device (vmc_blocking)."""
+        r = BlockingResult()
+        self._check(library().vmc_blocking(self._h, int(steps), int(burn_in), ctypes.byref(r)))
+        return r
+
     def status(self):
         out = np.zeros(self.W, np.uint32)
         self._check(library().vmc_get_status(self._h, _p(out)))
         return out
+
+
+def block_series(x):
+    """The reference's Blocker on a host series (vmc_block_series)."""
+    a = np.ascontiguousarray(x, np.float64)
+    b = Block()
+    Engine._check(library().vmc_block_series(_p(a), len(a), ctypes.byref(b)))
+    return b
 
 
 def measure_fma_peak(device=0, precision=1):
@@ -254,3 +330,86 @@ def measure_fma_peak(device=0, precision=1):
     t = ctypes.c_double()
     Engine._check(library().vmc_measure_fma_peak(device, precision, ctypes.byref(t)))
     return t.value
+
+
+class _Member(Engine):
+    """A system's engine inside a Batch (owned by the batch: closing it is a no-op)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        self._owned = False
+        info = Info()
+        self._check(library().vmc_get_info(self._h, ctypes.byref(info)))
+        self.info = info
+        self.W, self.D, self.E, self.P = info.n_walkers, info.n_coords, info.n_elements, info.p_max
+
+    def close(self):
+        self._h = None
+
+
+class Batch:
+    """Many systems (input.in texts), each with its own walkers and parameters,
+    iterated together by the persistent multi-system kernel and a captured graph."""
+
+    def __init__(self, texts, *, device=0, precision=None, refresh_interval=None, compat=None):
+        L = library()
+        arr = (ctypes.c_char_p * len(texts))(*[t.encode() for t in texts])
+        o = Options(device, -1 if precision is None else int(precision), 0, 0,
+                    -1 if refresh_interval is None else int(refresh_interval),
+                    -1 if compat is None else int(compat))
+        h = ctypes.c_void_p()
+        Engine._check(L.vmc_batch_create(arr, len(texts), ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.n = len(texts)
+        self.systems = []
+        for s in range(self.n):
+            eh = ctypes.c_void_p()
+            Engine._check(L.vmc_batch_system(self._h, s, ctypes.byref(eh)))
+            self.systems.append(_Member(eh))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.systems:
+                m.close()
+            library().vmc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def info(self):
+        i = BatchInfo()
+        Engine._check(library().vmc_batch_get_info(self._h, ctypes.byref(i)))
+        return i
+
+    def init_walkers(self, seeds=None):
+        sd = None if seeds is None else np.ascontiguousarray(seeds, np.uint64)
+        Engine._check(library().vmc_batch_init_walkers(self._h, _p(sd)))
+
+    def set_tile(self, walkers_per_block, walkers_per_item):
+        Engine._check(library().vmc_batch_set_tile(self._h, int(walkers_per_block), int(walkers_per_item)))
+
+    def run_iteration(self, iteration):
+        out = (Averages * self.n)()
+        Engine._check(library().vmc_batch_run_iteration(self._h, int(iteration), out))
+        return list(out)
+
+    def last_sums(self):
+        out = (Sums * self.n)()
+        Engine._check(library().vmc_batch_last_sums(self._h, out))
+        return list(out)
+
+    def tuning(self):
+        n = library().vmc_batch_tuning(self._h, None, 0)
+        out = (BatchCandidate * max(n, 1))()
+        library().vmc_batch_tuning(self._h, out, n)
+        return [(c.walkers_per_block, c.walkers_per_item, c.grid, c.ns_per_walker_move) for c in out[:n]]
