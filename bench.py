@@ -320,6 +320,9 @@ def run_engine_arm(args):
                 "mixed_sigma_same_iteration": energies[args.fp64_steps - 1][1]}
         eng64.close()
 
+    # the heterogeneous multi-system batch (every rank takes part)
+    batch = batch_line(args, pg, rank, local, world) if args.batch_iterations > 0 else None
+
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
@@ -367,6 +370,8 @@ def run_engine_arm(args):
     if args.learned > 0 and world == 1:
         from vmachine_b200.learned import compare
         line["learned"] = compare(budget_s=args.learned)
+    if batch:
+        line["batch"] = batch
     if not args.no_cpu_baseline and world == 1:
         cores = host_cores()
         v, err = reference_sample(cores, args.ref_steps)
@@ -379,6 +384,25 @@ def run_engine_arm(args):
     eng.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def batch_line(args, pg, rank, local, world):
+    """The heterogeneous workload (64 systems: 62 2D dots N = 2..56, He, Ne) through the
+    multi-system batch: systems bin-packed by cost over the ranks, each rank one batch
+    (persistent kernel, captured graph, tuned tile); walker-moves/s of the replayed
+    iterations, device-timed, max over ranks."""
+    from vmachine_b200.batch import mixed_systems, partition, run as batch_run
+    texts, desc = mixed_systems(5, 2000)
+    mine = partition(desc, world)[0][rank]
+    r = batch_run(args.batch_iterations, texts=[texts[i] for i in mine], device=local)
+    secs = max_over_ranks(pg, local, r["ms_per_iteration"] * 1e-3)
+    moves = sum(desc[i]["walkers"] for i in range(len(desc))) * 2000.0
+    return {"workload": "64 systems: 62 2D closed-shell dots N in {2,6,12,20,30,42,56}, omega ~ U[0.1, 1], "
+                        "256-4096 walkers each; He and Ne atoms (hydrogen orbitals x SimpleJastrow, FP64 general "
+                        "path); 2000 steps per walker per iteration, seed 5",
+            "walker_moves_per_s": moves / secs, "ms_per_iteration": secs * 1e3, "systems_per_rank": len(mine),
+            "tile": r["tile"], "graph_captures": r["graph_captures"], "replayed_iterations": r["replayed_iterations"],
+            "tuning_ns_per_move": [t[3] for t in r["tuning"]], "scaling": "strong"}
 
 
 def main():
@@ -396,6 +420,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-iterations", type=int, default=16,
+                    help="iterations of the 64-system heterogeneous batch (0: skip)")
     ap.add_argument("--learned", type=float, default=0.0,
                     help="seconds of training per wave function for the MLP-vs-Pade comparison "
                          "at N=20 omega=0.5 (0: skip)")

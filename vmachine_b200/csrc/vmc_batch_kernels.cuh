@@ -64,11 +64,14 @@ __device__ __forceinline__ bool batch_next(const BatchLaunch &b, int lane, int2 
 
 // The general-path walkers of an item, out of line: its FP64 code is register-hungry
 // and would otherwise raise the pressure in the dot paths of the same kernel.
+// The warp's slice: GEN_SCR scratch doubles, then the staged record and accumulators.
 static __device__ __noinline__ void batch_gen_walkers(const SweepArgs &a, int steps, int off, const GenParams &g, int w0,
                                                int w_end, double *scr)
 {
     TcMlp tc{};  // the general systems of a batch have no MLP factor
-    for (int w = w0; w < w_end; ++w) gen_sweep_walker<false>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr);
+    double *stage = gen_stage_doubles(g, a.P.nacc) ? scr + GEN_SCR : nullptr;
+    for (int w = w0; w < w_end; ++w)
+        gen_sweep_walker<false>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage);
 }
 
 template <typename T, int FX>

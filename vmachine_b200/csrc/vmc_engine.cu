@@ -509,8 +509,9 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     } else if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) {
         return reject("no kernel for this shape");
     }
+    // auto: start at 4 D steps (at least 512) and let the drift test tune it
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
-                          : (e->precision == VMC_PRECISION_MIXED ? 4 * e->D : 0);
+                          : (e->precision == VMC_PRECISION_MIXED ? std::max(4 * e->D, 512) : 0);
     e->refresh_auto = c.refresh_interval < 0 && e->precision == VMC_PRECISION_MIXED;
     e->seed = c.have_seed ? (unsigned long long)c.seed : 0x5eedULL;
 
@@ -1215,9 +1216,12 @@ int finish_sample(vmc_engine *e, const SamplePass &p, vmc_sums *out, std::vector
         // inverse: the 99th percentile over walkers (the maximum is set by the few
         // walkers sitting near a node of the determinant) halves the interval past
         // the tolerance and doubles it below 1/2.5 of it (drift grows about in
-        // proportion to the interval, so a doubling stays under the tolerance)
+        // proportion to the interval, so a doubling stays under the tolerance), up to
+        // 64 D steps or REFRESH_CAP_MIN (small blocks drift little: one refresh per
+        // sweep of a few thousand steps)
         if (q99_drift > e->drift_tol) e->refresh_interval = std::max(e->D, e->refresh_interval / 2);
-        else if (q99_drift < e->drift_tol / 2.5) e->refresh_interval = std::min(64 * e->D, e->refresh_interval * 2);
+        else if (q99_drift < e->drift_tol / 2.5)
+            e->refresh_interval = std::min(std::max(64 * e->D, REFRESH_CAP_MIN), e->refresh_interval * 2);
     }
     const double W = e->W;
     vmc_sums s{};

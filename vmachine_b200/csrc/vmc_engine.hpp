@@ -76,6 +76,9 @@ struct vmc_engine {
 
 namespace vmc {
 
+// Longest FP64 refresh interval the drift autotuner may choose for any system.
+constexpr int REFRESH_CAP_MIN = 8192;
+
 // Coefficients of the normalised Hermite recurrence (each kernel unit holds a copy
 // in constant memory).
 HermiteCoef hermite_coefficients();

@@ -60,7 +60,9 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
     if (TC) tc_ready(tc, &tc_slot);
     const bool active = w < P.W;
     if (!TC && !active) return;
-    gen_sweep_walker<TC>(a, a.steps, a.step_offset, g, w, active, scratch[wib], mw, tc, pre[wib]);
+    const int nst = gen_stage_doubles(g, P.nacc);  // 0 with the MLP (gsm holds its weights)
+    gen_sweep_walker<TC>(a, a.steps, a.step_offset, g, w, active, scratch[wib], mw, tc, pre[wib],
+                         nst ? gsm + (size_t)wib * nst : nullptr);
     if (TC) tc_teardown(tc, wib);
 }
 
@@ -378,7 +380,8 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
 cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st)
 {
     const bool tc = g.mlp && g.mlp_tc;
-    const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0);
+    const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0) +
+                        (size_t)GEN_WPB * gen_stage_doubles(g, a.P.nacc) * sizeof(double);
     const void *fn = tc ? (const void *)gen_sweep_kernel<true> : (const void *)gen_sweep_kernel<false>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -1003,22 +1003,45 @@ __device__ void tc_teardown(TcMlp &t, int wib)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(TC_COLS) : "memory");
 }
 
+// Shared doubles a warp needs to stage a walker of the general path (record and
+// accumulators), or 0 when the walker is not staged (MLP systems, whose record holds
+// the per-pair caches and the full parameter-gradient row, and records above 16 KB).
+constexpr int GEN_STAGE_MAX = 2048;
+__host__ __device__ inline int gen_stage_doubles(const GenParams &g, int nacc)
+{
+    const int n = g.rec + 2 * nacc;
+    return (g.mlp || n > GEN_STAGE_MAX) ? 0 : n;
+}
+
 // Steps step_offset .. step_offset + steps - 1 of walker w by the calling warp.  scr: the warp's
 // GEN_SCR shared doubles; mw: the CTA's staged MLP weights or null; with TC the
 // CTA's four warps run in lockstep (inactive ones join the tensor-core steps).
+// stage: shared memory for the walker's record and accumulators (gen_stage_doubles),
+// or null to work on them in global memory; staged, every step's reads and writes
+// stay on chip and the record goes back once at the end.
 template <bool TC>
 __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, int step_offset, const GenParams &g,
-                                                 int w, bool active, double *scr, float *mw, TcMlp &tc, float *pre_w)
+                                                 int w, bool active, double *scr, float *mw, TcMlp &tc, float *pre_w,
+                                                 double *stage = nullptr)
 {
     const Params &P = a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 
     const int N = P.N, D = g.D, dim = D / N;
     const int ws = active ? w : 0;  // record pointers of a warp without a walker are never used
-    double *rec = reinterpret_cast<double *>(P.state) + (size_t)ws * g.rec;
+    double *const grec = reinterpret_cast<double *>(P.state) + (size_t)ws * g.rec;
+    double *const gacc = P.acc + (size_t)ws * P.nacc * 2;
+    double *rec = grec, *acc = gacc;
+    const bool staged = stage && active;
+    if (staged) {
+        for (int i = lane; i < g.rec; i += 32) stage[i] = grec[i];
+        for (int i = lane; i < 2 * P.nacc; i += 32) stage[g.rec + i] = gacc[i];
+        __syncwarp();
+        rec = stage;
+        acc = stage + g.rec;
+    }
     double *x = rec, *fc = rec + g.off_fc;
     unsigned long long *mask = P.mask + (size_t)ws * N;
-    double *acc = P.acc + (size_t)ws * P.nacc * 2;
     unsigned long long ctr = active ? P.counter[ws] : 0ull;
     unsigned status = 0;
     const bool is = P.sampling == SAMPLER_IS;
@@ -1192,6 +1215,11 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
             }
             __syncwarp();
         }
+    }
+    if (staged) {
+        __syncwarp();
+        for (int i = lane; i < g.rec; i += 32) grec[i] = rec[i];
+        for (int i = lane; i < 2 * P.nacc; i += 32) gacc[i] = acc[i];
     }
     if (active && lane == 0) {
         P.counter[w] = ctr;
