@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define VMC_ABI_VERSION 3
+#define VMC_ABI_VERSION 4
 
 enum {
     VMC_OK = 0,
@@ -177,8 +177,17 @@ int vmc_set_replay(vmc_engine *e, const double *stream, int length);
 int vmc_get_status(const vmc_engine *e, uint32_t *status /* W */);
 
 /* Full run as System::runSimulation (system.cpp:81-139) without terminal output:
- * numIterations iterations; per-iteration averages to `history` (may be NULL,
- * n_iterations entries). */
+ * iterations until the last one (numIterations, or rangeOfAdaptiveSteps + 1 after
+ * convergence with checkConvergence: tolerance / numberOfEnergies), with
+ * applyAdaptiveSteps' longer last iterations (additionalSteps,
+ * additionalStepsLastIter), weights_<it>.dat every checkpointFreq iterations
+ * (printParametersToFile), energy.dat / kinetic.dat / external.dat / interaction.dat
+ * (printEnergyToFile), and in the last iteration the densities (onebody.dat,
+ * onebody2.dat, twobody.dat; computeOneBodyDensity / 2, computeTwoBodyDensity,
+ * numberOfBins, maxRadius) and the blocking of its energies (doResampling; see
+ * vmc_last_blocking), files in `path`.  Per-iteration averages to `history` (may be
+ * NULL, n_history entries).  Returns the number of iterations run (>= 0) or a
+ * negative error. */
 int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history);
 
 /* Device-side stopwatch on the engine's stream: mode 0 records the start; mode 1
@@ -220,6 +229,22 @@ int vmc_block_series(const double *x, long long n, vmc_block *out);
  * in device memory (W x steps x 24 bytes, released after), then blocking of E_L, T,
  * V_ext and V_int on the device.  Consumes a replay stream set by vmc_set_replay. */
 int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out);
+/* The blocking of the last iteration of the latest vmc_run_simulation with
+ * doResampling: true (Sampler::doResampling; the record must fit in 16 GB of device
+ * memory, W x steps x 24 bytes, else there is none: VMC_E_STATE). */
+int vmc_last_blocking(const vmc_engine *e, vmc_blocking_result *out);
+
+/* ---- Electron densities (Sampler::computeOneBodyDensity, computeOneBodyDensity2,
+ * computeTwoBodyDensity, sampler.cpp:639-692) ----
+ * `steps` moves per walker with the current parameters (no optimiser step; sums as
+ * vmc_sample with iteration 0), counting every sampled step of every walker into the
+ * requested histograms (NULL: not computed), bins = numberOfBins, step = max_radius /
+ * bins: radial[bins] counts floor(r / step) for r < max_radius; spatial[bins][bins]
+ * counts the cell (trunc(y / 2 step) + bins/2, trunc(x / 2 step) + bins/2) inside the
+ * grid (row = y); two_body[bins][bins] counts (floor(r_i / step) + 1, floor(r_j / step)
+ * + 1) for pairs i < j with both below bins.  64-bit counts summed over walkers. */
+int vmc_densities(vmc_engine *e, int steps, int burn_in, int bins, double max_radius, uint64_t *radial,
+                  uint64_t *spatial, uint64_t *two_body);
 
 /* ---- Checkpoint and resume ----
  *

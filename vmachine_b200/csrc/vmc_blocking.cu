@@ -293,44 +293,11 @@ int bl_fail(int code, const std::string &m) { return set_last_error(code, m.c_st
 
 }  // namespace
 
-extern "C" {
+namespace vmc {
 
-int vmc_block_series(const double *x, long long n, vmc_block *out)
+int block_record(vmc_engine *e, const double *rec, int steps, int burn_in, vmc_blocking_result *out)
 {
-    if (!out || (n > 0 && !x)) return bl_fail(VMC_E_ARG, "null argument");
-    if (n < 2 || (n & (n - 1))) {  // blocker.cpp:20-25
-        fail_block(*out);
-        return VMC_OK;
-    }
-    int d = 0;
-    while ((1LL << d) < n) ++d;
-    if (d > BL_MAX) return bl_fail(VMC_E_ARG, "series longer than 2^40");
-    double mean = 0.0;
-    for (long long i = 0; i < n; ++i) mean += x[i];
-    mean /= (double)n;
-    std::vector<double> v(x, x + n);
-    double gam[BL_MAX], s[BL_MAX];
-    long long m = n;
-    for (int k = 0; k < d; ++k) {
-        double g = 0.0, q = 0.0;
-        for (long long i = 0; i + 1 < m; ++i) g += (v[i] - mean) * (v[i + 1] - mean);
-        for (long long i = 0; i < m; ++i) q += (v[i] - mean) * (v[i] - mean);
-        gam[k] = g / m;
-        s[k] = q / m;
-        for (long long i = 0; i < m / 2; ++i) v[i] = 0.5 * (v[2 * i] + v[2 * i + 1]);
-        m /= 2;
-    }
-    double nK = 0.0;
-    const double var = jonsson(gam, s, d, chi2_table().data(), nK);
-    fill_block(*out, mean, var, nK);
-    return VMC_OK;
-}
-
-int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out)
-{
-    if (!e || !out) return bl_fail(VMC_E_ARG, "null argument");
-    if (!e->have_walkers) return bl_fail(VMC_E_STATE, "vmc_init_walkers first");
-    if (steps < 2 || burn_in < 0 || burn_in >= steps - 1) return bl_fail(VMC_E_ARG, "bad step counts");
+    if (steps - burn_in < 2) return bl_fail(VMC_E_ARG, "fewer than two sampled steps");
     std::memset(out, 0, sizeof(*out));
     int d = 0;
     while ((2LL << d) <= (long long)(steps - burn_in)) ++d;
@@ -340,10 +307,9 @@ int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out
     BLCUDA(cudaSetDevice(e->device));
     BLCUDA(cudaMemcpyToSymbolAsync(c_chi2, chi2_table().data(), sizeof(double) * BL_MAX, 0,
                                    cudaMemcpyHostToDevice, e->stream));
-    double *rec = nullptr, *scratch = nullptr, *stats = nullptr, *wout = nullptr, *wsum = nullptr, *red = nullptr,
+    double *scratch = nullptr, *stats = nullptr, *wout = nullptr, *wsum = nullptr, *red = nullptr,
            *mu = nullptr;
     auto release = [&]() {
-        cudaFree(rec);
         cudaFree(scratch);
         cudaFree(stats);
         cudaFree(wout);
@@ -352,21 +318,12 @@ int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out
         cudaFree(mu);
     };
     int rc = [&]() -> int {
-        BLCUDA(cudaMalloc(&rec, W * (size_t)steps * 3 * sizeof(double)));
         BLCUDA(cudaMalloc(&scratch, W * BL_PARTS * (size_t)n * sizeof(double)));
         BLCUDA(cudaMalloc(&stats, W * BL_PARTS * (size_t)d * BL_STATS * sizeof(double)));
         BLCUDA(cudaMalloc(&wout, W * BL_PARTS * 3 * sizeof(double)));
         BLCUDA(cudaMalloc(&wsum, W * BL_PARTS * sizeof(double)));
         BLCUDA(cudaMalloc(&red, (BL_PARTS * (size_t)d * 4 + BL_PARTS * 2) * sizeof(double)));
         BLCUDA(cudaMalloc(&mu, BL_PARTS * sizeof(double)));
-        // ---- sample with the per-step record
-        e->d_rec = rec;
-        e->rec_stride = steps;
-        vmc_sums s{};
-        int src = vmc_sample(e, 0, steps, burn_in, &s, nullptr, nullptr);
-        e->d_rec = nullptr;
-        e->rec_stride = 0;
-        if (src) return src;
         // ---- global means, then the levels
         block_sum_kernel<<<(unsigned)W, BL_THREADS, 0, e->stream>>>(rec, steps, burn_in, d, wsum);
         BLCUDA(cudaGetLastError());
@@ -441,6 +398,61 @@ int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out
     }();
     cudaStreamSynchronize(e->stream);
     release();
+    return rc;
+}
+
+}  // namespace vmc
+
+extern "C" {
+
+int vmc_block_series(const double *x, long long n, vmc_block *out)
+{
+    if (!out || (n > 0 && !x)) return bl_fail(VMC_E_ARG, "null argument");
+    if (n < 2 || (n & (n - 1))) {  // blocker.cpp:20-25
+        fail_block(*out);
+        return VMC_OK;
+    }
+    int d = 0;
+    while ((1LL << d) < n) ++d;
+    if (d > BL_MAX) return bl_fail(VMC_E_ARG, "series longer than 2^40");
+    double mean = 0.0;
+    for (long long i = 0; i < n; ++i) mean += x[i];
+    mean /= (double)n;
+    std::vector<double> v(x, x + n);
+    double gam[BL_MAX], s[BL_MAX];
+    long long m = n;
+    for (int k = 0; k < d; ++k) {
+        double g = 0.0, q = 0.0;
+        for (long long i = 0; i + 1 < m; ++i) g += (v[i] - mean) * (v[i + 1] - mean);
+        for (long long i = 0; i < m; ++i) q += (v[i] - mean) * (v[i] - mean);
+        gam[k] = g / m;
+        s[k] = q / m;
+        for (long long i = 0; i < m / 2; ++i) v[i] = 0.5 * (v[2 * i] + v[2 * i + 1]);
+        m /= 2;
+    }
+    double nK = 0.0;
+    const double var = jonsson(gam, s, d, chi2_table().data(), nK);
+    fill_block(*out, mean, var, nK);
+    return VMC_OK;
+}
+
+int vmc_blocking(vmc_engine *e, int steps, int burn_in, vmc_blocking_result *out)
+{
+    if (!e || !out) return bl_fail(VMC_E_ARG, "null argument");
+    if (!e->have_walkers) return bl_fail(VMC_E_STATE, "vmc_init_walkers first");
+    if (steps < 2 || burn_in < 0 || burn_in >= steps - 1) return bl_fail(VMC_E_ARG, "bad step counts");
+    BLCUDA(cudaSetDevice(e->device));
+    double *rec = nullptr;
+    BLCUDA(cudaMalloc(&rec, (size_t)e->W * steps * 3 * sizeof(double)));
+    e->d_rec = rec;
+    e->rec_stride = steps;
+    vmc_sums s{};
+    int rc = vmc_sample(e, 0, steps, burn_in, &s, nullptr, nullptr);
+    e->d_rec = nullptr;
+    e->rec_stride = 0;
+    if (!rc) rc = block_record(e, rec, steps, burn_in, out);
+    cudaStreamSynchronize(e->stream);
+    cudaFree(rec);
     return rc;
 }
 

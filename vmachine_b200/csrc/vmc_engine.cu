@@ -151,6 +151,9 @@ void free_engine(vmc_engine *e)
     cudaFree(e->d_snap_e);
     cudaFree(e->d_mlp_out);
     cudaFree(e->d_pos);
+    cudaFree(e->d_dens_radial);
+    cudaFree(e->d_dens_grid);
+    cudaFree(e->d_dens_pair);
     for (cudaEvent_t ev : e->sweep_events) cudaEventDestroy(ev);
     if (e->sw0) cudaEventDestroy(e->sw0);
     if (e->sw1) cudaEventDestroy(e->sw1);
@@ -255,7 +258,8 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
     a.wpb = e->wpb;
     a.smem_per_warp = sweep_smem_per_warp(e);
     const size_t smem = (size_t)a.wpb * a.smem_per_warp;
-    const void *fn = (!a.probe_k && !a.replay && !a.rec_en && !a.rec_acc) ? e->ks.sweep_plain : e->ks.sweep;
+    const void *fn = (!a.probe_k && !a.replay && !a.rec_en && !a.rec_acc && !a.dens_bins) ? e->ks.sweep_plain
+                                                                                         : e->ks.sweep;
     CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (e->W + a.wpb - 1) / a.wpb;
     return launch(fn, grid, 32 * a.wpb, smem, e->stream, &a);
@@ -745,6 +749,14 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
             a.rec_en = e->d_rec;
             a.rec_stride = e->rec_stride;
         }
+        if (e->dens_bins > 0) {
+            a.dens_radial = e->d_dens_radial;
+            a.dens_grid = e->d_dens_grid;
+            a.dens_pair = e->d_dens_pair;
+            a.dens_bins = e->dens_bins;
+            a.dens_step = e->dens_step;
+            a.dens_max = e->dens_max;
+        }
         if (e->d_replay) {
             if (e->replay_pos + steps > e->replay_len) return fail(VMC_E_ARG, "replay stream exhausted");
             a.replay = e->d_replay;
@@ -853,15 +865,104 @@ int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)
         int rc = vmc_init_walkers(e, nullptr, e->seed);
         if (rc) return rc;
     }
-    for (int it = 0; it < e->cfg.iterations; ++it) {
+    // System::runSimulation (system.cpp:81-139): the last iteration is number
+    // normal + rangeOfAdaptiveSteps; with adaptive steps the iterations from `normal`
+    // on sample 2^additionalSteps times the steps and the last 2^additionalStepsLastIter
+    // times (system.cpp:214-224); the convergence check moves `normal` to the next
+    // iteration once the energy of numberOfEnergies iterations ago is within
+    // `tolerance` of the latest (system.cpp:197-207)
+    const Config &c = e->cfg;
+    int normal = c.iterations - c.range_adaptive - 1;
+    bool check = c.check_convergence;
+    std::vector<double> window(std::max(1, c.n_energies), 0.0);
+    std::ofstream ef[4];
+    if (c.print_energy) {  // sampler.cpp:443-452, 491-498
+        const char *names[4] = {"energy.dat", "kinetic.dat", "external.dat", "interaction.dat"};
+        for (int q = 0; q < 4; ++q) {
+            ef[q].open(c.path + names[q]);
+            if (!ef[q]) return fail(VMC_E_ARG, "cannot write '" + c.path + names[q] + "'");
+        }
+    }
+    e->have_final = false;
+    const bool dens = c.ob_density || (c.ob_density2 && e->dim >= 2) || c.tb_density;
+    int it = 0;
+    for (; it < c.iterations; ++it) {
+        const bool last = it == normal + c.range_adaptive;
+        long long mult = 1;
+        if (c.adaptive_steps) mult = last ? (1LL << c.add_steps_last) : it >= normal ? (1LL << c.add_steps) : 1;
+        const long long sampled = (long long)e->steps_per_walker * mult;
+        if (sampled + e->burn_in > (1LL << 30)) return fail(VMC_E_ARG, "adaptive steps: too many steps per walker");
+        const int steps = (int)sampled + e->burn_in;
+        // the last iteration keeps every walker's energies for blocking (doResampling)
+        // when they fit in FINAL_RECORD_BYTES of device memory, and counts densities
+        double *rec = nullptr;
+        if (last && c.do_resampling && (double)e->W * steps * 24.0 <= FINAL_RECORD_BYTES) {
+            CUDA_TRY(cudaMalloc(&rec, (size_t)e->W * steps * 3 * sizeof(double)));
+            e->d_rec = rec;
+            e->rec_stride = steps;
+        }
+        int rc = (last && dens) ? density_begin(e, c.n_bins, c.max_radius, c.ob_density,
+                                                c.ob_density2 && e->dim >= 2, c.tb_density)
+                                : VMC_OK;
+        std::vector<double> g(e->EP), ge(e->EP);
+        vmc_sums s{};
         vmc_averages a{};
-        int rc = vmc_run_iteration(e, it, &a);
+        if (!rc) rc = vmc_sample(e, it, steps, e->burn_in, &s, g.data(), ge.data());
+        e->d_rec = nullptr;
+        e->rec_stride = 0;
+        if (!rc) rc = apply_sums(e, &s, g.data(), ge.data(), &a, true);
         if (history && it < n_history) history[it] = a;
+        if (!rc && last && rec) {
+            rc = block_record(e, rec, steps, e->burn_in, &e->final_blocking);
+            e->have_final = rc == VMC_OK;
+        }
+        if (rec) {
+            cudaStreamSynchronize(e->stream);
+            cudaFree(rec);
+        }
+        if (last && dens) {
+            const size_t b = (size_t)c.n_bins;
+            std::vector<uint64_t> r1(c.ob_density ? b : 0), r2(c.ob_density2 && e->dim >= 2 ? b * b : 0),
+                r3(c.tb_density ? b * b : 0);
+            const int drc = density_end(e, r1.empty() ? nullptr : r1.data(), r2.empty() ? nullptr : r2.data(),
+                                        r3.empty() ? nullptr : r3.data());
+            if (!rc) rc = drc;
+            // sampler.cpp:522-581: onebody.dat (a column), onebody2.dat, twobody.dat
+            if (!rc && !r1.empty()) rc = write_counts(c.path + "onebody.dat", r1.data(), c.n_bins, 1);
+            if (!rc && !r2.empty()) rc = write_counts(c.path + "onebody2.dat", r2.data(), c.n_bins, c.n_bins);
+            if (!rc && !r3.empty()) rc = write_counts(c.path + "twobody.dat", r3.data(), c.n_bins, c.n_bins);
+        }
         if (rc) return rc;
         // checkpointing (system.cpp:116-118, sampler.cpp:507-515)
-        if (e->cfg.print_params && e->cfg.checkpoint_freq > 0 && it % e->cfg.checkpoint_freq == 0)
-            if ((rc = write_weights_file(e, e->cfg.path + "weights_" + std::to_string(it) + ".dat", 6))) return rc;
+        if (c.print_params && c.checkpoint_freq > 0 && it % c.checkpoint_freq == 0)
+            if ((rc = write_weights_file(e, c.path + "weights_" + std::to_string(it) + ".dat", 6))) return rc;
+        if (c.print_energy) {
+            ef[0] << a.energy << std::endl;
+            ef[1] << a.kinetic << std::endl;
+            ef[2] << a.external << std::endl;
+            ef[3] << a.interaction << std::endl;
+        }
+        if (last) {
+            ++it;
+            break;
+        }
+        if (check) {
+            std::rotate(window.begin(), window.begin() + 1, window.end());
+            window.back() = a.energy;
+            if (std::fabs(window.front() - window.back()) < c.tolerance) {
+                normal = it + 1;
+                check = false;
+            }
+        }
     }
+    return it;
+}
+
+int vmc_last_blocking(const vmc_engine *e, vmc_blocking_result *out)
+{
+    if (!e || !out) return fail(VMC_E_ARG, "null argument");
+    if (!e->have_final) return fail(VMC_E_STATE, "no blocked final iteration (doResampling: true in vmc_run_simulation)");
+    *out = e->final_blocking;
     return VMC_OK;
 }
 

@@ -65,6 +65,13 @@ struct vmc_engine {
     // and step, W x rec_stride x 3 (the blocking analysis)
     double *d_rec = nullptr;
     int rec_stride = 0;
+    // optional electron-density histograms filled by vmc_sample (dens_bins > 0)
+    unsigned long long *d_dens_radial = nullptr, *d_dens_grid = nullptr, *d_dens_pair = nullptr;
+    int dens_bins = 0;
+    double dens_step = 0.0, dens_max = 0.0;
+    // blocking of the last vmc_run_simulation's final iteration (doResampling)
+    vmc_blocking_result final_blocking{};
+    bool have_final = false;
     // optional replayed random stream consumed by vmc_sample (W x replay_len x 3)
     double *d_replay = nullptr;
     int replay_len = 0, replay_pos = 0;
@@ -78,6 +85,8 @@ namespace vmc {
 
 // Longest FP64 refresh interval the drift autotuner may choose for any system.
 constexpr int REFRESH_CAP_MIN = 8192;
+// Device memory vmc_run_simulation may spend on the last iteration's energy record.
+constexpr double FINAL_RECORD_BYTES = 16.0e9;
 
 // Coefficients of the normalised Hermite recurrence (each kernel unit holds a copy
 // in constant memory).
@@ -118,5 +127,13 @@ int upload_parameters(vmc_engine *e);
 // values ("" or why not); write with `digits` significant digits.
 std::string read_weights_file(const std::string &path, int E, int P, std::vector<double> &theta);
 int write_weights_file(const vmc_engine *e, const std::string &path, int digits);
+// Electron-density histograms of the following vmc_sample calls (vmc_density.cu):
+// begin allocates and zeroes them, end copies them out (null: skip) and frees them.
+int density_begin(vmc_engine *e, int bins, double max_radius, bool radial, bool spatial, bool pair);
+int density_end(vmc_engine *e, uint64_t *radial, uint64_t *spatial, uint64_t *pair);
+// Integer counts as the reference prints Eigen integer vectors and matrices.
+int write_counts(const std::string &path, const uint64_t *v, int rows, int cols);
+// Blocking of an energy record of `steps` steps per walker (vmc_blocking.cu).
+int block_record(vmc_engine *e, const double *rec, int steps, int burn_in, vmc_blocking_result *out);
 
 }  // namespace vmc

@@ -1181,6 +1181,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                 o[1] = en[1];
                 o[2] = en[2];
             }
+            if (it_step >= a.burn_in && a.dens_bins > 0) density_sample<double>(a, x, N, dim, lane);
             if (it_step >= a.burn_in) {  // Sampler::sample (sampler.cpp:52-90)
                 const double el = en[0] + en[1] + en[2];
                 if (el != el) status |= ST_NAN_ENERGY;

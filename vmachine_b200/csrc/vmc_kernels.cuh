@@ -118,7 +118,62 @@ struct SweepArgs {
     float *snap_x;
     double *snap_e;
     int snap_stride, snap_interval, snap_first;  // slot = (step - win_lo) / interval - first
+    // electron densities over the sampled steps (0 bins: off): radial one-body counts
+    // (bins), the spatial one-body grid and the radial two-body counts (bins x bins,
+    // row-major), each optional
+    unsigned long long *dens_radial, *dens_grid, *dens_pair;
+    int dens_bins;
+    double dens_step, dens_max;  // maxRadius / bins, maxRadius
 };
+
+// Electron densities at a walker's current positions (Sampler::computeOneBodyDensity,
+// computeOneBodyDensity2, computeTwoBodyDensity: sampler.cpp:639-692), added to 64-bit
+// device histograms: radial bin floor(r / step) for r < maxRadius; spatial cell
+// (trunc(y / 2 step) + bins/2, trunc(x / 2 step) + bins/2) inside the grid; two-body
+// cell (floor(r_i / step) + 1, floor(r_j / step) + 1) for i < j, both below bins.
+// Lanes over particles (two per lane above 32); called by the whole warp.
+__device__ __forceinline__ int density_bin(double q)
+{
+    return (q == q && q < 2.0e9 && q > -2.0e9) ? (int)q : 2000000000;  // truncation toward zero
+}
+
+template <typename T>
+__device__ void density_sample(const SweepArgs &a, const T *x, int N, int dim, int lane)
+{
+    const int bins = a.dens_bins, half = bins / 2;
+    const double step = a.dens_step;
+    int pb0 = bins, pb1 = bins;  // two-body bins of particles lane and lane + 32
+    for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        if (i >= N) continue;
+        double r2 = 0.0;
+        for (int c = 0; c < dim; ++c) {
+            const double v = (double)x[i * dim + c];
+            r2 += v * v;
+        }
+        const double r = sqrt(r2);
+        if (a.dens_radial && r < a.dens_max) {
+            const int b = density_bin(r / step);
+            if (b < bins) atomicAdd(&a.dens_radial[b], 1ull);
+        }
+        if (a.dens_grid) {
+            const int ix = density_bin((double)x[i * dim] / (2.0 * step));
+            const int iy = density_bin((double)x[i * dim + 1] / (2.0 * step));
+            if (abs(ix) < half && abs(iy) < half)
+                atomicAdd(&a.dens_grid[(size_t)(iy + half) * bins + ix + half], 1ull);
+        }
+        const int pb = density_bin(r / step);
+        (h ? pb1 : pb0) = pb < bins ? pb + 1 : bins;
+    }
+    if (a.dens_pair) {
+        for (int j = 1; j < N; ++j) {
+            const int bj = __shfl_sync(0xffffffffu, j < 32 ? pb0 : pb1, j & 31);
+            if (bj >= bins) continue;  // uniform over the warp
+            if (lane < j && pb0 < bins) atomicAdd(&a.dens_pair[(size_t)pb0 * bins + bj], 1ull);
+            if (lane + 32 < j && pb1 < bins) atomicAdd(&a.dens_pair[(size_t)pb1 * bins + bj], 1ull);
+        }
+    }
+}
 
 // ------------------------------------------------------------------ helpers
 

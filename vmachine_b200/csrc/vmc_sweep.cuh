@@ -690,6 +690,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     const double qp = win ? (times_e ? g * el : g) : 0.0;
                     const double q = lane < 8 ? qe : lane == 8 ? (accept ? 1.0 : 0.0) : qp;
                     kadd(acc_s, acc_c, q);
+                    if (!PL && a.dens_bins > 0) density_sample<T>(a, x, N, DIM, lane);
                 }
             }
             if (rec_acc && lane == 0) rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;

@@ -82,7 +82,8 @@ EXPORTS = ["vmc_abi_version", "vmc_create", "vmc_destroy", "vmc_get_info", "vmc_
            "vmc_batch_create", "vmc_batch_destroy", "vmc_batch_get_info", "vmc_batch_system",
            "vmc_batch_init_walkers", "vmc_batch_set_tile", "vmc_batch_run_iteration",
            "vmc_batch_last_sums", "vmc_batch_tuning", "vmc_block_series", "vmc_blocking",
-           "vmc_format_weights", "vmc_write_weights", "vmc_read_weights", "vmc_save_state", "vmc_load_state"]
+           "vmc_format_weights", "vmc_write_weights", "vmc_read_weights", "vmc_save_state", "vmc_load_state",
+           "vmc_last_blocking", "vmc_densities"]
 
 
 def library():
@@ -121,6 +122,8 @@ def library():
     L.vmc_read_weights.argtypes = [vp, ctypes.c_char_p]
     L.vmc_save_state.argtypes = [vp, ctypes.c_char_p]
     L.vmc_load_state.argtypes = [vp, ctypes.c_char_p]
+    L.vmc_last_blocking.argtypes = [vp, ctypes.POINTER(BlockingResult)]
+    L.vmc_densities.argtypes = [vp, ip, ip, ip, dp, vp, vp, vp]
     L.vmc_block_series.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(Block)]
     L.vmc_blocking.argtypes = [vp, ip, ip, ctypes.POINTER(BlockingResult)]
     L.vmc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ctypes.POINTER(Options), ctypes.POINTER(vp)]
@@ -137,7 +140,6 @@ def library():
         if name not in ("vmc_destroy", "vmc_last_error", "vmc_batch_destroy"):
             getattr(L, name).restype = ip
     L.vmc_format_weights.restype = ctypes.c_longlong
-    del dp
     _lib = L
     return L
 
@@ -231,10 +233,27 @@ class Engine:
         return a
 
     def run_simulation(self):
+        """System::runSimulation: the per-iteration averages of the iterations run."""
         n = self.info.n_iterations
         hist = (Averages * n)()
-        self._check(library().vmc_run_simulation(self._h, hist, n))
-        return list(hist)
+        rc = library().vmc_run_simulation(self._h, hist, n)
+        if rc < 0:
+            self._check(rc)
+        return list(hist)[:rc]
+
+    def last_blocking(self):
+        r = BlockingResult()
+        self._check(library().vmc_last_blocking(self._h, ctypes.byref(r)))
+        return r
+
+    def densities(self, steps, burn_in=0, bins=1000, max_radius=5.0, radial=True, spatial=False, two_body=False):
+        """Electron-density counts over `steps` moves per walker (vmc_densities)."""
+        r = np.zeros(bins, np.uint64) if radial else None
+        sp = np.zeros((bins, bins), np.uint64) if spatial else None
+        tb = np.zeros((bins, bins), np.uint64) if two_body else None
+        self._check(library().vmc_densities(self._h, int(steps), int(burn_in), int(bins), float(max_radius),
+                                            _p(r), _p(sp), _p(tb)))
+        return r, sp, tb
 
     def walker_energies(self):
         out = np.zeros(self.W)
