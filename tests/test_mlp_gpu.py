@@ -83,6 +83,28 @@ def test_fixed_positions(N):
             assert abs(en2[w, 0] - kin) < 2e-5 * max(1.0, abs(kin))
 
 
+@pytest.mark.parametrize("N", [6, 20])
+def test_tensor_core_backward_at_fixed_positions(N):
+    """dJ/dtheta from the tensor-core backward (bfloat16 high/low operands, FP32
+    accumulation) against the FP64 oracle and the CUDA-core backward, per walker."""
+    from vmachine_b200 import Engine
+    theta = theta_for(N + 3)
+    rng = np.random.default_rng(200 + N)
+    W = 6
+    pos = rng.normal(0.0, 1.0, (W, 2 * N))
+    pg = {}
+    for tc in ("false", "true"):
+        with Engine(config(N, extra=[f"mlpTensorCores: {tc}"]), walkers=W, precision=0) as eng:
+            eng.set_parameters(theta)
+            eng.init_walkers(pos)
+            pg[tc] = eng.eval()[2][:, 2]
+            assert not (eng.status() & 8).any()
+    for w in range(W):
+        want = mj.param_gradient(theta[2], pos[w], N, 2)
+        assert rel(pg["true"][w], want) < 2e-4
+        assert rel(pg["true"][w], pg["false"][w]) < 2e-4
+
+
 def test_sampled_gradient_sums():
     """One iteration: the MLP rows of the gradient sums come from the window's
     snapshots, scaled to the window's sample count; dJ/db3 is the pair count, so its
@@ -100,6 +122,7 @@ def test_sampled_gradient_sums():
         lo, hi = max(1, info.burn_in), min(bs - 1, info.steps_per_walker + info.burn_in - 1)
         n_win = hi - lo + 1
         assert abs(g[2, 4416] - N * (N - 1) / 2 * W * n_win) < 1e-9 * g[2, 4416]
+
 
 
 @pytest.mark.parametrize("compat,sampling", [(0, "importanceSampling"), (0, "bruteForce")])

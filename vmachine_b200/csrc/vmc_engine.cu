@@ -776,7 +776,7 @@ int vmc_sample(vmc_engine *e, int iteration, int steps, int burn_in, vmc_sums *o
     if (n_slots > 0) {
         CUDA_TRY(cudaMemsetAsync(e->d_mlp_out, 0, 2 * MLP_PARAMS * sizeof(double), e->stream));
         CUDA_TRY(mlp_launch_grad(e->gen, e->N, e->dim, e->d_snap_x, e->d_snap_e, (long long)W * n_slots,
-                                 e->d_mlp_out, e->stream));
+                                 e->d_mlp_out, e->stream, e->d_status));
     }
     CUDA_TRY(cudaEventRecord(e->ev1, e->stream));
     if (e->d_replay) e->replay_pos += steps;
@@ -1012,7 +1012,8 @@ int vmc_eval(vmc_engine *e, double *grad, double *lap, double *pgrad, double *en
         cudaError_t ge = cudaMemcpyAsync(dx, xf.data(), xf.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream);
         if (ge == cudaSuccess) ge = cudaMemsetAsync(dout, 0, W * 2 * MLP_PARAMS * sizeof(double), e->stream);
         for (size_t w = 0; w < W && ge == cudaSuccess; ++w)
-            ge = mlp_launch_grad(e->gen, e->N, e->dim, dx + w * e->D, nullptr, 1, dout + w * 2 * MLP_PARAMS, e->stream);
+            ge = mlp_launch_grad(e->gen, e->N, e->dim, dx + w * e->D, nullptr, 1, dout + w * 2 * MLP_PARAMS, e->stream,
+                                 e->d_status + w);
         std::vector<double> g(W * 2 * MLP_PARAMS);
         if (ge == cudaSuccess)
             ge = cudaMemcpyAsync(g.data(), dout, g.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream);

@@ -284,6 +284,353 @@ __global__ void __launch_bounds__(256) mlp_grad_kernel(const GenParams g, int N,
     }
 }
 
+// The same gradient sums with the pair network's GEMM-shaped work on the tensor
+// cores.  The pair rows of all snapshots (n_snap x N(N-1)/2) go through in tiles of
+// 128 rows, one row per thread of a 4-warp CTA (TMEM lane = row):
+//   G1  z2 = h1 W2^T                  M 128, N 64,  K 64   A = h1 (rows r, k inputs)
+//   G2  e1 = delta2 W2                M 128, N 64,  K 64   A = delta2 (rows r, j outputs)
+//   G3  [dW2 | db2] += [delta2^T; (E delta2)^T] [h1 | 1]      M 128 (j, then j E-weighted),
+//                                     N 80, K 128 (the tile's rows), accumulated in TMEM
+//   G4  [delta1 sums | h2 sums] += [delta1^T; h2^T] [1, E, r, s, E r, E s]
+//                                     M 128, N 16, K 128, accumulated in TMEM
+// with delta2 = w3 (1 - h2^2), h2 = tanh(z2 + b2), delta1 = e1 (1 - h1^2): G4 gives
+// db1, dW1 (r and s columns) and dw3 with their E-weighted forms.  Operands are
+// bfloat16, every non-weight operand as a high and a low part (the products of the
+// parts, 2 or 3 MMAs per K step, keep about 16 significant bits); W2 is bfloat16
+// already.  FP32 accumulation in TMEM, added to the FP64 output once per CTA.  The
+// one-body network (N rows per snapshot) runs on the CUDA cores as in
+// mlp_grad_kernel.  Every completion wait is bounded (TC_WAIT_LIMIT polls); on
+// expiry the CTA stops, sets *fail and still releases its tensor memory.
+constexpr int BT_ROWS = 128;
+constexpr int BT_A1 = 0;                   // h1 [r][k] K64: hi 16 KB, lo 16 KB
+constexpr int BT_A2 = 32768;               // delta2 [r][j] K64: hi, lo; later A4 hi [128][128]
+constexpr int BT_A3 = 65536;               // [delta2^T; E delta2^T] [128][K128]: hi 32 KB, lo 32 KB; A4 lo in the first half
+constexpr int BT_B3 = 131072;              // [h1^T; 1; 0] [80][K128]: hi 20 KB, lo 20 KB
+constexpr int BT_B4 = BT_B3 + 40960;       // [1, E, r, s, E r, E s, 0] [16][K128]: hi 4 KB, lo 4 KB
+constexpr int BT_W2 = BT_B4 + 8192;        // W2 [j][m] K64
+constexpr int BT_W2T = BT_W2 + 8192;       // W2^T [m][j] K64
+constexpr int BT_TILES = BT_W2T + 8192;    // 196 608 bytes of operand tiles
+constexpr int BT_SMEM = BT_TILES + 1024;  // + alignment slack
+constexpr int BT_COLS = 256;               // TMEM: G1 [0,64), G2 [64,128), G3 [128,208), G4 [208,224)
+__host__ __device__ constexpr uint32_t bt_idesc(int n) { return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24); }
+
+__device__ __forceinline__ uint32_t bt_off128(int row, int k)
+{
+    return (row & 7) * 16 + (row >> 3) * 2048 + (k >> 3) * 128 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint64_t bt_desc(uint32_t saddr, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+__device__ __forceinline__ void bt_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+                 "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bt_put(unsigned char *t, uint32_t off_hi, uint32_t lo_bytes, float v)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    *reinterpret_cast<__nv_bfloat16 *>(t + off_hi) = h;
+    *reinterpret_cast<__nv_bfloat16 *>(t + off_hi + lo_bytes) = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// The CTA's MMAs are visible and this thread's earlier TMEM reads are done; thread
+// 0 issues, the commit arrives on bar.  Returns false when the wait gave up.
+__device__ bool bt_commit_wait(uint32_t bar, uint32_t &phase)
+{
+    if (threadIdx.x == 0)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+    uint32_t done = 0;
+    for (long it = 0; it < TC_WAIT_LIMIT && !done; ++it)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar), "r"(phase)
+                     : "memory");
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return done != 0;
+}
+
+// tile writes by every thread visible to the tensor cores, then thread 0 may issue
+__device__ __forceinline__ void bt_publish()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(BT_ROWS) mlp_grad_tc_kernel(const GenParams g, int N, int dim,
+                                                              const float *__restrict__ snap_x,
+                                                              const double *__restrict__ snap_e, long long n_snap,
+                                                              double *out, unsigned *fail)
+{
+    extern __shared__ __align__(16) unsigned char btsm[];
+    __shared__ __align__(8) unsigned long long bar_mem;
+    __shared__ uint32_t tslot;
+    __shared__ int stop;
+    unsigned char *T = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(btsm) + 1023) & ~uintptr_t(1023));
+    const float *w = g.mlp;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int D = N * dim, npair = N * (N - 1) / 2;
+    const long long rows = n_snap * npair, tiles = (rows + BT_ROWS - 1) / BT_ROWS;
+    const uint32_t ts = (uint32_t)__cvta_generic_to_shared(T);
+    // constant tiles: W2 and W2^T, the ones row of B3, zero rows of B3 and B4
+    for (int i = t; i < MLP_H * MLP_H; i += BT_ROWS) {
+        const int a = i >> 6, b = i & 63;  // W2[a][b]: output a, input b
+        const __nv_bfloat16 v = __float2bfloat16_rn(w[MW_W2 + i]);
+        *reinterpret_cast<__nv_bfloat16 *>(T + BT_W2 + tc_off(a, b)) = v;
+        *reinterpret_cast<__nv_bfloat16 *>(T + BT_W2T + tc_off(b, a)) = v;
+    }
+    for (int i = t; i < 16 * BT_ROWS; i += BT_ROWS) {
+        const int n = i / BT_ROWS, k = i % BT_ROWS;
+        if (n >= 1) {  // B3 rows 65..79 stay zero (row 64 = ones, written per tile)
+            *reinterpret_cast<__nv_bfloat16 *>(T + BT_B3 + bt_off128(64 + n, k)) = __float2bfloat16_rn(0.0f);
+            *reinterpret_cast<__nv_bfloat16 *>(T + BT_B3 + 20480 + bt_off128(64 + n, k)) = __float2bfloat16_rn(0.0f);
+        }
+        if (n >= 6) {
+            *reinterpret_cast<__nv_bfloat16 *>(T + BT_B4 + bt_off128(n, k)) = __float2bfloat16_rn(0.0f);
+            *reinterpret_cast<__nv_bfloat16 *>(T + BT_B4 + 4096 + bt_off128(n, k)) = __float2bfloat16_rn(0.0f);
+        }
+    }
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&bar_mem);
+    uint32_t phase = 0;
+    if (t == 0) {
+        stop = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(&tslot)),
+                     "r"(BT_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tslot;
+    const uint32_t lb = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes
+    bool first = true;
+    double n_rows = 0.0, e_rows = 0.0;
+
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        // ---- this thread's row: pair (i, j) of snapshot sn
+        const long long R = tile * BT_ROWS + t;
+        const bool valid = R < rows;
+        float r = 0.0f, sv = 0.0f, E = 0.0f;
+        if (valid) {
+            const long long sn = R / npair;
+            int i, j;
+            pair_of((int)(R - sn * npair), N, i, j);
+            float r2 = 0.0f;
+            for (int c = 0; c < dim; ++c) {
+                const float d = snap_x[sn * D + i * dim + c] - snap_x[sn * D + j * dim + c];
+                r2 += d * d;
+            }
+            r = sqrtf(r2);
+            sv = same_spin(i, j, N) ? 1.0f : 0.0f;
+            E = snap_e ? (float)snap_e[sn] : 0.0f;
+            n_rows += 1.0;
+            e_rows += snap_e ? snap_e[sn] : 0.0;
+        }
+        // ---- h1 into A1 (rows) and B3 (columns); the ones row; B4's weights
+        for (int c = 0; c < 8; ++c) {
+            uint32_t hv[4], lv[4];
+            for (int e = 0; e < 4; ++e) {
+                float h[2];
+                for (int q = 0; q < 2; ++q) {
+                    const int k = 8 * c + 2 * e + q;
+                    h[q] = valid ? mlp_tanh(fmaf(w[MW_W1 + 2 * k], r, fmaf(w[MW_W1 + 2 * k + 1], sv, w[MW_B1 + k])))
+                                 : 0.0f;
+                    bt_put(T + BT_B3, bt_off128(k, t), 20480, h[q]);
+                }
+                hv[e] = pack_bf16(h[0], h[1]);
+                const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&hv[e]);
+                lv[e] = pack_bf16(h[0] - __bfloat162float(hi.x), h[1] - __bfloat162float(hi.y));
+            }
+            *reinterpret_cast<uint4 *>(T + BT_A1 + tc_off(t, 8 * c)) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+            *reinterpret_cast<uint4 *>(T + BT_A1 + 16384 + tc_off(t, 8 * c)) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+        }
+        bt_put(T + BT_B3, bt_off128(64, t), 20480, valid ? 1.0f : 0.0f);
+        const float wv[6] = {valid ? 1.0f : 0.0f, E, r, sv, E * r, E * sv};
+        for (int n = 0; n < 6; ++n) bt_put(T + BT_B4, bt_off128(n, t), 4096, wv[n]);
+        // ---- G1: z2 = h1 W2^T
+        bt_publish();
+        if (t == 0)
+            for (int st = 0; st < 4; ++st) {
+                const uint64_t b = bt_desc(ts + BT_W2 + st * 256, 1024);
+                bt_mma(tmem, bt_desc(ts + BT_A1 + st * 256, 1024), b, bt_idesc(64), st > 0);
+                bt_mma(tmem, bt_desc(ts + BT_A1 + 16384 + st * 256, 1024), b, bt_idesc(64), 1);
+            }
+        if (!bt_commit_wait(bar, phase)) stop = 1;
+        __syncthreads();
+        if (stop) break;
+        // ---- delta2 into A2 (rows) and A3 (columns, plain and E-weighted)
+        for (int c = 0; c < 4; ++c) {
+            uint32_t z[16];
+            tmem_ld16(lb + 16 * c, z);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            for (int e = 0; e < 16; e += 8) {
+                uint32_t dh[4], dl[4];
+                for (int q = 0; q < 8; q += 2) {
+                    float dd[2];
+                    for (int u = 0; u < 2; ++u) {
+                        const int m = 16 * c + e + q + u;
+                        const float h2 = mlp_tanh(__uint_as_float(z[e + q + u]) + w[MW_B2 + m]);
+                        dd[u] = valid ? w[MW_W3 + m] * (1.0f - h2 * h2) : 0.0f;
+                        bt_put(T + BT_A3, bt_off128(m, t), 32768, dd[u]);
+                        bt_put(T + BT_A3, bt_off128(64 + m, t), 32768, E * dd[u]);
+                    }
+                    dh[q / 2] = pack_bf16(dd[0], dd[1]);
+                    const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&dh[q / 2]);
+                    dl[q / 2] = pack_bf16(dd[0] - __bfloat162float(hi.x), dd[1] - __bfloat162float(hi.y));
+                }
+                const uint32_t off = tc_off(t, 16 * c + e);
+                *reinterpret_cast<uint4 *>(T + BT_A2 + off) = make_uint4(dh[0], dh[1], dh[2], dh[3]);
+                *reinterpret_cast<uint4 *>(T + BT_A2 + 16384 + off) = make_uint4(dl[0], dl[1], dl[2], dl[3]);
+            }
+        }
+        // ---- G2: e1 = delta2 W2;  G3: [dW2 | db2] += A3 B3
+        bt_publish();
+        if (t == 0) {
+            for (int st = 0; st < 4; ++st) {
+                const uint64_t b = bt_desc(ts + BT_W2T + st * 256, 1024);
+                bt_mma(tmem + 64, bt_desc(ts + BT_A2 + st * 256, 1024), b, bt_idesc(64), st > 0);
+                bt_mma(tmem + 64, bt_desc(ts + BT_A2 + 16384 + st * 256, 1024), b, bt_idesc(64), 1);
+            }
+            for (int st = 0; st < 8; ++st) {
+                const uint64_t ah = bt_desc(ts + BT_A3 + st * 256, 2048), al = bt_desc(ts + BT_A3 + 32768 + st * 256, 2048);
+                const uint64_t bh = bt_desc(ts + BT_B3 + st * 256, 2048), bl = bt_desc(ts + BT_B3 + 20480 + st * 256, 2048);
+                bt_mma(tmem + 128, ah, bh, bt_idesc(80), (first && st == 0) ? 0u : 1u);
+                bt_mma(tmem + 128, ah, bl, bt_idesc(80), 1);
+                bt_mma(tmem + 128, al, bh, bt_idesc(80), 1);
+            }
+        }
+        if (!bt_commit_wait(bar, phase)) stop = 1;
+        __syncthreads();
+        if (stop) break;
+        // ---- delta1 (from e1 and h1) and h2 (from z2) into A4 = [delta1^T; h2^T]:
+        // hi in the A2 region, lo in the first half of the A3 region (both free now)
+        for (int c = 0; c < 4; ++c) {
+            uint32_t ez[16], z[16];
+            tmem_ld16(lb + 64 + 16 * c, ez);
+            tmem_ld16(lb + 16 * c, z);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            for (int e = 0; e < 16; ++e) {
+                const int k = 16 * c + e;
+                const uint32_t o = tc_off(t, k);
+                const float hk = __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(T + BT_A1 + o)) +
+                                 __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(T + BT_A1 + 16384 + o));
+                const float d1 = valid ? __uint_as_float(ez[e]) * (1.0f - hk * hk) : 0.0f;
+                const float h2 = valid ? mlp_tanh(__uint_as_float(z[e]) + w[MW_B2 + k]) : 0.0f;
+                const uint32_t o1 = bt_off128(k, t), o2 = bt_off128(64 + k, t);
+                const __nv_bfloat16 a = __float2bfloat16_rn(d1), b = __float2bfloat16_rn(h2);
+                *reinterpret_cast<__nv_bfloat16 *>(T + BT_A2 + o1) = a;
+                *reinterpret_cast<__nv_bfloat16 *>(T + BT_A3 + o1) = __float2bfloat16_rn(d1 - __bfloat162float(a));
+                *reinterpret_cast<__nv_bfloat16 *>(T + BT_A2 + o2) = b;
+                *reinterpret_cast<__nv_bfloat16 *>(T + BT_A3 + o2) = __float2bfloat16_rn(h2 - __bfloat162float(b));
+            }
+        }
+        // ---- G4: [delta1 | h2] sums += A4 B4
+        bt_publish();
+        if (t == 0)
+            for (int st = 0; st < 8; ++st) {
+                const uint64_t ah = bt_desc(ts + BT_A2 + st * 256, 2048), al = bt_desc(ts + BT_A3 + st * 256, 2048);
+                const uint64_t bh = bt_desc(ts + BT_B4 + st * 256, 2048), bl = bt_desc(ts + BT_B4 + 4096 + st * 256, 2048);
+                bt_mma(tmem + 208, ah, bh, bt_idesc(16), (first && st == 0) ? 0u : 1u);
+                bt_mma(tmem + 208, ah, bl, bt_idesc(16), 1);
+                bt_mma(tmem + 208, al, bh, bt_idesc(16), 1);
+            }
+        if (!bt_commit_wait(bar, phase)) stop = 1;
+        __syncthreads();
+        if (stop) break;
+        first = false;
+    }
+    // ---- the TMEM sums to the FP64 output: row t of G3 and G4
+    const int P = MLP_PARAMS;
+    if (!stop && !first) {
+        const int j = t & 63;
+        double *o = out + (t < 64 ? 0 : P);  // rows 64..127: E-weighted
+        for (int c = 0; c < 5; ++c) {
+            uint32_t v[16];
+            tmem_ld16(lb + 128 + 16 * c, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            for (int e = 0; e < 16; ++e) {
+                const int m = 16 * c + e;
+                const double x = (double)__uint_as_float(v[e]);
+                if (m < 64) atomicAdd(&o[MW_W2 + j * MLP_H + m], x);
+                else if (m == 64) atomicAdd(&o[MW_B2 + j], x);
+            }
+        }
+        uint32_t v[16];
+        tmem_ld16(lb + 208, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (t < 64) {  // delta1 rows: 1, E, r, s, E r, E s
+            const int k = t;
+            atomicAdd(&out[MW_B1 + k], (double)__uint_as_float(v[0]));
+            atomicAdd(&out[P + MW_B1 + k], (double)__uint_as_float(v[1]));
+            atomicAdd(&out[MW_W1 + 2 * k], (double)__uint_as_float(v[2]));
+            atomicAdd(&out[MW_W1 + 2 * k + 1], (double)__uint_as_float(v[3]));
+            atomicAdd(&out[P + MW_W1 + 2 * k], (double)__uint_as_float(v[4]));
+            atomicAdd(&out[P + MW_W1 + 2 * k + 1], (double)__uint_as_float(v[5]));
+        } else {  // h2 rows: 1, E
+            atomicAdd(&out[MW_W3 + (t - 64)], (double)__uint_as_float(v[0]));
+            atomicAdd(&out[P + MW_W3 + (t - 64)], (double)__uint_as_float(v[1]));
+        }
+    }
+    if (stop && t == 0) atomicOr(fail, (unsigned)ST_TC_TIMEOUT);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BT_COLS) : "memory");
+    // b3: one per pair row
+    if (!stop) {
+        atomicAdd(&out[MW_B3], n_rows);
+        atomicAdd(&out[P + MW_B3], e_rows);
+    }
+    // ---- the one-body network of each snapshot, warp per particle (CUDA cores)
+    for (long long sn = blockIdx.x; sn < n_snap && !stop; sn += gridDim.x) {
+        const double Es = snap_e ? snap_e[sn] : 0.0;
+        for (int i = warp; i < N; i += BT_ROWS / 32) {
+            float r2 = 0.0f;
+            for (int c = 0; c < dim; ++c) r2 += snap_x[sn * D + i * dim + c] * snap_x[sn * D + i * dim + c];
+            const float r = sqrtf(r2);
+            const float h = mlp_tanh(fmaf(w[MW_V1 + lane], r, w[MW_C1 + lane]));
+            float z = w[MW_C2 + lane];
+            for (int k = 0; k < MLP_G; ++k) z = fmaf(w[MW_V2 + lane * MLP_G + k], __shfl_sync(FULL, h, k), z);
+            const float h2 = mlp_tanh(z), e2 = w[MW_V3 + lane] * (1.0f - h2 * h2);
+            float acc = 0.0f;
+            for (int m = 0; m < MLP_G; ++m) acc = fmaf(__shfl_sync(FULL, e2, m), w[MW_V2 + m * MLP_G + lane], acc);
+            const float e1 = acc * (1.0f - h * h);
+            for (int k = 0; k < MLP_G; ++k) {
+                const float v = e2 * __shfl_sync(FULL, h, k);
+                atomicAdd(&out[MW_V2 + lane * MLP_G + k], (double)v);
+                atomicAdd(&out[P + MW_V2 + lane * MLP_G + k], Es * v);
+            }
+            const int idx[4] = {MW_V1 + lane, MW_C1 + lane, MW_C2 + lane, MW_V3 + lane};
+            const float vals[4] = {e1 * r, e1, e2, h2};
+            for (int q = 0; q < 4; ++q) {
+                atomicAdd(&out[idx[q]], (double)vals[q]);
+                atomicAdd(&out[P + idx[q]], Es * vals[q]);
+            }
+        }
+        if (t == 0) {
+            atomicAdd(&out[MW_C3], (double)N);
+            atomicAdd(&out[P + MW_C3], Es * N);
+        }
+    }
+}
+
 }  // namespace
 
 cudaError_t upload_hermite_gen(const HermiteCoef &h) { return cudaMemcpyToSymbol(c_herm, &h, sizeof(h)); }
@@ -397,15 +744,23 @@ cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_
 namespace vmc {
 
 cudaError_t mlp_launch_grad(const GenParams &g, int N, int dim, const float *snap_x, const double *snap_e,
-                            long long n_snap, double *out, cudaStream_t st)
+                            long long n_snap, double *out, cudaStream_t st, unsigned *fail)
 {
     if (n_snap <= 0) return cudaSuccess;
-    const size_t smem = (size_t)MG_SMEM_FLOATS * sizeof(float);
-    cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g.mlp_tc && fail) {  // pair network on the tensor cores
+        cudaError_t e = cudaFuncSetAttribute(mlp_grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BT_SMEM);
+        if (e != cudaSuccess) return e;
+        const long long rows = n_snap * (N * (N - 1) / 2), tiles = (rows + BT_ROWS - 1) / BT_ROWS;
+        const long long grid = std::min<long long>(std::max(1LL, tiles), (long long)sms);
+        mlp_grad_tc_kernel<<<(unsigned)grid, BT_ROWS, BT_SMEM, st>>>(g, N, dim, snap_x, snap_e, n_snap, out, fail);
+        return cudaGetLastError();
+    }
+    const size_t smem = (size_t)MG_SMEM_FLOATS * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     const long long grid = std::min<long long>(n_snap, (long long)sms);
     mlp_grad_kernel<<<(unsigned)grid, 256, smem, st>>>(g, N, dim, snap_x, snap_e, n_snap, out);
     return cudaGetLastError();

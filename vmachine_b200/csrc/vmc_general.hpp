@@ -47,8 +47,10 @@ cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_
 cudaError_t upload_hermite_gen(const HermiteCoef &h);
 // dJ/dtheta of the MLP Jastrow summed over snapshots (positions n_snap x D floats,
 // local energies n_snap, or null = weights 0): out[0..P) += sum dJ/dtheta,
-// out[P..2P) += sum E dJ/dtheta (FP64 accumulators, zeroed by the caller).
+// out[P..2P) += sum E dJ/dtheta (FP64 accumulators, zeroed by the caller).  With
+// g.mlp_tc and a fail word, the pair network's products run on the tensor cores and
+// a completion wait that gives up ORs ST_TC_TIMEOUT into *fail.
 cudaError_t mlp_launch_grad(const GenParams &g, int N, int dim, const float *snap_x, const double *snap_e,
-                            long long n_snap, double *out, cudaStream_t st);
+                            long long n_snap, double *out, cudaStream_t st, unsigned *fail = nullptr);
 
 }  // namespace vmc
