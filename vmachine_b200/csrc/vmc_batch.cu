@@ -335,10 +335,12 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
         if (!e->general && e->refresh_interval > 0) b->any_refresh = true;
         if (!e->general)
             b->rebuild_smem = std::max(b->rebuild_smem, engine_rebuild_smem_per_warp(e));
-        b->sweep_smem = std::max(b->sweep_smem,
-                                 e->general ? (int)((GEN_SCR + gen_stage_doubles(e->gen, e->nacc_dev)) * sizeof(double))
-                                            : engine_sweep_smem_per_warp(e));
+        b->sweep_smem = std::max(b->sweep_smem, e->general ? (int)(GEN_SCR * sizeof(double)) : engine_sweep_smem_per_warp(e));
     }
+    if (dot_precision < 0)  // general-path systems only: slices as large as their staging
+        for (vmc_engine *e : b->sys)
+            b->sweep_smem = std::max(b->sweep_smem,
+                                     (int)((GEN_SCR + gen_stage_doubles(e->gen, e->nacc_dev)) * sizeof(double)));
     b->precision = dot_precision >= 0 ? dot_precision : VMC_PRECISION_FP64;
     if (b->compat < 0) b->compat = b->sys[0]->compat;
     b->stride = b->max_nacc + BATCH_EXTRA;

@@ -64,14 +64,18 @@ __device__ __forceinline__ bool batch_next(const BatchLaunch &b, int lane, int2 
 
 // The general-path walkers of an item, out of line: its FP64 code is register-hungry
 // and would otherwise raise the pressure in the dot paths of the same kernel.
-// The warp's slice: GEN_SCR scratch doubles, then the staged record and accumulators.
+// The warp's slice (`slice` doubles): GEN_SCR scratch doubles, then the staged record
+// and, when they fit too, the accumulators (the slice is sized by the batch's largest
+// dot record, so a large general-path walker stages less or nothing).
 static __device__ __noinline__ void batch_gen_walkers(const SweepArgs &a, int steps, int off, const GenParams &g, int w0,
-                                               int w_end, double *scr)
+                                               int w_end, double *scr, int slice)
 {
     TcMlp tc{};  // the general systems of a batch have no MLP factor
-    double *stage = gen_stage_doubles(g, a.P.nacc) ? scr + GEN_SCR : nullptr;
+    const int full = gen_stage_doubles(g, a.P.nacc);
+    const bool rec_fits = !g.mlp && GEN_SCR + g.rec <= slice, acc_fits = full && GEN_SCR + full <= slice;
+    double *stage = rec_fits ? scr + GEN_SCR : nullptr;
     for (int w = w0; w < w_end; ++w)
-        gen_sweep_walker<false>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage);
+        gen_sweep_walker<false>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage, acc_fits);
 }
 
 template <typename T, int FX>
@@ -96,7 +100,8 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3) batch_sweep_ker
         case 6: sweep_walkers<T, 2, 6, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
         case 7: sweep_walkers<T, 2, 7, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
         default:
-            batch_gen_walkers(sy.a, steps, off, c_gen[sy.gen], item.y, w_end, reinterpret_cast<double *>(ws));
+            batch_gen_walkers(sy.a, steps, off, c_gen[sy.gen], item.y, w_end, reinterpret_cast<double *>(ws),
+                              b.smem_per_warp / (int)sizeof(double));
             break;
         }
     }

@@ -696,7 +696,8 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     }
     const bool rbmp = std::count(c.elements.begin(), c.elements.end(), (int)E_RBMPRODUCT) > 0;
     if (rbmp && (D > GEN_SCR / 4 || c.hidden > 64)) return "RBMProduct: at most 64 coordinates and 64 hidden units";
-    // record layout (doubles): x | fc | grad | energies (4) | pgrad (E p_max) | inverse (2 n n)
+    // record layout (doubles): x | fc | grad | energies (4) | pgrad (E p_max) | inverse (2 n n) |
+    // orbital derivatives at every particle (N n 2 dim) | MLP caches
     g.off_fc = D;
     g.off_g = 2 * D;
     g.off_en = 3 * D;
@@ -704,7 +705,8 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     g.off_inv = round_up(g.off_pg + g.EP, 2);
     const bool mlp = std::count(c.elements.begin(), c.elements.end(), (int)E_MLP) > 0;
     if (mlp && (N > 32 || dim * N > 96)) return "MLP Jastrow: at most 32 particles on this engine";
-    g.off_uc = g.off_inv + 2 * g.n * g.n;                 // MLP caches: N x N x 3, N x 3
+    g.off_dphi = g.off_inv + 2 * g.n * g.n;               // orbital derivatives: N x n x 2 dim
+    g.off_uc = g.off_dphi + N * g.n * 2 * dim;             // MLP caches: N x N x 3, N x 3
     g.off_oc = g.off_uc + (mlp ? N * N * 3 : 0);
     g.rec = round_up(g.off_oc + (mlp ? N * 3 : 0), 2);
     return "";

@@ -22,6 +22,7 @@ struct GenParams {
     const double *theta;        // E x p_max parameters on the device
     const float *mlp;           // MLP Jastrow weights rounded to bfloat16 (MLP_PARAMS), or null
     int off_uc, off_oc;         // MLP caches: (u, u', u'') per pair i < j, (chi, chi', chi'') per particle
+    int off_dphi;               // Slater: d phi_o / dx_c and d2 phi_o / dx_c^2 at particle q, [q][o][2 dim]
     // parameters accumulated per walker (all but padding and the MLP row, whose
     // gradient comes from snapshots): accumulator 9 + c holds parameter act[c]
     const int *act;

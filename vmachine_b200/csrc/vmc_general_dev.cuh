@@ -290,10 +290,12 @@ __device__ __forceinline__ void pair_of(int q, int N, int &i, int &j)
 // gradient, energies and parameter gradients into the record and, when given,
 // the per-element outputs of one walker (grad E x D, lap E, pgrad E x p_max,
 // energies 3).
+// moved: the particle whose position changed since the last evaluation (its cached
+// orbital derivatives are refreshed), or -1 to refresh every particle's.
 __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, double *rec,
                              const unsigned long long *mask, double *scr, int lane, double *o_grad,
                              double *o_lap, double *o_pg, double *o_en, const float *mw = nullptr,
-                             bool full = true)
+                             bool full = true, int moved = -1)
 {
     const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
     const double *x = rec;
@@ -326,17 +328,31 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 1: {  // Slater determinant (slaterdeterminant.cpp:155-191)
-            const int n = g.n;
+            const int n = g.n, nd = 2 * dim;
+            double *dphi = rec + g.off_dphi;
+            // orbital derivatives of the particles that moved (lanes over (particle,
+            // orbital)); the other particles' are unchanged in the cache
+            const int q0 = moved < 0 ? 0 : moved, nq = moved < 0 ? N : 1;
+            for (int t = lane; t < nq * n; t += 32) {
+                const int q = q0 + t / n, o = t - (t / n) * n;
+                double v, d1[3], d2[3];
+                gen_orbital(g, dim, P.Z, o, x + q * dim, v, d1, d2);
+                double *cq = dphi + (size_t)(q * n + o) * nd;
+                for (int c = 0; c < dim; ++c) {
+                    cq[c] = d1[c];
+                    cq[dim + c] = d2[c];
+                }
+            }
+            __syncwarp();
             for (int q = lane; q < N; q += 32) {
                 const int b = q / n, il = q - b * n;
                 const double *row = inv + (size_t)(b * n + il) * n;
                 double dd[3] = {0.0, 0.0, 0.0}, sdd[3] = {0.0, 0.0, 0.0};
                 for (int o = 0; o < n; ++o) {
-                    double v, d1[3], d2[3];
-                    gen_orbital(g, dim, P.Z, o, x + q * dim, v, d1, d2);
+                    const double *cq = dphi + (size_t)(q * n + o) * nd;
                     for (int c = 0; c < dim; ++c) {
-                        dd[c] += d1[c] * row[o];
-                        sdd[c] += d2[c] * row[o];
+                        dd[c] += cq[c] * row[o];
+                        sdd[c] += cq[dim + c] * row[o];
                     }
                 }
                 for (int c = 0; c < dim; ++c) {
@@ -1016,13 +1032,14 @@ __host__ __device__ inline int gen_stage_doubles(const GenParams &g, int nacc)
 // Steps step_offset .. step_offset + steps - 1 of walker w by the calling warp.  scr: the warp's
 // GEN_SCR shared doubles; mw: the CTA's staged MLP weights or null; with TC the
 // CTA's four warps run in lockstep (inactive ones join the tensor-core steps).
-// stage: shared memory for the walker's record and accumulators (gen_stage_doubles),
-// or null to work on them in global memory; staged, every step's reads and writes
-// stay on chip and the record goes back once at the end.
+// stage: shared memory for the walker's record (g.rec doubles) and, with stage_acc,
+// its accumulators after it (gen_stage_doubles in all), or null to work on them in
+// global memory; staged, every step's reads and writes stay on chip and the record
+// goes back once at the end.
 template <bool TC>
 __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, int step_offset, const GenParams &g,
                                                  int w, bool active, double *scr, float *mw, TcMlp &tc, float *pre_w,
-                                                 double *stage = nullptr)
+                                                 double *stage = nullptr, bool stage_acc = true)
 {
     const Params &P = a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1032,13 +1049,14 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
     double *const grec = reinterpret_cast<double *>(P.state) + (size_t)ws * g.rec;
     double *const gacc = P.acc + (size_t)ws * P.nacc * 2;
     double *rec = grec, *acc = gacc;
-    const bool staged = stage && active;
+    const bool staged = stage && active, acc_staged = staged && stage_acc;
     if (staged) {
         for (int i = lane; i < g.rec; i += 32) stage[i] = grec[i];
-        for (int i = lane; i < 2 * P.nacc; i += 32) stage[g.rec + i] = gacc[i];
+        if (acc_staged)
+            for (int i = lane; i < 2 * P.nacc; i += 32) stage[g.rec + i] = gacc[i];
         __syncwarp();
         rec = stage;
-        acc = stage + g.rec;
+        if (acc_staged) acc = stage + g.rec;
     }
     double *x = rec, *fc = rec + g.off_fc;
     unsigned long long *mask = P.mask + (size_t)ws * N;
@@ -1171,7 +1189,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                     if (lane == 0) mask[p] = ~0ull;
                 }
                 __syncwarp();
-                gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false);
+                gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false, p);
             }
             if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
             const double *en = rec + g.off_en;
@@ -1220,7 +1238,8 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
     if (staged) {
         __syncwarp();
         for (int i = lane; i < g.rec; i += 32) grec[i] = rec[i];
-        for (int i = lane; i < 2 * P.nacc; i += 32) gacc[i] = acc[i];
+        if (acc_staged)
+            for (int i = lane; i < 2 * P.nacc; i += 32) gacc[i] = acc[i];
     }
     if (active && lane == 0) {
         P.counter[w] = ctr;
