@@ -189,3 +189,54 @@ def test_tensor_core_layer_tracks_fp32(N):
         el32, eltc = e32[w, :upto].sum(-1), etc[w, :upto].sum(-1)
         assert np.max(np.abs(eltc - el32) / np.abs(el32)) < 1e-3
     assert agree > 0.8 * W * steps
+
+
+@pytest.mark.parametrize("N", [6, 20])
+def test_mlp_dot_sweep_tracks_general_path(N):
+    """The MLP Jastrow on the FP32 dot sweep (mixed precision: incremental pair and
+    one-body caches, the tensor-core layer with the CTA in lockstep, FP64 rebuilds)
+    against the general FP64 path on one replayed stream: the same decisions for most
+    of the run and local energies within 1e-3 relative while the chains agree."""
+    from vmachine_b200 import Engine
+    from vmachine_b200.engine import KERNEL_DOT, KERNEL_GENERAL
+    W, steps = 8, 300
+    omega = 1.0 if N == 6 else 0.5
+    rng = np.random.default_rng(N + 70)
+    pos = rng.normal(0.0, 1.0 / np.sqrt(omega), (W, 2 * N))
+    stream = np.stack([rng.random((W, steps)), rng.normal(size=(W, steps)), rng.random((W, steps))], -1)
+    theta = theta_for(N + 2)
+    theta[2] *= 0.5
+    res = {}
+    for prec, variant in ((0, KERNEL_GENERAL), (1, KERNEL_DOT)):
+        with Engine(config(N, omega=omega), walkers=W, precision=prec, compat=0) as eng:
+            assert eng.info.kernel_variant == variant
+            eng.set_parameters(theta)
+            eng.init_walkers(pos)
+            res[prec] = eng.replay(stream)
+            assert not (eng.status() & 8).any()
+    (a64, e64), (a32, e32) = res[0], res[1]
+    agree = 0
+    for w in range(W):
+        diff = np.nonzero(a64[w] != a32[w])[0]
+        upto = diff[0] if len(diff) else steps
+        agree += upto
+        el64, el32 = e64[w, :upto].sum(-1), e32[w, :upto].sum(-1)
+        assert np.max(np.abs(el32 - el64) / np.abs(el64)) < 1e-3, w
+    assert agree > 0.8 * W * steps
+
+
+def test_mlp_dot_trains():
+    """One short optimisation on the dot sweep: finite energies and gradients, the
+    network's rows move, no walker flagged beyond rejected NaN proposals."""
+    from vmachine_b200 import Engine
+    N, W = 6, 256
+    text = config(N, steps=W * 400, extra=["numWalkers: 256", "precision: mixed", "compat: corrected"])
+    with Engine(text) as eng:
+        eng.init_walkers(None, seed=2)
+        t0 = eng.parameters()
+        hist = [eng.run_iteration(it) for it in range(5)]
+        t1 = eng.parameters()
+        assert all(np.isfinite(a.energy) for a in hist)
+        assert np.abs(t1[2] - t0[2]).max() > 0
+        assert (int(np.bitwise_or.reduce(eng.status())) & ~2) == 0
+

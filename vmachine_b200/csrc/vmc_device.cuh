@@ -40,6 +40,9 @@ enum : int {
 constexpr int FX_DOT_COMPAT = F_GAUSS | F_SLATER | F_PADE | F_COULOMB | F_IS | Q_PADE_RATIO |
                               Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
 constexpr int FX_DOT_CORRECTED = F_GAUSS | F_SLATER | F_PADE | F_COULOMB | F_IS;
+// the same dot with the learned MLP Jastrow in place of the Pade factor (corrected
+// mode): the sweep runs the CTA's walkers in lockstep for the tensor-core layer
+constexpr int FX_MLP_DOT = F_GAUSS | F_SLATER | F_MLP | F_COULOMB | F_IS;
 
 enum : int { SAMPLER_IS = 0, SAMPLER_BF = 1 };
 

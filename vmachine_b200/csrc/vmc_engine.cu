@@ -151,6 +151,7 @@ void free_engine(vmc_engine *e)
     cudaFree(e->d_snap_e);
     cudaFree(e->d_mlp_out);
     cudaFree(e->d_pos);
+    cudaFree(e->d_mlp_cache);
     cudaFree(e->d_dens_radial);
     cudaFree(e->d_dens_grid);
     cudaFree(e->d_dens_pair);
@@ -204,6 +205,14 @@ Params make_params(const vmc_engine *e)
         }
     }
     P.gamma_prev = e->gamma_prev;
+    P.mlpw = e->d_mlpw;
+    P.mlp_cache = e->d_mlp_cache;
+    P.mlp_cache_stride = e->N * e->N * 3 + e->N * 3;
+    if (e->flags == FX_MLP_DOT) {  // compact accumulators: the Gaussian's alpha only
+        P.ep = (int)e->act.size();
+        P.idx_alpha = 0;
+        P.idx_gamma = -1;
+    }
     // Pade spin coefficients (padejastrow.cpp:140-170)
     P.beta_same = e->dim == 2 ? 1.0 / 3 : e->dim == 3 ? 1.0 / 4 : 1.0 / 5;
     P.beta_anti = e->dim == 2 ? 1.0 : e->dim == 3 ? 1.0 / 2 : 1.0 / 3;
@@ -245,7 +254,9 @@ int run_rebuild(vmc_engine *e, int mode, double *drift)
     const size_t smem = (size_t)a.wpb * a.smem_per_warp;
     CUDA_TRY(cudaFuncSetAttribute(e->ks.rebuild, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (e->W + a.wpb - 1) / a.wpb;
-    return launch(e->ks.rebuild, grid, 32 * a.wpb, smem, e->stream, &a);
+    int rc = launch(e->ks.rebuild, grid, 32 * a.wpb, smem, e->stream, &a);
+    if (!rc && e->ks.rebuild_mlp) rc = launch(e->ks.rebuild_mlp, (e->W + 3) / 4, 128, 0, e->stream, &a);
+    return rc;
 }
 
 int run_sweep(vmc_engine *e, SweepArgs &a)
@@ -257,7 +268,8 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
     }
     a.wpb = e->wpb;
     a.smem_per_warp = sweep_smem_per_warp(e);
-    const size_t smem = (size_t)a.wpb * a.smem_per_warp;
+    // the MLP dot adds the CTA's weight block and tensor-core tiles in front
+    const size_t smem = (size_t)a.wpb * a.smem_per_warp + (e->flags == FX_MLP_DOT ? MLP_FAST_BYTES + TC_SMEM : 0);
     const void *fn = (!a.probe_k && !a.replay && !a.rec_en && !a.rec_acc && !a.dens_bins) ? e->ks.sweep_plain
                                                                                          : e->ks.sweep;
     CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -269,6 +281,10 @@ int choose_wpb(vmc_engine *e)
 {
     if (e->general) {
         e->wpb = 4;  // the general kernels' fixed warps per CTA
+        return VMC_OK;
+    }
+    if (e->flags == FX_MLP_DOT) {
+        e->wpb = 4;  // the CTA's four walkers fill one 128-row tensor-core tile
         return VMC_OK;
     }
     if (e->cfg.walkers_per_block > 0) {
@@ -360,12 +376,14 @@ int initial_weights(vmc_engine *e)
 
 int upload_theta(vmc_engine *e)
 {
-    if (!e->general) return VMC_OK;  // the quantum-dot kernels take their scalars by value
-    CUDA_TRY(cudaMemcpyAsync(e->d_theta, e->theta.data(), e->theta.size() * sizeof(double),
-                             cudaMemcpyHostToDevice, e->stream));
+    if (!e->general && e->mlp_e < 0) return VMC_OK;  // the quantum-dot kernels take their scalars by value
+    if (e->general)
+        CUDA_TRY(cudaMemcpyAsync(e->d_theta, e->theta.data(), e->theta.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, e->stream));
     if (e->mlp_e >= 0) {
-        // the networks run with their weights rounded to bfloat16 (nearest even)
-        std::vector<float> w(MLP_PARAMS);
+        // the networks run with their weights rounded to bfloat16 (nearest even); the
+        // device block also holds W2 and V2 transposed (MW_W2T, MW_V2T)
+        std::vector<float> w(MLP_SMEM_FLOATS, 0.0f);
         for (int i = 0; i < MLP_PARAMS; ++i) {
             const float f = (float)e->theta[(size_t)e->mlp_e * e->Pmax + i];
             uint32_t b;
@@ -373,6 +391,10 @@ int upload_theta(vmc_engine *e)
             b = ((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16) << 16;
             std::memcpy(&w[i], &b, 4);
         }
+        for (int k = 0; k < MLP_H; ++k)
+            for (int m = 0; m < MLP_H; ++m) w[MW_W2T + k * MLP_H + m] = w[MW_W2 + m * MLP_H + k];
+        for (int k = 0; k < MLP_G; ++k)
+            for (int m = 0; m < MLP_G; ++m) w[MW_V2T + k * MLP_G + m] = w[MW_V2 + m * MLP_G + k];
         CUDA_TRY(cudaMemcpyAsync(e->d_mlpw, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
         CUDA_TRY(cudaStreamSynchronize(e->stream));  // w is a local buffer
     }
@@ -432,6 +454,19 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     for (int el : c.elements)
         general |= el == E_SIMPLEJASTROW || el == E_RBMGAUSSIAN || el == E_RBMPRODUCT || el == E_MLP ||
                    (el == E_SLATER && c.basis == "hydrogenOrbital");
+    // the learned MLP Jastrow on the FP32 dot sweep: mixed precision, 2D closed-shell
+    // Slater(Hermite) x Gaussian x MLP, Coulomb, importance sampling, corrected mode,
+    // N <= 30 (one partner per lane); the general FP64 path takes the rest
+    bool mlp_dot = false;
+    if (c.precision == VMC_PRECISION_MIXED && c.mlp_tc && c.dim == 2 && c.basis == "hermite" && c.coulomb && !c.compat &&
+        c.sampling != "bruteForce" && c.elements.size() == 3 && c.hamiltonian == "harmonicOscillator") {
+        const auto has = [&](int el) { return std::count(c.elements.begin(), c.elements.end(), el) == 1; };
+        const int k = closed_shells_2d(c.N, 2);
+        if (has(E_SLATER) && has(E_GAUSSIAN) && has(E_MLP) && k >= 1 && k <= 5) {
+            mlp_dot = true;
+            general = false;
+        }
+    }
     for (int el : c.elements) {
         switch (el) {
         case E_GAUSSIAN: flags |= F_GAUSS; break;
@@ -481,8 +516,16 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     for (int el : c.elements) e->Pmax = std::max(e->Pmax, element_parameters(c, el));
     e->EP = e->E * e->Pmax;
     e->nacc = 9 + 2 * e->EP;
-    if (!general && e->nacc > 32) return reject("more than 11 parameters per walker is not supported");
+    if (!general && !mlp_dot && e->nacc > 32) return reject("more than 11 parameters per walker is not supported");
     e->nacc_dev = e->nacc;
+    if (mlp_dot) {  // per walker: the Gaussian's alpha; the network's gradient comes from snapshots
+        for (int i = 0; i < e->E; ++i) {
+            if (c.elements[i] == E_MLP) e->mlp_e = i;
+            if (c.elements[i] == E_GAUSSIAN) e->act.push_back(i * e->Pmax);
+        }
+        e->nacc_dev = 9 + 2 * (int)e->act.size();
+        e->gen.mlp_tc = c.mlp_tc ? 1 : 0;
+    }
     if (general) {
         if (e->precision == VMC_PRECISION_MIXED)
             return reject("mixed precision covers Gaussian, Hermite Slater, Pade and hydrogen-like "
@@ -547,8 +590,13 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
                 e->gen.act = e->d_act;
                 e->gen.n_act = (int)e->act.size();
             }
+            if (mlp_dot) {
+                const size_t stride = (size_t)e->N * e->N * 3 + e->N * 3;
+                CUDA_TRY(cudaMalloc(&e->d_mlp_cache, W * stride * sizeof(float)));
+                CUDA_TRY(cudaMemsetAsync(e->d_mlp_cache, 0, W * stride * sizeof(float), e->stream));
+            }
             if (e->mlp_e >= 0) {
-                CUDA_TRY(cudaMalloc(&e->d_mlpw, MLP_PARAMS * sizeof(float)));
+                CUDA_TRY(cudaMalloc(&e->d_mlpw, MLP_SMEM_FLOATS * sizeof(float)));
                 CUDA_TRY(cudaMalloc(&e->d_mlp_out, 2 * MLP_PARAMS * sizeof(double)));
                 e->gen.mlp = e->d_mlpw;
             }
@@ -603,7 +651,7 @@ int vmc_get_info(const vmc_engine *e, vmc_info *o)
     o->refresh_interval = e->refresh_interval;
     for (int i = 0; i < e->E && i < 8; ++i) o->element_kind[i] = e->cfg.elements[i];
     o->kernel_variant = e->general ? VMC_KERNEL_GENERAL
-                        : (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED) && e->K > 0
+                        : (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED || e->flags == FX_MLP_DOT) && e->K > 0
                             ? VMC_KERNEL_DOT : VMC_KERNEL_RUNTIME_FLAGS;
     return VMC_OK;
 }
@@ -983,6 +1031,11 @@ int vmc_eval(vmc_engine *e, double *grad, double *lap, double *pgrad, double *en
     a.pgrad = d + ng + nl;
     a.energies = d + ng + nl + np;
     int rc = VMC_OK;
+    if (e->flags == FX_MLP_DOT) {
+        cudaFree(d);
+        return fail(VMC_E_UNSUPPORTED, "vmc_eval: the MLP Jastrow dot in mixed precision samples only; "
+                                       "evaluate with precision: fp64");
+    }
     if (e->general) {
         const cudaError_t ge = gen_launch_state(a.P, e->gen, GEN_STATE, a.grad, a.lap, a.pgrad, a.energies, e->stream);
         if (ge != cudaSuccess) rc = fail(VMC_E_CUDA, cudaGetErrorString(ge));
@@ -1295,7 +1348,7 @@ int finish_sample(vmc_engine *e, const SamplePass &p, vmc_sums *out, std::vector
 {
     const double *dev_sums = p.dev_sums;
     sums.assign(e->nacc, 0.0);
-    if (e->general) {  // active parameters back to their (element, parameter) slots
+    if (e->general || e->flags == FX_MLP_DOT) {  // active parameters back to their (element, parameter) slots
         std::copy(dev_sums, dev_sums + 9, sums.begin());
         const size_t na = e->act.size();
         for (size_t c = 0; c < na; ++c) {

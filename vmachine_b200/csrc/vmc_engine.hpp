@@ -43,6 +43,7 @@ struct vmc_engine {
     // MLP Jastrow: bf16-rounded weights, parameter-gradient snapshots and sums
     int mlp_e = -1;                // element index, or -1
     float *d_mlpw = nullptr;
+    float *d_mlp_cache = nullptr;  // MLP Jastrow dot: per-walker pair and one-body caches
     float *d_snap_x = nullptr;
     double *d_snap_e = nullptr, *d_mlp_out = nullptr;
     size_t snap_cap = 0;           // snapshots the buffers hold

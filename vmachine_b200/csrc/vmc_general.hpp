@@ -31,12 +31,6 @@ struct GenParams {
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
 };
 
-// MLP Jastrow weight offsets (floats) in the packed parameter row
-enum : int {
-    MW_W1 = 0, MW_B1 = 128, MW_W2 = 192, MW_B2 = 4288, MW_W3 = 4352, MW_B3 = 4416,
-    MW_V1 = 4417, MW_C1 = 4449, MW_V2 = 4481, MW_C2 = 5505, MW_V3 = 5537, MW_C3 = 5569,
-};
-static_assert(MW_C3 + 1 == MLP_PARAMS, "MLP layout");
 
 // "" when the general path takes the configuration (fills g except theta), else why not.
 std::string gen_configure(const Config &c, int n_elements, int p_max, GenParams &g);

@@ -18,6 +18,7 @@
 // of Pade pairs computed with the current gamma, and the Philox step counter.
 #pragma once
 #include "vmc_device.cuh"
+#include "vmc_mlp.cuh"
 
 namespace vmc {
 
@@ -98,6 +99,13 @@ struct Params {
     unsigned long long *counter;  // W Philox step counters
     double *acc;               // W x nacc x 2 (sum, compensation)
     unsigned *status;          // W
+    // MLP Jastrow on the dot sweep: the weights (bfloat16-rounded floats in the CTA
+    // block layout, MLP_SMEM_FLOATS) and per walker the pair and one-body caches,
+    // (u, u', u'') of every ordered pair [i][j] then (chi, chi', chi'') of every
+    // particle, mlp_cache_stride floats
+    const float *mlpw;
+    float *mlp_cache;
+    int mlp_cache_stride;
 };
 
 struct SweepArgs {
@@ -191,6 +199,23 @@ __device__ __forceinline__ bool same_spin(int i, int j, int N)
     const int h = N >> 1;
     return (i < h) == (j < h);
 }
+
+}  // namespace vmc
+
+namespace vmc {
+
+// The tensor-core context of the MLP dot sweep: the CTA's weight block, its
+// tcgen05 state, and this warp's slot for the layer's per-partner outputs.
+struct MlpCtx {
+    float *w;
+    TcMlp *tc;
+    float *pre;
+};
+// shared-memory weight block of the MLP dot sweep: the packed row (its FP32 W2 slot
+// holds the value's low-part A tile) and V2 transposed in the W2^T slot
+constexpr int MLP_FAST_FLOATS = MLP_PARAMS + 2 + MLP_G * MLP_G;
+constexpr int MLP_FAST_BYTES = MLP_FAST_FLOATS * 4;
+static_assert(MLP_FAST_BYTES % 16 == 0 && (MW_W2 * 4) % 16 == 0, "MLP block alignment");
 
 }  // namespace vmc
 
@@ -460,6 +485,79 @@ __device__ __forceinline__ void rebuild_walkers(const Params &P, int mode, doubl
     }
 }
 
+// The MLP Jastrow part of a rebuild, after rebuild_kernel (which leaves the Jastrow
+// gradient vector and Laplacian sum at zero for these systems): every ordered pair's
+// (u, u', u'') and every particle's (chi, chi', chi'') from the FP32 network into the
+// walker's cache, the gradient vector gj, the Laplacian sum, and at initialisation
+// the Jastrow part of the importance-sampling force.  One warp per walker.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(128) rebuild_mlp_kernel(const RebuildArgs a)
+{
+    const Params &P = a.P;
+    const Layout L = P.L;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int w = blockIdx.x * 4 + wib;
+    if (w >= P.W) return;
+    const int N = P.N;
+    const float *wt = P.mlpw;
+    T *rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
+    const T *x = rec + L.off_x;
+    T *gj = rec + L.off_gj, *fc = rec + L.off_fc;
+    float *cache = P.mlp_cache + (size_t)w * P.mlp_cache_stride, *oc = cache + (size_t)N * N * 3;
+    for (int i = 0; i < N; ++i) {
+        double r2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) r2 += (double)x[i * DIM + c] * (double)x[i * DIM + c];
+        float c0, c1, c2;
+        mlp_body(wt, wt + MW_V2T, (float)sqrt(r2), lane, c0, c1, c2);
+        if (lane == 0) {
+            oc[i * 3] = c0;
+            oc[i * 3 + 1] = c1;
+            oc[i * 3 + 2] = c2;
+        }
+    }
+    __syncwarp();
+    double lap = 0.0;
+    for (int i = lane; i < N; i += 32) {
+        double g[DIM], ri2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            g[c] = 0.0;
+            ri2 += (double)x[i * DIM + c] * (double)x[i * DIM + c];
+        }
+        for (int j = 0; j < N; ++j) {
+            if (j == i) continue;
+            double dxv[DIM], r2 = 0.0;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+                dxv[c] = (double)x[i * DIM + c] - (double)x[j * DIM + c];
+                r2 += dxv[c] * dxv[c];
+            }
+            const double r = sqrt(r2);
+            const bool same = same_spin(i, j, N);
+            float u, du, ddu;
+            mlp_pair(wt, (float)r, same ? 1.0f : 0.0f, mlp_cusp(DIM, same), u, du, ddu);
+            float *c3 = cache + (size_t)(i * N + j) * 3;
+            c3[0] = u;
+            c3[1] = du;
+            c3[2] = ddu;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) g[c] += du * dxv[c] / r;
+            lap += ddu + (DIM - 1) * du / r;  // grad_i^2 u(r_ij); every ordered pair once
+        }
+        const double ri = sqrt(ri2), dc = oc[i * 3 + 1];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            const double gc = g[c] + dc * (double)x[i * DIM + c] / ri;
+            gj[i * DIM + c] = T(gc);
+            if (a.mode == RB_INIT && P.sampling == SAMPLER_IS) fc[i * DIM + c] += T(2.0 * gc);
+        }
+        lap += oc[i * 3 + 2] + (DIM - 1) * dc / ri;
+    }
+    lap = warp_sum(lap);
+    if (lane == 0) P.scal[(size_t)w * NSCAL + SC_LAPJ] = lap;
+}
+
 template <typename T, int DIM, int K>
 __global__ void __launch_bounds__(128, 3) rebuild_kernel(const RebuildArgs a)
 {
@@ -605,6 +703,7 @@ struct KernelSet {
     const void *sweep = nullptr, *rebuild = nullptr, *eval = nullptr, *initpos = nullptr;
     const void *sweep_plain = nullptr;  // production sweep: no probe, replay or recording
     const void *scatter = nullptr, *gather = nullptr;  // positions in and out of the records
+    const void *rebuild_mlp = nullptr;                  // MLP Jastrow dot: completes each rebuild
 };
 
 template <typename T, int DIM, int K, int FX>
@@ -625,6 +724,13 @@ KernelSet make_set()
 template <typename T, int K>
 bool select_2d(int flags, KernelSet &out)
 {
+    if constexpr (sizeof(T) == 4 && K >= 1 && K <= 5) {
+        if (flags == FX_MLP_DOT) {
+            out = make_set<T, 2, K, FX_MLP_DOT>();
+            out.rebuild_mlp = reinterpret_cast<const void *>(&rebuild_mlp_kernel<T, 2>);
+            return true;
+        }
+    }
     if (K > 0 && flags == FX_DOT_COMPAT) { out = make_set<T, 2, K, (K > 0 ? FX_DOT_COMPAT : 0)>(); return true; }
     if (K > 0 && flags == FX_DOT_CORRECTED) { out = make_set<T, 2, K, (K > 0 ? FX_DOT_CORRECTED : 0)>(); return true; }
     out = make_set<T, 2, K, 0>();

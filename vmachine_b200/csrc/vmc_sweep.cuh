@@ -235,8 +235,11 @@ __device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
 // walkers of one work item.
 template <typename T, int DIM, int K, int FX, bool PL>
 __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int step_offset,
-                                              unsigned char *warp_smem, int w_first, int w_end, int w_stride)
+                                              unsigned char *warp_smem, int w_first, int w_end, int w_stride,
+                                              MlpCtx *mctx = nullptr)
 {
+    // the MLP Jastrow dot: the CTA's warps step in lockstep (one tensor-core layer per step)
+    constexpr bool MLPJ = FX == FX_MLP_DOT;
     // PL: the production form (Philox numbers, no probe, no recording), with the
     // branches of the test and replay modes compiled out
     const int *const probe_k = PL ? nullptr : a.probe_k;
@@ -262,6 +265,9 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
     T *gj = sm + L.off_gj, *inv = sm + L.off_inv;
     const int flags = FX ? FX : P.flags;
     const bool is = flags & F_IS;
+    const int jas = flags & (F_PADE | F_MLP);  // a pair Jastrow with gradient vector gj and Laplacian sum
+    const int wib_l = threadIdx.x >> 5;
+    bool tc_fail = false;
 
     // accumulator slot of this lane: 0..7 energy moments, 8 accepts, then the
     // parameter gradients (kind 1 alpha, 2 gamma, 3 hydrogen-like alpha) and
@@ -275,7 +281,16 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
         pkind = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : j == P.idx_alpha_h ? 3 : 0;
     }
 
-    for (int w = w_first; w < w_end; w += w_stride) {
+    for (int w = w_first; MLPJ ? (w - wib_l < w_end) : (w < w_end); w += w_stride) {
+        if constexpr (MLPJ) {
+            if (w >= w_end || tc_fail) {  // no walker for this warp: join the CTA's tensor-core steps
+                for (int s = 0; s < steps && !tc_fail; ++s) {
+                    const unsigned st = tc_pair_layer(*mctx->tc, mctx->w, false, 0.0f, 0.0f, 0.0f, lane, wib_l, mctx->pre);
+                    tc_fail = __syncthreads_or(st != 0u);
+                }
+                continue;
+            }
+        }
         T *g_rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
         copy_in(sm, g_rec, L.rec, lane);
         for (int j = lane; j < N; j += 32) smask[j] = P.mask[(size_t)w * N + j];
@@ -293,7 +308,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
         __syncwarp();
 
         const bool use_philox = !probe_k && !replay;
-        for (int s0 = 0; s0 < steps; s0 += 32) {
+        float *mcache = MLPJ ? P.mlp_cache + (size_t)w * P.mlp_cache_stride : nullptr;
+        for (int s0 = 0; s0 < steps && !(MLPJ && tc_fail); s0 += 32) {
           if (use_philox) {
             // Lane-parallel Philox: lane i draws the numbers of step counter ctr + i
             // (the same per-step stream as a serial draw); each step of this block
@@ -317,7 +333,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             rng_u = v.w;
           }
           const int s_end = min(s0 + 32, steps);
-          for (int s = s0; s < s_end; ++s) {
+          for (int s = s0; s < s_end && !(MLPJ && tc_fail); ++s) {
             const int it_step = step_offset + s;
             const T wa = T(P.omega * P.alpha);
             // ---- 1. random numbers and the proposal
@@ -345,7 +361,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             T Gk = T(0);
             if (flags & F_GAUSS) Gk += -wa * xo;
             if (K > 0) Gk += dd[k];
-            if (flags & F_PADE) Gk += gj[k];
+            if (jas) Gk += gj[k];
             T rpo = T(0);
             if (flags & (F_HYDROGENLIKE | F_ATOM)) {
                 T r2s = T(0);
@@ -398,7 +414,67 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
 #pragma unroll
                 for (int jj = 0; jj < NJ; ++jj) gdel[jj][c] = T(0);
             }
-            if (flags & (F_PADE | F_COULOMB)) {
+            float mlp_un = 0.0f, mlp_dun = 0.0f, mlp_ddun = 0.0f, mlp_cn = 0.0f, mlp_dcn = 0.0f, mlp_ddcn = 0.0f;
+            if constexpr (MLPJ) {
+                // pair values of the moved particle's partners (lane j; N <= 32): new ones
+                // from the network (second layer on the tensor cores, the CTA in lockstep),
+                // old ones from the walker's cache
+                const int j = lane;
+                const bool pv = j < N && j != p;
+                float dvo[DIM], dvn[DIM], r2o = 0.0f, r2n = 0.0f;
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) {
+                    const float xj = pv ? (float)x[j * DIM + c] : 0.0f;
+                    const float xp = (float)((c == adim) ? xo : xpn[c]);
+                    dvo[c] = xp - xj;
+                    dvn[c] = (float)xpn[c] - xj;
+                    r2o = fmaf(dvo[c], dvo[c], r2o);
+                    r2n = fmaf(dvn[c], dvn[c], r2n);
+                }
+                const float iro = pv ? rsqrtf(r2o) : 0.0f, irn = pv ? rsqrtf(r2n) : 0.0f;
+                const bool same = same_spin(p, j, N);
+                const unsigned tst = tc_pair_layer(*mctx->tc, mctx->w, pv, r2n * irn, same ? 1.0f : 0.0f,
+                                                   mlp_cusp(DIM, same), lane, wib_l, mctx->pre);
+                tc_fail = __syncthreads_or(tst != 0u);
+                if (tc_fail) break;
+                if (pv) {
+                    mlp_un = mctx->pre[lane];
+                    mlp_dun = mctx->pre[32 + lane];
+                    mlp_ddun = mctx->pre[64 + lane];
+                    const float *co = mcache + (size_t)(p * N + j) * 3;
+                    const float uo = co[0], duo = co[1], dduo = co[2];
+                    sum_ratio = T(mlp_un - uo);
+#pragma unroll
+                    for (int c = 0; c < DIM; ++c) {
+                        gp_new[c] = T(mlp_dun * dvn[c] * irn);
+                        gdel[0][c] = T(duo * dvo[c] * iro - mlp_dun * dvn[c] * irn);
+                    }
+                    d_lap = T(2.0f * ((mlp_ddun + (DIM - 1) * mlp_dun * irn) - (dduo + (DIM - 1) * duo * iro)));
+                    d_vint = T(irn - iro);
+                }
+                // one-body term of the moved particle (lanes over the 32 hidden units)
+                float rp2n = 0.0f, rp2o = 0.0f;
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) {
+                    const float xp = (float)((c == adim) ? xo : xpn[c]);
+                    rp2n = fmaf((float)xpn[c], (float)xpn[c], rp2n);
+                    rp2o = fmaf(xp, xp, rp2o);
+                }
+                const float rpn1 = sqrtf(rp2n), rpo1 = sqrtf(rp2o);
+                mlp_body(mctx->w, mctx->w + MW_W2T, rpn1, lane, mlp_cn, mlp_dcn, mlp_ddcn);
+                if (lane == 0) {
+                    const float *oc = mcache + (size_t)N * N * 3 + p * 3;
+                    sum_ratio += T(mlp_cn - oc[0]);
+#pragma unroll
+                    for (int c = 0; c < DIM; ++c) gp_new[c] += T(mlp_dcn * (float)xpn[c] / rpn1);
+                    d_lap += T((mlp_ddcn + (DIM - 1) * mlp_dcn / rpn1) - (oc[2] + (DIM - 1) * oc[1] / rpo1));
+                }
+                T vals[8] = {sum_ratio, d_lap, T(0), d_vint, T(0), T(0), T(0), T(0)};
+#pragma unroll
+                for (int c = 0; c < DIM; ++c) vals[4 + c] = gp_new[c];
+                pair_total = warp_reduce_scatter8(vals, lane);
+                sum_ratio = __shfl_sync(FULL, pair_total, 0);
+            } else if (flags & (F_PADE | F_COULOMB)) {
                 const unsigned long long mp = smask[p];
                 const T gam = T(P.gamma), gamp = T(P.gamma_prev);
                 // old and new position of the moved particle side by side: every pair
@@ -463,7 +539,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 rpn = r2s * F::rsqrt(r2s);
             }
             const T rat_g = (flags & F_GAUSS) ? F::exp(wa * (xo * xo - xn * xn)) : T(1);
-            const T rat_p = (flags & F_PADE) ? F::exp(T(2) * sum_ratio) : T(1);
+            const T rat_p = jas ? F::exp(T(2) * sum_ratio) : T(1);
             const T rat_h = (flags & F_HYDROGENLIKE) ? F::exp(T(2 * P.alpha_h * P.Z) * (rpo - rpn)) : T(1);
             double prob = 1.0;
             if (FX && !probe_k) {
@@ -472,7 +548,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             } else {
                 for (int e = 0; e < P.n_elem; ++e) {
                     const int kind = P.elem_kind[e];
-                    const T r = kind == 0 ? rat_g : kind == 1 ? R * R : kind == 2 ? rat_p : kind == 6 ? rat_h : T(1);
+                    const T r = kind == 0 ? rat_g : kind == 1 ? R * R : (kind == 2 || kind == 7) ? rat_p
+                                : kind == 6 ? rat_h : T(1);
                     prob *= (double)r;
                     if (probe_k && lane == 0) a.probe_ratio[(size_t)w * P.n_elem + e] = (double)r;
                 }
@@ -490,7 +567,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     } else {
                         T gy = T(0);
                         if (flags & F_GAUSS) gy += -wa * xn;
-                        if (flags & F_PADE) gy += __shfl_sync(FULL, pair_total, 16 + 4 * adim);
+                        if (jas) gy += __shfl_sync(FULL, pair_total, 16 + 4 * adim);
                         if (flags & F_HYDROGENLIKE) gy += -T(P.alpha_h * P.Z) * xn / rpn;
                         if constexpr (K > 0) gy += slater_grad_new<T, DIM, K>(inv + (b * NO + pl) * IS, xpn, adim, R);
                         const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
@@ -519,12 +596,26 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 }
                 // owners of the reduced pair sums apply them: value v (lanes 4v..4v+3)
                 // 1, 2 -> SC_LAPJ, SC_BH2 (= v); 3 -> SC_VINT (= v); 4 + c -> gj of p
-                if ((flags & (F_PADE | F_COULOMB)) && (lane & 3) == 0 && lane >= 4 && lane < 16 + 4 * DIM) {
+                if ((flags & (F_PADE | F_MLP | F_COULOMB)) && (lane & 3) == 0 && lane >= 4 && lane < 16 + 4 * DIM) {
                     const int v = lane >> 2;
                     if (v < 4) {
-                        if ((v == 3) ? (flags & F_COULOMB) : (flags & F_PADE)) ssc[v] += (double)pair_total;
-                    } else if (flags & F_PADE) {
+                        if ((v == 3) ? (flags & F_COULOMB) : jas) ssc[v] += (double)pair_total;
+                    } else if (jas) {
                         gj[p * DIM + v - 4] = pair_total;
+                    }
+                }
+                if constexpr (MLPJ) {  // the moved particle's pair and one-body values into the cache
+                    if (lane < N && lane != p) {
+                        float *c1 = mcache + (size_t)(p * N + lane) * 3, *c2 = mcache + (size_t)(lane * N + p) * 3;
+                        c1[0] = c2[0] = mlp_un;
+                        c1[1] = c2[1] = mlp_dun;
+                        c1[2] = c2[2] = mlp_ddun;
+                    }
+                    if (lane == 0) {
+                        float *oc = mcache + (size_t)N * N * 3 + p * 3;
+                        oc[0] = mlp_cn;
+                        oc[1] = mlp_dcn;
+                        oc[2] = mlp_ddcn;
                     }
                 }
                 if constexpr (K > 0) {
@@ -577,7 +668,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         store_coords<T, DIM>(sdd, b * NO + lane, sd);
                     }
                 }
-                if (flags & F_PADE) {
+                if (jas) {
 #pragma unroll
                     for (int jj = 0; jj < NJ; ++jj) {
                         const int j = lane + 32 * jj;
@@ -587,10 +678,10 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
 #pragma unroll
                             for (int c = 0; c < DIM; ++c) gv[c] += gdel[jj][c];
                             store_coords<T, DIM>(gj, j, gv);
-                            smask[j] |= (1ull << p);
+                            if (flags & F_PADE) smask[j] |= (1ull << p);
                         }
                     }
-                    if (lane == (p & 31)) smask[p] = ~0ull;
+                    if ((flags & F_PADE) && lane == (p & 31)) smask[p] = ~0ull;
                 }
                 __syncwarp();
             }
@@ -610,7 +701,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         G += g_s;
                         lc += s_s - g_s * g_s;
                     }
-                    if (flags & F_PADE) G += g_j;
+                    if (jas) G += g_j;
                     if (flags & F_HYDROGENLIKE) {
                         const int q = c / DIM;
                         T r2s = T(0);
@@ -640,7 +731,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                                 for (int e = 0; e < VW; e += 2) {
                                     Two<T> A = two(T(0), T(0));
                                     if (flags & F_GAUSS) A = mul2(two(-wa, -wa), two(ax[e], ax[e + 1]));
-                                    if (flags & F_PADE) A = add2(A, two(aj[e], aj[e + 1]));
+                                    if (jas) A = add2(A, two(aj[e], aj[e + 1]));
                                     const Two<T> B = fma2(two(T(2), T(2)), two(ad[e], ad[e + 1]), A);
                                     k2 = fma2(A, B, add2(k2, two(as[e], as[e + 1])));
                                 }
@@ -658,12 +749,12 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         const int c = lane + 32 * i;
                         if (c < D)
                             coord_term(c, x[c], K > 0 ? dd[c] : T(0), K > 0 ? sdd[c] : T(0),
-                                       (flags & F_PADE) ? gj[c] : T(0));
+                                       jas ? gj[c] : T(0));
                     }
                 }
                 ks = warp_sum(ks);
                 double lap = (double)ks;
-                if (flags & F_PADE) lap += ssc[SC_LAPJ];
+                if (jas) lap += ssc[SC_LAPJ];
                 if (flags & F_GAUSS) lap -= P.omega * P.alpha * D;
                 if (flags & F_HYDROGENLIKE) lap -= 2.0 * P.alpha_h * P.Z * ssc[SC_INVR];
                 const double ekin = -0.5 * lap;
@@ -691,6 +782,18 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     const double q = lane < 8 ? qe : lane == 8 ? (accept ? 1.0 : 0.0) : qp;
                     kadd(acc_s, acc_c, q);
                     if (!PL && a.dens_bins > 0) density_sample<T>(a, x, N, DIM, lane);
+                    if constexpr (MLPJ) {
+                        // the MLP row's parameter gradient: positions and E_L every
+                        // snap_interval steps of the window, for the backward kernel
+                        if (win && a.snap_x && (it_step - a.win_lo) % a.snap_interval == 0) {
+                            const int slot = (it_step - a.win_lo) / a.snap_interval - a.snap_first;
+                            if (slot >= 0 && slot < a.snap_stride) {
+                                const size_t base = (size_t)w * a.snap_stride + slot;
+                                for (int t = lane; t < D; t += 32) a.snap_x[base * D + t] = (float)x[t];
+                                if (lane == 0) a.snap_e[base] = el;
+                            }
+                        }
+                    }
                 }
             }
             if (rec_acc && lane == 0) rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
@@ -712,6 +815,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             P.acc[((size_t)w * P.nacc + lane) * 2] = acc_s;
             P.acc[((size_t)w * P.nacc + lane) * 2 + 1] = acc_c;
         }
+        if (MLPJ && tc_fail) status |= ST_TC_TIMEOUT;
         status = __reduce_or_sync(FULL, status);
         if (lane == 0 && status) P.status[w] |= status;
         __syncwarp();
@@ -719,13 +823,32 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
 }
 
 template <typename T, int DIM, int K, int FX, bool PL>
-__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3)
+__global__ void __launch_bounds__(FX == FX_MLP_DOT ? 128 : sizeof(T) == 4 ? 256 : 128, FX == FX_MLP_DOT ? 2 : 3)
     sweep_kernel(const SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5;
-    sweep_walkers<T, DIM, K, FX, PL>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
-                                     blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb);
+    if constexpr (FX == FX_MLP_DOT) {
+        // shared memory: the MLP weight block | the tensor-core tiles | the warps' walkers
+        __shared__ __align__(8) unsigned long long tc_bar;
+        __shared__ uint32_t tc_slot;
+        __shared__ float tc_pre[4][96];
+        float *mw = reinterpret_cast<float *>(smem_raw);
+        for (int i = threadIdx.x; i < MLP_PARAMS; i += blockDim.x) mw[i] = a.P.mlpw[i];
+        for (int i = threadIdx.x; i < MLP_G * MLP_G; i += blockDim.x) mw[MW_W2T + i] = a.P.mlpw[MW_V2T + i];
+        TcMlp tc{};
+        tc_setup(tc, smem_raw + MLP_FAST_BYTES, mw, a.P.mlpw, &tc_bar, &tc_slot, wib, mw + MW_W2);
+        __syncthreads();
+        tc_ready(tc, &tc_slot);
+        MlpCtx ctx{mw, &tc, tc_pre[wib & 3]};
+        sweep_walkers<T, DIM, K, FX, PL>(a, a.steps, a.step_offset,
+                                         smem_raw + MLP_FAST_BYTES + TC_SMEM + (size_t)wib * a.smem_per_warp,
+                                         blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb, &ctx);
+        tc_teardown(tc, wib);
+    } else {
+        sweep_walkers<T, DIM, K, FX, PL>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
+                                         blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb);
+    }
 }
 
 }  // namespace vmc

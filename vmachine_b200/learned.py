@@ -15,13 +15,15 @@ import numpy as np
 from .engine import Engine
 
 
-def dot_config(N, omega, jastrow, walkers, steps, lr, dt=0.01, seed=7, extra=()):
+def dot_config(N, omega, jastrow, walkers, steps, lr, dt=0.01, seed=7, extra=(), precision="mixed"):
+    """Mixed precision runs both Jastrow factors on the FP32 dot sweep (the MLP's
+    second layer on the tensor cores); fp64 runs the MLP on the general path."""
     lines = [f"numParticles: {N}", "numDimensions: 2", "hamiltonian: harmonicOscillator",
              f"omega: {omega!r}", "interactionStyle: coulomb",
              "waveFunctionElement: slaterDeterminant", "waveFunctionElement: gaussian",
              f"waveFunctionElement: {jastrow}", "basis: hermite", "sampling: importanceSampling",
              f"stepLength: {dt!r}", "optimization: adam", f"learningRate: {lr!r}",
-             f"numSteps: {walkers * steps}", f"numWalkers: {walkers}", "precision: fp64",
+             f"numSteps: {walkers * steps}", f"numWalkers: {walkers}", f"precision: {precision}",
              f"rng: MersenneTwister {seed}", "compat: corrected"]
     return "\n".join(lines + list(extra)) + "\n"
 
@@ -66,10 +68,13 @@ def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps
     return out
 
 
-def sweep_speed(walkers=8192, steps=100, N=20, omega=0.5, tensor_cores=True, iterations=2):
+def sweep_speed(walkers=8192, steps=100, N=20, omega=0.5, tensor_cores=True, iterations=2, precision="mixed"):
     """Walker-moves per second of the MLP-Jastrow sweep (sampling and the backward
-    kernel included) over `iterations` optimisation iterations after one warm-up."""
-    text = dot_config(N, omega, "mlpJastrow", walkers, steps, 3e-4,
+    kernel included) over `iterations` optimisation iterations after one warm-up.
+    precision mixed: the FP32 dot sweep (tensor cores required); fp64: the general path."""
+    if not tensor_cores:
+        precision = "fp64"
+    text = dot_config(N, omega, "mlpJastrow", walkers, steps, 3e-4, precision=precision,
                       extra=[f"mlpTensorCores: {'true' if tensor_cores else 'false'}"])
     eng = Engine(text)
     try:
@@ -80,7 +85,7 @@ def sweep_speed(walkers=8192, steps=100, N=20, omega=0.5, tensor_cores=True, ite
             a = eng.run_iteration(1 + it)
         ms = eng.stopwatch_stop()
         moves = iterations * walkers * (eng.info.steps_per_walker + eng.info.burn_in)
-        return {"walkers": walkers, "steps_per_walker": steps, "tensor_cores": tensor_cores,
+        return {"walkers": walkers, "steps_per_walker": steps, "tensor_cores": tensor_cores, "precision": precision,
                 "ms_per_iteration": ms / iterations, "walker_moves_per_s": moves / (ms * 1e-3),
                 "energy": a.energy, "status": int(np.bitwise_or.reduce(eng.status()))}
     finally:
@@ -95,13 +100,15 @@ def main(argv=None):
     s = sub.add_parser("speed", help="sweep throughput of the MLP-Jastrow wave function")
     s.add_argument("--walkers", type=int, default=8192)
     s.add_argument("--steps", type=int, default=100)
-    s.add_argument("--cuda-cores", action="store_true", help="second layer on the CUDA cores")
+    s.add_argument("--cuda-cores", action="store_true", help="second layer on the CUDA cores (general path)")
+    s.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                   help="mixed: the FP32 dot sweep; fp64: the general path")
     c = sub.add_parser("compare", help="MLP against Pade at equal wall time")
     c.add_argument("--budget", type=float, default=120.0)
     c.add_argument("--walkers", type=int, default=4096)
     a = ap.parse_args(argv)
     if a.cmd == "speed":
-        print(json.dumps(sweep_speed(a.walkers, a.steps, tensor_cores=not a.cuda_cores)))
+        print(json.dumps(sweep_speed(a.walkers, a.steps, tensor_cores=not a.cuda_cores, precision=a.precision)))
     else:
         print(json.dumps(compare(walkers=a.walkers, budget_s=a.budget)))
 
