@@ -5,8 +5,9 @@ forward and backward kernels (N = 20, omega = 0.5 quantum dot).
   start (the network's output layers start at zero, so the untrained factor is the
   cusp term alone, with alpha = 1).
 - At equal wall time the trained MLP is not worse than the Pade-Jastrow trained by
-  the same engine (the difference is printed; the longer run in
-  vmachine_b200.learned.compare measured the MLP 0.018 +- 0.009 lower).
+  the same engine (the difference is printed; the 150 s run of
+  vmachine_b200.learned.compare measured the MLP 0.072 +- 0.008 lower).
+Both factors run on the mixed-precision dot sweep.
 Energies are of the frozen wave functions, with error bars over walkers.
 """
 import pytest
