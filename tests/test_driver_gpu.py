@@ -7,7 +7,8 @@ system.cpp:81-139) and its electron densities (sampler.cpp:639-692), on the GPU.
 - vmc_run_simulation: the convergence check ends the run rangeOfAdaptiveSteps + 1
   iterations after convergence, adaptive steps lengthen the last iterations, the
   energy files get one line per iteration, the last iteration writes the density
-  files and blocks its energies (doResampling)."""
+  files, blocks its energies and writes them to the instant-energy file
+  (doResampling)."""
 import os
 
 import numpy as np
@@ -93,6 +94,9 @@ def test_run_simulation_driver(tmp_path):
     assert one.shape == (bins,) and 0.9 * W * 4 * spw * 6 < one.sum() <= W * 4 * spw * 6
     grid = np.loadtxt(tmp_path / "onebody2.dat")
     assert grid.shape == (bins, bins) and grid.sum() > 0
+    inst = np.loadtxt(tmp_path / "0_0.dat")  # the last iteration's E_L, walker after walker
+    assert inst.shape == (W * 4 * spw,)
+    assert abs(inst.mean() - hist[-1].energy) < 1e-4 * abs(hist[-1].energy)
     del burn
 
 

@@ -963,6 +963,23 @@ int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)
         if (!rc && last && rec) {
             rc = block_record(e, rec, steps, e->burn_in, &e->final_blocking);
             e->have_final = rc == VMC_OK;
+            // the instant energies the reference blocks (sampler.cpp:624-632, appended over
+            // ranks by appendInstantFiles, sampler.cpp:407-425): the walkers' sampled E_L,
+            // walker after walker, one per line, into <path>0_0.dat (its instant number
+            // is 0 here), when at most INSTANT_FILE_LINES
+            const double lines = (double)e->W * (steps - e->burn_in);
+            if (!rc && lines <= INSTANT_FILE_LINES) {
+                std::vector<double> h((size_t)e->W * steps * 3);
+                CUDA_TRY(cudaMemcpyAsync(h.data(), rec, h.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+                CUDA_TRY(cudaStreamSynchronize(e->stream));
+                std::ofstream f(c.path + "0_0.dat");
+                if (!f) rc = fail(VMC_E_ARG, "cannot write '" + c.path + "0_0.dat'");
+                for (int w = 0; w < e->W && !rc; ++w)
+                    for (int t = e->burn_in; t < steps; ++t) {
+                        const double *q = h.data() + ((size_t)w * steps + t) * 3;
+                        f << (q[0] + q[1]) + q[2] << '\n';
+                    }
+            }
         }
         if (rec) {
             cudaStreamSynchronize(e->stream);

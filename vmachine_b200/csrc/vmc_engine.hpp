@@ -86,8 +86,10 @@ namespace vmc {
 
 // Longest FP64 refresh interval the drift autotuner may choose for any system.
 constexpr int REFRESH_CAP_MIN = 8192;
-// Device memory vmc_run_simulation may spend on the last iteration's energy record.
+// Device memory vmc_run_simulation may spend on the last iteration's energy record,
+// and the most lines it writes to the instant-energy file.
 constexpr double FINAL_RECORD_BYTES = 16.0e9;
+constexpr double INSTANT_FILE_LINES = 1.0e8;
 
 // Coefficients of the normalised Hermite recurrence (each kernel unit holds a copy
 // in constant memory).
