@@ -140,12 +140,13 @@ __device__ __forceinline__ double block_sum(double v, double *red)
 
 __global__ void __launch_bounds__(BL_THREADS) block_levels_kernel(const LevelArgs a)
 {
-    __shared__ double red[BL_THREADS / 32];
     __shared__ double st[BL_PARTS][BL_MAX][BL_STATS];
     const int w = blockIdx.x, d = a.d;
     const long long n = 1LL << d;
     double *scr = a.scratch + (size_t)w * BL_PARTS * n;
     const double *rw = a.rec + ((size_t)w * a.stride + a.first) * 3;
+    __shared__ double vred[BL_THREADS / 32][3 * BL_PARTS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int k = 0; k < d; ++k) {
         const long long m = n >> k;
         // level k values: level 0 from the record, level k >= 1 at scratch[n - 2m .. n - m)
@@ -158,27 +159,44 @@ __global__ void __launch_bounds__(BL_THREADS) block_levels_kernel(const LevelArg
             }
             return scr[(size_t)p * n + in_off + i];
         };
-        for (long long i = threadIdx.x; i < m; i += BL_THREADS) {
+        // thread t takes the pairs (2i, 2i + 1), i = t, t + BL_THREADS, ...: their sums,
+        // the lag-1 products inside the pair and to the next pair's first value, and the
+        // pair mean (the next level)
+        for (long long i2 = 2 * threadIdx.x; i2 < m; i2 += 2 * BL_THREADS) {
             for (int p = 0; p < BL_PARTS; ++p) {
-                const double x = value(i, p), X = x - a.mu[p];
-                S[p] += X;
-                Q[p] += X * X;
-                if (i + 1 < m) C[p] += X * (value(i + 1, p) - a.mu[p]);
-                if ((i & 1) == 0)  // next level: pairwise means (m is even)
-                    scr[(size_t)p * n + out_off + i / 2] = 0.5 * (x + value(i + 1, p));
+                const double x0 = value(i2, p), x1 = value(i2 + 1, p);
+                const double X0 = x0 - a.mu[p], X1 = x1 - a.mu[p];
+                S[p] += X0 + X1;
+                Q[p] += X0 * X0 + X1 * X1;
+                C[p] += X0 * X1;
+                if (i2 + 2 < m) C[p] += X1 * (value(i2 + 2, p) - a.mu[p]);
+                scr[(size_t)p * n + out_off + i2 / 2] = 0.5 * (x0 + x1);
             }
         }
+        // one block reduction for the twelve sums: shuffles, then one shared round
+        double v[3 * BL_PARTS];
         for (int p = 0; p < BL_PARTS; ++p) {
-            const double s1 = block_sum(S[p], red), s2 = block_sum(Q[p], red), s3 = block_sum(C[p], red);
-            if (threadIdx.x == 0) {
-                st[p][k][0] = s1;
-                st[p][k][1] = s2;
-                st[p][k][2] = s3;
-                st[p][k][3] = value(0, p) - a.mu[p];
-                st[p][k][4] = value(m - 1, p) - a.mu[p];
-            }
+            v[3 * p] = S[p];
+            v[3 * p + 1] = Q[p];
+            v[3 * p + 2] = C[p];
         }
-        __syncthreads();  // the next level reads what this one wrote
+#pragma unroll
+        for (int q = 0; q < 3 * BL_PARTS; ++q)
+            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 3 * BL_PARTS; ++q) vred[wid][q] = v[q];
+        __syncthreads();  // also: the next level reads what this one wrote
+        if (threadIdx.x < 3 * BL_PARTS) {
+            double t = 0.0;
+            for (int q = 0; q < BL_THREADS / 32; ++q) t += vred[q][threadIdx.x];
+            st[threadIdx.x / 3][k][threadIdx.x % 3] = t;
+        } else if (threadIdx.x < 4 * BL_PARTS) {
+            const int p = threadIdx.x - 3 * BL_PARTS;
+            st[p][k][3] = value(0, p) - a.mu[p];
+            st[p][k][4] = value(m - 1, p) - a.mu[p];
+        }
+        __syncthreads();  // vred reused by the next level
     }
     if (threadIdx.x == 0) {
         for (int p = 0; p < BL_PARTS; ++p) {
