@@ -74,6 +74,41 @@ __device__ __forceinline__ T orbital_dot(const T (&hv)[DIM][K], V &&v)
     return s;
 }
 
+// phi(r) . v and d_A phi(r) . v together, the orbital sum factorised along axis A:
+// part[m] = sum over orbitals with m_A = m of prod_{c != A} h_{m_c}(x_c) v_o, then
+// phi . v = sum_m h_m(x_A) part[m] and d_A phi . v = sum_m h'_m(x_A) part[m].
+template <typename T, int DIM, int K, int A, typename V>
+__device__ __forceinline__ T orbital_dot_axis(const T (&hv)[DIM][K], V &&v, T &grad)
+{
+    T part[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) part[m] = T(0);
+    for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
+        const int mc[3] = {m0, m1, m2};
+        T f = T(1);
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+            if (c != A) f = (c == (A == 0 ? 1 : 0)) ? hv[c][mc[c]] : f * hv[c][mc[c]];
+        part[mc[A]] += f * v(o);
+    });
+    T s = T(0), g = T(0);
+#pragma unroll
+    for (int m = 0; m < K; ++m) s += hv[A][m] * part[m];
+#pragma unroll
+    for (int m = 1; m < K; ++m) g += hC<T>(m) * hv[A][m - 1] * part[m];
+    grad = g;
+    return s;
+}
+
+// orbital_dot_axis with the axis chosen at run time (a warp-uniform branch).
+template <typename T, int DIM, int K, typename V>
+__device__ __forceinline__ T orbital_dot_grad(const T (&hv)[DIM][K], V &&v, int axis, T &grad)
+{
+    if (axis == 0) return orbital_dot_axis<T, DIM, K, 0>(hv, v, grad);
+    if (DIM == 2 || axis == 1) return orbital_dot_axis<T, DIM, K, (DIM > 1 ? 1 : 0)>(hv, v, grad);
+    return orbital_dot_axis<T, DIM, K, DIM - 1>(hv, v, grad);
+}
+
 // Per-degree partial sums of the derivative vectors: orbital o = (m0, m1, m2) with
 // inverse entry v adds, for each dimension c, prod_{c' != c} h_{m_c'} * v to
 // part[c][m_c].
@@ -175,24 +210,6 @@ __device__ __forceinline__ void store_coords(T *x, int j, const T (&in)[DIM])
 #pragma unroll
         for (int c = 0; c < DIM; ++c) x[j * DIM + c] = in[c];
     }
-}
-
-// d ln Psi / d x_k at the proposed point for the corrected Fokker-Planck Green's
-// ratio (compat off): Slater part (d_a phi(r_p') . inv[:, p]) / R.  Out of line so
-// its registers stay off the common path; compiled out of the compat kernels.
-template <typename T, int DIM, int K>
-__device__ __noinline__ T slater_grad_new(const T *row_p, const T *xpn, int adim, T R)
-{
-    T hv[DIM][K];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
-    T gd[DIM], sd[DIM];
-    orbital_derivs<T, DIM, K>(hv, [&](int o) { return row_p[o]; }, gd, sd);
-    T g = gd[0];
-#pragma unroll
-    for (int c = 1; c < DIM; ++c)
-        if (c == adim) g = gd[c];
-    return g / R;
 }
 
 // Reduce-scatter of 8 per-lane values over the warp (xor butterfly that halves the
@@ -385,7 +402,11 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             for (int c = 0; c < DIM; ++c) xpn[c] = (c == adim) ? xn : x[p * DIM + c];
 
             // ---- 2a. Slater: S_j = phi(r_p') . inv[:, j] for lane j, R = S_pl
-            T Sj = T(0), R = T(1);
+            // the corrected Green's ratio needs d ln Psi / d x_k at the proposed point:
+            // its Slater part d_adim phi(r_p') . inv[:, p] / R comes out of the same
+            // row contraction as R (lane pl)
+            const bool green_grad = is && !(flags & Q_IS_GREEN) && !probe_k;
+            T Sj = T(0), R = T(1), Gs = T(0);
             int b = 0, pl = 0;
             if constexpr (K > 0) {
                 b = p / NO;
@@ -393,15 +414,20 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 T hv[DIM][K];
 #pragma unroll
                 for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
+                T Gj = T(0);
                 if (lane < NO) {
                     // this lane's row (column `lane` of A^{-1}), 16-byte vector loads
                     T rv[NQ * VE];
                     const T *row = inv + (b * NO + lane) * IS;
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) vload<T>(row + q * VE, rv + q * VE);
-                    Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return rv[o]; });
+                    if (green_grad)
+                        Sj = orbital_dot_grad<T, DIM, K>(hv, [&](int o) { return rv[o]; }, adim, Gj);
+                    else
+                        Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return rv[o]; });
                 }
                 R = __shfl_sync(FULL, Sj, pl);
+                if (green_grad) Gs = __shfl_sync(FULL, Gj, pl);
             }
 
             // ---- 2b. pair terms of the moved particle (Pade, Coulomb)
@@ -569,7 +595,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         if (flags & F_GAUSS) gy += -wa * xn;
                         if (jas) gy += __shfl_sync(FULL, pair_total, 16 + 4 * adim);
                         if (flags & F_HYDROGENLIKE) gy += -T(P.alpha_h * P.Z) * xn / rpn;
-                        if constexpr (K > 0) gy += slater_grad_new<T, DIM, K>(inv + (b * NO + pl) * IS, xpn, adim, R);
+                        if constexpr (K > 0) gy += Gs / R;
                         const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
                         wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
                     }
