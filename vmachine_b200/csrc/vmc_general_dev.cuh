@@ -105,15 +105,15 @@ __device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const 
     if (nq == 2 && l == 0) { f = 2.0 - k * rr; fp = -k; }
     if (nq == 3 && l == 0) { f = 2.0 * k * k * rr * rr - 18.0 * k * rr + 27.0; fp = 4.0 * k * k * rr - 18.0 * k; fpp = 4.0 * k * k; }
     if (nq == 3 && l == 1) { f = k * rr - 6.0; fp = k; }
-    const double a = k / nq, ex = exp(-a * rr);
+    const double a = k * (nq == 1 ? 1.0 : nq == 2 ? 0.5 : 1.0 / 3.0), ex = exp(-a * rr), irr = 1.0 / rr;
     const double R = f * ex, R1 = (fp - a * f) * ex, R2 = (fpp - 2.0 * a * fp + a * a * f) * ex;
     const int ca = l == 1 ? (m == 1 ? 0 : m == -1 ? 1 : 2) : -1;  // m = 1: x, -1: y, 0: z
     const double A = ca >= 0 ? r[ca] : 1.0;
     v = A * R;
     for (int c = 0; c < 3; ++c) {
-        const double xc = r[c], u = xc / rr, dA = (c == ca) ? 1.0 : 0.0;
+        const double xc = r[c], u = xc * irr, dA = (c == ca) ? 1.0 : 0.0;
         d1[c] = dA * R + A * R1 * u;
-        d2[c] = 2.0 * dA * R1 * u + A * (R2 * u * u + R1 * (1.0 / rr - u * u / rr));
+        d2[c] = 2.0 * dA * R1 * u + A * (R2 * u * u + R1 * (1.0 - u * u) * irr);
         if (nq == 3 && g.horb3) {
             // compat: the reference's n = 3 "second derivatives" (hydrogenorbital.cpp:351-364),
             // which are not d^2/dx_c^2
@@ -282,6 +282,47 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 3: {  // SimpleJastrow (simplejastrow.cpp:67-111)
+            const int npair = N * (N - 1) / 2;
+            if (npair * dim <= GEN_SCR) {
+                // lanes over the pairs i < j: beta (x_i - x_j) / r into the scratch,
+                // the pair's Laplacian term and dJ/dbeta_ij = r; then lanes over the
+                // particles sum their pairs' terms (j ascending, as the reference)
+                double *tp = scr;
+                for (int q = lane; q < npair; q += 32) {
+                    int i, j;
+                    pair_of(q, N, i, j);
+                    double d[3], r2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        d[c] = x[i * dim + c] - x[j * dim + c];
+                        r2 += d[c] * d[c];
+                    }
+                    const double r = sqrt(r2), ir = 1.0 / r, beta = th[i + N * j];
+                    double c2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        const double cc = d[c] * ir;
+                        tp[q * dim + c] = beta * cc;
+                        c2 += 2.0 * beta * (1.0 - cc * cc) * ir;
+                    }
+                    lap_l += c2;
+                    pge[i + N * j] = r;
+                }
+                __syncwarp();
+                for (int i = lane; i < N; i += 32) {
+                    double gi[3] = {0.0, 0.0, 0.0};
+                    for (int j = 0; j < N; ++j) {
+                        if (j == i) continue;
+                        const int lo = min(i, j), hi = max(i, j);
+                        const double *t = tp + (lo * (2 * N - lo - 1) / 2 + hi - lo - 1) * dim;
+                        for (int c = 0; c < dim; ++c) gi[c] += i < j ? t[c] : -t[c];
+                    }
+                    for (int c = 0; c < dim; ++c) {
+                        G[i * dim + c] += gi[c];
+                        if (oge) oge[i * dim + c] = gi[c];
+                    }
+                }
+                __syncwarp();  // the scratch is free again for the next element
+                break;
+            }
             for (int i = lane; i < N; i += 32) {
                 double gi[3] = {0.0, 0.0, 0.0};
                 for (int j = 0; j < N; ++j) {
@@ -431,16 +472,19 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
     } else {
         for (int k = lane; k < D; k += 32) vx += x[k] * x[k];
     }
-    if (P.flags & F_COULOMB)
-        for (int i = lane; i < N; i += 32)
-            for (int j = i + 1; j < N; ++j) {
-                double r2 = 0.0;
-                for (int c = 0; c < dim; ++c) {
-                    const double t = x[i * dim + c] - x[j * dim + c];
-                    r2 += t * t;
-                }
-                vi += rsqrt(r2);
+    if (P.flags & F_COULOMB) {  // lanes over the pairs i < j
+        const int npair = N * (N - 1) / 2;
+        for (int q = lane; q < npair; q += 32) {
+            int i, j;
+            pair_of(q, N, i, j);
+            double r2 = 0.0;
+            for (int c = 0; c < dim; ++c) {
+                const double t = x[i * dim + c] - x[j * dim + c];
+                r2 += t * t;
             }
+            vi += rsqrt(r2);
+        }
+    }
     g2 = warp_sum(g2);
     vx = warp_sum(vx);
     vi = warp_sum(vi);
