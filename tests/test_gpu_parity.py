@@ -159,6 +159,38 @@ def test_corrected_mode_matches_oracle_chain():
     del Q_RBM_SORT
 
 
+@pytest.mark.parametrize("Z,elements,compat", [
+    (2, (SLATER, SIMPLEJASTROW), 1), (10, (SLATER, SIMPLEJASTROW), 1),
+    (10, (SLATER, SIMPLEJASTROW), 0), (10, (SLATER, PADE, SIMPLEJASTROW), 0)])
+def test_atom_sweep_matches_oracle_chain(Z, elements, compat):
+    """Atoms (hydrogen-orbital Slater determinant with SimpleJastrow and Pade-Jastrow
+    factors) take the general path's compiled 3D form: replayed chains of four
+    walkers against the oracle, reference Green's ratio and corrected."""
+    spec = SystemSpec(N=Z, d=3, Z=Z, atom=True, basis="hydrogenOrbital", elements=elements, step=0.01,
+                      quirks=SystemSpec().quirks if compat else 0)
+    rng = np.random.default_rng(Z + 7 * compat)
+    W, steps = 4, 300
+    pos = rng.normal(size=(W, spec.D))
+    stream = np.stack([rng.random((W, steps)), rng.normal(size=(W, steps)), rng.random((W, steps))], -1)
+    theta = np.zeros((len(elements), spec.p_max))
+    for e, el in enumerate(elements):
+        if el == SIMPLEJASTROW:
+            theta[e, :Z * Z] = rng.uniform(0.1, 0.5, Z * Z)
+        elif el == PADE:
+            theta[e, 0] = 0.8
+    with make_engine(spec, W, compat=compat) as eng:
+        eng.set_parameters(theta)
+        eng.init_walkers(pos)
+        acc, en = eng.replay(stream)
+        final = eng.positions()
+    p = pos.copy()
+    f = np.zeros_like(p)
+    out = Oracle().run(spec, theta, p, f, steps, 0, 0, 1, stream=stream)
+    assert np.array_equal(acc, out["accepted"])
+    assert rel(en, out["energies"]) < 1e-10
+    assert rel(final, p) < 1e-11
+
+
 @pytest.mark.parametrize("n", [6, 20, 56])
 def test_mixed_precision_tracks_fp64(n):
     """FP32 sweep with FP64 rebuilds: same decisions on a replayed stream (a flip

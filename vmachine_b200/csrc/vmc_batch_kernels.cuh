@@ -74,8 +74,12 @@ static __device__ __noinline__ void batch_gen_walkers(const SweepArgs &a, int st
     const int full = gen_stage_doubles(g, a.P.nacc);
     const bool rec_fits = !g.mlp && GEN_SCR + g.rec <= slice, acc_fits = full && GEN_SCR + full <= slice;
     double *stage = rec_fits ? scr + GEN_SCR : nullptr;
-    for (int w = w0; w < w_end; ++w)
-        gen_sweep_walker<false>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage, acc_fits);
+    for (int w = w0; w < w_end; ++w) {
+        if (g.variant == GV_ATOM)
+            gen_sweep_walker<false, GV_ATOM>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage, acc_fits);
+        else
+            gen_sweep_walker<false>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage, acc_fits);
+    }
 }
 
 template <typename T, int FX>

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
     if (lane == 0 && status) P.status[w] |= status;
 }
 
-template <bool TC>
+template <bool TC, int GV>
 __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs a, const GenParams g)
 {
     extern __shared__ __align__(16) double gsm[];
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
     const bool active = w < P.W;
     if (!TC && !active) return;
     const int nst = gen_stage_doubles(g, P.nacc);  // 0 with the MLP (gsm holds its weights)
-    gen_sweep_walker<TC>(a, a.steps, a.step_offset, g, w, active, scratch[wib], mw, tc, pre[wib],
+    gen_sweep_walker<TC, GV>(a, a.steps, a.step_offset, g, w, active, scratch[wib], mw, tc, pre[wib],
                          nst ? gsm + (size_t)wib * nst : nullptr);
     if (TC) tc_teardown(tc, wib);
 }
@@ -709,6 +709,9 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     g.off_uc = g.off_dphi + N * g.n * 2 * dim;             // MLP caches: N x N x 3, N x 3
     g.off_oc = g.off_uc + (mlp ? N * N * 3 : 0);
     g.rec = round_up(g.off_oc + (mlp ? N * 3 : 0), 2);
+    bool atom_set = slater && dim == 3 && g.basis == BASIS_HYDROGEN;
+    for (int e : c.elements) atom_set = atom_set && (e == (int)E_SLATER || e == (int)E_PADE || e == (int)E_SIMPLEJASTROW);
+    g.variant = atom_set ? GV_ATOM : GV_ANY;
     return "";
 }
 
@@ -731,13 +734,19 @@ cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_
     const bool tc = g.mlp && g.mlp_tc;
     const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0) +
                         (size_t)GEN_WPB * gen_stage_doubles(g, a.P.nacc) * sizeof(double);
-    const void *fn = tc ? (const void *)gen_sweep_kernel<true> : (const void *)gen_sweep_kernel<false>;
+    const bool atom = !tc && g.variant == GV_ATOM;
+    const void *fn = tc     ? (const void *)gen_sweep_kernel<true, GV_ANY>
+                     : atom ? (const void *)gen_sweep_kernel<false, GV_ATOM>
+                            : (const void *)gen_sweep_kernel<false, GV_ANY>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    const unsigned grid = (a.P.W + GEN_WPB - 1) / GEN_WPB;
     if (tc)
-        gen_sweep_kernel<true><<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(a, g);
+        gen_sweep_kernel<true, GV_ANY><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
+    else if (atom)
+        gen_sweep_kernel<false, GV_ATOM><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
     else
-        gen_sweep_kernel<false><<<(a.P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(a, g);
+        gen_sweep_kernel<false, GV_ANY><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
     return cudaGetLastError();
 }
 

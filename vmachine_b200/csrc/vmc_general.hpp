@@ -10,6 +10,14 @@ namespace vmc {
 
 enum : int { BASIS_HERMITE = 1, BASIS_HYDROGEN = 2 };
 enum : int { GEN_INIT = 0, GEN_STATE = 1 };
+// Compiled variants of the general path: GV_ANY takes every element, basis and
+// dimension at run time; GV_ATOM is the atoms' form (3D, a Slater determinant of
+// hydrogen orbitals with SimpleJastrow and/or Pade-Jastrow) with the dimension and the
+// element set compiled in, so per-coordinate arrays stay in registers and the
+// sweep's code is a fraction of the generic one.
+enum : int { GV_ANY = 0, GV_ATOM = 1 };
+__host__ __device__ constexpr int gv_dim(int gv, int dim) { return gv == GV_ATOM ? 3 : dim; }
+__host__ __device__ constexpr bool gv_has(int gv, int kind) { return gv == GV_ANY || (kind >= 1 && kind <= 3); }
 
 // Record layout (offsets in doubles), element data and orbital table of the
 // general path; passed by value to its kernels.
@@ -28,6 +36,7 @@ struct GenParams {
     const int *act;
     int n_act;
     int mlp_tc;                 // MLP sweep with the second layer on the tensor cores
+    int variant;                // GV_*: the compiled sweep that takes this system
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
 };
 

@@ -81,10 +81,12 @@ __device__ __forceinline__ void herm3(int m, double x, double &h, double &h1, do
 // R(r) = f(r) exp(-k r / n); derivatives by the chain rule:
 //   d_i phi   = (d_i A) R + A R' x_i / r
 //   d_i^2 phi = 2 (d_i A) R' x_i / r + A (R'' x_i^2 / r^2 + R' (1/r - x_i^2 / r^3))
-__device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const double *r, double &v,
-                            double *d1, double *d2)
+template <int GV>
+__device__ __forceinline__ void gen_orbital_t(const GenParams &g, int dim_rt, double Z, int o, const double *r,
+                                              double &v, double *d1, double *d2)
 {
-    if (g.basis == BASIS_HERMITE) {
+    const int dim = gv_dim(GV, dim_rt);
+    if (GV == GV_ANY && g.basis == BASIS_HERMITE) {
         double h[3], h1[3], h2[3];
         for (int c = 0; c < dim; ++c) herm3(g.orb[o][c], r[c], h[c], h1[c], h2[c]);
         v = 1.0;
@@ -123,6 +125,24 @@ __device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const 
                            : pre * A * (kr - 18.0) * (kr - 6.0) / rr;
         }
     }
+}
+
+__device__ void gen_orbital(const GenParams &g, int dim, double Z, int o, const double *r, double &v,
+                            double *d1, double *d2)
+{
+    gen_orbital_t<GV_ANY>(g, dim, Z, o, r, v, d1, d2);
+}
+
+// orbital o at r in variant GV: the generic variant calls the out-of-line function,
+// the compiled-in variants inline their own
+template <int GV>
+__device__ __forceinline__ void gen_orb(const GenParams &g, int dim, double Z, int o, const double *r, double &v,
+                                        double *d1, double *d2)
+{
+    if constexpr (GV == GV_ANY)
+        gen_orbital(g, dim, Z, o, r, v, d1, d2);
+    else
+        gen_orbital_t<GV>(g, dim, Z, o, r, v, d1, d2);
 }
 
 // RBMProduct visible vector: the coordinates, sorted ascending under the
@@ -172,6 +192,28 @@ __device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
     return same_spin(i, j, P.N) ? P.beta_same : P.beta_anti;
 }
 
+// Per-particle sums of pair vectors: tp holds t(i, j) for each pair i < j (pair
+// index as pair_of), particle i takes +t(i, j) for j > i and -t(j, i) for j < i, j
+// ascending; lanes over particles add the sums to G (and the per-element output).
+__device__ __forceinline__ void gen_pair_gather(const double *tp, int N, int dim, double *G, double *oge, int lane)
+{
+    __syncwarp();
+    for (int i = lane; i < N; i += 32) {
+        double gi[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < N; ++j) {
+            if (j == i) continue;
+            const int lo = min(i, j), hi = max(i, j);
+            const double *t = tp + (lo * (2 * N - lo - 1) / 2 + hi - lo - 1) * dim;
+            for (int c = 0; c < dim; ++c) gi[c] += i < j ? t[c] : -t[c];
+        }
+        for (int c = 0; c < dim; ++c) {
+            G[i * dim + c] += gi[c];
+            if (oge) oge[i * dim + c] = gi[c];
+        }
+    }
+    __syncwarp();  // the scratch is free again for the next element
+}
+
 // Evaluate the walker at its positions (eval_impl): per-element gradient,
 // Laplacian and parameter gradient, the local-energy parts.  Writes the total
 // gradient, energies and parameter gradients into the record and, when given,
@@ -179,12 +221,13 @@ __device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
 // energies 3).
 // moved: the particle whose position changed since the last evaluation (its cached
 // orbital derivatives are refreshed), or -1 to refresh every particle's.
-__device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, double *rec,
+template <int GV = GV_ANY>
+__device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, double *rec,
                              const unsigned long long *mask, double *scr, int lane, double *o_grad,
                              double *o_lap, double *o_pg, double *o_en, const float *mw = nullptr,
                              bool full = true, int moved = -1)
 {
-    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
+    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max, dim = gv_dim(GV, dim_rt);
     const double *x = rec;
     double *G = rec + g.off_g, *pg = rec + g.off_pg;
     const double *inv = rec + g.off_inv;
@@ -201,6 +244,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
         double *oge = o_grad ? o_grad + (size_t)e * D : nullptr;
         switch (P.elem_kind[e]) {
         case 0: {  // Gaussian (gaussian.cpp:62-78)
+            if (!gv_has(GV, 0)) break;
             const double wa = P.omega * th[0];
             double x2 = 0.0;
             for (int k = lane; k < D; k += 32) {
@@ -215,6 +259,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 1: {  // Slater determinant (slaterdeterminant.cpp:155-191)
+            if (!gv_has(GV, 1)) break;
             const int n = g.n, nd = 2 * dim;
             double *dphi = rec + g.off_dphi;
             // orbital derivatives of the particles that moved (lanes over (particle,
@@ -223,7 +268,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             for (int t = lane; t < nq * n; t += 32) {
                 const int q = q0 + t / n, o = t - (t / n) * n;
                 double v, d1[3], d2[3];
-                gen_orbital(g, dim, P.Z, o, x + q * dim, v, d1, d2);
+                gen_orb<GV>(g, dim, P.Z, o, x + q * dim, v, d1, d2);
                 double *cq = dphi + (size_t)(q * n + o) * nd;
                 for (int c = 0; c < dim; ++c) {
                     cq[c] = d1[c];
@@ -251,8 +296,38 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 2: {  // Pade-Jastrow (padejastrow.cpp:75-116)
+            if (!gv_has(GV, 2)) break;
             const double gam = th[0];
             double dg = 0.0;
+            const int npair = N * (N - 1) / 2;
+            if (npair * dim <= GEN_SCR) {
+                // lanes over the pairs i < j (as SimpleJastrow below)
+                double *tp = scr;
+                for (int q = lane; q < npair; q += 32) {
+                    int i, j;
+                    pair_of(q, N, i, j);
+                    double d[3], r2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        d[c] = x[i * dim + c] - x[j * dim + c];
+                        r2 += d[c] * d[c];
+                    }
+                    const double r = sqrt(r2), ir = 1.0 / r, beta = pade_beta_of(P, i, j);
+                    const double gp = pade_gamma(P, mask, i, j, gam);
+                    const double f1 = 1.0 / (1.0 + gp * r), f = beta * f1 * f1, h = r * f1;
+                    double c2 = 0.0;
+                    for (int c = 0; c < dim; ++c) {
+                        const double cc = d[c] * ir;
+                        tp[q * dim + c] = f * cc;
+                        c2 += 2.0 * f * (1.0 - (1.0 + 2.0 * gam * h) * cc * cc) * ir;
+                    }
+                    lap_l += c2;
+                    dg += beta * h * h;
+                }
+                gen_pair_gather(tp, N, dim, G, oge, lane);
+                dg = warp_sum(dg);
+                if (lane == 0) pge[0] = (P.flags & Q_PADE_DGAMMA) ? -0.5 * dg : -dg;
+                break;
+            }
             for (int i = lane; i < N; i += 32) {
                 double gi[3] = {0.0, 0.0, 0.0};
                 for (int j = 0; j < N; ++j) {
@@ -282,6 +357,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 3: {  // SimpleJastrow (simplejastrow.cpp:67-111)
+            if (!gv_has(GV, 3)) break;
             const int npair = N * (N - 1) / 2;
             if (npair * dim <= GEN_SCR) {
                 // lanes over the pairs i < j: beta (x_i - x_j) / r into the scratch,
@@ -306,21 +382,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
                     lap_l += c2;
                     pge[i + N * j] = r;
                 }
-                __syncwarp();
-                for (int i = lane; i < N; i += 32) {
-                    double gi[3] = {0.0, 0.0, 0.0};
-                    for (int j = 0; j < N; ++j) {
-                        if (j == i) continue;
-                        const int lo = min(i, j), hi = max(i, j);
-                        const double *t = tp + (lo * (2 * N - lo - 1) / 2 + hi - lo - 1) * dim;
-                        for (int c = 0; c < dim; ++c) gi[c] += i < j ? t[c] : -t[c];
-                    }
-                    for (int c = 0; c < dim; ++c) {
-                        G[i * dim + c] += gi[c];
-                        if (oge) oge[i * dim + c] = gi[c];
-                    }
-                }
-                __syncwarp();  // the scratch is free again for the next element
+                gen_pair_gather(tp, N, dim, G, oge, lane);
                 break;
             }
             for (int i = lane; i < N; i += 32) {
@@ -348,6 +410,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 4: {  // RBMGaussian (rbmgaussian.cpp:67-87)
+            if (!gv_has(GV, 4)) break;
             const double s2 = g.sigma * g.sigma;
             for (int k = lane; k < D; k += 32) {
                 const double t = (x[k] - th[k]) / s2;
@@ -359,6 +422,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 5: {  // RBMProduct (rbmproduct.cpp:167-189)
+            if (!gv_has(GV, 5)) break;
             const int H = g.hidden;
             const double s2 = 100.0 * g.sigma * g.sigma, s4 = s2 * s2;
             double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
@@ -385,6 +449,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;
         }
         case 7: {  // MLP Jastrow: caches of (u, u', u'') per pair and (chi, chi', chi'') per particle
+            if (!gv_has(GV, 7)) break;
             double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
             if (full) {  // from scratch (initialisation, parameter update, evaluation)
                 const int npair = N * (N - 1) / 2;
@@ -440,6 +505,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
             break;  // parameter gradients: mlp_grad_kernel, from snapshots
         }
         case 6: {  // HydrogenLike (hydrogenlike.cpp:268-286)
+            if (!gv_has(GV, 6)) break;
             const double az = th[0] * P.Z;
             double rs = 0.0;
             for (int i = lane; i < N; i += 32) {
@@ -510,12 +576,13 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim, doubl
 // and, when grad_y is given, d ln Psi / d y_k at the proposal (the corrected
 // Fokker-Planck Green's ratio).  Orbital values at the proposal go to the scratch
 // (the Sherman-Morrison update reuses them).  Returns the product in element order.
-__device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const double *rec,
+template <int GV = GV_ANY>
+__device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, const double *rec,
                              const unsigned long long *mask, double *scr, int lane, int k, double xn,
                              double *ratios, double *grad_y, double &R_out, const float *mw = nullptr,
                              const float *pre = nullptr)
 {
-    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max;
+    const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max, dim = gv_dim(GV, dim_rt);
     const double *x = rec;
     const int p = k / dim, adim = k - p * dim;
     double yp[3];
@@ -528,15 +595,17 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
         double r = 1.0;
         switch (P.elem_kind[e]) {
         case 0:  // gaussian.cpp:23-28
+            if (!gv_has(GV, 0)) break;
             r = exp(P.omega * th[0] * (xo * xo - xn * xn));
             gy += -P.omega * th[0] * xn;
             break;
         case 1: {  // slaterdeterminant.cpp:150-153, 177-180
+            if (!gv_has(GV, 1)) break;
             const int n = g.n, b = p / n, pl = p - b * n;
             double s = 0.0, sg = 0.0;
             if (lane < n) {
                 double v, d1[3], d2[3];
-                gen_orbital(g, dim, P.Z, lane, yp, v, d1, d2);
+                gen_orb<GV>(g, dim, P.Z, lane, yp, v, d1, d2);
                 scr[SCR_PHI + lane] = v;
                 const double iv = rec[g.off_inv + (size_t)(b * n + pl) * n + lane];
                 s = v * iv;
@@ -550,6 +619,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
             break;
         }
         case 2: {  // padejastrow.cpp:211-218
+            if (!gv_has(GV, 2)) break;
             const double gam = th[0];
             const int j0 = (P.flags & Q_PADE_RATIO) ? p + 1 : 0;
             double acc = 0.0, gyl = 0.0;
@@ -573,6 +643,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
             break;
         }
         case 3: {  // simplejastrow.cpp:145-156
+            if (!gv_has(GV, 3)) break;
             const int j0 = (P.flags & Q_SJ_RATIO) ? p + 1 : 0;
             double acc = 0.0, gyl = 0.0;
             for (int j = lane; j < N; j += 32) {
@@ -593,12 +664,14 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
             break;
         }
         case 4: {  // rbmgaussian.cpp:34-46
+            if (!gv_has(GV, 4)) break;
             const double s2 = g.sigma * g.sigma, a = xo - th[k], bn = xn - th[k];
             r = exp((a * a - bn * bn) / (2.0 * s2));
             gy += -bn / s2;
             break;
         }
         case 5: {  // rbmproduct.cpp:199-203
+            if (!gv_has(GV, 5)) break;
             const int H = g.hidden;
             const double s2 = 100.0 * g.sigma * g.sigma;
             double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
@@ -629,6 +702,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
             break;
         }
         case 7: {  // MLP Jastrow: exp(2 (J(y) - J(x))); the new pair and one-body values
+            if (!gv_has(GV, 7)) break;
                    // go to the scratch for an accepted move
             const double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
             double acc = 0.0, gyl = 0.0;
@@ -672,6 +746,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim, const
             break;
         }
         case 6: {  // hydrogenlike.cpp:231-242
+            if (!gv_has(GV, 6)) break;
             double rn2 = 0.0;
             for (int c = 0; c < dim; ++c) rn2 += yp[c] * yp[c];
             const double rn = sqrt(rn2);
@@ -762,7 +837,7 @@ __host__ __device__ inline int gen_stage_doubles(const GenParams &g, int nacc)
 // its accumulators after it (gen_stage_doubles in all), or null to work on them in
 // global memory; staged, every step's reads and writes stay on chip and the record
 // goes back once at the end.
-template <bool TC>
+template <bool TC, int GV = GV_ANY>
 __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, int step_offset, const GenParams &g,
                                                  int w, bool active, double *scr, float *mw, TcMlp &tc, float *pre_w,
                                                  double *stage = nullptr, bool stage_acc = true)
@@ -770,7 +845,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
     const Params &P = a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 
-    const int N = P.N, D = g.D, dim = D / N;
+    const int N = P.N, D = g.D, dim = gv_dim(GV, D / N);
     const int ws = active ? w : 0;  // record pointers of a warp without a walker are never used
     double *const grec = reinterpret_cast<double *>(P.state) + (size_t)ws * g.rec;
     double *const gacc = P.acc + (size_t)ws * P.nacc * 2;
@@ -857,7 +932,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
             const bool corrected = is && !(P.flags & Q_IS_GREEN) && !a.probe_k;
             double gy = 0.0, R = 1.0;
             double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
-            const double prob = gen_ratios(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
+            const double prob = gen_ratios<GV>(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
                                            corrected ? &gy : nullptr, R, mw, TC ? pre_w : nullptr);
             bool accept = true;
             if (!a.probe_k) {
@@ -915,7 +990,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                     if (lane == 0) mask[p] = ~0ull;
                 }
                 __syncwarp();
-                gen_evaluate(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false, p);
+                gen_evaluate<GV>(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false, p);
             }
             if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
             const double *en = rec + g.off_en;
