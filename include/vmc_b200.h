@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define VMC_ABI_VERSION 4
+#define VMC_ABI_VERSION 5
 
 enum {
     VMC_OK = 0,
@@ -58,6 +58,7 @@ typedef struct {
     int walkers_per_block, refresh_interval;
     int element_kind[8];                        /* VMC_ELEM_* in configuration order    */
     int kernel_variant;                         /* VMC_KERNEL_* of the sweep            */
+    int walkers_per_warp;                       /* production sweep: 1, or 2 (small dots) */
 } vmc_info;
 
 /* Sweep implementations: element flags read at run time, the quantum-dot flag

@@ -1,0 +1,57 @@
+"""Two walkers per warp for the small dots.
+
+Dots of at most three Hermite shells (N = 2, 6, 12) have at most 6 orbitals per spin
+block and 11 partners per particle, so one walker fills few of a warp's 32 lanes; the
+production sweep then gives each walker a 16-lane half of the warp.  The walkers see
+the same random numbers and the same arithmetic either way, so the iterations of a
+population swept two per warp equal those swept one per warp (`walkersPerWarp: 1`).
+An odd population leaves the last warp with one walker.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def run(text, iterations):
+    from vmachine_b200 import Engine
+    out = []
+    with Engine(text, device=0) as e:
+        e.init_walkers(None, seed=3)
+        info = e.info
+        for it in range(iterations):
+            a = e.run_iteration(it)
+            out.append((a.energy, a.kinetic, a.interaction, a.acceptance, e.parameters().copy()))
+        pos = e.positions()
+    return info, out, pos
+
+
+@pytest.mark.parametrize("N,omega", [(2, 1.0), (6, 0.5), (12, 0.8)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("compat", ["reference", "corrected"])
+def test_two_walkers_per_warp_equal_one(N, omega, precision, compat):
+    from vmachine_b200.batch import dot_text
+    text = dot_text(N, omega, 37, 300, precision, seed=11, compat=compat)
+    i2, two, p2 = run(text, 3)
+    i1, one, p1 = run(text + "walkersPerWarp: 1\n", 3)
+    assert i2.walkers_per_warp == 2 and i1.walkers_per_warp == 1
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    for (e2, k2, v2, a2, t2), (e1, k1, v1, a1, t1) in zip(two, one):
+        assert abs(e2 - e1) <= tol * abs(e1), (e2, e1)
+        assert abs(k2 - k1) <= tol * abs(k1)
+        assert abs(v2 - v1) <= tol * max(abs(v1), 1e-300)
+        assert abs(a2 - a1) <= 1e-3
+        assert np.allclose(t2, t1, rtol=tol, atol=0)
+    assert np.allclose(p2, p1, rtol=tol * 10, atol=tol * 10)
+
+
+def test_walkers_per_warp_selection():
+    """Two per warp only for the small compiled-in dots; larger dots and the general
+    path keep one walker per warp."""
+    from vmachine_b200 import Engine
+    from vmachine_b200.batch import atom_text, dot_text
+    for N, expect in ((2, 2), (6, 2), (12, 2), (20, 1), (56, 1)):
+        with Engine(dot_text(N, 0.5, 64, 10, "mixed"), device=0) as e:
+            assert e.info.walkers_per_warp == expect, N
+    with Engine(atom_text(2, 64, 10), device=0) as e:
+        assert e.info.walkers_per_warp == 1

@@ -9,8 +9,9 @@
 // system's sampling pass and optimiser step on the host exactly as vmc_sample and
 // vmc_apply_sums do for one engine.
 //
-// Work items and the tile.  Items are runs of `per_item` walkers of one system,
-// ordered by decreasing walker-steps x cost per step; the autotuner times one
+// Work items and the tile.  Items are runs of `per_item` walkers of one system
+// (`per_item` pairs for the dots of at most three shells, whose warps carry two
+// walkers), ordered by decreasing walker-steps x cost per step; the autotuner times one
 // iteration per (walkers per block, walkers per item) candidate and keeps the
 // fastest; the graph is re-captured when the schedule (rounds, refresh rounds,
 // tile) changes, e.g. while the refresh intervals settle.
@@ -145,8 +146,10 @@ int build_items(vmc_batch *b, int per_item)
     std::vector<It> v;
     for (size_t s = 0; s < b->sys.size(); ++s) {
         const vmc_engine *e = b->sys[s];
+        // an item is per_item warps' worth: per_item walkers, or pairs for two-walker warps
         const double c = b->cost[s] * (double)(e->steps_per_walker + e->burn_in) * per_item;
-        for (int w0 = 0; w0 < e->W; w0 += per_item) v.push_back({c, (int)s, w0});
+        const int width = per_item * (e->general ? 1 : e->ks.seg);
+        for (int w0 = 0; w0 < e->W; w0 += width) v.push_back({c, (int)s, w0});
     }
     std::stable_sort(v.begin(), v.end(), [](const It &x, const It &y) { return x.c > y.c; });
     std::vector<int2> items(v.size());
@@ -335,7 +338,8 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
         if (!e->general && e->refresh_interval > 0) b->any_refresh = true;
         if (!e->general)
             b->rebuild_smem = std::max(b->rebuild_smem, engine_rebuild_smem_per_warp(e));
-        b->sweep_smem = std::max(b->sweep_smem, e->general ? (int)(GEN_SCR * sizeof(double)) : engine_sweep_smem_per_warp(e));
+        b->sweep_smem = std::max(b->sweep_smem, e->general ? (int)(GEN_SCR * sizeof(double))
+                                                           : e->ks.seg * engine_sweep_smem_per_warp(e));
     }
     if (dot_precision < 0)  // general-path systems only: slices as large as their staging
         for (vmc_engine *e : b->sys)
@@ -486,6 +490,7 @@ int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *avg)
         h.refresh = (b->kind[s] != BATCH_GENERAL && e->refresh_interval > 0) ? 1 : 0;
         h.theta_refresh = (b->kind[s] != BATCH_GENERAL && b->theta_dirty[s]) ? 1 : 0;
         h.samples = steps - burn;
+        h.seg = e->general ? 1 : e->ks.seg;
         h.drift = e->d_drift;
         theta_refresh |= h.theta_refresh != 0;
         if (b->kind[s] == BATCH_GENERAL) {

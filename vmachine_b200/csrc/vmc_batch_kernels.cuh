@@ -38,6 +38,7 @@ struct BatchSys {
     int refresh;        // FP64 rebuild after each round
     int theta_refresh;  // parameters changed: re-derive the walkers before round 0
     int samples;        // sampled steps per walker (total_steps - burn-in)
+    int seg;            // walkers per warp in the sweep: the engine's (2: dots of at most 3 shells)
     double *drift;      // W: inverse drift of the refreshes
 };
 
@@ -94,11 +95,21 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3) batch_sweep_ker
         const int off = b.round * sy.a.steps;
         if (off >= sy.total_steps) continue;
         const int steps = min(sy.a.steps, sy.total_steps - off);
-        const int w_end = min(item.y + b.per_item, sy.a.P.W);
+        const int w_end = min(item.y + b.per_item * sy.seg, sy.a.P.W);
+        const int seg_stride = (b.smem_per_warp / 2) & ~15;  // two 16-byte aligned walker slices
         switch (sy.kind) {
-        case 1: sweep_walkers<T, 2, 1, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
-        case 2: sweep_walkers<T, 2, 2, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
-        case 3: sweep_walkers<T, 2, 3, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
+        case 1:
+            if (sy.seg == 2) sweep_walkers<T, 2, 1, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            else sweep_walkers<T, 2, 1, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
+        case 2:
+            if (sy.seg == 2) sweep_walkers<T, 2, 2, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            else sweep_walkers<T, 2, 2, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
+        case 3:
+            if (sy.seg == 2) sweep_walkers<T, 2, 3, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            else sweep_walkers<T, 2, 3, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
         case 4: sweep_walkers<T, 2, 4, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
         case 5: sweep_walkers<T, 2, 5, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
         case 6: sweep_walkers<T, 2, 6, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
@@ -128,7 +139,7 @@ __global__ void __launch_bounds__(128, 3) batch_rebuild_kernel(const BatchLaunch
             if (!sy.refresh || b.round * sy.a.steps >= sy.total_steps) continue;
             drift = sy.drift;
         }
-        const int w_end = min(item.y + b.per_item, sy.a.P.W);
+        const int w_end = min(item.y + b.per_item * sy.seg, sy.a.P.W);
         switch (sy.kind) {
         case 1: rebuild_walkers<T, 2, 1>(sy.a.P, RB_REFRESH, drift, ws, item.y, w_end, 1); break;
         case 2: rebuild_walkers<T, 2, 2>(sy.a.P, RB_REFRESH, drift, ws, item.y, w_end, 1); break;

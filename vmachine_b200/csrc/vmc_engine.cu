@@ -266,14 +266,15 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
         CUDA_TRY(gen_launch_sweep(a, e->gen, e->stream));
         return VMC_OK;
     }
+    const bool plain = !a.probe_k && !a.replay && !a.rec_en && !a.rec_acc && !a.dens_bins;
+    const void *fn = plain ? e->ks.sweep_plain : e->ks.sweep;
+    const int g = plain ? e->ks.seg : 1;  // walkers per warp
     a.wpb = e->wpb;
-    a.smem_per_warp = sweep_smem_per_warp(e);
+    a.smem_per_warp = g * sweep_smem_per_warp(e);
     // the MLP dot adds the CTA's weight block and tensor-core tiles in front
     const size_t smem = (size_t)a.wpb * a.smem_per_warp + (e->flags == FX_MLP_DOT ? MLP_FAST_BYTES + TC_SMEM : 0);
-    const void *fn = (!a.probe_k && !a.replay && !a.rec_en && !a.rec_acc && !a.dens_bins) ? e->ks.sweep_plain
-                                                                                         : e->ks.sweep;
     CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = (e->W + a.wpb - 1) / a.wpb;
+    const int grid = (e->W + a.wpb * g - 1) / (a.wpb * g);
     return launch(fn, grid, 32 * a.wpb, smem, e->stream, &a);
 }
 
@@ -291,7 +292,7 @@ int choose_wpb(vmc_engine *e)
         e->wpb = e->cfg.walkers_per_block;
         return VMC_OK;
     }
-    const int per_warp = sweep_smem_per_warp(e);
+    const int per_warp = e->ks.seg * sweep_smem_per_warp(e);
     cudaFuncAttributes fa;
     CUDA_TRY(cudaFuncGetAttributes(&fa, e->ks.sweep_plain));
     int best = 1, best_warps = -1;
@@ -556,6 +557,12 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     } else if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) {
         return reject("no kernel for this shape");
     }
+    // two walkers per warp unless configured off or the accumulators need more than
+    // a 16-lane segment (one lane each)
+    if (e->ks.seg > 1 && (c.walkers_per_warp == 1 || e->nacc_dev > 32 / e->ks.seg)) {
+        e->ks.sweep_plain = e->ks.sweep_plain1;
+        e->ks.seg = 1;
+    }
     // auto: start at 4 D steps (at least 512) and let the drift test tune it
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
                           : (e->precision == VMC_PRECISION_MIXED ? std::max(4 * e->D, 512) : 0);
@@ -653,6 +660,7 @@ int vmc_get_info(const vmc_engine *e, vmc_info *o)
     o->kernel_variant = e->general ? VMC_KERNEL_GENERAL
                         : (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED || e->flags == FX_MLP_DOT) && e->K > 0
                             ? VMC_KERNEL_DOT : VMC_KERNEL_RUNTIME_FLAGS;
+    o->walkers_per_warp = e->general ? 1 : e->ks.seg;
     return VMC_OK;
 }
 

@@ -704,6 +704,8 @@ struct KernelSet {
     const void *sweep_plain = nullptr;  // production sweep: no probe, replay or recording
     const void *scatter = nullptr, *gather = nullptr;  // positions in and out of the records
     const void *rebuild_mlp = nullptr;                  // MLP Jastrow dot: completes each rebuild
+    int seg = 1;                                        // walkers per warp of sweep_plain
+    const void *sweep_plain1 = nullptr;                 // production sweep, one walker per warp
 };
 
 template <typename T, int DIM, int K, int FX>
@@ -711,8 +713,16 @@ KernelSet make_set()
 {
     KernelSet s;
     s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, false>);
-    if constexpr (FX != 0) s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
-    else s.sweep_plain = s.sweep;
+    if constexpr (FX != 0 && FX != FX_MLP_DOT && DIM == 2 && K >= 1 && K <= 3) {
+        // small dots: two walkers per warp in the production sweep
+        s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 2>);
+        s.seg = 2;
+        s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
+    } else if constexpr (FX != 0) {
+        s.sweep_plain = s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
+    } else {
+        s.sweep_plain = s.sweep_plain1 = s.sweep;
+    }
     s.rebuild = reinterpret_cast<const void *>(&rebuild_kernel<T, DIM, K>);
     s.eval = reinterpret_cast<const void *>(&eval_kernel<T, DIM, K>);
     s.initpos = reinterpret_cast<const void *>(&initial_positions_kernel<T>);

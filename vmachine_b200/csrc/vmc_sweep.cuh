@@ -212,33 +212,43 @@ __device__ __forceinline__ void store_coords(T *x, int j, const T (&in)[DIM])
     }
 }
 
-// Reduce-scatter of 8 per-lane values over the warp (xor butterfly that halves the
-// value set at each stage): returns, in lane L, the warp total of value L >> 2.
-// 9 shuffles instead of 40 for eight all-reduces.
-template <typename R>
+// Reduce-scatter of 8 per-lane values over a segment of SEG lanes (the warp, or
+// half of it when a warp carries two walkers): an xor butterfly that halves the
+// value set at each stage returns, in segment lane L, the segment total of value
+// L / (SEG / 8).  9 shuffles instead of 40 for eight all-reduces over a warp.
+template <typename R, int SEG = 32>
 __device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
 {
-    const bool h4 = lane & 16;
+    const bool h4 = lane & (SEG / 2);
     R w[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const R mine = h4 ? v[4 + i] : v[i];
         const R other = h4 ? v[i] : v[4 + i];
-        w[i] = mine + __shfl_xor_sync(FULL, other, 16);
+        w[i] = mine + __shfl_xor_sync(FULL, other, SEG / 2);
     }
-    const bool h3 = lane & 8;
+    const bool h3 = lane & (SEG / 4);
     R u[2];
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
         const R mine = h3 ? w[2 + i] : w[i];
         const R other = h3 ? w[i] : w[2 + i];
-        u[i] = mine + __shfl_xor_sync(FULL, other, 8);
+        u[i] = mine + __shfl_xor_sync(FULL, other, SEG / 4);
     }
-    const bool h2 = lane & 4;
-    R t = (h2 ? u[1] : u[0]) + __shfl_xor_sync(FULL, h2 ? u[0] : u[1], 4);
-    t += __shfl_xor_sync(FULL, t, 2);
-    t += __shfl_xor_sync(FULL, t, 1);
+    const bool h2 = lane & (SEG / 8);
+    R t = (h2 ? u[1] : u[0]) + __shfl_xor_sync(FULL, h2 ? u[0] : u[1], SEG / 8);
+#pragma unroll
+    for (int o = SEG / 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
     return t;
+}
+
+// Sum over a segment of SEG lanes (every lane of the segment gets the total).
+template <int SEG, typename R>
+__device__ __forceinline__ R seg_sum(R v)
+{
+#pragma unroll
+    for (int o = SEG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
 }
 
 // A register-resident inverse (each lane keeping its two rows in registers) was
@@ -250,11 +260,23 @@ __device__ __forceinline__ R warp_reduce_scatter8(const R (&v)[8], int lane)
 // shared memory starts at warp_smem.  The single-system kernel below
 // strides over its whole population; the multi-system kernel hands each warp the
 // walkers of one work item.
-template <typename T, int DIM, int K, int FX, bool PL>
+//
+// G walkers per warp: G = 2 splits the warp into two 16-lane segments, segment s
+// sweeping walker w + s of each pair (its record at warp_smem + s * seg_stride), for
+// the small dots (N <= 12: at most 6 orbitals per block, 11 partners, 13
+// accumulators), which would leave most of a 32-lane warp idle.  The two walkers
+// step in lockstep; every shuffle stays inside a segment, and a segment whose
+// walker does not exist (odd populations) replays its partner's walker on its own
+// shared memory and writes nothing back.
+template <typename T, int DIM, int K, int FX, bool PL, int G = 1>
 __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int step_offset,
                                               unsigned char *warp_smem, int w_first, int w_end, int w_stride,
-                                              MlpCtx *mctx = nullptr)
+                                              MlpCtx *mctx = nullptr, int seg_stride = 0)
 {
+    static_assert(G == 1 || (G == 2 && PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && K <= 3),
+                  "two walkers per warp: production dot sweeps with at most 6 orbitals per block");
+    constexpr int SEG = 32 / G;        // lanes per walker
+    constexpr int VL = SEG / 8;        // lanes per reduce-scatter value
     // the MLP Jastrow dot: the CTA's warps step in lockstep (one tensor-core layer per step)
     constexpr bool MLPJ = FX == FX_MLP_DOT;
     // PL: the production form (Philox numbers, no probe, no recording), with the
@@ -272,8 +294,10 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
     constexpr int NQ = (NO + VE - 1) / VE;                        // vectors per inverse row
     const Params &P = a.P;
     const Layout L = P.L;
-    const int lane = threadIdx.x & 31;
-    T *sm = reinterpret_cast<T *>(warp_smem);
+    const int lane = threadIdx.x & (SEG - 1);   // lane within the walker's segment
+    const int seg = (threadIdx.x & 31) / SEG;
+    const unsigned segmask = G == 1 ? FULL : (0xFFFFu << (16 * seg));
+    T *sm = reinterpret_cast<T *>(warp_smem + (size_t)seg * seg_stride);
     const int N = K > 0 ? NK : P.N;
     const int D = K > 0 ? DK : L.D;
     unsigned long long *smask = reinterpret_cast<unsigned long long *>(sm + L.rec);
@@ -298,7 +322,9 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
         pkind = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : j == P.idx_alpha_h ? 3 : 0;
     }
 
-    for (int w = w_first; MLPJ ? (w - wib_l < w_end) : (w < w_end); w += w_stride) {
+    for (int w0 = w_first; MLPJ ? (w0 - wib_l < w_end) : (w0 < w_end); w0 += w_stride) {
+        const bool wact = G == 1 || w0 + seg < w_end;  // this segment has a walker to write back
+        const int w = G == 1 ? w0 : (wact ? w0 + seg : w0);
         if constexpr (MLPJ) {
             if (w >= w_end || tc_fail) {  // no walker for this warp: join the CTA's tensor-core steps
                 for (int s = 0; s < steps && !tc_fail; ++s) {
@@ -309,8 +335,13 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             }
         }
         T *g_rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
-        copy_in(sm, g_rec, L.rec, lane);
-        for (int j = lane; j < N; j += 32) smask[j] = P.mask[(size_t)w * N + j];
+        {
+            const int nv = L.rec * (int)sizeof(T) / 16;
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(g_rec);
+            uint4 *d4 = reinterpret_cast<uint4 *>(sm);
+            for (int i = lane; i < nv; i += SEG) d4[i] = s4[i];
+        }
+        for (int j = lane; j < N; j += SEG) smask[j] = P.mask[(size_t)w * N + j];
         if (lane < NSCAL) ssc[lane] = P.scal[(size_t)w * NSCAL + lane];
         double acc_s = 0.0, acc_c = 0.0;
         if (lane < P.nacc) {
@@ -319,14 +350,14 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
         }
         unsigned long long ctr = P.counter[w];
         unsigned status = 0;
-        int rng_k = 0;        // this lane's step of the current 32-step random block
+        int rng_k = 0;        // this lane's step of the current SEG-step random block
         T rng_z = T(0);
         unsigned rng_u = 0u;
-        __syncwarp();
+        __syncwarp(segmask);
 
         const bool use_philox = !probe_k && !replay;
         float *mcache = MLPJ ? P.mlp_cache + (size_t)w * P.mlp_cache_stride : nullptr;
-        for (int s0 = 0; s0 < steps && !(MLPJ && tc_fail); s0 += 32) {
+        for (int s0 = 0; s0 < steps && !(MLPJ && tc_fail); s0 += SEG) {
           if (use_philox) {
             // Lane-parallel Philox: lane i draws the numbers of step counter ctr + i
             // (the same per-step stream as a serial draw); each step of this block
@@ -349,7 +380,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             }
             rng_u = v.w;
           }
-          const int s_end = min(s0 + 32, steps);
+          const int s_end = min(s0 + SEG, steps);
           for (int s = s0; s < s_end && !(MLPJ && tc_fail); ++s) {
             const int it_step = step_offset + s;
             const T wa = T(P.omega * P.alpha);
@@ -367,11 +398,11 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 r1 = T(q[1]);
                 r2 = q[2];
             } else {
-                const int slot = (s - s0) & 31;  // s - s0 < 32 (the mask frees a register)
+                const int slot = (s - s0) & (SEG - 1);  // s - s0 < SEG (the mask frees a register)
                 ++ctr;
-                k = __shfl_sync(FULL, rng_k, slot);
-                r1 = __shfl_sync(FULL, rng_z, slot);
-                r2 = __shfl_sync(FULL, rng_u, slot) * TWO_M32;
+                k = __shfl_sync(FULL, rng_k, slot, SEG);
+                r1 = __shfl_sync(FULL, rng_z, slot, SEG);
+                r2 = __shfl_sync(FULL, rng_u, slot, SEG) * TWO_M32;
             }
             const int p = k / DIM, adim = k - p * DIM;
             const T xo = x[k];
@@ -426,12 +457,12 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     else
                         Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return rv[o]; });
                 }
-                R = __shfl_sync(FULL, Sj, pl);
-                if (green_grad) Gs = __shfl_sync(FULL, Gj, pl);
+                R = __shfl_sync(FULL, Sj, pl, SEG);
+                if (green_grad) Gs = __shfl_sync(FULL, Gj, pl, SEG);
             }
 
             // ---- 2b. pair terms of the moved particle (Pade, Coulomb)
-            constexpr int NJ = K > 0 ? (NK + 31) / 32 : 2;
+            constexpr int NJ = K > 0 ? (NK + SEG - 1) / SEG : 2;
             T sum_ratio = T(0), d_lap = T(0), d_bh2 = T(0), d_vint = T(0), pair_total = T(0);
             T gp_new[DIM], gdel[NJ][DIM];
 #pragma unroll
@@ -498,8 +529,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 T vals[8] = {sum_ratio, d_lap, T(0), d_vint, T(0), T(0), T(0), T(0)};
 #pragma unroll
                 for (int c = 0; c < DIM; ++c) vals[4 + c] = gp_new[c];
-                pair_total = warp_reduce_scatter8(vals, lane);
-                sum_ratio = __shfl_sync(FULL, pair_total, 0);
+                pair_total = warp_reduce_scatter8<T, SEG>(vals, lane);
+                sum_ratio = __shfl_sync(FULL, pair_total, 0, SEG);
             } else if (flags & (F_PADE | F_COULOMB)) {
                 const unsigned long long mp = smask[p];
                 const T gam = T(P.gamma), gamp = T(P.gamma_prev);
@@ -511,7 +542,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 const Two<T> lap_c = two(T(DIM - 1), T(DIM - 1)), m2gam = two(T(-2) * gam, T(-2) * gam);
 #pragma unroll
                 for (int jj = 0; jj < NJ; ++jj) {
-                    const int j = lane + 32 * jj;
+                    const int j = lane + SEG * jj;
                     if (j < N && j != p) {
                         T xjv[DIM];
                         load_coords<T, DIM>(x, j, xjv);
@@ -552,8 +583,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 T vals[8] = {sum_ratio, d_lap, d_bh2, d_vint, T(0), T(0), T(0), T(0)};
 #pragma unroll
                 for (int c = 0; c < DIM; ++c) vals[4 + c] = gp_new[c];
-                pair_total = warp_reduce_scatter8(vals, lane);
-                sum_ratio = __shfl_sync(FULL, pair_total, 0);
+                pair_total = warp_reduce_scatter8<T, SEG>(vals, lane);
+                sum_ratio = __shfl_sync(FULL, pair_total, 0, SEG);
             }
 
             // ---- 2c. element ratios, multiplied in configuration order
@@ -593,7 +624,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     } else {
                         T gy = T(0);
                         if (flags & F_GAUSS) gy += -wa * xn;
-                        if (jas) gy += __shfl_sync(FULL, pair_total, 16 + 4 * adim);
+                        if (jas) gy += __shfl_sync(FULL, pair_total, VL * (4 + adim), SEG);
                         if (flags & F_HYDROGENLIKE) gy += -T(P.alpha_h * P.Z) * xn / rpn;
                         if constexpr (K > 0) gy += Gs / R;
                         const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
@@ -610,7 +641,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
 
             if (accept) {
                 // ---- 3. state update
-                __syncwarp();
+                __syncwarp(segmask);
                 if (lane == 0) {
                     x[k] = xn;
                     if (is) fc[k] = Fn;
@@ -620,10 +651,10 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         ssc[SC_SUMR] += (double)rpn - (double)rpo;
                     }
                 }
-                // owners of the reduced pair sums apply them: value v (lanes 4v..4v+3)
+                // owners of the reduced pair sums apply them: value v (lanes VL v ..)
                 // 1, 2 -> SC_LAPJ, SC_BH2 (= v); 3 -> SC_VINT (= v); 4 + c -> gj of p
-                if ((flags & (F_PADE | F_MLP | F_COULOMB)) && (lane & 3) == 0 && lane >= 4 && lane < 16 + 4 * DIM) {
-                    const int v = lane >> 2;
+                if ((flags & (F_PADE | F_MLP | F_COULOMB)) && (lane % VL) == 0 && lane >= VL && lane < VL * (4 + DIM)) {
+                    const int v = lane / VL;
                     if (v < 4) {
                         if ((v == 3) ? (flags & F_COULOMB) : jas) ssc[v] += (double)pair_total;
                     } else if (jas) {
@@ -654,7 +685,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     // row p += (1 / R - 1) row p (exact when 1 / R lies in [0.5, 2]):
                     // one fused multiply-add per entry on every lane
                     const T tl = (lane == pl) ? rinv - T(1) : -(Sj * rinv);
-                    __syncwarp();  // x[k] written by lane 0
+                    __syncwarp(segmask);  // x[k] written by lane 0
                     const int lr = lane < NO ? lane : pl;   // lanes >= NO shadow row pl, store nothing
                     T *row_j = inv + (b * NO + lr) * IS;
                     const T *row_p = inv + (b * NO + pl) * IS;
@@ -675,7 +706,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         T cv[VE], vv[VE];
                         vload<T>(row_p + q * VE, cv);   // old row of the moved particle
                         vload<T>(row_j + q * VE, vv);
-                        __syncwarp();                   // row p read by all before it changes
+                        __syncwarp(segmask);            // row p read by all before it changes
 #pragma unroll
                         for (int e = 0; e < VE; e += 2) {
                             const Two<T> nv = fma2(two(cv[e], cv[e + 1]), two(tl, tl), two(vv[e], vv[e + 1]));
@@ -697,7 +728,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 if (jas) {
 #pragma unroll
                     for (int jj = 0; jj < NJ; ++jj) {
-                        const int j = lane + 32 * jj;
+                        const int j = lane + SEG * jj;
                         if (j < N && j != p) {
                             T gv[DIM];
                             load_coords<T, DIM>(gj, j, gv);
@@ -707,9 +738,9 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                             if (flags & F_PADE) smask[j] |= (1ull << p);
                         }
                     }
-                    if ((flags & F_PADE) && lane == (p & 31)) smask[p] = ~0ull;
+                    if ((flags & F_PADE) && lane == (p & (SEG - 1))) smask[p] = ~0ull;
                 }
-                __syncwarp();
+                __syncwarp(segmask);
             }
 
             // ---- 4. local energy and parameter gradients (Sampler::sample)
@@ -740,8 +771,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 if constexpr (VEC) {
                     using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 #pragma unroll
-                    for (int i = 0; i < (NV + 31) / 32; ++i) {
-                        const int vi = lane + 32 * i;
+                    for (int i = 0; i < (NV + SEG - 1) / SEG; ++i) {
+                        const int vi = lane + SEG * i;
                         if (vi < NV) {
                             const V vx = reinterpret_cast<const V *>(x)[vi];
                             const V vd = reinterpret_cast<const V *>(dd)[vi];
@@ -769,16 +800,16 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         }
                     }
                 } else {
-                    constexpr int NC = K > 0 ? (DK + 31) / 32 : 6;
+                    constexpr int NC = K > 0 ? (DK + SEG - 1) / SEG : 6;
 #pragma unroll
                     for (int i = 0; i < NC; ++i) {
-                        const int c = lane + 32 * i;
+                        const int c = lane + SEG * i;
                         if (c < D)
                             coord_term(c, x[c], K > 0 ? dd[c] : T(0), K > 0 ? sdd[c] : T(0),
                                        jas ? gj[c] : T(0));
                     }
                 }
-                ks = warp_sum(ks);
+                ks = seg_sum<SEG>(ks);
                 double lap = (double)ks;
                 if (jas) lap += ssc[SC_LAPJ];
                 if (flags & F_GAUSS) lap -= P.omega * P.alpha * D;
@@ -827,28 +858,30 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
         }
 
         // ---- write the walker back
-        __syncwarp();
-        {
+        __syncwarp(segmask);
+        if (MLPJ && tc_fail) status |= ST_TC_TIMEOUT;
+#pragma unroll
+        for (int o = SEG / 2; o > 0; o >>= 1) status |= __shfl_xor_sync(FULL, status, o);
+        if (wact) {
             const int nv = L.rec * (int)sizeof(T) / 16;
             const uint4 *s4 = reinterpret_cast<const uint4 *>(sm);
             uint4 *d4 = reinterpret_cast<uint4 *>(g_rec);
-            for (int i = lane; i < nv; i += 32) d4[i] = s4[i];
+            for (int i = lane; i < nv; i += SEG) d4[i] = s4[i];
+            for (int j = lane; j < N; j += SEG) P.mask[(size_t)w * N + j] = smask[j];
+            if (lane < NSCAL) P.scal[(size_t)w * NSCAL + lane] = ssc[lane];
+            if (lane == 0) P.counter[w] = ctr;
+            if (lane < P.nacc) {
+                P.acc[((size_t)w * P.nacc + lane) * 2] = acc_s;
+                P.acc[((size_t)w * P.nacc + lane) * 2 + 1] = acc_c;
+            }
+            if (lane == 0 && status) P.status[w] |= status;
         }
-        for (int j = lane; j < N; j += 32) P.mask[(size_t)w * N + j] = smask[j];
-        if (lane < NSCAL) P.scal[(size_t)w * NSCAL + lane] = ssc[lane];
-        if (lane == 0) P.counter[w] = ctr;
-        if (lane < P.nacc) {
-            P.acc[((size_t)w * P.nacc + lane) * 2] = acc_s;
-            P.acc[((size_t)w * P.nacc + lane) * 2 + 1] = acc_c;
-        }
-        if (MLPJ && tc_fail) status |= ST_TC_TIMEOUT;
-        status = __reduce_or_sync(FULL, status);
-        if (lane == 0 && status) P.status[w] |= status;
-        __syncwarp();
+        __syncwarp(segmask);
     }
 }
 
-template <typename T, int DIM, int K, int FX, bool PL>
+// G walkers per warp (see sweep_walkers): a.smem_per_warp holds G walker slices.
+template <typename T, int DIM, int K, int FX, bool PL, int G = 1>
 __global__ void __launch_bounds__(FX == FX_MLP_DOT ? 128 : sizeof(T) == 4 ? 256 : 128, FX == FX_MLP_DOT ? 2 : 3)
     sweep_kernel(const SweepArgs a)
 {
@@ -872,8 +905,9 @@ __global__ void __launch_bounds__(FX == FX_MLP_DOT ? 128 : sizeof(T) == 4 ? 256 
                                          blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb, &ctx);
         tc_teardown(tc, wib);
     } else {
-        sweep_walkers<T, DIM, K, FX, PL>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
-                                         blockIdx.x * a.wpb + wib, a.P.W, gridDim.x * a.wpb);
+        sweep_walkers<T, DIM, K, FX, PL, G>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
+                                            (blockIdx.x * a.wpb + wib) * G, a.P.W, gridDim.x * a.wpb * G, nullptr,
+                                            a.smem_per_warp / G);
     }
 }
 
