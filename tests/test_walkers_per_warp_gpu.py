@@ -1,11 +1,12 @@
-"""Two walkers per warp for the small dots.
+"""Several walkers per warp for the small dots.
 
 Dots of at most three Hermite shells (N = 2, 6, 12) have at most 6 orbitals per spin
 block and 11 partners per particle, so one walker fills few of a warp's 32 lanes; the
-production sweep then gives each walker a 16-lane half of the warp.  The walkers see
-the same random numbers and the same arithmetic either way, so the iterations of a
-population swept two per warp equal those swept one per warp (`walkersPerWarp: 1`).
-An odd population leaves the last warp with one walker.
+production sweep then gives each walker a 16-lane half (N = 12) or an 8-lane quarter
+(N <= 6) of the warp.  The walkers see the same random numbers and the same
+arithmetic either way, so the iterations of a population swept several per warp
+equal those swept one per warp (`walkersPerWarp: 1`).  A population of 37 leaves
+the last warp with one walker.
 """
 import numpy as np
 import pytest
@@ -26,15 +27,15 @@ def run(text, iterations):
     return info, out, pos
 
 
-@pytest.mark.parametrize("N,omega", [(2, 1.0), (6, 0.5), (12, 0.8)])
+@pytest.mark.parametrize("N,omega,per_warp", [(2, 1.0, 4), (6, 0.5, 4), (6, 0.5, 2), (12, 0.8, 2)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("compat", ["reference", "corrected"])
-def test_two_walkers_per_warp_equal_one(N, omega, precision, compat):
+def test_walkers_per_warp_equal_one(N, omega, per_warp, precision, compat):
     from vmachine_b200.batch import dot_text
     text = dot_text(N, omega, 37, 300, precision, seed=11, compat=compat)
-    i2, two, p2 = run(text, 3)
+    i2, two, p2 = run(text + f"walkersPerWarp: {per_warp}\n", 3)
     i1, one, p1 = run(text + "walkersPerWarp: 1\n", 3)
-    assert i2.walkers_per_warp == 2 and i1.walkers_per_warp == 1
+    assert i2.walkers_per_warp == per_warp and i1.walkers_per_warp == 1
     tol = 1e-12 if precision == "fp64" else 1e-5
     for (e2, k2, v2, a2, t2), (e1, k1, v1, a1, t1) in zip(two, one):
         assert abs(e2 - e1) <= tol * abs(e1), (e2, e1)
@@ -46,11 +47,11 @@ def test_two_walkers_per_warp_equal_one(N, omega, precision, compat):
 
 
 def test_walkers_per_warp_selection():
-    """Two per warp only for the small compiled-in dots; larger dots and the general
-    path keep one walker per warp."""
+    """Four per warp for the compiled-in dots of N <= 6, two for N = 12; larger dots
+    and the general path keep one walker per warp."""
     from vmachine_b200 import Engine
     from vmachine_b200.batch import atom_text, dot_text
-    for N, expect in ((2, 2), (6, 2), (12, 2), (20, 1), (56, 1)):
+    for N, expect in ((2, 4), (6, 4), (12, 2), (20, 1), (56, 1)):
         with Engine(dot_text(N, 0.5, 64, 10, "mixed"), device=0) as e:
             assert e.info.walkers_per_warp == expect, N
     with Engine(atom_text(2, 64, 10), device=0) as e:

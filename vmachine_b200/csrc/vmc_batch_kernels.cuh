@@ -96,14 +96,16 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3) batch_sweep_ker
         if (off >= sy.total_steps) continue;
         const int steps = min(sy.a.steps, sy.total_steps - off);
         const int w_end = min(item.y + b.per_item * sy.seg, sy.a.P.W);
-        const int seg_stride = (b.smem_per_warp / 2) & ~15;  // two 16-byte aligned walker slices
+        const int seg_stride = (b.smem_per_warp / max(1, sy.seg)) & ~15;  // 16-byte aligned walker slices
         switch (sy.kind) {
         case 1:
-            if (sy.seg == 2) sweep_walkers<T, 2, 1, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            if (sy.seg == 4) sweep_walkers<T, 2, 1, FX, true, 4>(sy.a, steps, off, ws, item.y, w_end, 4, nullptr, seg_stride);
+            else if (sy.seg == 2) sweep_walkers<T, 2, 1, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
             else sweep_walkers<T, 2, 1, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
         case 2:
-            if (sy.seg == 2) sweep_walkers<T, 2, 2, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            if (sy.seg == 4) sweep_walkers<T, 2, 2, FX, true, 4>(sy.a, steps, off, ws, item.y, w_end, 4, nullptr, seg_stride);
+            else if (sy.seg == 2) sweep_walkers<T, 2, 2, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
             else sweep_walkers<T, 2, 2, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
         case 3:

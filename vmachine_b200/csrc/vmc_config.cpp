@@ -304,8 +304,8 @@ std::string parse_config(const std::string &text, Config &c)
                 c.walkers_per_block = std::stoi(v0);
             } else if (key == "walkersPerWarp") {
                 if (v0 == "auto") c.walkers_per_warp = 0;
-                else if (v0 == "1" || v0 == "2") c.walkers_per_warp = std::stoi(v0);
-                else return err("walkersPerWarp must be auto, 1 or 2");
+                else if (v0 == "1" || v0 == "2" || v0 == "4") c.walkers_per_warp = std::stoi(v0);
+                else return err("walkersPerWarp must be auto, 1, 2 or 4");
             } else if (key == "seed") {
                 c.have_seed = true;
                 c.seed = std::stoll(v0);

@@ -557,11 +557,15 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     } else if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) {
         return reject("no kernel for this shape");
     }
-    // two walkers per warp unless configured off or the accumulators need more than
-    // a 16-lane segment (one lane each)
-    if (e->ks.seg > 1 && (c.walkers_per_warp == 1 || e->nacc_dev > 32 / e->ks.seg)) {
-        e->ks.sweep_plain = e->ks.sweep_plain1;
-        e->ks.seg = 1;
+    // several walkers per warp for the small dots, at most the configured count; the
+    // accumulators need at most two slots per lane of a segment
+    if (e->ks.seg > 1) {
+        const int cap = c.walkers_per_warp > 0 ? c.walkers_per_warp : 4;
+        if (e->ks.seg > cap || e->nacc_dev > 2 * (32 / e->ks.seg)) {
+            const bool two = cap >= 2 && e->ks.sweep_plain2 && e->nacc_dev <= 16;
+            e->ks.sweep_plain = two ? e->ks.sweep_plain2 : e->ks.sweep_plain1;
+            e->ks.seg = two ? 2 : 1;
+        }
     }
     // auto: start at 4 D steps (at least 512) and let the drift test tune it
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval

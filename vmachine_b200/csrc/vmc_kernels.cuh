@@ -706,6 +706,7 @@ struct KernelSet {
     const void *rebuild_mlp = nullptr;                  // MLP Jastrow dot: completes each rebuild
     int seg = 1;                                        // walkers per warp of sweep_plain
     const void *sweep_plain1 = nullptr;                 // production sweep, one walker per warp
+    const void *sweep_plain2 = nullptr;                 // two walkers per warp (dots of N <= 12), or null
 };
 
 template <typename T, int DIM, int K, int FX>
@@ -714,10 +715,16 @@ KernelSet make_set()
     KernelSet s;
     s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, false>);
     if constexpr (FX != 0 && FX != FX_MLP_DOT && DIM == 2 && K >= 1 && K <= 3) {
-        // small dots: two walkers per warp in the production sweep
-        s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 2>);
-        s.seg = 2;
+        // small dots: two (N <= 12) or four (N <= 6) walkers per warp in the production sweep
+        s.sweep_plain2 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 2>);
         s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
+        if constexpr (K <= 2) {
+            s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 4>);
+            s.seg = 4;
+        } else {
+            s.sweep_plain = s.sweep_plain2;
+            s.seg = 2;
+        }
     } else if constexpr (FX != 0) {
         s.sweep_plain = s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
     } else {

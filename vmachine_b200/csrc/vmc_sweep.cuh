@@ -261,22 +261,25 @@ __device__ __forceinline__ R seg_sum(R v)
 // strides over its whole population; the multi-system kernel hands each warp the
 // walkers of one work item.
 //
-// G walkers per warp: G = 2 splits the warp into two 16-lane segments, segment s
-// sweeping walker w + s of each pair (its record at warp_smem + s * seg_stride), for
-// the small dots (N <= 12: at most 6 orbitals per block, 11 partners, 13
-// accumulators), which would leave most of a 32-lane warp idle.  The two walkers
-// step in lockstep; every shuffle stays inside a segment, and a segment whose
-// walker does not exist (odd populations) replays its partner's walker on its own
-// shared memory and writes nothing back.
+// G walkers per warp: G = 2 (4) splits the warp into 16-lane (8-lane) segments,
+// segment s sweeping walker w + s of each group (its record at warp_smem +
+// s * seg_stride), for the small dots (G = 2: N <= 12, at most 6 orbitals per block
+// and 11 partners; G = 4: N <= 6, with two accumulator slots per lane for the 15
+// accumulators), which would leave most of a 32-lane warp idle.  The walkers step in
+// lockstep; every shuffle stays inside a segment, and a segment whose walker does not
+// exist (a population that is not a multiple of G) replays the group's first walker
+// on its own shared memory and writes nothing back.
 template <typename T, int DIM, int K, int FX, bool PL, int G = 1>
 __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int step_offset,
                                               unsigned char *warp_smem, int w_first, int w_end, int w_stride,
                                               MlpCtx *mctx = nullptr, int seg_stride = 0)
 {
-    static_assert(G == 1 || (G == 2 && PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && K <= 3),
-                  "two walkers per warp: production dot sweeps with at most 6 orbitals per block");
+    static_assert(G == 1 || (PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && ((G == 2 && K <= 3) || (G == 4 && K <= 2))),
+                  "several walkers per warp: production dot sweeps with at most 6 (G = 2) or 3 (G = 4) "
+                  "orbitals per block");
     constexpr int SEG = 32 / G;        // lanes per walker
     constexpr int VL = SEG / 8;        // lanes per reduce-scatter value
+    constexpr int NSLOT = G == 4 ? 2 : 1;  // accumulator slots per lane (slot lane + SEG i)
     // the MLP Jastrow dot: the CTA's warps step in lockstep (one tensor-core layer per step)
     constexpr bool MLPJ = FX == FX_MLP_DOT;
     // PL: the production form (Philox numbers, no probe, no recording), with the
@@ -296,7 +299,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
     const Layout L = P.L;
     const int lane = threadIdx.x & (SEG - 1);   // lane within the walker's segment
     const int seg = (threadIdx.x & 31) / SEG;
-    const unsigned segmask = G == 1 ? FULL : (0xFFFFu << (16 * seg));
+    const unsigned segmask = G == 1 ? FULL : (((1u << SEG) - 1u) << (SEG * seg));
     T *sm = reinterpret_cast<T *>(warp_smem + (size_t)seg * seg_stride);
     const int N = K > 0 ? NK : P.N;
     const int D = K > 0 ? DK : L.D;
@@ -310,16 +313,22 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
     const int wib_l = threadIdx.x >> 5;
     bool tc_fail = false;
 
-    // accumulator slot of this lane: 0..7 energy moments, 8 accepts, then the
-    // parameter gradients (kind 1 alpha, 2 gamma, 3 hydrogen-like alpha) and
-    // the same times E_L.
-    int pkind = 0;
-    bool times_e = false;
-    if (lane >= 9 && lane < P.nacc) {
-        int j = lane - 9;
-        times_e = j >= P.ep;
-        if (times_e) j -= P.ep;
-        pkind = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : j == P.idx_alpha_h ? 3 : 0;
+    // accumulator slots of this lane (lane + SEG i): 0..7 energy moments, 8 accepts,
+    // then the parameter gradients (kind 1 alpha, 2 gamma, 3 hydrogen-like alpha)
+    // and the same times E_L.
+    int pkind[NSLOT];
+    bool times_e[NSLOT];
+#pragma unroll
+    for (int i = 0; i < NSLOT; ++i) {
+        const int slot = lane + SEG * i;
+        pkind[i] = 0;
+        times_e[i] = false;
+        if (slot >= 9 && slot < P.nacc) {
+            int j = slot - 9;
+            times_e[i] = j >= P.ep;
+            if (times_e[i]) j -= P.ep;
+            pkind[i] = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : j == P.idx_alpha_h ? 3 : 0;
+        }
     }
 
     for (int w0 = w_first; MLPJ ? (w0 - wib_l < w_end) : (w0 < w_end); w0 += w_stride) {
@@ -343,10 +352,15 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
         }
         for (int j = lane; j < N; j += SEG) smask[j] = P.mask[(size_t)w * N + j];
         if (lane < NSCAL) ssc[lane] = P.scal[(size_t)w * NSCAL + lane];
-        double acc_s = 0.0, acc_c = 0.0;
-        if (lane < P.nacc) {
-            acc_s = P.acc[((size_t)w * P.nacc + lane) * 2];
-            acc_c = P.acc[((size_t)w * P.nacc + lane) * 2 + 1];
+        double acc_s[NSLOT], acc_c[NSLOT];
+#pragma unroll
+        for (int i = 0; i < NSLOT; ++i) {
+            const int slot = lane + SEG * i;
+            acc_s[i] = acc_c[i] = 0.0;
+            if (slot < P.nacc) {
+                acc_s[i] = P.acc[((size_t)w * P.nacc + slot) * 2];
+                acc_c[i] = P.acc[((size_t)w * P.nacc + slot) * 2 + 1];
+            }
         }
         unsigned long long ctr = P.counter[w];
         unsigned status = 0;
@@ -827,17 +841,21 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     o[2] = vint;
                 }
                 if (it_step >= a.burn_in) {
-                    // branch-free slot selection; lanes past the accumulators add zero
-                    const int g2 = (lane >> 1) & 3;
-                    const double base = g2 == 0 ? el : g2 == 1 ? ekin : g2 == 2 ? vext : vint;
-                    const double qe = (lane & 1) ? base * base : base;
+                    // branch-free slot selection; slots past the accumulators add zero
                     const bool win = it_step > a.win_lo && it_step < a.win_hi;
-                    const double g = pkind == 1 ? -0.5 * P.omega * ssc[SC_SUMX2]
-                                   : pkind == 2 ? ((flags & Q_PADE_DGAMMA) ? -0.5 : -1.0) * ssc[SC_BH2]
-                                   : pkind == 3 ? -P.Z * ssc[SC_SUMR] : 0.0;
-                    const double qp = win ? (times_e ? g * el : g) : 0.0;
-                    const double q = lane < 8 ? qe : lane == 8 ? (accept ? 1.0 : 0.0) : qp;
-                    kadd(acc_s, acc_c, q);
+#pragma unroll
+                    for (int i = 0; i < NSLOT; ++i) {
+                        const int slot = lane + SEG * i;
+                        const int g2 = (slot >> 1) & 3;
+                        const double base = g2 == 0 ? el : g2 == 1 ? ekin : g2 == 2 ? vext : vint;
+                        const double qe = (slot & 1) ? base * base : base;
+                        const double g = pkind[i] == 1 ? -0.5 * P.omega * ssc[SC_SUMX2]
+                                       : pkind[i] == 2 ? ((flags & Q_PADE_DGAMMA) ? -0.5 : -1.0) * ssc[SC_BH2]
+                                       : pkind[i] == 3 ? -P.Z * ssc[SC_SUMR] : 0.0;
+                        const double qp = win ? (times_e[i] ? g * el : g) : 0.0;
+                        const double q = slot < 8 ? qe : slot == 8 ? (accept ? 1.0 : 0.0) : qp;
+                        kadd(acc_s[i], acc_c[i], q);
+                    }
                     if (!PL && a.dens_bins > 0) density_sample<T>(a, x, N, DIM, lane);
                     if constexpr (MLPJ) {
                         // the MLP row's parameter gradient: positions and E_L every
@@ -870,9 +888,13 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             for (int j = lane; j < N; j += SEG) P.mask[(size_t)w * N + j] = smask[j];
             if (lane < NSCAL) P.scal[(size_t)w * NSCAL + lane] = ssc[lane];
             if (lane == 0) P.counter[w] = ctr;
-            if (lane < P.nacc) {
-                P.acc[((size_t)w * P.nacc + lane) * 2] = acc_s;
-                P.acc[((size_t)w * P.nacc + lane) * 2 + 1] = acc_c;
+#pragma unroll
+            for (int i = 0; i < NSLOT; ++i) {
+                const int slot = lane + SEG * i;
+                if (slot < P.nacc) {
+                    P.acc[((size_t)w * P.nacc + slot) * 2] = acc_s[i];
+                    P.acc[((size_t)w * P.nacc + slot) * 2 + 1] = acc_c[i];
+                }
             }
             if (lane == 0 && status) P.status[w] |= status;
         }
