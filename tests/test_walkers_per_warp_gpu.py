@@ -27,7 +27,8 @@ def run(text, iterations):
     return info, out, pos
 
 
-@pytest.mark.parametrize("N,omega,per_warp", [(2, 1.0, 4), (6, 0.5, 4), (6, 0.5, 2), (12, 0.8, 2)])
+@pytest.mark.parametrize("N,omega,per_warp", [(2, 1.0, 4), (6, 0.5, 4), (6, 0.5, 2), (12, 0.8, 2), (20, 0.5, 2),
+                                                (30, 0.6, 2)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("compat", ["reference", "corrected"])
 def test_walkers_per_warp_equal_one(N, omega, per_warp, precision, compat):
@@ -51,7 +52,7 @@ def test_walkers_per_warp_selection():
     and the general path keep one walker per warp."""
     from vmachine_b200 import Engine
     from vmachine_b200.batch import atom_text, dot_text
-    for N, expect in ((2, 4), (6, 4), (12, 2), (20, 1), (56, 1)):
+    for N, expect in ((2, 4), (6, 4), (12, 2), (20, 2), (30, 2), (42, 1), (56, 1)):
         with Engine(dot_text(N, 0.5, 64, 10, "mixed"), device=0) as e:
             assert e.info.walkers_per_warp == expect, N
     with Engine(atom_text(2, 64, 10), device=0) as e:

@@ -112,8 +112,14 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3) batch_sweep_ker
             if (sy.seg == 2) sweep_walkers<T, 2, 3, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
             else sweep_walkers<T, 2, 3, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
-        case 4: sweep_walkers<T, 2, 4, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
-        case 5: sweep_walkers<T, 2, 5, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
+        case 4:
+            if (sy.seg == 2) sweep_walkers<T, 2, 4, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            else sweep_walkers<T, 2, 4, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
+        case 5:
+            if (sy.seg == 2) sweep_walkers<T, 2, 5, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
+            else sweep_walkers<T, 2, 5, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
         case 6: sweep_walkers<T, 2, 6, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
         case 7: sweep_walkers<T, 2, 7, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
         default:

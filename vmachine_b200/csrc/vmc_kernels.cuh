@@ -714,8 +714,8 @@ KernelSet make_set()
 {
     KernelSet s;
     s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, false>);
-    if constexpr (FX != 0 && FX != FX_MLP_DOT && DIM == 2 && K >= 1 && K <= 3) {
-        // small dots: two (N <= 12) or four (N <= 6) walkers per warp in the production sweep
+    if constexpr (FX != 0 && FX != FX_MLP_DOT && DIM == 2 && K >= 1 && K <= 5) {
+        // dots up to N = 30: two (N <= 30) or four (N <= 6) walkers per warp in the production sweep
         s.sweep_plain2 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 2>);
         s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
         if constexpr (K <= 2) {

@@ -263,9 +263,10 @@ __device__ __forceinline__ R seg_sum(R v)
 //
 // G walkers per warp: G = 2 (4) splits the warp into 16-lane (8-lane) segments,
 // segment s sweeping walker w + s of each group (its record at warp_smem +
-// s * seg_stride), for the small dots (G = 2: N <= 12, at most 6 orbitals per block
-// and 11 partners; G = 4: N <= 6, with two accumulator slots per lane for the 15
-// accumulators), which would leave most of a 32-lane warp idle.  The walkers step in
+// s * seg_stride), for the dots up to N = 30 (G = 2: at most 15 orbitals per block,
+// one row per lane, partners in two passes above 16; G = 4: N <= 6, with two
+// accumulator slots per lane for the 15 accumulators), which would leave much of a
+// 32-lane warp idle.  The walkers step in
 // lockstep; every shuffle stays inside a segment, and a segment whose walker does not
 // exist (a population that is not a multiple of G) replays the group's first walker
 // on its own shared memory and writes nothing back.
@@ -274,8 +275,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                                               unsigned char *warp_smem, int w_first, int w_end, int w_stride,
                                               MlpCtx *mctx = nullptr, int seg_stride = 0)
 {
-    static_assert(G == 1 || (PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && ((G == 2 && K <= 3) || (G == 4 && K <= 2))),
-                  "several walkers per warp: production dot sweeps with at most 6 (G = 2) or 3 (G = 4) "
+    static_assert(G == 1 || (PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && ((G == 2 && K <= 5) || (G == 4 && K <= 2))),
+                  "several walkers per warp: production dot sweeps with at most 15 (G = 2) or 3 (G = 4) "
                   "orbitals per block");
     constexpr int SEG = 32 / G;        // lanes per walker
     constexpr int VL = SEG / 8;        // lanes per reduce-scatter value
