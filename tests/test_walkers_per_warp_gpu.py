@@ -1,9 +1,10 @@
 """Several walkers per warp for the small dots.
 
-Dots of at most three Hermite shells (N = 2, 6, 12) have at most 6 orbitals per spin
-block and 11 partners per particle, so one walker fills few of a warp's 32 lanes; the
-production sweep then gives each walker a 16-lane half (N = 12) or an 8-lane quarter
-(N <= 6) of the warp.  The walkers see the same random numbers and the same
+A walker of a small dot fills few of a warp's 32 lanes (one per orbital row, partner
+or coordinate group), so the production sweep gives each walker an 8-lane quarter
+(N <= 6) or a 16-lane half (N = 12 to 30) of the warp; N = 42 and 56 keep one walker
+per warp by default and take two on request (`walkersPerWarp: 2`, rows of the 21 x 21
+and 28 x 28 inverse blocks in two passes).  The walkers see the same random numbers and the same
 arithmetic either way, so the iterations of a population swept several per warp
 equal those swept one per warp (`walkersPerWarp: 1`).  A population of 37 leaves
 the last warp with one walker.
@@ -28,7 +29,7 @@ def run(text, iterations):
 
 
 @pytest.mark.parametrize("N,omega,per_warp", [(2, 1.0, 4), (6, 0.5, 4), (6, 0.5, 2), (12, 0.8, 2), (20, 0.5, 2),
-                                                (30, 0.6, 2)])
+                                                (30, 0.6, 2), (42, 0.4, 2), (56, 0.28, 2)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("compat", ["reference", "corrected"])
 def test_walkers_per_warp_equal_one(N, omega, per_warp, precision, compat):
@@ -48,8 +49,8 @@ def test_walkers_per_warp_equal_one(N, omega, per_warp, precision, compat):
 
 
 def test_walkers_per_warp_selection():
-    """Four per warp for the compiled-in dots of N <= 6, two for N = 12; larger dots
-    and the general path keep one walker per warp."""
+    """Four per warp for the compiled-in dots of N <= 6, two for N = 12 to 30; larger
+    dots and the general path keep one walker per warp."""
     from vmachine_b200 import Engine
     from vmachine_b200.batch import atom_text, dot_text
     for N, expect in ((2, 4), (6, 4), (12, 2), (20, 2), (30, 2), (42, 1), (56, 1)):

@@ -135,6 +135,14 @@ void free_batch(vmc_batch *b)
     delete b;
 }
 
+// Walkers per warp of a system in the batch sweep: the engine's choice for the dots
+// up to N = 30 (Hermite shells K <= 5), one otherwise (the batch kernel carries the
+// several-walker forms only for those).
+static int batch_walkers_per_warp(const vmc_engine *e, int kind)
+{
+    return (!e->general && kind >= 1 && kind <= 5) ? e->ks.seg : 1;
+}
+
 // Items of per_item walkers, longest work first (ties: system order, then walker).
 int build_items(vmc_batch *b, int per_item)
 {
@@ -148,7 +156,7 @@ int build_items(vmc_batch *b, int per_item)
         const vmc_engine *e = b->sys[s];
         // an item is per_item warps' worth: per_item walkers, or pairs for two-walker warps
         const double c = b->cost[s] * (double)(e->steps_per_walker + e->burn_in) * per_item;
-        const int width = per_item * (e->general ? 1 : e->ks.seg);
+        const int width = per_item * batch_walkers_per_warp(e, b->kind[s]);
         for (int w0 = 0; w0 < e->W; w0 += width) v.push_back({c, (int)s, w0});
     }
     std::stable_sort(v.begin(), v.end(), [](const It &x, const It &y) { return x.c > y.c; });
@@ -339,7 +347,7 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
         if (!e->general)
             b->rebuild_smem = std::max(b->rebuild_smem, engine_rebuild_smem_per_warp(e));
         b->sweep_smem = std::max(b->sweep_smem, e->general ? (int)(GEN_SCR * sizeof(double))
-                                                           : e->ks.seg * engine_sweep_smem_per_warp(e));
+                                                           : batch_walkers_per_warp(e, kind) * engine_sweep_smem_per_warp(e));
     }
     if (dot_precision < 0)  // general-path systems only: slices as large as their staging
         for (vmc_engine *e : b->sys)
@@ -490,7 +498,7 @@ int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *avg)
         h.refresh = (b->kind[s] != BATCH_GENERAL && e->refresh_interval > 0) ? 1 : 0;
         h.theta_refresh = (b->kind[s] != BATCH_GENERAL && b->theta_dirty[s]) ? 1 : 0;
         h.samples = steps - burn;
-        h.seg = e->general ? 1 : e->ks.seg;
+        h.seg = batch_walkers_per_warp(e, b->kind[s]);
         h.drift = e->d_drift;
         theta_refresh |= h.theta_refresh != 0;
         if (b->kind[s] == BATCH_GENERAL) {

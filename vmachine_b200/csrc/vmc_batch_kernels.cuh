@@ -38,7 +38,7 @@ struct BatchSys {
     int refresh;        // FP64 rebuild after each round
     int theta_refresh;  // parameters changed: re-derive the walkers before round 0
     int samples;        // sampled steps per walker (total_steps - burn-in)
-    int seg;            // walkers per warp in the sweep: the engine's (2: dots of at most 3 shells)
+    int seg;            // walkers per warp in the sweep: the engine's for N <= 30, else 1
     double *drift;      // W: inverse drift of the refreshes
 };
 

@@ -557,14 +557,22 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     } else if (!select_set(e->precision, e->dim, K, e->flags, e->ks)) {
         return reject("no kernel for this shape");
     }
-    // several walkers per warp for the small dots, at most the configured count; the
-    // accumulators need at most two slots per lane of a segment
-    if (e->ks.seg > 1) {
-        const int cap = c.walkers_per_warp > 0 ? c.walkers_per_warp : 4;
-        if (e->ks.seg > cap || e->nacc_dev > 2 * (32 / e->ks.seg)) {
-            const bool two = cap >= 2 && e->ks.sweep_plain2 && e->nacc_dev <= 16;
-            e->ks.sweep_plain = two ? e->ks.sweep_plain2 : e->ks.sweep_plain1;
-            e->ks.seg = two ? 2 : 1;
+    // walkers per warp of the compiled-in dots: the kernel set's default, or at most
+    // the configured count; the accumulators (one lane each, two with 8-lane segments)
+    // must fit 16 slots
+    if (e->ks.sweep_plain2) {
+        const void *four = e->ks.seg == 4 ? e->ks.sweep_plain : nullptr;
+        int want = c.walkers_per_warp > 0 ? c.walkers_per_warp : e->ks.seg;
+        if (e->nacc_dev > 16) want = 1;
+        if (want >= 4 && four) {
+            e->ks.sweep_plain = four;
+            e->ks.seg = 4;
+        } else if (want >= 2) {
+            e->ks.sweep_plain = e->ks.sweep_plain2;
+            e->ks.seg = 2;
+        } else {
+            e->ks.sweep_plain = e->ks.sweep_plain1;
+            e->ks.seg = 1;
         }
     }
     // auto: start at 4 D steps (at least 512) and let the drift test tune it

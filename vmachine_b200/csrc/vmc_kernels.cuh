@@ -714,16 +714,21 @@ KernelSet make_set()
 {
     KernelSet s;
     s.sweep = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, false>);
-    if constexpr (FX != 0 && FX != FX_MLP_DOT && DIM == 2 && K >= 1 && K <= 5) {
-        // dots up to N = 30: two (N <= 30) or four (N <= 6) walkers per warp in the production sweep
+    if constexpr (FX != 0 && FX != FX_MLP_DOT && DIM == 2 && K >= 1) {
+        // compiled-in dots: four (N <= 6), two (N <= 30) or one walker per warp by
+        // default (two on request for N = 42 and 56: rows in two passes, measured at
+        // 1.05x and 0.89x, the 5-9 KB records of two walkers halving the warps per SM)
         s.sweep_plain2 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 2>);
         s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
         if constexpr (K <= 2) {
             s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 4>);
             s.seg = 4;
-        } else {
+        } else if constexpr (K <= 5) {
             s.sweep_plain = s.sweep_plain2;
             s.seg = 2;
+        } else {
+            s.sweep_plain = s.sweep_plain1;
+            s.seg = 1;
         }
     } else if constexpr (FX != 0) {
         s.sweep_plain = s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);

@@ -275,9 +275,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                                               unsigned char *warp_smem, int w_first, int w_end, int w_stride,
                                               MlpCtx *mctx = nullptr, int seg_stride = 0)
 {
-    static_assert(G == 1 || (PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && ((G == 2 && K <= 5) || (G == 4 && K <= 2))),
-                  "several walkers per warp: production dot sweeps with at most 15 (G = 2) or 3 (G = 4) "
-                  "orbitals per block");
+    static_assert(G == 1 || (PL && FX != 0 && FX != FX_MLP_DOT && K > 0 && (G == 2 || (G == 4 && K <= 2))),
+                  "several walkers per warp: production dot sweeps (G = 4: at most 3 orbitals per block)");
     constexpr int SEG = 32 / G;        // lanes per walker
     constexpr int VL = SEG / 8;        // lanes per reduce-scatter value
     constexpr int NSLOT = G == 4 ? 2 : 1;  // accumulator slots per lane (slot lane + SEG i)
@@ -296,6 +295,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
     constexpr int VE = 16 / (int)sizeof(T);                     // entries per 16-byte vector
     constexpr int IS = K > 0 ? inv_row_stride(NO, sizeof(T)) : 0; // inverse row stride
     constexpr int NQ = (NO + VE - 1) / VE;                        // vectors per inverse row
+    constexpr int RP = K > 0 ? (NO + 32 / G - 1) / (32 / G) : 1;  // inverse rows per lane
     const Params &P = a.P;
     const Layout L = P.L;
     const int lane = threadIdx.x & (SEG - 1);   // lane within the walker's segment
@@ -452,28 +452,41 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             // its Slater part d_adim phi(r_p') . inv[:, p] / R comes out of the same
             // row contraction as R (lane pl)
             const bool green_grad = is && !(flags & Q_IS_GREEN) && !probe_k;
-            T Sj = T(0), R = T(1), Gs = T(0);
+            // rows per lane: lane holds rows lane + SEG rp (more than one only when a
+            // segment is narrower than a Slater block)
+            T Sj[RP], R = T(1), Gs = T(0);
             int b = 0, pl = 0;
+#pragma unroll
+            for (int rp = 0; rp < RP; ++rp) Sj[rp] = T(0);
             if constexpr (K > 0) {
                 b = p / NO;
                 pl = p - b * NO;
                 T hv[DIM][K];
 #pragma unroll
                 for (int c = 0; c < DIM; ++c) hermite_values<K>(xpn[c], hv[c]);
-                T Gj = T(0);
-                if (lane < NO) {
-                    // this lane's row (column `lane` of A^{-1}), 16-byte vector loads
-                    T rv[NQ * VE];
-                    const T *row = inv + (b * NO + lane) * IS;
+                T Gj[RP], Sp = T(0), Gp = T(0);
 #pragma unroll
-                    for (int q = 0; q < NQ; ++q) vload<T>(row + q * VE, rv + q * VE);
-                    if (green_grad)
-                        Sj = orbital_dot_grad<T, DIM, K>(hv, [&](int o) { return rv[o]; }, adim, Gj);
-                    else
-                        Sj = orbital_dot<T, DIM, K>(hv, [&](int o) { return rv[o]; });
+                for (int rp = 0; rp < RP; ++rp) {
+                    const int r = lane + SEG * rp;
+                    Gj[rp] = T(0);
+                    if (r < NO) {
+                        // row r (column r of A^{-1}), 16-byte vector loads
+                        T rv[NQ * VE];
+                        const T *row = inv + (b * NO + r) * IS;
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) vload<T>(row + q * VE, rv + q * VE);
+                        if (green_grad)
+                            Sj[rp] = orbital_dot_grad<T, DIM, K>(hv, [&](int o) { return rv[o]; }, adim, Gj[rp]);
+                        else
+                            Sj[rp] = orbital_dot<T, DIM, K>(hv, [&](int o) { return rv[o]; });
+                    }
+                    if (rp == pl / SEG) {
+                        Sp = Sj[rp];
+                        Gp = Gj[rp];
+                    }
                 }
-                R = __shfl_sync(FULL, Sj, pl, SEG);
-                if (green_grad) Gs = __shfl_sync(FULL, Gj, pl, SEG);
+                R = __shfl_sync(FULL, Sp, pl & (SEG - 1), SEG);
+                if (green_grad) Gs = __shfl_sync(FULL, Gp, pl & (SEG - 1), SEG);
             }
 
             // ---- 2b. pair terms of the moved particle (Pade, Coulomb)
@@ -699,45 +712,56 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     // row j -= (S_j / R) row p for j != p; row p *= 1 / R, written as
                     // row p += (1 / R - 1) row p (exact when 1 / R lies in [0.5, 2]):
                     // one fused multiply-add per entry on every lane
-                    const T tl = (lane == pl) ? rinv - T(1) : -(Sj * rinv);
                     __syncwarp(segmask);  // x[k] written by lane 0
-                    const int lr = lane < NO ? lane : pl;   // lanes >= NO shadow row pl, store nothing
-                    T *row_j = inv + (b * NO + lr) * IS;
                     const T *row_p = inv + (b * NO + pl) * IS;
-                    T hv[DIM][K];
-                    {
-                        T xq[DIM];
-                        load_coords<T, DIM>(x, b * NO + lr, xq);
+                    // with several rows per lane the pass holding row p goes last, so
+                    // every other row reads row p before it changes
+#pragma unroll 1
+                    for (int i = 0; i < RP; ++i) {
+                        const int rp = RP == 1 ? 0 : (pl / SEG + 1 + i) % RP;
+                        const int r = lane + SEG * rp;
+                        T s_r = Sj[0];
 #pragma unroll
-                        for (int c = 0; c < DIM; ++c) hermite_values<K>(xq[c], hv[c]);
-                    }
-                    T part[DIM][K];
+                        for (int q = 1; q < RP; ++q)
+                            if (q == rp) s_r = Sj[q];
+                        const T tl = (r == pl) ? rinv - T(1) : -(s_r * rinv);
+                        const int lr = r < NO ? r : pl;   // rows >= NO shadow row pl, store nothing
+                        T *row_j = inv + (b * NO + lr) * IS;
+                        T hv[DIM][K];
+                        {
+                            T xq[DIM];
+                            load_coords<T, DIM>(x, b * NO + lr, xq);
 #pragma unroll
-                    for (int c = 0; c < DIM; ++c)
-#pragma unroll
-                        for (int m = 0; m < K; ++m) part[c][m] = T(0);
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) {
-                        T cv[VE], vv[VE];
-                        vload<T>(row_p + q * VE, cv);   // old row of the moved particle
-                        vload<T>(row_j + q * VE, vv);
-                        __syncwarp(segmask);            // row p read by all before it changes
-#pragma unroll
-                        for (int e = 0; e < VE; e += 2) {
-                            const Two<T> nv = fma2(two(cv[e], cv[e + 1]), two(tl, tl), two(vv[e], vv[e + 1]));
-                            vv[e] = nv.x;
-                            vv[e + 1] = nv.y;
+                            for (int c = 0; c < DIM; ++c) hermite_values<K>(xq[c], hv[c]);
                         }
-                        if (lane < NO) vstore<T>(row_j + q * VE, vv);
-                        for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
-                            if (o / VE == q) accumulate_orbital<T, DIM, K>(hv, part, vv[o % VE], m0, m1, m2);
-                        });
-                    }
-                    if (lane < NO) {
-                        T gd[DIM], sd[DIM];
-                        contract_orbitals<T, DIM, K>(hv, part, gd, sd);
-                        store_coords<T, DIM>(dd, b * NO + lane, gd);
-                        store_coords<T, DIM>(sdd, b * NO + lane, sd);
+                        T part[DIM][K];
+#pragma unroll
+                        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+                            for (int m = 0; m < K; ++m) part[c][m] = T(0);
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            T cv[VE], vv[VE];
+                            vload<T>(row_p + q * VE, cv);   // old row of the moved particle
+                            vload<T>(row_j + q * VE, vv);
+                            __syncwarp(segmask);            // row p read by all before it changes
+#pragma unroll
+                            for (int e = 0; e < VE; e += 2) {
+                                const Two<T> nv = fma2(two(cv[e], cv[e + 1]), two(tl, tl), two(vv[e], vv[e + 1]));
+                                vv[e] = nv.x;
+                                vv[e + 1] = nv.y;
+                            }
+                            if (r < NO) vstore<T>(row_j + q * VE, vv);
+                            for_each_orbital<DIM, K>([&](int o, int m0, int m1, int m2) {
+                                if (o / VE == q) accumulate_orbital<T, DIM, K>(hv, part, vv[o % VE], m0, m1, m2);
+                            });
+                        }
+                        if (r < NO) {
+                            T gd[DIM], sd[DIM];
+                            contract_orbitals<T, DIM, K>(hv, part, gd, sd);
+                            store_coords<T, DIM>(dd, b * NO + r, gd);
+                            store_coords<T, DIM>(sdd, b * NO + r, sd);
+                        }
                     }
                 }
                 if (jas) {
