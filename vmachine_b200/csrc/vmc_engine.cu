@@ -537,9 +537,15 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         e->nacc_dev = 0;  // set below from the active parameters
         for (int i = 0; i < e->E; ++i)
             if (c.elements[i] == E_MLP) e->mlp_e = i;
+        // every parameter but the MLP row's, less SimpleJastrow's beta_ij with i >= j,
+        // whose gradient is identically zero (the reference's distance matrix holds only
+        // i < j, simplejastrow.cpp:106-111): their sums stay exact zeros on the host
         for (int i = 0; i < e->E; ++i)
             if (i != e->mlp_e)
-                for (int q = 0; q < element_parameters(c, c.elements[i]); ++q) e->act.push_back(i * e->Pmax + q);
+                for (int q = 0; q < element_parameters(c, c.elements[i]); ++q) {
+                    if (c.elements[i] == E_SIMPLEJASTROW && q % c.N >= q / c.N) continue;
+                    e->act.push_back(i * e->Pmax + q);
+                }
         e->nacc_dev = 9 + 2 * (int)e->act.size();
     }
     // userinput.cpp:60-81 with walkers in place of ranks: numSteps is the total
