@@ -49,12 +49,17 @@ def test_walkers_per_warp_equal_one(N, omega, per_warp, precision, compat):
 
 
 def test_walkers_per_warp_selection():
-    """Four per warp for the compiled-in dots of N <= 6, two for N = 12 to 30; larger
-    dots and the general path keep one walker per warp."""
+    """Four per warp for the compiled-in dots of N <= 6, two for N = 12 to 30, one for
+    larger dots; four for the atoms of at most 4 electrons, one for the rest of the
+    general path."""
     from vmachine_b200 import Engine
     from vmachine_b200.batch import atom_text, dot_text
     for N, expect in ((2, 4), (6, 4), (12, 2), (20, 2), (30, 2), (42, 1), (56, 1)):
         with Engine(dot_text(N, 0.5, 64, 10, "mixed"), device=0) as e:
             assert e.info.walkers_per_warp == expect, N
+    # atoms on the general path: four per warp for He (at most 4 electrons; its
+    # replayed chains against the oracle run in this form), one for Ne
     with Engine(atom_text(2, 64, 10), device=0) as e:
+        assert e.info.walkers_per_warp == 4
+    with Engine(atom_text(10, 64, 10), device=0) as e:
         assert e.info.walkers_per_warp == 1

@@ -136,11 +136,12 @@ void free_batch(vmc_batch *b)
 }
 
 // Walkers per warp of a system in the batch sweep: the engine's choice for the dots
-// up to N = 30 (Hermite shells K <= 5), one otherwise (the batch kernel carries the
-// several-walker forms only for those).
+// up to N = 30 (Hermite shells K <= 5) and for the general path's small atoms, one
+// otherwise (the batch kernel carries the several-walker forms only for those).
 static int batch_walkers_per_warp(const vmc_engine *e, int kind)
 {
-    return (!e->general && kind >= 1 && kind <= 5) ? e->ks.seg : 1;
+    if (e->general) return e->gen.variant == GV_ATOM ? e->gen.seg : 1;
+    return (kind >= 1 && kind <= 5) ? e->ks.seg : 1;
 }
 
 // Items of per_item walkers, longest work first (ties: system order, then walker).

@@ -75,6 +75,20 @@ static __device__ __noinline__ void batch_gen_walkers(const SweepArgs &a, int st
     const int full = gen_stage_doubles(g, a.P.nacc);
     const bool rec_fits = !g.mlp && GEN_SCR + g.rec <= slice, acc_fits = full && GEN_SCR + full <= slice;
     double *stage = rec_fits ? scr + GEN_SCR : nullptr;
+    if (g.variant == GV_ATOM && g.seg == 4) {
+        // four walkers per warp: 8-lane segments, each with a quarter of the scratch and,
+        // when they fit after it, its own staged record and accumulators
+        const int seg = (threadIdx.x & 31) >> 3;
+        const bool fits4 = !g.mlp && GEN_SCR + 4 * full <= slice && full > 0;
+        double *st4 = fits4 ? scr + GEN_SCR + seg * full : nullptr;
+        for (int wb = w0; wb < w_end; wb += 4) {
+            const int w = wb + seg;
+            if (w < w_end)
+                gen_sweep_walker<false, GV_ATOM, 8>(a, steps, off, g, w, true, scr + seg * (GEN_SCR / 4), nullptr, tc,
+                                                    nullptr, st4, fits4);
+        }
+        return;
+    }
     for (int w = w0; w < w_end; ++w) {
         if (g.variant == GV_ATOM)
             gen_sweep_walker<false, GV_ATOM>(a, steps, off, g, w, true, scr, nullptr, tc, nullptr, stage, acc_fits);

@@ -678,7 +678,7 @@ int vmc_get_info(const vmc_engine *e, vmc_info *o)
     o->kernel_variant = e->general ? VMC_KERNEL_GENERAL
                         : (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED || e->flags == FX_MLP_DOT) && e->K > 0
                             ? VMC_KERNEL_DOT : VMC_KERNEL_RUNTIME_FLAGS;
-    o->walkers_per_warp = e->general ? 1 : e->ks.seg;
+    o->walkers_per_warp = e->general ? (e->gen.variant == GV_ATOM ? e->gen.seg : 1) : e->ks.seg;
     return VMC_OK;
 }
 

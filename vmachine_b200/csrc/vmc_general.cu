@@ -40,7 +40,9 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
     if (lane == 0 && status) P.status[w] |= status;
 }
 
-template <bool TC, int GV>
+// G walkers per warp (compiled forms only): each takes a 32 / G-lane segment, a
+// GEN_SCR / G slice of the warp's scratch and its own staging area.
+template <bool TC, int GV, int G = 1>
 __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs a, const GenParams g)
 {
     extern __shared__ __align__(16) double gsm[];
@@ -49,8 +51,8 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
     __shared__ __align__(8) unsigned long long tc_bar;
     __shared__ uint32_t tc_slot;
     const Params &P = a.P;
-    const int wib = threadIdx.x >> 5;
-    const int w = blockIdx.x * GEN_WPB + wib;
+    const int wib = threadIdx.x >> 5, seg = (threadIdx.x & 31) / (32 / G);
+    const int w = (blockIdx.x * GEN_WPB + wib) * G + seg;
     float *mw = g.mlp ? reinterpret_cast<float *>(gsm) : nullptr;
     if (mw) mlp_stage(g.mlp, mw, !TC);
     TcMlp tc{};
@@ -61,8 +63,8 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
     const bool active = w < P.W;
     if (!TC && !active) return;
     const int nst = gen_stage_doubles(g, P.nacc);  // 0 with the MLP (gsm holds its weights)
-    gen_sweep_walker<TC, GV>(a, a.steps, a.step_offset, g, w, active, scratch[wib], mw, tc, pre[wib],
-                         nst ? gsm + (size_t)wib * nst : nullptr);
+    gen_sweep_walker<TC, GV, 32 / G>(a, a.steps, a.step_offset, g, w, active, scratch[wib] + seg * (GEN_SCR / G), mw,
+                                     tc, pre[wib], nst ? gsm + (size_t)(wib * G + seg) * nst : nullptr);
     if (TC) tc_teardown(tc, wib);
 }
 
@@ -712,6 +714,9 @@ std::string gen_configure(const Config &c, int E, int p_max, GenParams &g)
     bool atom_set = slater && dim == 3 && g.basis == BASIS_HYDROGEN;
     for (int e : c.elements) atom_set = atom_set && (e == (int)E_SLATER || e == (int)E_PADE || e == (int)E_SIMPLEJASTROW);
     g.variant = atom_set ? GV_ATOM : GV_ANY;
+    // at most 2 orbitals per block, 6 pairs and 12 coordinates: an 8-lane segment and a
+    // 64-double scratch slice hold a walker
+    g.seg = atom_set && N <= 4 ? 4 : 1;
     return "";
 }
 
@@ -732,17 +737,23 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
 cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_t st)
 {
     const bool tc = g.mlp && g.mlp_tc;
-    const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0) +
-                        (size_t)GEN_WPB * gen_stage_doubles(g, a.P.nacc) * sizeof(double);
     const bool atom = !tc && g.variant == GV_ATOM;
-    const void *fn = tc     ? (const void *)gen_sweep_kernel<true, GV_ANY>
-                     : atom ? (const void *)gen_sweep_kernel<false, GV_ATOM>
-                            : (const void *)gen_sweep_kernel<false, GV_ANY>;
+    // four walkers per warp for the small atoms (not while sampling densities, whose
+    // histogram code takes a whole warp per walker)
+    const int G = atom && g.seg == 4 && a.dens_bins == 0 ? 4 : 1;
+    const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0) +
+                        (size_t)GEN_WPB * G * gen_stage_doubles(g, a.P.nacc) * sizeof(double);
+    const void *fn = tc       ? (const void *)gen_sweep_kernel<true, GV_ANY>
+                     : G == 4 ? (const void *)gen_sweep_kernel<false, GV_ATOM, 4>
+                     : atom   ? (const void *)gen_sweep_kernel<false, GV_ATOM>
+                              : (const void *)gen_sweep_kernel<false, GV_ANY>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const unsigned grid = (a.P.W + GEN_WPB - 1) / GEN_WPB;
+    const unsigned grid = (a.P.W + GEN_WPB * G - 1) / (GEN_WPB * G);
     if (tc)
         gen_sweep_kernel<true, GV_ANY><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
+    else if (G == 4)
+        gen_sweep_kernel<false, GV_ATOM, 4><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
     else if (atom)
         gen_sweep_kernel<false, GV_ATOM><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
     else

@@ -37,6 +37,7 @@ struct GenParams {
     int n_act;
     int mlp_tc;                 // MLP sweep with the second layer on the tensor cores
     int variant;                // GV_*: the compiled sweep that takes this system
+    int seg;                    // walkers per warp of the sweep (4: atoms of at most 4 electrons)
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
 };
 

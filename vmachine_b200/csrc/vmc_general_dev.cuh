@@ -192,13 +192,31 @@ __device__ __forceinline__ double pade_beta_of(const Params &P, int i, int j)
     return same_spin(i, j, P.N) ? P.beta_same : P.beta_anti;
 }
 
+// Lanes of the calling thread's segment when a warp carries 32 / SEG walkers of the
+// general path (SEG = 32: the whole warp), and sums over them.
+template <int SEG>
+__device__ __forceinline__ unsigned gen_segmask()
+{
+    return SEG == 32 ? FULL : (((1u << SEG) - 1u) << ((threadIdx.x & 31) & ~(SEG - 1)));
+}
+
+template <int SEG>
+__device__ __forceinline__ double seg_reduce(unsigned mask, double v)
+{
+#pragma unroll
+    for (int o = SEG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
 // Per-particle sums of pair vectors: tp holds t(i, j) for each pair i < j (pair
 // index as pair_of), particle i takes +t(i, j) for j > i and -t(j, i) for j < i, j
 // ascending; lanes over particles add the sums to G (and the per-element output).
+template <int SEG = 32>
 __device__ __forceinline__ void gen_pair_gather(const double *tp, int N, int dim, double *G, double *oge, int lane)
 {
-    __syncwarp();
-    for (int i = lane; i < N; i += 32) {
+    const unsigned segmask = gen_segmask<SEG>();
+    __syncwarp(segmask);
+    for (int i = lane; i < N; i += SEG) {
         double gi[3] = {0.0, 0.0, 0.0};
         for (int j = 0; j < N; ++j) {
             if (j == i) continue;
@@ -211,7 +229,7 @@ __device__ __forceinline__ void gen_pair_gather(const double *tp, int N, int dim
             if (oge) oge[i * dim + c] = gi[c];
         }
     }
-    __syncwarp();  // the scratch is free again for the next element
+    __syncwarp(segmask);  // the scratch is free again for the next element
 }
 
 // Evaluate the walker at its positions (eval_impl): per-element gradient,
@@ -221,21 +239,23 @@ __device__ __forceinline__ void gen_pair_gather(const double *tp, int N, int dim
 // energies 3).
 // moved: the particle whose position changed since the last evaluation (its cached
 // orbital derivatives are refreshed), or -1 to refresh every particle's.
-template <int GV = GV_ANY>
+template <int GV = GV_ANY, int SEG = 32>
 __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, double *rec,
                              const unsigned long long *mask, double *scr, int lane, double *o_grad,
                              double *o_lap, double *o_pg, double *o_en, const float *mw = nullptr,
                              bool full = true, int moved = -1)
 {
     const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max, dim = gv_dim(GV, dim_rt);
+    const unsigned segmask = gen_segmask<SEG>();
+    constexpr int SCR = GEN_SCR * SEG / 32;  // this walker's scratch doubles
     const double *x = rec;
     double *G = rec + g.off_g, *pg = rec + g.off_pg;
     const double *inv = rec + g.off_inv;
-    for (int k = lane; k < D; k += 32) G[k] = 0.0;
+    for (int k = lane; k < D; k += SEG) G[k] = 0.0;
     // only the accumulated parameters are ever written (padding and the MLP row stay
     // zero from the record's initialisation): clear those
-    for (int c = lane; c < g.n_act; c += 32) pg[g.act[c]] = 0.0;
-    __syncwarp();
+    for (int c = lane; c < g.n_act; c += SEG) pg[g.act[c]] = 0.0;
+    __syncwarp(segmask);
     double lap_total = 0.0;
     for (int e = 0; e < E; ++e) {
         const double *th = g.theta + (size_t)e * PM;
@@ -247,13 +267,13 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             if (!gv_has(GV, 0)) break;
             const double wa = P.omega * th[0];
             double x2 = 0.0;
-            for (int k = lane; k < D; k += 32) {
+            for (int k = lane; k < D; k += SEG) {
                 const double gk = -wa * x[k];
                 G[k] += gk;
                 if (oge) oge[k] = gk;
                 x2 += x[k] * x[k];
             }
-            x2 = warp_sum(x2);
+            x2 = seg_reduce<SEG>(segmask, x2);
             lap_u = -wa * D;
             if (lane == 0) pge[0] = -0.5 * P.omega * x2;
             break;
@@ -265,7 +285,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             // orbital derivatives of the particles that moved (lanes over (particle,
             // orbital)); the other particles' are unchanged in the cache
             const int q0 = moved < 0 ? 0 : moved, nq = moved < 0 ? N : 1;
-            for (int t = lane; t < nq * n; t += 32) {
+            for (int t = lane; t < nq * n; t += SEG) {
                 const int q = q0 + t / n, o = t - (t / n) * n;
                 double v, d1[3], d2[3];
                 gen_orb<GV>(g, dim, P.Z, o, x + q * dim, v, d1, d2);
@@ -275,8 +295,8 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                     cq[dim + c] = d2[c];
                 }
             }
-            __syncwarp();
-            for (int q = lane; q < N; q += 32) {
+            __syncwarp(segmask);
+            for (int q = lane; q < N; q += SEG) {
                 const int b = q / n, il = q - b * n;
                 const double *row = inv + (size_t)(b * n + il) * n;
                 double dd[3] = {0.0, 0.0, 0.0}, sdd[3] = {0.0, 0.0, 0.0};
@@ -300,10 +320,10 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             const double gam = th[0];
             double dg = 0.0;
             const int npair = N * (N - 1) / 2;
-            if (npair * dim <= GEN_SCR) {
+            if (npair * dim <= SCR) {
                 // lanes over the pairs i < j (as SimpleJastrow below)
                 double *tp = scr;
-                for (int q = lane; q < npair; q += 32) {
+                for (int q = lane; q < npair; q += SEG) {
                     int i, j;
                     pair_of(q, N, i, j);
                     double d[3], r2 = 0.0;
@@ -323,12 +343,12 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                     lap_l += c2;
                     dg += beta * h * h;
                 }
-                gen_pair_gather(tp, N, dim, G, oge, lane);
-                dg = warp_sum(dg);
+                gen_pair_gather<SEG>(tp, N, dim, G, oge, lane);
+                dg = seg_reduce<SEG>(segmask, dg);
                 if (lane == 0) pge[0] = (P.flags & Q_PADE_DGAMMA) ? -0.5 * dg : -dg;
                 break;
             }
-            for (int i = lane; i < N; i += 32) {
+            for (int i = lane; i < N; i += SEG) {
                 double gi[3] = {0.0, 0.0, 0.0};
                 for (int j = 0; j < N; ++j) {
                     if (j == i) continue;
@@ -352,19 +372,19 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                     if (oge) oge[i * dim + c] = gi[c];
                 }
             }
-            dg = warp_sum(dg);
+            dg = seg_reduce<SEG>(segmask, dg);
             if (lane == 0) pge[0] = (P.flags & Q_PADE_DGAMMA) ? -0.5 * dg : -dg;
             break;
         }
         case 3: {  // SimpleJastrow (simplejastrow.cpp:67-111)
             if (!gv_has(GV, 3)) break;
             const int npair = N * (N - 1) / 2;
-            if (npair * dim <= GEN_SCR) {
+            if (npair * dim <= SCR) {
                 // lanes over the pairs i < j: beta (x_i - x_j) / r into the scratch,
                 // the pair's Laplacian term and dJ/dbeta_ij = r; then lanes over the
                 // particles sum their pairs' terms (j ascending, as the reference)
                 double *tp = scr;
-                for (int q = lane; q < npair; q += 32) {
+                for (int q = lane; q < npair; q += SEG) {
                     int i, j;
                     pair_of(q, N, i, j);
                     double d[3], r2 = 0.0;
@@ -382,10 +402,10 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                     lap_l += c2;
                     pge[i + N * j] = r;
                 }
-                gen_pair_gather(tp, N, dim, G, oge, lane);
+                gen_pair_gather<SEG>(tp, N, dim, G, oge, lane);
                 break;
             }
-            for (int i = lane; i < N; i += 32) {
+            for (int i = lane; i < N; i += SEG) {
                 double gi[3] = {0.0, 0.0, 0.0};
                 for (int j = 0; j < N; ++j) {
                     if (j == i) continue;
@@ -412,7 +432,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
         case 4: {  // RBMGaussian (rbmgaussian.cpp:67-87)
             if (!gv_has(GV, 4)) break;
             const double s2 = g.sigma * g.sigma;
-            for (int k = lane; k < D; k += 32) {
+            for (int k = lane; k < D; k += SEG) {
                 const double t = (x[k] - th[k]) / s2;
                 G[k] += -t;
                 if (oge) oge[k] = -t;
@@ -428,7 +448,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             double *xs = scr + SCR_XS, *pn = scr + SCR_PN, *nn = scr + SCR_NN;
             rbm_visible(x, D, -1, 0.0, P.flags & Q_RBM_SORT, xs, lane);
             rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
-            for (int k = lane; k < D; k += 32) {
+            for (int k = lane; k < D; k += SEG) {
                 double acc = 0.0, acc2 = 0.0;
                 for (int j = 0; j < H; ++j) {
                     const double w = th[H + k + D * j];
@@ -439,7 +459,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                 if (oge) oge[k] = acc / s2;
                 lap_l += acc2 / s4;
             }
-            for (int t = lane; t < H * (D + 1); t += 32) {
+            for (int t = lane; t < H * (D + 1); t += SEG) {
                 if (t < H) pge[t] = nn[t];
                 else {
                     const int j = (t - H) / D, i = (t - H) - j * D;
@@ -453,7 +473,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
             if (full) {  // from scratch (initialisation, parameter update, evaluation)
                 const int npair = N * (N - 1) / 2;
-                for (int q = lane; q < npair; q += 32) {
+                for (int q = lane; q < npair; q += SEG) {
                     int i, j;
                     pair_of(q, N, i, j);
                     const bool same = same_spin(i, j, N);
@@ -473,10 +493,10 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                         oc[i * 3 + 2] = ddc;
                     }
                 }
-                __syncwarp();
+                __syncwarp(segmask);
             }
             // from the caches in FP32 (the network values are FP32 already)
-            for (int i = lane; i < N; i += 32) {
+            for (int i = lane; i < N; i += SEG) {
                 float gi[3] = {0.0f, 0.0f, 0.0f}, li = 0.0f, xi[3];
                 for (int c = 0; c < dim; ++c) xi[c] = (float)x[i * dim + c];
                 for (int j = 0; j < N; ++j) {
@@ -508,7 +528,7 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             if (!gv_has(GV, 6)) break;
             const double az = th[0] * P.Z;
             double rs = 0.0;
-            for (int i = lane; i < N; i += 32) {
+            for (int i = lane; i < N; i += SEG) {
                 const double r = gen_radius(x, dim, i);
                 rs += r;
                 for (int c = 0; c < dim; ++c) {
@@ -518,29 +538,29 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
                 }
                 lap_l -= 2.0 / r;
             }
-            rs = warp_sum(rs);
+            rs = seg_reduce<SEG>(segmask, rs);
             lap_l *= az;
             if (lane == 0) pge[0] = -P.Z * rs;
             break;
         }
         default: break;
         }
-        __syncwarp();
-        const double lap_e = warp_sum(lap_l) + lap_u;
+        __syncwarp(segmask);
+        const double lap_e = seg_reduce<SEG>(segmask, lap_l) + lap_u;
         lap_total += lap_e;
         if (o_lap && lane == 0) o_lap[e] = lap_e;
     }
     // System::getKineticEnergy (elementoperation.cpp:95-109) and the potentials
     double g2 = 0.0, vx = 0.0, vi = 0.0;
-    for (int k = lane; k < D; k += 32) g2 += G[k] * G[k];
+    for (int k = lane; k < D; k += SEG) g2 += G[k] * G[k];
     if (P.flags & F_ATOM) {
-        for (int i = lane; i < N; i += 32) vx += 1.0 / gen_radius(x, dim, i);
+        for (int i = lane; i < N; i += SEG) vx += 1.0 / gen_radius(x, dim, i);
     } else {
-        for (int k = lane; k < D; k += 32) vx += x[k] * x[k];
+        for (int k = lane; k < D; k += SEG) vx += x[k] * x[k];
     }
     if (P.flags & F_COULOMB) {  // lanes over the pairs i < j
         const int npair = N * (N - 1) / 2;
-        for (int q = lane; q < npair; q += 32) {
+        for (int q = lane; q < npair; q += SEG) {
             int i, j;
             pair_of(q, N, i, j);
             double r2 = 0.0;
@@ -551,9 +571,9 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
             vi += rsqrt(r2);
         }
     }
-    g2 = warp_sum(g2);
-    vx = warp_sum(vx);
-    vi = warp_sum(vi);
+    g2 = seg_reduce<SEG>(segmask, g2);
+    vx = seg_reduce<SEG>(segmask, vx);
+    vi = seg_reduce<SEG>(segmask, vi);
     const double ekin = -0.5 * (lap_total + g2);
     const double vext = (P.flags & F_ATOM) ? -P.Z * vx : 0.5 * P.omega * P.omega * vx;
     double *en = rec + g.off_en;
@@ -563,26 +583,27 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, do
         en[2] = vi;
     }
     if (o_pg)
-        for (int j = lane; j < g.EP; j += 32) o_pg[j] = pg[j];
+        for (int j = lane; j < g.EP; j += SEG) o_pg[j] = pg[j];
     if (o_en && lane == 0) {
         o_en[0] = ekin;
         o_en[1] = vext;
         o_en[2] = vi;
     }
-    __syncwarp();
+    __syncwarp(segmask);
 }
 
 // Element ratios |Psi(y)|^2 / |Psi(x)|^2 for coordinate k moved to xn (ratio_impl)
 // and, when grad_y is given, d ln Psi / d y_k at the proposal (the corrected
 // Fokker-Planck Green's ratio).  Orbital values at the proposal go to the scratch
 // (the Sherman-Morrison update reuses them).  Returns the product in element order.
-template <int GV = GV_ANY>
+template <int GV = GV_ANY, int SEG = 32>
 __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, const double *rec,
                              const unsigned long long *mask, double *scr, int lane, int k, double xn,
                              double *ratios, double *grad_y, double &R_out, const float *mw = nullptr,
                              const float *pre = nullptr)
 {
     const int N = P.N, D = g.D, E = P.n_elem, PM = g.p_max, dim = gv_dim(GV, dim_rt);
+    const unsigned segmask = gen_segmask<SEG>();
     const double *x = rec;
     const int p = k / dim, adim = k - p * dim;
     double yp[3];
@@ -603,19 +624,19 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
             if (!gv_has(GV, 1)) break;
             const int n = g.n, b = p / n, pl = p - b * n;
             double s = 0.0, sg = 0.0;
-            if (lane < n) {
+            for (int o = lane; o < n; o += SEG) {
                 double v, d1[3], d2[3];
-                gen_orb<GV>(g, dim, P.Z, lane, yp, v, d1, d2);
-                scr[SCR_PHI + lane] = v;
-                const double iv = rec[g.off_inv + (size_t)(b * n + pl) * n + lane];
-                s = v * iv;
-                sg = d1[adim] * iv;
+                gen_orb<GV>(g, dim, P.Z, o, yp, v, d1, d2);
+                scr[SCR_PHI + o] = v;
+                const double iv = rec[g.off_inv + (size_t)(b * n + pl) * n + o];
+                s += v * iv;
+                sg += d1[adim] * iv;
             }
-            const double R = warp_sum(s);
+            const double R = seg_reduce<SEG>(segmask, s);
             R_out = R;
             r = R * R;
-            if (grad_y) gy += warp_sum(sg) / R;
-            __syncwarp();
+            if (grad_y) gy += seg_reduce<SEG>(segmask, sg) / R;
+            __syncwarp(segmask);
             break;
         }
         case 2: {  // padejastrow.cpp:211-218
@@ -623,7 +644,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
             const double gam = th[0];
             const int j0 = (P.flags & Q_PADE_RATIO) ? p + 1 : 0;
             double acc = 0.0, gyl = 0.0;
-            for (int j = lane; j < N; j += 32) {
+            for (int j = lane; j < N; j += SEG) {
                 if (j == p) continue;
                 const int lo = min(p, j), hi = max(p, j);
                 double rn2 = 0.0;
@@ -637,16 +658,16 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
                 const double f1 = 1.0 / (1.0 + gam * rn);
                 gyl += beta * f1 * f1 * (yp[adim] - x[j * dim + adim]) / rn;
             }
-            acc = warp_sum(acc);
+            acc = seg_reduce<SEG>(segmask, acc);
             r = exp(2.0 * acc);
-            if (grad_y) gy += warp_sum(gyl);
+            if (grad_y) gy += seg_reduce<SEG>(segmask, gyl);
             break;
         }
         case 3: {  // simplejastrow.cpp:145-156
             if (!gv_has(GV, 3)) break;
             const int j0 = (P.flags & Q_SJ_RATIO) ? p + 1 : 0;
             double acc = 0.0, gyl = 0.0;
-            for (int j = lane; j < N; j += 32) {
+            for (int j = lane; j < N; j += SEG) {
                 if (j == p) continue;
                 const int lo = min(p, j), hi = max(p, j);
                 double rn2 = 0.0;
@@ -658,9 +679,9 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
                 if (j >= j0) acc += beta * (rn - gen_dist(x, dim, p, j));
                 gyl += beta * (yp[adim] - x[j * dim + adim]) / rn;
             }
-            acc = warp_sum(acc);
+            acc = seg_reduce<SEG>(segmask, acc);
             r = exp(2.0 * acc);
-            if (grad_y) gy += warp_sum(gyl);
+            if (grad_y) gy += seg_reduce<SEG>(segmask, gyl);
             break;
         }
         case 4: {  // rbmgaussian.cpp:34-46
@@ -683,7 +704,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
                 const int j = lane + 32 * t;
                 if (j < H) po[t] = pn[j];
             }
-            __syncwarp();
+            __syncwarp(segmask);
             rbm_visible(x, D, k, xn, sort, xs, lane);
             rbm_hidden(th, D, H, s2, xs, pn, nn, lane);
             double prod = 1.0, gyl = 0.0;
@@ -697,8 +718,8 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) prod *= __shfl_xor_sync(FULL, prod, o);
             r = prod * prod;
-            if (grad_y) gy += warp_sum(gyl) / s2;
-            __syncwarp();
+            if (grad_y) gy += seg_reduce<SEG>(segmask, gyl) / s2;
+            __syncwarp(segmask);
             break;
         }
         case 7: {  // MLP Jastrow: exp(2 (J(y) - J(x))); the new pair and one-body values
@@ -706,7 +727,7 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
                    // go to the scratch for an accepted move
             const double *uc = rec + g.off_uc, *oc = rec + g.off_oc;
             double acc = 0.0, gyl = 0.0;
-            for (int j = lane; j < N; j += 32) {
+            for (int j = lane; j < N; j += SEG) {
                 if (j == p) continue;
                 double rn2 = 0.0;
                 for (int c = 0; c < dim; ++c) {
@@ -739,10 +760,10 @@ __device__ double gen_ratios(const Params &P, const GenParams &g, int dim_rt, co
                 scr[SCR_PN + 33] = dcn;
                 scr[SCR_PN + 34] = ddcn;
             }
-            const double dj = warp_sum(acc) + ((double)cn - oc[p * 3]);
+            const double dj = seg_reduce<SEG>(segmask, acc) + ((double)cn - oc[p * 3]);
             r = exp(2.0 * dj);
-            if (grad_y) gy += warp_sum(gyl) + dcn * yp[adim] / rp;
-            __syncwarp();
+            if (grad_y) gy += seg_reduce<SEG>(segmask, gyl) + dcn * yp[adim] / rp;
+            __syncwarp(segmask);
             break;
         }
         case 6: {  // hydrogenlike.cpp:231-242
@@ -837,13 +858,15 @@ __host__ __device__ inline int gen_stage_doubles(const GenParams &g, int nacc)
 // its accumulators after it (gen_stage_doubles in all), or null to work on them in
 // global memory; staged, every step's reads and writes stay on chip and the record
 // goes back once at the end.
-template <bool TC, int GV = GV_ANY>
+template <bool TC, int GV = GV_ANY, int SEG = 32>
 __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, int step_offset, const GenParams &g,
                                                  int w, bool active, double *scr, float *mw, TcMlp &tc, float *pre_w,
                                                  double *stage = nullptr, bool stage_acc = true)
 {
+    static_assert(SEG == 32 || (!TC && GV != GV_ANY), "several walkers per warp: compiled forms only");
     const Params &P = a.P;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int lane = threadIdx.x & (SEG - 1), wib = threadIdx.x >> 5;
+    const unsigned segmask = gen_segmask<SEG>();
 
     const int N = P.N, D = g.D, dim = gv_dim(GV, D / N);
     const int ws = active ? w : 0;  // record pointers of a warp without a walker are never used
@@ -852,10 +875,10 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
     double *rec = grec, *acc = gacc;
     const bool staged = stage && active, acc_staged = staged && stage_acc;
     if (staged) {
-        for (int i = lane; i < g.rec; i += 32) stage[i] = grec[i];
+        for (int i = lane; i < g.rec; i += SEG) stage[i] = grec[i];
         if (acc_staged)
-            for (int i = lane; i < 2 * P.nacc; i += 32) stage[g.rec + i] = gacc[i];
-        __syncwarp();
+            for (int i = lane; i < 2 * P.nacc; i += SEG) stage[g.rec + i] = gacc[i];
+        __syncwarp(segmask);
         rec = stage;
         if (acc_staged) acc = stage + g.rec;
     }
@@ -932,7 +955,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
             const bool corrected = is && !(P.flags & Q_IS_GREEN) && !a.probe_k;
             double gy = 0.0, R = 1.0;
             double *ratios = (a.probe_k && lane == 0) ? a.probe_ratio + (size_t)w * P.n_elem : nullptr;
-            const double prob = gen_ratios<GV>(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
+            const double prob = gen_ratios<GV, SEG>(P, g, dim, rec, mask, scr, lane, k, xn, ratios,
                                            corrected ? &gy : nullptr, R, mw, TC ? pre_w : nullptr);
             bool accept = true;
             if (!a.probe_k) {
@@ -956,17 +979,17 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                     // Sherman-Morrison on the moved particle's block (slaterdeterminant.cpp:165-175)
                     const int n = g.n, b = p / n, pl = p - b * n;
                     double *rows = rec + g.off_inv + (size_t)b * n * n;
-                    for (int o = lane; o < n; o += 32) scr[SCR_ROW + o] = rows[(size_t)pl * n + o];
-                    __syncwarp();
-                    if (lane < n) {
-                        double *row = rows + (size_t)lane * n;
+                    for (int o = lane; o < n; o += SEG) scr[SCR_ROW + o] = rows[(size_t)pl * n + o];
+                    __syncwarp(segmask);
+                    for (int r = lane; r < n; r += SEG) {
+                        double *row = rows + (size_t)r * n;
                         double S = 0.0;
                         for (int o = 0; o < n; ++o) S += scr[SCR_PHI + o] * row[o];
                         const double c = S / R;
                         for (int o = 0; o < n; ++o)
-                            row[o] = lane == pl ? scr[SCR_ROW + o] / R : row[o] - c * scr[SCR_ROW + o];
+                            row[o] = r == pl ? scr[SCR_ROW + o] / R : row[o] - c * scr[SCR_ROW + o];
                     }
-                    __syncwarp();
+                    __syncwarp(segmask);
                 }
                 if (lane == 0) {
                     x[k] = xn;
@@ -974,7 +997,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                 }
                 if (P.flags & F_MLP) {  // the moved particle's pair and one-body values from the proposal
                     double *uc = rec + g.off_uc;
-                    for (int j = lane; j < N; j += 32)
+                    for (int j = lane; j < N; j += SEG)
                         if (j != p) {
                             double *c3 = uc + (size_t)(min(p, j) * N + max(p, j)) * 3;
                             c3[0] = scr[SCR_XS + j];
@@ -985,12 +1008,12 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                         for (int t = 0; t < 3; ++t) rec[g.off_oc + p * 3 + t] = scr[SCR_PN + 32 + t];
                 }
                 if (P.flags & Q_PADE_STALE) {  // the moved particle's pairs take the current gamma
-                    for (int j = lane; j < N; j += 32)
+                    for (int j = lane; j < N; j += SEG)
                         if (j != p) mask[j] |= 1ull << p;
                     if (lane == 0) mask[p] = ~0ull;
                 }
-                __syncwarp();
-                gen_evaluate<GV>(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false, p);
+                __syncwarp(segmask);
+                gen_evaluate<GV, SEG>(P, g, dim, rec, mask, scr, lane, nullptr, nullptr, nullptr, nullptr, mw, false, p);
             }
             if (a.rec_acc && lane == 0) a.rec_acc[(size_t)w * a.rec_stride + it_step] = accept ? 1 : 0;
             const double *en = rec + g.off_en;
@@ -1000,7 +1023,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                 o[1] = en[1];
                 o[2] = en[2];
             }
-            if (it_step >= a.burn_in && a.dens_bins > 0) density_sample<double>(a, x, N, dim, lane);
+            if (SEG == 32 && it_step >= a.burn_in && a.dens_bins > 0) density_sample<double>(a, x, N, dim, lane);
             if (it_step >= a.burn_in) {  // Sampler::sample (sampler.cpp:52-90)
                 const double el = en[0] + en[1] + en[2];
                 if (el != el) status |= ST_NAN_ENERGY;
@@ -1010,13 +1033,13 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                     const int slot = (it_step - a.win_lo) / a.snap_interval - a.snap_first;
                     if (slot >= 0 && slot < a.snap_stride) {
                         const size_t base = (size_t)w * a.snap_stride + slot;
-                        for (int t = lane; t < D; t += 32) a.snap_x[base * D + t] = (float)x[t];
+                        for (int t = lane; t < D; t += SEG) a.snap_x[base * D + t] = (float)x[t];
                         if (lane == 0) a.snap_e[base] = el;
                     }
                 }
                 const int top = win ? 9 + 2 * g.n_act : 9;  // == P.nacc inside the window
                 const double *pg = rec + g.off_pg;
-                for (int t = lane; t < top; t += 32) {
+                for (int t = lane; t < top; t += SEG) {
                     double q;
                     if (t < 8) {
                         const double base = t < 2 ? el : en[(t >> 1) - 1];
@@ -1033,14 +1056,14 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                     acc[2 * t + 1] = c1;
                 }
             }
-            __syncwarp();
+            __syncwarp(segmask);
         }
     }
     if (staged) {
-        __syncwarp();
-        for (int i = lane; i < g.rec; i += 32) grec[i] = rec[i];
+        __syncwarp(segmask);
+        for (int i = lane; i < g.rec; i += SEG) grec[i] = rec[i];
         if (acc_staged)
-            for (int i = lane; i < 2 * P.nacc; i += 32) gacc[i] = acc[i];
+            for (int i = lane; i < 2 * P.nacc; i += SEG) gacc[i] = acc[i];
     }
     if (active && lane == 0) {
         P.counter[w] = ctr;
