@@ -185,15 +185,6 @@ __device__ void density_sample(const SweepArgs &a, const T *x, int N, int dim, i
 
 // ------------------------------------------------------------------ helpers
 
-template <typename T>
-__device__ __forceinline__ void copy_in(T *dst, const T *src, int n_elems, int lane)
-{
-    const int nv = n_elems * (int)sizeof(T) / 16;
-    const uint4 *s = reinterpret_cast<const uint4 *>(src);
-    uint4 *d = reinterpret_cast<uint4 *>(dst);
-    for (int i = lane; i < nv; i += 32) d[i] = s[i];
-}
-
 __device__ __forceinline__ bool same_spin(int i, int j, int N)
 {
     const int h = N >> 1;

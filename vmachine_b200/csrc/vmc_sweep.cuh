@@ -1,4 +1,5 @@
-// Metropolis sweep kernel: one warp per walker, WPB walkers per CTA.
+// Metropolis sweep kernel: one warp per walker (or, for the dots up to N = 30, two or
+// four walkers per warp in 16- or 8-lane segments), WPB warps per CTA.
 //
 // Per step (System::runMetropolisCycles body, src/system.cpp:149-163):
 //   1. draw (k, displacement, uniform) from the walker's Philox stream (or a replay
@@ -21,7 +22,7 @@
 // Template FX: 0 = element flags read at run time (any supported system); a
 // non-zero flag set compiles the flags in (the quantum-dot paths).
 //
-// Shared memory per warp: the walker record (see Layout), the Pade pair mask
+// Shared memory per walker: the walker record (see Layout), the Pade pair mask
 // (N x u64) and the FP64 running scalars (NSCAL doubles).
 #pragma once
 #include <type_traits>
