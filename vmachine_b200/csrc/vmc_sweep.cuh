@@ -494,6 +494,9 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             constexpr int NJ = K > 0 ? (NK + SEG - 1) / SEG : 2;
             T sum_ratio = T(0), d_lap = T(0), d_bh2 = T(0), d_vint = T(0), pair_total = T(0);
             T gp_new[DIM], gdel[NJ][DIM];
+            // Pade pairs keep the previous gamma until one of their particles moves
+            // (reference quirk, the pair masks); without the quirk the masks are unused
+            const bool stale = flags & Q_PADE_STALE;
 #pragma unroll
             for (int c = 0; c < DIM; ++c) {
                 gp_new[c] = T(0);
@@ -561,7 +564,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 pair_total = warp_reduce_scatter8<T, SEG>(vals, lane);
                 sum_ratio = __shfl_sync(FULL, pair_total, 0, SEG);
             } else if (flags & (F_PADE | F_COULOMB)) {
-                const unsigned long long mp = smask[p];
+                const unsigned long long mp = stale ? smask[p] : ~0ull;
                 const T gam = T(P.gamma), gamp = T(P.gamma_prev);
                 // old and new position of the moved particle side by side: every pair
                 // quantity below is a (before, after) pair computed by packed instructions
@@ -585,7 +588,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         if (flags & F_PADE) {
                             const Two<T> r = mul2(r2, ir);
                             const T beta = same_spin(p, j, N) ? T(P.beta_same) : T(P.beta_anti);
-                            const T gpair = ((flags & Q_PADE_STALE) && !((mp >> j) & 1ull)) ? gamp : gam;
+                            const T gpair = (stale && !((mp >> j) & 1ull)) ? gamp : gam;
                             const Two<T> den = fma2(two(gpair, gam), r, two(T(1), T(1)));
                             const Two<T> f1 = two(F::rcp(den.x), F::rcp(den.y));
                             const Two<T> h = mul2(r, f1);                              // r / (1 + g r)
@@ -775,10 +778,10 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
 #pragma unroll
                             for (int c = 0; c < DIM; ++c) gv[c] += gdel[jj][c];
                             store_coords<T, DIM>(gj, j, gv);
-                            if (flags & F_PADE) smask[j] |= (1ull << p);
+                            if (stale) smask[j] |= (1ull << p);
                         }
                     }
-                    if ((flags & F_PADE) && lane == (p & (SEG - 1))) smask[p] = ~0ull;
+                    if (stale && lane == (p & (SEG - 1))) smask[p] = ~0ull;
                 }
                 __syncwarp(segmask);
             }
