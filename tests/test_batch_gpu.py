@@ -56,6 +56,23 @@ def test_batch_equals_alone_fixed_tile(precision):
         assert np.allclose(params[s], th_ref, rtol=TOL, atol=TOL), (s, params[s], th_ref)
 
 
+@pytest.mark.parametrize("tile", [(4, 1), (2, 4)])
+def test_batch_equals_alone_partial_warps(tile):
+    """Populations that are not a multiple of the walkers per warp (four for N <= 6 and
+    He, two for N = 12 to 30): the last item of each system leaves segments without a
+    walker, in the batch and alone alike."""
+    from vmachine_b200.batch import atom_text, dot_text
+    texts = [dot_text(2, 0.7, 37, 300, "mixed", seed=21), dot_text(6, 0.5, 45, 300, "mixed", seed=22),
+             dot_text(12, 0.9, 51, 300, "mixed", seed=23), dot_text(30, 0.6, 33, 300, "mixed", seed=24),
+             atom_text(2, 41, 300, seed=25)]
+    seeds = np.arange(300, 300 + len(texts), dtype=np.uint64)
+    ref = alone(texts, seeds, 3)
+    en, params, info, _ = batched(texts, seeds, 3, tile=tile)
+    for s, (e_ref, th_ref) in enumerate(ref):
+        assert np.allclose(en[:, s], e_ref, rtol=TOL, atol=0), (s, en[:, s], e_ref)
+        assert np.allclose(params[s], th_ref, rtol=TOL, atol=TOL), (s, params[s], th_ref)
+
+
 def test_batch_tuner_keeps_results():
     texts = small_texts("mixed")
     seeds = np.arange(7, 7 + len(texts), dtype=np.uint64)
