@@ -53,11 +53,23 @@ def evaluate(eng, eval_steps, burn_steps=200):
 
 
 def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps=4000,
-            lr_pade=0.01, lr_mlp=3e-4, seed=7):
+            lr_pade=0.01, lr_mlp=3e-4, seed=7, mlp_iterations=None):
+    """Pade against MLP Jastrow at equal wall time: both train for budget_s seconds,
+    or, with mlp_iterations, the MLP trains for that many iterations and the Pade
+    factor for the MLP's wall time; then each frozen wave function is evaluated."""
     out = {"system": f"2D dot N={N} omega={omega}", "walkers": walkers, "steps_per_iteration": steps,
            "budget_s": budget_s, "eval_steps_per_walker": eval_steps}
-    for name, jastrow, lr in (("pade", "padeJastrow", lr_pade), ("mlp", "mlpJastrow", lr_mlp)):
-        eng, hist = train(dot_config(N, omega, jastrow, walkers, steps, lr, seed=seed), budget_s, seed=seed)
+    runs = (("pade", "padeJastrow", lr_pade), ("mlp", "mlpJastrow", lr_mlp))
+    if mlp_iterations:
+        runs = runs[::-1]
+    for name, jastrow, lr in runs:
+        text = dot_config(N, omega, jastrow, walkers, steps, lr, seed=seed)
+        if name == "mlp" and mlp_iterations:
+            eng, hist = train(text, float("inf"), max_iterations=mlp_iterations, seed=seed)
+            budget_s = hist[-1][0]
+            out["budget_s"] = budget_s
+        else:
+            eng, hist = train(text, budget_s, seed=seed)
         energy, err, W = evaluate(eng, eval_steps)
         out[name] = {"iterations": len(hist), "train_seconds": hist[-1][0], "lr": lr,
                      "last_iteration_energy": hist[-1][1], "energy": energy, "error": err}
@@ -106,11 +118,16 @@ def main(argv=None):
     c = sub.add_parser("compare", help="MLP against Pade at equal wall time")
     c.add_argument("--budget", type=float, default=120.0)
     c.add_argument("--walkers", type=int, default=4096)
+    c.add_argument("--steps", type=int, default=800, help="steps per walker per iteration")
+    c.add_argument("--iterations", type=int, default=0,
+                   help="train the MLP for this many iterations and the Pade factor for the same wall time")
+    c.add_argument("--lr-mlp", type=float, default=3e-4)
     a = ap.parse_args(argv)
     if a.cmd == "speed":
         print(json.dumps(sweep_speed(a.walkers, a.steps, tensor_cores=not a.cuda_cores, precision=a.precision)))
     else:
-        print(json.dumps(compare(walkers=a.walkers, budget_s=a.budget)))
+        print(json.dumps(compare(walkers=a.walkers, steps=a.steps, budget_s=a.budget, lr_mlp=a.lr_mlp,
+                                 mlp_iterations=a.iterations or None)))
 
 
 if __name__ == "__main__":
