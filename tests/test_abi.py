@@ -40,6 +40,8 @@ def test_library_exports_every_declared_symbol():
     ("numParticles: 2\nhamiltonian: harmonicOscillator\nwaveFunctionElement: fnn\n", -1),
     ("numParticles: 2\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
      "precision: fp16\n", -1),
+    ("numParticles: 2\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
+     "walkersPerWarp: 3\n", -1),
     # parsed, but not on the engine's path
     ("numParticles: 2\nhamiltonian: doubleWell 1.0\nwaveFunctionElement: gaussian\n", -2),
     ("numParticles: 4\nhamiltonian: harmonicOscillator\nwaveFunctionElement: slaterDeterminant\n"
