@@ -301,7 +301,9 @@ static __device__ unsigned tc_pair_layer(TcMlp &t, const float *w, bool valid, f
                      : "memory");
     t.phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    float u = w[MW_B3], du = 0.0f, ddu = 0.0f;
+    // third layer, two output units at a time in packed FP32 (FADD2 / FMUL2 / FFMA2):
+    // with ng = h^2 - 1 = -(1 - h^2) the sums collect -du and -d2u
+    float2 u2 = make_float2(0.0f, 0.0f), ndu2 = u2, nddu2 = u2;
     const uint32_t lb = t.tmem + ((uint32_t)(wib * 32) << 16);
 #pragma unroll 1
     for (int c = 0; c < 4; ++c) {
@@ -311,16 +313,28 @@ static __device__ unsigned tc_pair_layer(TcMlp &t, const float *w, bool valid, f
         tmem_ld16(lb + 128 + 16 * c, ddz);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int e = 0; e < 16; ++e) {
+        for (int e = 0; e < 16; e += 4) {
             const int m = 16 * c + e;
-            const float zz = __uint_as_float(z[e]) + w[MW_B2 + m], d1 = __uint_as_float(dz[e]),
-                        d2 = __uint_as_float(ddz[e]);
-            const float h2 = mlp_tanh(zz), g2 = 1.0f - h2 * h2, w3 = w[MW_W3 + m];
-            u = fmaf(w3, h2, u);
-            du = fmaf(w3, g2 * d1, du);
-            ddu = fmaf(w3, g2 * (d2 - 2.0f * h2 * d1 * d1), ddu);
+            const float4 b4 = *reinterpret_cast<const float4 *>(w + MW_B2 + m);
+            const float4 w4 = *reinterpret_cast<const float4 *>(w + MW_W3 + m);
+#pragma unroll
+            for (int hp = 0; hp < 2; ++hp) {
+                const int q = e + 2 * hp;
+                const float2 bb = hp ? make_float2(b4.z, b4.w) : make_float2(b4.x, b4.y);
+                const float2 ww = hp ? make_float2(w4.z, w4.w) : make_float2(w4.x, w4.y);
+                const float2 zz = __fadd2_rn(make_float2(__uint_as_float(z[q]), __uint_as_float(z[q + 1])), bb);
+                const float2 d1 = make_float2(__uint_as_float(dz[q]), __uint_as_float(dz[q + 1]));
+                const float2 d2 = make_float2(__uint_as_float(ddz[q]), __uint_as_float(ddz[q + 1]));
+                const float2 h2 = make_float2(mlp_tanh(zz.x), mlp_tanh(zz.y));
+                const float2 ng = __ffma2_rn(h2, h2, make_float2(-1.0f, -1.0f));
+                u2 = __ffma2_rn(ww, h2, u2);
+                ndu2 = __ffma2_rn(ww, __fmul2_rn(ng, d1), ndu2);
+                const float2 inner = __ffma2_rn(__fmul2_rn(h2, __fmul2_rn(d1, d1)), make_float2(-2.0f, -2.0f), d2);
+                nddu2 = __ffma2_rn(ww, __fmul2_rn(ng, inner), nddu2);
+            }
         }
     }
+    const float u = w[MW_B3] + (u2.x + u2.y), du = -(ndu2.x + ndu2.y), ddu = -(nddu2.x + nddu2.y);
     const float q = 1.0f / (1.0f + r);
     pre[lane] = u + a * r * q;
     pre[32 + lane] = du + a * q * q;
