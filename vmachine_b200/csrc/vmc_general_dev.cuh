@@ -35,10 +35,12 @@ namespace vmc {
 namespace {
 
 
-constexpr int GEN_WPB = 4;     // walkers (warps) per CTA
-constexpr int GEN_SCR = 256;   // shared doubles per warp
-// shared scratch of a warp: orbital values at the proposal | moved row | RBM visible
-// (sorted) | RBM hidden p_j = 1/(1+e^v) | RBM hidden e^v/(1+e^v)
+constexpr int GEN_WPB = 4;     // warps per CTA
+constexpr int GEN_SCR = 256;   // shared doubles per warp (a warp of G walkers: GEN_SCR / G each)
+// shared scratch of a walker: orbital values at the proposal | moved row | RBM visible
+// (sorted) | RBM hidden p_j = 1/(1+e^v) | RBM hidden e^v/(1+e^v); the pair elements'
+// per-pair terms reuse it from offset 0 during an evaluation (the compiled atom form
+// with four walkers per warp has 64 doubles: the proposal's orbitals and moved row)
 constexpr int SCR_PHI = 0, SCR_ROW = 32, SCR_XS = 64, SCR_PN = 128, SCR_NN = 192;
 
 __device__ __forceinline__ double gen_dist(const double *x, int dim, int i, int j)
