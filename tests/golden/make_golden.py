@@ -7,6 +7,7 @@ reference nor its build.
 
     python tests/golden/make_golden.py            # rewrites tests/golden/*.npz
     python tests/golden/make_golden.py hydrogen   # only hydrogen_orbitals.npz
+    python tests/golden/make_golden.py hydrogen_sj   # only hydrogen_simplejastrow.npz
     python tests/golden/make_golden.py weights    # only weights_format.npz
 
 Every input is seeded synthetic data: walker positions ~ N(0, 1/sqrt(omega)),
@@ -244,6 +245,28 @@ def make_weights(rng):
     return out
 
 
+# The same atoms with a SimpleJastrow factor (the general path's compiled atom form),
+# in a file of their own so the fixtures above stay as they are.
+HYDROGEN_SJ_EVAL = [
+    ("he_horb_sj", SystemSpec(N=2, Z=2, elements=(S, SIMPLEJASTROW), **H_ORB), 1.0, "random"),
+    ("ne_horb_sj", SystemSpec(N=10, Z=10, elements=(S, SIMPLEJASTROW), **H_ORB), 0.6, "random"),
+    ("ne_horb_pade_sj", SystemSpec(N=10, Z=10, elements=(S, P, SIMPLEJASTROW), **H_ORB), 0.6, "random"),
+]
+HYDROGEN_SJ_CHAINS = [
+    ("he_horb_sj_is", SystemSpec(N=2, Z=2, elements=(S, SIMPLEJASTROW), step=0.05, **H_ORB), 300),
+    ("ne_horb_sj_is", SystemSpec(N=10, Z=10, elements=(S, SIMPLEJASTROW), step=0.01, **H_ORB), 300),
+    ("ne_horb_sj_bf", SystemSpec(N=10, Z=10, elements=(S, SIMPLEJASTROW), sampling="bruteForce", step=0.02,
+                                 **H_ORB), 300),
+]
+
+
+def make_hydrogen_sj():
+    rng = np.random.default_rng(20261206)
+    out = make_eval(rng, HYDROGEN_SJ_EVAL)
+    out.update({f"chain_{k}": v for k, v in make_chains(rng, HYDROGEN_SJ_CHAINS).items()})
+    np.savez_compressed(os.path.join(HERE, "hydrogen_simplejastrow.npz"), **out)
+
+
 def make_hydrogen():
     rng = np.random.default_rng(20261204)
     out = make_eval(rng, HYDROGEN_EVAL)
@@ -255,11 +278,15 @@ def main():
     if sys.argv[1:] == ["hydrogen"]:
         make_hydrogen()
         return
+    if sys.argv[1:] == ["hydrogen_sj"]:
+        make_hydrogen_sj()
+        return
     if sys.argv[1:] == ["weights"]:
         np.savez_compressed(os.path.join(HERE, "weights_format.npz"),
                             **make_weights(np.random.default_rng(20261205)))
         return
     make_hydrogen()
+    make_hydrogen_sj()
     rng = np.random.default_rng(20261203)
     np.savez_compressed(os.path.join(HERE, "eval_fixed.npz"), **make_eval(rng))
     np.savez_compressed(os.path.join(HERE, "chains.npz"), **make_chains(rng))

@@ -22,9 +22,10 @@ GOLD = os.path.join(HERE, "golden")
 EVAL = load_cases(os.path.join(GOLD, "eval_fixed.npz"))
 CHAINS = load_cases(os.path.join(GOLD, "chains.npz"))
 ITERS = load_cases(os.path.join(GOLD, "iterations.npz"))
-_H = load_cases(os.path.join(GOLD, "hydrogen_orbitals.npz"))
-EVAL.update({k: v for k, v in _H.items() if not k.startswith("chain_")})
-CHAINS.update({k[len("chain_"):]: v for k, v in _H.items() if k.startswith("chain_")})
+for _f in ("hydrogen_orbitals.npz", "hydrogen_simplejastrow.npz"):
+    _H = load_cases(os.path.join(GOLD, _f))
+    EVAL.update({k: v for k, v in _H.items() if not k.startswith("chain_")})
+    CHAINS.update({k[len("chain_"):]: v for k, v in _H.items() if k.startswith("chain_")})
 ENGINE_ELEMENTS = {GAUSSIAN, SLATER, PADE, HYDROGENLIKE, SIMPLEJASTROW, RBMGAUSSIAN, RBMPRODUCT}
 
 

@@ -36,9 +36,10 @@ CHAINS = load_cases(os.path.join(GOLD, "chains.npz"))
 ITERS = load_cases(os.path.join(GOLD, "iterations.npz"))
 BLOCK = load_cases(os.path.join(GOLD, "blocking.npz"))
 # Slater determinants of hydrogen orbitals (He, Be, Ne, Mg, Ar): fixed positions and chains
-_H = load_cases(os.path.join(GOLD, "hydrogen_orbitals.npz"))
-EVAL.update({k: v for k, v in _H.items() if not k.startswith("chain_")})
-CHAINS.update({k[len("chain_"):]: v for k, v in _H.items() if k.startswith("chain_")})
+for _f in ("hydrogen_orbitals.npz", "hydrogen_simplejastrow.npz"):
+    _H = load_cases(os.path.join(GOLD, _f))
+    EVAL.update({k: v for k, v in _H.items() if not k.startswith("chain_")})
+    CHAINS.update({k[len("chain_"):]: v for k, v in _H.items() if k.startswith("chain_")})
 
 
 @pytest.mark.parametrize("name", sorted(EVAL))
