@@ -192,6 +192,35 @@ def test_atom_sweep_matches_oracle_chain(Z, elements, compat):
     assert rel(final, p) < 1e-11
 
 
+@pytest.mark.parametrize("n,walkers,compat", [(2, 37, 1), (6, 37, 1), (12, 37, 0), (20, 19, 1), (56, 5, 1)])
+def test_production_sweep_matches_oracle(n, walkers, compat):
+    """The production sweep (Philox numbers drawn lane-parallel, nothing recorded; four
+    walkers per warp for N <= 6, two for N = 12 and 20, one for N = 56) against the
+    oracle on the same per-walker Philox streams, FP64: the same final positions and
+    the same sums of sampled energies and accepts."""
+    omega = {2: 1.0, 6: 1.0, 12: 0.8, 20: 0.5, 56: 0.28}[n]
+    steps, seed = 300, 4321
+    spec = SystemSpec(N=n, omega=omega, elements=(SLATER, GAUSSIAN, PADE), step=0.01,
+                      num_steps=walkers * steps, quirks=SystemSpec().quirks if compat else 0)
+    rng = np.random.default_rng(n)
+    pos = rng.normal(0, 1 / np.sqrt(omega), size=(walkers, spec.D))
+    theta = np.array([[0.0], [1.0], [0.5]])
+    with make_engine(spec, walkers, compat=compat) as eng:
+        eng.set_parameters(theta)
+        eng.init_walkers(pos, seed=seed)
+        s, _, _ = eng.sample(0, steps, 0)
+        final = eng.positions()
+    O = Oracle()
+    p = pos.copy()
+    # the importance-sampling force cache as initialised (ImportanceSampling::initialize);
+    # the reference-mode Green's ratio reads it for coordinates not yet moved
+    f = np.stack([O.quantum_force(spec, theta, pos[w]) for w in range(walkers)])
+    out = O.run(spec, theta, p, f, steps, 0, 0, 10, stream=None, seed=seed, counter=np.zeros(walkers, np.uint64))
+    assert rel(final, p) < 1e-11
+    assert abs(s.accepts - out["sums"][:, 8].sum()) < 0.5
+    assert abs(s.energy - out["sums"][:, 0].sum()) < 1e-10 * abs(out["sums"][:, 0].sum())
+
+
 @pytest.mark.parametrize("n", [6, 20, 56])
 def test_mixed_precision_tracks_fp64(n):
     """FP32 sweep with FP64 rebuilds: same decisions on a replayed stream (a flip
