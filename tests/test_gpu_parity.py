@@ -221,6 +221,31 @@ def test_production_sweep_matches_oracle(n, walkers, compat):
     assert abs(s.energy - out["sums"][:, 0].sum()) < 1e-10 * abs(out["sums"][:, 0].sum())
 
 
+@pytest.mark.parametrize("Z,walkers", [(2, 37), (10, 9)])
+def test_atom_sweep_matches_oracle_philox(Z, walkers):
+    """The atoms' sweep on its own Philox streams (He four walkers per warp, a last warp
+    with one; Ne one per warp) against the oracle: final positions and sampled sums."""
+    steps, seed = 300, 977
+    spec = SystemSpec(N=Z, d=3, Z=Z, atom=True, basis="hydrogenOrbital", elements=(SLATER, SIMPLEJASTROW),
+                      step=0.01, num_steps=walkers * steps)
+    rng = np.random.default_rng(Z)
+    pos = rng.normal(size=(walkers, spec.D))
+    theta = np.zeros((2, spec.p_max))
+    theta[1, :Z * Z] = rng.uniform(0.1, 0.5, Z * Z)
+    with make_engine(spec, walkers) as eng:
+        eng.set_parameters(theta)
+        eng.init_walkers(pos, seed=seed)
+        s, _, _ = eng.sample(0, steps, 0)
+        final = eng.positions()
+    O = Oracle()
+    p = pos.copy()
+    f = np.stack([O.quantum_force(spec, theta, pos[w]) for w in range(walkers)])
+    out = O.run(spec, theta, p, f, steps, 0, 0, 10, stream=None, seed=seed, counter=np.zeros(walkers, np.uint64))
+    assert rel(final, p) < 1e-11
+    assert abs(s.accepts - out["sums"][:, 8].sum()) < 0.5
+    assert abs(s.energy - out["sums"][:, 0].sum()) < 1e-10 * abs(out["sums"][:, 0].sum())
+
+
 @pytest.mark.parametrize("n", [6, 20, 56])
 def test_mixed_precision_tracks_fp64(n):
     """FP32 sweep with FP64 rebuilds: same decisions on a replayed stream (a flip
