@@ -65,7 +65,9 @@ def sweep_traffic():
 def flops_per_step(N, d=2):
     """Algorithmic flops of one accepted move plus one E_L / dlnPsi sample in the
     engine's incremental, degree-factorised scheme (FMA = 2, MUL/ADD = 1,
-    div/sqrt/exp = 1); derived term by term in DESIGN.md."""
+    div/sqrt/exp = 1), term by term below: Hermite tables at the proposal, the ratio
+    row contractions, the Sherman-Morrison update, the block's derivative refresh, the
+    moved particle's pair terms, the kinetic sum and the scalar bookkeeping."""
     n = N // 2
     K = next(k for k in range(1, 12) if (k * (k + 1) // 2 if d == 2 else k * (k + 1) * (k + 2) // 6) == n)
     tables = d * 4 * (K - 1)                             # Hermite recurrence at one point

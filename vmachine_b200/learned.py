@@ -6,7 +6,7 @@ ADAM steps (forward and backward kernels on the GPU) for the same wall-clock
 budget each, then evaluated with their parameters frozen: every walker samples
 `eval_steps` moves, and the energy's error bar is the spread of the walkers' mean
 energies over sqrt(walkers) (the walkers are independent Markov chains).  The
-variational principle judges: the lower energy at comparable error bars wins.
+variational principle decides: the lower energy at comparable error bars wins.
 """
 import time
 
