@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define VMC_ABI_VERSION 5
+#define VMC_ABI_VERSION 6
 
 enum {
     VMC_OK = 0,
@@ -32,6 +32,8 @@ enum {
     VMC_E_NAN = -5,         /* NaN kinetic energy (sampler.cpp:219-225 aborts with 143)        */
     VMC_E_SINGULAR = -6,    /* singular Slater block at (re)initialisation                     */
     VMC_E_STATE = -7,       /* call out of order (e.g. sampling before walkers exist)          */
+    VMC_E_TIMEOUT = -8,     /* a bounded device wait gave up: the pass is incomplete, its sums
+                               are not applied; vmc_init_walkers or vmc_load_state clears it  */
 };
 
 enum { VMC_PRECISION_FP64 = 0, VMC_PRECISION_MIXED = 1 };
@@ -59,7 +61,13 @@ typedef struct {
     int element_kind[8];                        /* VMC_ELEM_* in configuration order    */
     int kernel_variant;                         /* VMC_KERNEL_* of the sweep            */
     int walkers_per_warp;                       /* production sweep: 1, or 2 (small dots) */
+    int sweep_form;                             /* VMC_SWEEP_* of the production sweep    */
 } vmc_info;
+
+/* Forms of the production sweep: the walker record staged in shared memory (one, two
+ * or four walkers per warp), or the dots' owner form (one walker per warp, each lane
+ * holding two particles' state in registers; `sweepForm:` key). */
+enum { VMC_SWEEP_STAGED = 1, VMC_SWEEP_OWNER = 2 };
 
 /* Sweep implementations: element flags read at run time, the quantum-dot flag
  * set compiled in, or the general FP64 path (SimpleJastrow, RBM, hydrogen orbitals). */

@@ -21,7 +21,8 @@ SOURCES = ["vmc_engine.cu", "vmc_inst_f32.cu", "vmc_inst_f64.cu", "vmc_config.cp
            "vmc_noalloc.cu", "vmc_general.cu", "vmc_batch.cu", "vmc_batch_f32.cu", "vmc_batch_f64.cu",
            "vmc_blocking.cu", "vmc_checkpoint.cu", "vmc_density.cu"]
 HEADERS = ["vmc_device.cuh", "vmc_kernels.cuh", "vmc_sweep.cuh", "vmc_config.hpp", "vmc_general.hpp",
-           "vmc_general_dev.cuh", "vmc_engine.hpp", "vmc_batch_kernels.cuh", "vmc_mlp.cuh"]
+           "vmc_general_dev.cuh", "vmc_engine.hpp", "vmc_batch_kernels.cuh", "vmc_mlp.cuh",
+           "vmc_owner_sweep.cuh"]
 FLAGS = ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 

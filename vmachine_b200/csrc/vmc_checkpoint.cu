@@ -17,7 +17,8 @@
 //
 // Layout: "VMCSTATE" | u32 version | u32 header ints (n) | n x i32 header |
 // u64 seed | f64 gamma_prev | sections, each u64 byte count + bytes, in the order
-// theta, opt_m, opt_v, state, scal, mask, counter, status.
+// theta, opt_m, opt_v, state, scal, mask, counter, status, and the learned MLP
+// Jastrow dot's per-walker pair and one-body caches (empty for every other system).
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -65,7 +66,7 @@ std::string format_weights(const double *theta, int E, int P, int digits)
 }
 
 const char MAGIC[8] = {'V', 'M', 'C', 'S', 'T', 'A', 'T', 'E'};
-constexpr uint32_t STATE_VERSION = 1;
+constexpr uint32_t STATE_VERSION = 2;
 
 // header ints: what must match between the saving and the loading engine, then the
 // run's progress
@@ -95,6 +96,10 @@ void header(const vmc_engine *e, int32_t *h)
     h[H_OPT_STEP] = e->opt_step;
     h[H_HAVE] = e->have_walkers ? 1 : 0;
 }
+
+// floats of one walker's MLP Jastrow caches: (u, u', u'') of every ordered pair, then
+// (chi, chi', chi'') of every particle
+size_t mlp_cache_floats(const vmc_engine *e) { return (size_t)e->N * e->N * 3 + (size_t)e->N * 3; }
 
 struct Section {
     void *dev;       // device buffer, or null
@@ -187,6 +192,7 @@ int vmc_save_state(const vmc_engine *e, const char *path)
         {e->d_mask, nullptr, W * e->N * sizeof(unsigned long long)},
         {e->d_counter, nullptr, W * sizeof(unsigned long long)},
         {e->d_status, nullptr, W * sizeof(unsigned)},
+        {e->d_mlp_cache, nullptr, e->d_mlp_cache ? W * mlp_cache_floats(e) * sizeof(float) : 0},
     };
     std::ofstream out(path, std::ios::binary);
     if (!out) return ck_fail(VMC_E_ARG, std::string("cannot write '") + path + "'");
@@ -250,6 +256,7 @@ int vmc_load_state(vmc_engine *e, const char *path)
         {e->d_mask, nullptr, W * e->N * sizeof(unsigned long long)},
         {e->d_counter, nullptr, W * sizeof(unsigned long long)},
         {e->d_status, nullptr, W * sizeof(unsigned)},
+        {e->d_mlp_cache, nullptr, e->d_mlp_cache ? W * mlp_cache_floats(e) * sizeof(float) : 0},
     };
     std::vector<std::vector<char>> dev_bytes;
     for (const Section &s : secs) {

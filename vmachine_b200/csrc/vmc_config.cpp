@@ -306,6 +306,11 @@ std::string parse_config(const std::string &text, Config &c)
                 if (v0 == "auto") c.walkers_per_warp = 0;
                 else if (v0 == "1" || v0 == "2" || v0 == "4") c.walkers_per_warp = std::stoi(v0);
                 else return err("walkersPerWarp must be auto, 1, 2 or 4");
+            } else if (key == "sweepForm") {
+                if (v0 == "auto") c.sweep_form = 0;
+                else if (v0 == "staged") c.sweep_form = 1;
+                else if (v0 == "owner") c.sweep_form = 2;
+                else return err("sweepForm must be auto, staged or owner");
             } else if (key == "seed") {
                 c.have_seed = true;
                 c.seed = std::stoll(v0);

@@ -60,6 +60,7 @@ struct Config {
     bool mlp_tc = true;          // MLP Jastrow second layer on the tensor cores (mlpTensorCores)
     int walkers_per_block = 0;   // 0 auto
     int walkers_per_warp = 0;    // at most this many walkers per warp: 0 auto (4 for dots of N <= 6, 2 for N = 12 to 30), 1, 2, 4
+    int sweep_form = 0;          // production dot sweep: 0 auto (owner for one walker per warp), 1 staged, 2 owner
 };
 
 // Returns empty string on success, else an error message.

@@ -267,6 +267,13 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
         return VMC_OK;
     }
     const bool plain = !a.probe_k && !a.replay && !a.rec_en && !a.rec_acc && !a.dens_bins;
+    if (plain && e->owner) {
+        a.wpb = OWNER_WPB;
+        a.smem_per_warp = e->ks.owner_smem;
+        const size_t smem = (size_t)OWNER_WPB * a.smem_per_warp;
+        CUDA_TRY(cudaFuncSetAttribute(e->ks.sweep_owner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        return launch(e->ks.sweep_owner, (e->W + OWNER_WPB - 1) / OWNER_WPB, 32 * OWNER_WPB, smem, e->stream, &a);
+    }
     const void *fn = plain ? e->ks.sweep_plain : e->ks.sweep;
     const int g = plain ? e->ks.seg : 1;  // walkers per warp
     a.wpb = e->wpb;
@@ -581,6 +588,11 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
             e->ks.seg = 1;
         }
     }
+    // the owner form of the production dot sweep: by default where one walker per warp
+    // remains (N = 42 and 56), on request for N = 20 and 30
+    if (c.sweep_form == 2 && !e->ks.sweep_owner) return reject("sweepForm: owner covers the 2D dots of N = 20 to 56");
+    e->owner = e->ks.sweep_owner && (c.sweep_form == 2 || (c.sweep_form == 0 && e->ks.seg == 1));
+    if (e->owner) e->ks.seg = 1;
     // auto: start at 4 D steps (at least 512) and let the drift test tune it
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
                           : (e->precision == VMC_PRECISION_MIXED ? std::max(4 * e->D, 512) : 0);
@@ -679,6 +691,8 @@ int vmc_get_info(const vmc_engine *e, vmc_info *o)
                         : (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED || e->flags == FX_MLP_DOT) && e->K > 0
                             ? VMC_KERNEL_DOT : VMC_KERNEL_RUNTIME_FLAGS;
     o->walkers_per_warp = e->general ? (e->gen.variant == GV_ATOM ? e->gen.seg : 1) : e->ks.seg;
+    o->sweep_form = e->owner ? VMC_SWEEP_OWNER : VMC_SWEEP_STAGED;
+    if (e->owner) o->walkers_per_block = OWNER_WPB;
     return VMC_OK;
 }
 
@@ -1389,6 +1403,11 @@ int apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum, con
 
 int finish_sample(vmc_engine *e, const SamplePass &p, vmc_sums *out, std::vector<double> &sums)
 {
+    // a walker whose tensor-core wait gave up stopped sampling part-way: its sums are
+    // incomplete and its record may be too, so neither the pass nor the walkers are used
+    // until they are set up again (the status words are cumulative)
+    if (p.status & ST_TC_TIMEOUT)
+        return fail(VMC_E_TIMEOUT, "a tensor-core completion wait gave up; re-initialise the walkers");
     const double *dev_sums = p.dev_sums;
     sums.assign(e->nacc, 0.0);
     if (e->general || e->flags == FX_MLP_DOT) {  // active parameters back to their (element, parameter) slots

@@ -31,6 +31,7 @@ struct vmc_engine {
     int precision = 0, compat = 1, flags = 0, sampling = 0;
     int steps_per_walker = 0, burn_in = 0, batches = 1;
     int wpb = 0, refresh_interval = 0, sweep_chunk = 2048;
+    bool owner = false;  // production dot sweep in the owner form (vmc_owner_sweep.cuh)
     bool refresh_auto = false;          // refreshInterval: auto (mixed precision)
     double drift_tol = 1e-4;            // inverse drift that halves the interval
     size_t elem_bytes = 8;

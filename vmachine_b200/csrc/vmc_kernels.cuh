@@ -211,6 +211,7 @@ static_assert(MLP_FAST_BYTES % 16 == 0 && (MW_W2 * 4) % 16 == 0, "MLP block alig
 }  // namespace vmc
 
 #include "vmc_sweep.cuh"
+#include "vmc_owner_sweep.cuh"
 
 namespace vmc {
 
@@ -698,6 +699,8 @@ struct KernelSet {
     int seg = 1;                                        // walkers per warp of sweep_plain
     const void *sweep_plain1 = nullptr;                 // production sweep, one walker per warp
     const void *sweep_plain2 = nullptr;                 // two walkers per warp (dots of N <= 12), or null
+    const void *sweep_owner = nullptr;                  // production dot sweep, owner form, or null
+    int owner_smem = 0;                                 // its shared bytes per warp
 };
 
 template <typename T, int DIM, int K, int FX>
@@ -711,6 +714,12 @@ KernelSet make_set()
         // 1.05x and 0.89x, the 5-9 KB records of two walkers halving the warps per SM)
         s.sweep_plain2 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 2>);
         s.sweep_plain1 = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true>);
+        if constexpr (K >= 4) {
+            // the owner form: the default for one walker per warp (N = 42, 56), on request
+            // for N = 20 and 30
+            s.sweep_owner = reinterpret_cast<const void *>(&owner_sweep_kernel<T, K, FX>);
+            s.owner_smem = owner_smem_per_warp(K, (int)sizeof(T));
+        }
         if constexpr (K <= 2) {
             s.sweep_plain = reinterpret_cast<const void *>(&sweep_kernel<T, DIM, K, FX, true, 4>);
             s.seg = 4;

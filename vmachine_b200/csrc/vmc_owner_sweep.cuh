@@ -1,0 +1,667 @@
+// Production Metropolis sweep of the 2D closed-shell quantum dots with one walker per
+// warp (N = 42 and 56; N = 20 and 30 on request: Slater(Hermite) x Gaussian x
+// Pade-Jastrow, Coulomb, importance sampling), in the "owner" form: every lane owns two
+// particles of its walker.
+//
+// Lane l < n (n = N / 2 orbitals per spin block) owns particle l (spin up, row l of the
+// first inverse block) and particle n + l (spin down, row l of the second block).  For
+// those two particles it keeps, in registers, one pair (particle l, particle n + l) per
+// coordinate of: the positions, d ln det / dx, (d^2 det / dx^2) / det and the Pade
+// gradient.  The pair terms of a move (the moved particle against both of a lane's
+// particles), the Jastrow gradient update and the kinetic energy are therefore packed
+// two-wide instructions on register operands.  Shared memory holds what the whole warp
+// reads at one index: the inverse blocks and, per coordinate, the position, the drift
+// gradient d ln Psi / dx and the importance-sampling force cache of the proposal.
+//
+// Per step (System::runMetropolisCycles body, src/system.cpp:149-163; the quantities
+// are those of the staged sweep in vmc_sweep.cuh, whose comments cite the reference for
+// every term):
+//   1. k, the normal and the accept uniform from the walker's Philox stream (drawn 32
+//      steps at a time, lane-parallel); the drifted proposal of coordinate k;
+//   2. the Slater ratio R = sigma_p phi(r_p') . row p (lane l: its row of the moved
+//      particle's block), the Pade / Coulomb pair terms of both own particles against the
+//      moved one, one reduce-scatter of the pair sums (which also carries the previous
+//      step's per-lane kinetic terms, so the kinetic energy costs no reduction of its own);
+//   3. accept: Sherman-Morrison through the row scales (below), the block's derivative
+//      vectors recomputed from the updated rows, the Pade gradient, the running sums;
+//   4. E_L and dlnPsi/dtheta of every step after burn-in (one step late: the kinetic sum of
+//      step s is the total carried by the reduce-scatter of step s + 1).
+//
+// Staged inverse rows.  Orbitals are reordered in shared memory so that the transposed
+// pair (a, b), (b, a) sits in adjacent slots (the diagonal orbitals (a, a) last), and the
+// entries are written for the basis hh_m(u) = He_m(u) / m!, u = sqrt(2) x (probabilists'
+// Hermite polynomials), whose derivatives are hh'_m = hh_{m-1}: the engine's normalised
+// functions are h_m(x) = H_m(x) / sqrt(2^m m!) = sqrt(m!) hh_m(sqrt(2) x), so a staged
+// entry is the record's entry times sqrt(m0! m1!), a column scaling of the Slater matrix
+// under which ratios and derivative vectors are unchanged.  Each row also carries a scale
+// sigma (true row = sigma x staged row): an accepted move divides the moved particle's
+// row by R through its sigma alone, so the rank-1 pass updates every other row from a
+// row that nobody writes (no warp barrier between the reads and the writes).
+//
+// Sums.  The running pair sums (Pade Laplacian, sum beta h^2, Coulomb) and sum x^2 are
+// FP64 per walker.  In the FP32 form the per-step changes go to FP32 partial sums that
+// are added to the FP64 values every 32 steps, and each lane's accumulator slot adds its
+// per-step sample, shifted by the walker's value at the start of the launch, to an FP32
+// partial sum folded into the lane's FP64 Neumaier accumulator every 32 steps.  The FP64
+// form adds to the FP64 sums and accumulators every step, as the staged sweep does.
+#pragma once
+
+namespace vmc {
+
+// Orbital order of the staged inverse rows: slot 2q holds orbital (a, b) and slot 2q + 1
+// orbital (b, a) of the q-th transposed pair (a < b, a + b < K, by a then b); the
+// diagonal orbitals (d, d), 2d < K, follow.  Per slot: the Hermite degrees along x (m0)
+// and y (m1), the orbital's index in the record (the reference's order: shell s = m0 + m1,
+// then m1) and the staging scale sqrt(m0! m1!).
+struct PairTable {
+    int m0[32], m1[32], orb[32];
+    double scale[32];
+};
+
+__host__ __device__ constexpr double owner_factorial(int m) { return m <= 1 ? 1.0 : m * owner_factorial(m - 1); }
+// square root by Newton's iteration (compile-time staging scales)
+__host__ __device__ constexpr double owner_sqrt(double v)
+{
+    double r = v > 1.0 ? v : 1.0;
+    for (int i = 0; i < 64; ++i) r = 0.5 * (r + v / r);
+    return r;
+}
+
+template <int K> __host__ __device__ constexpr PairTable make_pair_table()
+{
+    PairTable t{};
+    int i = 0;
+    for (int a = 0; a < K; ++a)
+        for (int b = a + 1; a + b < K; ++b) {
+            t.m0[i] = a;
+            t.m1[i] = b;
+            t.m0[i + 1] = b;
+            t.m1[i + 1] = a;
+            i += 2;
+        }
+    for (int d = 0; 2 * d < K; ++d) {
+        t.m0[i] = d;
+        t.m1[i] = d;
+        ++i;
+    }
+    for (int j = 0; j < i; ++j) {
+        const int s = t.m0[j] + t.m1[j];
+        t.orb[j] = s * (s + 1) / 2 + t.m1[j];
+        t.scale[j] = owner_sqrt(owner_factorial(t.m0[j]) * owner_factorial(t.m1[j]));
+    }
+    return t;
+}
+
+template <typename T> __device__ __forceinline__ T fmaT(T a, T b, T c);
+template <> __device__ __forceinline__ float fmaT<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <> __device__ __forceinline__ double fmaT<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// hh_0..hh_{K-1} at u: hh_{m+1} = (u hh_m - hh_{m-1}) / (m + 1)
+template <int K, typename T>
+__device__ __forceinline__ void hermite_pe(T u, T (&h)[K])
+{
+    h[0] = T(1);
+    if (K > 1) h[1] = u;
+#pragma unroll
+    for (int m = 1; m + 1 < K; ++m) h[m + 1] = (u * h[m] - h[m - 1]) * T(1.0 / (m + 1));
+}
+
+constexpr int OWNER_WPB = 4;  // walkers (warps) per CTA
+
+// Shared bytes per warp: the inverse blocks, then per coordinate the positions, drift
+// gradients and force cache, then the Pade pair masks.
+__host__ __device__ constexpr int owner_smem_per_warp(int K, int elem_bytes)
+{
+    const int n = K * (K + 1) / 2, D = 4 * n;
+    return (2 * n * inv_row_stride(n, elem_bytes) + 3 * D) * elem_bytes + 2 * n * 8;
+}
+
+template <typename T, int K, int FX>
+__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_sweep_kernel(const SweepArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr PairTable PO = make_pair_table<K>();
+    using T2 = Two<T>;
+    using Fs = Fast<T>;
+    constexpr int n = K * (K + 1) / 2, N = 2 * n, D = 2 * N;
+    constexpr int VE = 16 / (int)sizeof(T);
+    constexpr int IS = inv_row_stride(n, (int)sizeof(T));
+    constexpr int NQ = (n + VE - 1) / VE;
+    constexpr bool F32 = sizeof(T) == 4;
+    constexpr bool GREEN_Q = (FX & Q_IS_GREEN) != 0;
+    constexpr bool STALE = (FX & Q_PADE_STALE) != 0;
+    constexpr bool RATIO_Q = (FX & Q_PADE_RATIO) != 0;
+    static_assert(n <= 32 && (FX & F_IS) && (FX & F_PADE) && (FX & F_COULOMB) && (FX & F_GAUSS) &&
+                      (FX & F_SLATER) && !(FX & (F_ATOM | F_HYDROGENLIKE | F_MLP)),
+                  "the owner sweep covers the 2D closed-shell dots with Pade and Coulomb");
+
+    const Params &P = a.P;
+    const Layout L = P.L;
+    const int l = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const bool own = l < n;
+    const int lc = own ? l : n - 1;  // lanes without particles shadow the last row and store nothing
+    unsigned char *ws = smem_raw + (size_t)wib * a.smem_per_warp;
+    T *inv = reinterpret_cast<T *>(ws);
+    T *xs = inv + 2 * n * IS, *gs = xs + D, *fcs = gs + D;
+    unsigned long long *msk = reinterpret_cast<unsigned long long *>(fcs + D);
+
+    const T wa = T(P.omega * P.alpha);
+    const T hdt = T(0.5 * P.step), sdt = T(sqrt(P.step));
+    const T gam = T(P.gamma), gamp = T(P.gamma_prev);
+    const T2 gam2 = two(gam, gam), m2gam = two(T(-2) * gam, T(-2) * gam), one2 = two(T(1), T(1));
+    const T2 mwa2 = two(-wa, -wa);
+    const T bsame = T(P.beta_same), banti = T(P.beta_anti);
+    const T sq2 = T(1.4142135623730951);
+    const double dgk = (FX & Q_PADE_DGAMMA) ? -0.5 : -1.0;  // dlnPsi/dgamma = dgk sum beta h^2
+    const double lapc = P.omega * P.alpha * D;              // the Gaussian's -Laplacian
+    const double w2h = 0.5 * P.omega * P.omega;
+    // accumulator slot of this lane: 0..7 energy moments, 8 accepts, then the parameter
+    // gradients (1 alpha, 2 gamma) and the same times E_L
+    int pk = 0;
+    bool te = false;
+    if (l >= 9 && l < P.nacc) {
+        int j = l - 9;
+        te = j >= P.ep;
+        if (te) j -= P.ep;
+        pk = j == P.idx_alpha ? 1 : j == P.idx_gamma ? 2 : 0;
+    }
+    const int eg = (l >> 1) & 3;  // energy slots: 0 E, 1 T, 2 V_ext, 3 V_int
+
+    for (int w = blockIdx.x * OWNER_WPB + wib; w < P.W; w += gridDim.x * OWNER_WPB) {
+        T *rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
+        // ---- stage the walker: inverse rows reordered and rescaled, own particles' arrays
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const T *src = rec + L.off_inv + (size_t)(h * n + lc) * L.inv_stride;
+            T *dst = inv + (h * n + lc) * IS;
+            T v[IS];
+#pragma unroll
+            for (int i = 0; i < IS; ++i) v[i] = i < n ? src[PO.orb[i < n ? i : 0]] * T(PO.scale[i < n ? i : 0]) : T(0);
+            if (own)
+#pragma unroll
+                for (int q = 0; q < IS / VE; ++q) vstore<T>(dst + q * VE, v + q * VE);
+        }
+        T2 X[2], DD[2], SD[2], GJ[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int ka = 2 * lc + c, kb = 2 * (n + lc) + c;
+            const T z = T(0);
+            X[c] = own ? two(rec[L.off_x + ka], rec[L.off_x + kb]) : two(z, z);
+            DD[c] = own ? two(rec[L.off_dd + ka], rec[L.off_dd + kb]) : two(z, z);
+            SD[c] = own ? two(rec[L.off_sdd + ka], rec[L.off_sdd + kb]) : two(z, z);
+            GJ[c] = own ? two(rec[L.off_gj + ka], rec[L.off_gj + kb]) : two(z, z);
+        }
+        for (int i = l; i < D; i += 32) {
+            xs[i] = rec[L.off_x + i];
+            fcs[i] = rec[L.off_fc + i];
+        }
+        // Pade pairs keep the previous gamma until one of their particles moves (the
+        // reference quirk); once every particle of the walker has moved, all pairs are
+        // current and the masks are left alone
+        bool allcur = true, mdirty = false;
+        if constexpr (STALE) {
+            if (P.gamma != P.gamma_prev) {
+                const unsigned long long *gm = P.mask + (size_t)w * N;
+                for (int j = l; j < N; j += 32) msk[j] = gm[j];
+                const unsigned long long mm = own ? (gm[l] & gm[n + l]) : ~0ull;
+                allcur = __all_sync(FULL, mm == ~0ull);
+                mdirty = !allcur;
+            }
+        }
+        const double *sc = P.scal + (size_t)w * NSCAL;
+        double sumx2 = sc[SC_SUMX2], lapj = sc[SC_LAPJ], bh2 = sc[SC_BH2], vint = sc[SC_VINT];
+        T2 SIG = two(T(1), T(1));
+
+        // drift gradient G = -omega alpha x + d ln det + Pade gradient of the own particles
+        // into shared memory, and this lane's kinetic terms (G^2 + d2det/det - dd^2)
+        auto publish = [&]() -> T {
+            T2 k2 = add2(SD[0], SD[1]);
+            T2 G[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                G[c] = fma2(mwa2, X[c], add2(DD[c], GJ[c]));
+                k2 = fma2(G[c], G[c], k2);
+                k2 = fma2(two(-DD[c].x, -DD[c].y), DD[c], k2);
+            }
+            if (own) {
+                reinterpret_cast<T2 *>(gs)[l] = two(G[0].x, G[1].x);
+                reinterpret_cast<T2 *>(gs)[n + l] = two(G[0].y, G[1].y);
+            }
+            return k2.x + k2.y;
+        };
+        T kp = publish();  // this lane's kinetic terms after the last update
+        const T ks0 = seg_sum<32>(kp);
+        __syncwarp();
+
+        double acc_s = 0.0, acc_c = 0.0;
+        if (l < P.nacc) {
+            acc_s = P.acc[((size_t)w * P.nacc + l) * 2];
+            acc_c = P.acc[((size_t)w * P.nacc + l) * 2 + 1];
+        }
+        // FP32 form: the walker's energies at the start of the launch (the shifts of the
+        // per-step samples) and the FP32 parts of the running sums since the last fold
+        const double T0 = -0.5 * ((double)ks0 + lapj - lapc), V0 = w2h * sumx2, I0 = vint, E0 = T0 + V0 + I0;
+        const double myref = l < 8 ? (eg == 0 ? E0 : eg == 1 ? T0 : eg == 2 ? V0 : I0) : E0;
+        T cT = T(0), cV = T(0), cI = T(0), gA = T(0), gG = T(0);  // FP32 shifted bases at the fold
+        T dlap = T(0), dbh2 = T(0), dvint = T(0), dsx2 = T(0);    // FP32 changes since the fold
+        T accf = T(0);
+        int ns = 0;
+        auto fp32_bases = [&]() {
+            cT = T(-0.5 * lapj + 0.5 * lapc - T0);
+            cV = T(w2h * sumx2 - V0);
+            cI = T(vint - I0);
+            gA = T(-0.5 * P.omega * sumx2);
+            gG = T(dgk * bh2);
+        };
+        auto fold = [&]() {
+            if constexpr (F32) {
+                const T part = __shfl_xor_sync(FULL, accf, 1);  // odd energy slots: the linear sum
+                const T gsum = __shfl_sync(FULL, accf, te ? l - P.ep : l);
+                double v = (double)accf;
+                if (l < 8) v += (l & 1) ? ns * myref * myref + 2.0 * myref * (double)part : ns * myref;
+                else if (te) v += myref * (double)gsum;
+                kadd(acc_s, acc_c, v);
+                accf = T(0);
+                ns = 0;
+                // the FP32 running-sum changes into the FP64 sums
+                lapj += (double)dlap;
+                bh2 += (double)dbh2;
+                vint += (double)dvint;
+                sumx2 += (double)dsx2;
+                dlap = dbh2 = dvint = dsx2 = T(0);
+                fp32_bases();
+            }
+        };
+        if constexpr (F32) fp32_bases();
+
+        unsigned long long ctr = P.counter[w];
+        unsigned status = 0;
+        // the step whose sample is pending (taken with the next step's reduce-scatter)
+        bool pend = false, pend_acc = false, pend_win = false;
+
+        // E_L and dlnPsi/dtheta of the pending step from its kinetic sum ks
+        auto sample = [&](T ks) {
+            if constexpr (F32) {
+                const T Ts = fmaT(T(-0.5), ks + dlap, cT);
+                const T Vs = fmaT(T(w2h), dsx2, cV);
+                const T Is = cI + dvint;
+                const T Es = Ts + Vs + Is;
+                if (Es != Es) status |= ST_NAN_ENERGY;
+                const T eb = eg == 0 ? Es : eg == 1 ? Ts : eg == 2 ? Vs : Is;
+                const T gl = pk == 1 ? fmaT(T(-0.5 * P.omega), dsx2, gA) : pk == 2 ? fmaT(T(dgk), dbh2, gG) : T(0);
+                const T gq = pend_win ? (te ? Es * gl : gl) : T(0);
+                accf += l < 8 ? ((l & 1) ? eb * eb : eb) : l == 8 ? (pend_acc ? T(1) : T(0)) : gq;
+                ++ns;
+            } else {
+                const double lap = (double)ks + lapj - lapc;
+                const double ekin = -0.5 * lap, vext = w2h * sumx2, el = ekin + vext + vint;
+                if (el != el) status |= ST_NAN_ENERGY;
+                const double base = eg == 0 ? el : eg == 1 ? ekin : eg == 2 ? vext : vint;
+                const double qe = (l & 1) ? base * base : base;
+                const double g = pk == 1 ? -0.5 * P.omega * sumx2 : pk == 2 ? dgk * bh2 : 0.0;
+                const double qp = pend_win ? (te ? g * el : g) : 0.0;
+                kadd(acc_s, acc_c, l < 8 ? qe : l == 8 ? (pend_acc ? 1.0 : 0.0) : qp);
+            }
+        };
+
+        for (int s0 = 0; s0 < a.steps; s0 += 32) {
+            // lane i draws the numbers of step ctr + i; step s0 + i reads them by shuffle
+            int rng_k;
+            T rng_z;
+            unsigned rng_u;
+            {
+                const unsigned long long c = ctr + (unsigned long long)l;
+                const uint4 v = philox(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)w, 0u),
+                                       make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
+                rng_k = (int)__umulhi(v.x, (unsigned)D);
+                if constexpr (F32) {
+                    const float u1 = ((float)v.y + 1.0f) * 2.3283064e-10f;
+                    const float u2 = (float)v.z * 2.3283064e-10f;
+                    rng_z = sqrtf(-2.0f * __logf(u1)) * __cosf(6.2831853f * u2);
+                } else {
+                    const double u1 = ((double)v.y + 1.0) * TWO_M32, u2 = v.z * TWO_M32;
+                    rng_z = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+                }
+                rng_u = v.w;
+            }
+            if constexpr (STALE) {
+                if (!allcur) {
+                    const unsigned long long mm = own ? (msk[l] & msk[n + l]) : ~0ull;
+                    allcur = __all_sync(FULL, mm == ~0ull);
+                }
+            }
+            const int s_end = min(s0 + 32, a.steps);
+            for (int s = s0; s < s_end; ++s) {
+                const int it_step = a.step_offset + s;
+                const int slot = (s - s0) & 31;
+                ++ctr;
+                const int k = __shfl_sync(FULL, rng_k, slot);
+                const T zr = __shfl_sync(FULL, rng_z, slot);
+                const unsigned ur = __shfl_sync(FULL, rng_u, slot);
+                // ---- 1. proposal of coordinate k (particle p, axis adim; owner lane pl of block b)
+                const int p = k >> 1, adim = k & 1;
+                const int b = p >= n ? 1 : 0;
+                const int pl = p - b * n;
+                const T2 xp = reinterpret_cast<const T2 *>(xs)[p];
+                const T xo = adim ? xp.y : xp.x;
+                const T Fn = T(2) * gs[k];
+                const T dx = hdt * Fn + zr * sdt;
+                const T xn = xo + dx;
+                const T qx = adim ? xp.x : xn, qy = adim ? xn : xp.y;  // proposed position of p
+
+                // ---- 2a. Slater: s_l = phi(r_p') . staged row l of block b (lane l), R = sigma_p s_pl
+                T hu[K], hv[K];
+                hermite_pe<K>(sq2 * qx, hu);
+                hermite_pe<K>(sq2 * qy, hv);
+                T sl, gl_ = T(0);
+                {
+                    const T *row = inv + (b * n + lc) * IS;
+                    T part[K];
+#pragma unroll
+                    for (int m = 0; m < K; ++m) part[m] = T(0);
+                    if (GREEN_Q || adim == 0) {
+                        // factorised along x: part[m0] = sum_m1 hh_m1(v) row
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            T v[VE];
+                            vload<T>(row + q * VE, v);
+#pragma unroll
+                            for (int e = 0; e < VE; ++e) {
+                                const int i = q * VE + e;
+                                if (i < n) part[PO.m0[i]] = fmaT(hv[PO.m1[i]], v[e], part[PO.m0[i]]);
+                            }
+                        }
+                        T s2 = T(0), g2 = T(0);
+#pragma unroll
+                        for (int m = 0; m < K; ++m) s2 = fmaT(hu[m], part[m], s2);
+                        if (!GREEN_Q)
+#pragma unroll
+                            for (int m = 1; m < K; ++m) g2 = fmaT(hu[m - 1], part[m], g2);
+                        sl = s2;
+                        gl_ = g2;
+                    } else {
+                        // factorised along y (corrected mode, a move along y)
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            T v[VE];
+                            vload<T>(row + q * VE, v);
+#pragma unroll
+                            for (int e = 0; e < VE; ++e) {
+                                const int i = q * VE + e;
+                                if (i < n) part[PO.m1[i]] = fmaT(hu[PO.m0[i]], v[e], part[PO.m1[i]]);
+                            }
+                        }
+                        T s2 = T(0), g2 = T(0);
+#pragma unroll
+                        for (int m = 0; m < K; ++m) s2 = fmaT(hv[m], part[m], s2);
+#pragma unroll
+                        for (int m = 1; m < K; ++m) g2 = fmaT(hv[m - 1], part[m], g2);
+                        sl = s2;
+                        gl_ = g2;
+                    }
+                }
+                const T sig_l = b ? SIG.y : SIG.x;  // this lane's row scale in block b
+                const T R = __shfl_sync(FULL, sig_l * sl, pl);
+
+                // ---- 2b. pair terms: the moved particle against both own particles (packed)
+                T2 gdx, gdy;  // Pade gradient change of the own particles
+                T vals[8];
+                {
+                    const T2 pxo = two(-xp.x, -xp.x), pyo = two(-xp.y, -xp.y);
+                    const T2 pxn = two(-qx, -qx), pyn = two(-qy, -qy);
+                    const T2 dxo = add2(X[0], pxo), dyo = add2(X[1], pyo);
+                    const T2 dxn = add2(X[0], pxn), dyn = add2(X[1], pyn);
+                    const T2 r2o = fma2(dyo, dyo, mul2(dxo, dxo)), r2n = fma2(dyn, dyn, mul2(dxn, dxn));
+                    // partners: particle l (block 0) and n + l (block 1), not the moved one
+                    const bool va = own && !(b == 0 && l == pl), vb = own && !(b == 1 && l == pl);
+                    const T2 iro = two(va ? Fs::rsqrt(r2o.x) : T(0), vb ? Fs::rsqrt(r2o.y) : T(0));
+                    const T2 irn = two(va ? Fs::rsqrt(r2n.x) : T(0), vb ? Fs::rsqrt(r2n.y) : T(0));
+                    const T2 ro = mul2(r2o, iro), rn = mul2(r2n, irn);
+                    // spin coefficients: particle l has spin up, n + l spin down
+                    const T2 B = b ? two(banti, bsame) : two(bsame, banti);
+                    T2 gpo = gam2;
+                    if constexpr (STALE) {
+                        if (!allcur) {
+                            const unsigned long long mp = msk[p];
+                            gpo = two(((mp >> l) & 1ull) ? gam : gamp, ((mp >> (n + l)) & 1ull) ? gam : gamp);
+                        }
+                    }
+                    const T2 deno = fma2(gpo, ro, one2), denn = fma2(gam2, rn, one2);
+                    const T2 f1o = two(Fs::rcp(deno.x), Fs::rcp(deno.y)), f1n = two(Fs::rcp(denn.x), Fs::rcp(denn.y));
+                    const T2 ho = mul2(ro, f1o), hn = mul2(rn, f1n);
+                    const T2 fio = mul2(mul2(f1o, f1o), mul2(B, iro));  // beta f1^2 / r
+                    const T2 fin = mul2(mul2(f1n, f1n), mul2(B, irn));
+                    T2 dh = add2(hn, two(-ho.x, -ho.y));
+                    if constexpr (RATIO_Q) dh = two(l > p ? dh.x : T(0), n + l > p ? dh.y : T(0));
+                    const T2 sr = mul2(B, dh);
+                    const T2 tnx = mul2(fin, dxn), tny = mul2(fin, dyn);
+                    gdx = fma2(fio, dxo, two(-tnx.x, -tnx.y));
+                    gdy = fma2(fio, dyo, two(-tny.x, -tny.y));
+                    // 2 f (DIM - (1 + 2 gamma h)) / r, new minus old (DIM = 2)
+                    const T2 lqo = mul2(fio, fma2(m2gam, ho, one2)), lqn = mul2(fin, fma2(m2gam, hn, one2));
+                    const T2 dl = add2(lqn, two(-lqo.x, -lqo.y));
+                    const T2 hh = fma2(hn, hn, mul2(two(-ho.x, -ho.y), ho));
+                    const T2 db = mul2(B, hh);
+                    const T2 dv = add2(irn, two(-iro.x, -iro.y));
+                    vals[0] = sr.x + sr.y;
+                    vals[1] = T(2) * (dl.x + dl.y);
+                    vals[2] = db.x + db.y;
+                    vals[3] = dv.x + dv.y;
+                    vals[4] = tnx.x + tnx.y;
+                    vals[5] = tny.x + tny.y;
+                    vals[6] = kp;  // the previous step's kinetic terms
+                    vals[7] = T(0);
+                }
+                // one reduce-scatter: lane L ends with the total of value L / 4
+                const T tot = warp_reduce_scatter8<T, 32>(vals, l);
+                const T sum_ratio = __shfl_sync(FULL, tot, 0);
+                if (pend) sample(__shfl_sync(FULL, tot, 24));  // E_L of the previous step
+                pend = false;
+
+                // ---- 2c/2d. ratio, Green's ratio, accept
+                const T rat_g = Fs::exp(wa * (xo * xo - xn * xn));
+                const T rat_p = Fs::exp(T(2) * sum_ratio);
+                bool accept;
+                if constexpr (GREEN_Q) {
+                    // importancesampling.cpp:43-47: exp(0.5 (F_old(k) - F_new(k)) dx) + 1
+                    const T ex = Fs::exp(T(0.5) * (fcs[k] - Fn) * dx);
+                    if constexpr (F32) {
+                        const float wgt = (ex + 1.0f) * (R * R * rat_g * rat_p);
+                        if (wgt != wgt) status |= ST_BAD_RATIO;
+                        accept = wgt >= __uint2float_rn(ur) * 2.3283064365386963e-10f;
+                    } else {
+                        const double wgt = ((double)ex + 1.0) * ((double)(R * R) * (double)rat_g * (double)rat_p);
+                        if (wgt != wgt) status |= ST_BAD_RATIO;
+                        accept = wgt >= ur * TWO_M32;
+                    }
+                } else {
+                    // Fokker-Planck Green's ratio with the drift at the proposed point
+                    const T gsl = __shfl_sync(FULL, sig_l * gl_, pl) * sq2;
+                    const T gy = -wa * xn + __shfl_sync(FULL, tot, 16 + 4 * adim) + gsl / R;
+                    const double prob = (double)(R * R) * (double)rat_g * (double)rat_p;
+                    const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
+                    const double wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
+                    if (wgt != wgt) status |= ST_BAD_RATIO;
+                    accept = wgt >= ur * TWO_M32;
+                }
+
+                if (accept) {
+                    // ---- 3. state update
+                    const bool mine = l == pl;
+                    if (adim == 0) {
+                        if (mine) X[0] = b ? two(X[0].x, xn) : two(xn, X[0].y);
+                    } else {
+                        if (mine) X[1] = b ? two(X[1].x, xn) : two(xn, X[1].y);
+                    }
+                    if (l == 0) {
+                        xs[k] = xn;
+                        fcs[k] = Fn;
+                    }
+                    // running sums (the pair totals sit in lanes 4, 8, 12; the new
+                    // gradient of the moved particle in lanes 16, 20)
+                    const T tl = __shfl_sync(FULL, tot, 4), tb = __shfl_sync(FULL, tot, 8);
+                    const T tv = __shfl_sync(FULL, tot, 12);
+                    const T tgx = __shfl_sync(FULL, tot, 16), tgy = __shfl_sync(FULL, tot, 20);
+                    if constexpr (F32) {
+                        dlap += tl;
+                        dbh2 += tb;
+                        dvint += tv;
+                        dsx2 += (xn - xo) * (xn + xo);
+                    } else {
+                        sumx2 += (double)xn * (double)xn - (double)xo * (double)xo;
+                        lapj += (double)tl;
+                        bh2 += (double)tb;
+                        vint += (double)tv;
+                    }
+                    // Pade gradients: partners by their change, the moved particle anew
+                    GJ[0] = add2(GJ[0], gdx);
+                    GJ[1] = add2(GJ[1], gdy);
+                    if (mine) {
+                        GJ[0] = b ? two(GJ[0].x, tgx) : two(tgx, GJ[0].y);
+                        GJ[1] = b ? two(GJ[1].x, tgy) : two(tgy, GJ[1].y);
+                    }
+                    if constexpr (STALE) {
+                        if (!allcur) {
+                            if (own && l != p) msk[l] |= 1ull << p;
+                            if (own && n + l != p) msk[n + l] |= 1ull << p;
+                            if (mine) msk[p] = ~0ull;
+                        }
+                    }
+                    // Sherman-Morrison on block b (slaterdeterminant.cpp:165-175) through the
+                    // row scales: row l += t_l row p with t_l = -s_l sigma_p / R (staged
+                    // rows), sigma_p /= R; then the block's derivative vectors
+                    // (slaterdeterminant.cpp:155-163) from the updated rows
+                    const T sig_p = __shfl_sync(FULL, sig_l, pl);
+                    const T rinv = Fs::rcp(R);
+                    const T tcoef = (own && !mine) ? -(sl * sig_p * rinv) : T(0);
+                    const T sig_new = mine ? sig_l * rinv : sig_l;
+                    if (b) SIG.y = sig_new;
+                    else SIG.x = sig_new;
+                    const T ux = sq2 * (b ? X[0].y : X[0].x), uy = sq2 * (b ? X[1].y : X[1].x);
+                    T au[K], av[K];
+                    hermite_pe<K>(ux, au);
+                    hermite_pe<K>(uy, av);
+                    T *rowj = inv + (b * n + lc) * IS;
+                    const T *rowp = inv + (b * n + pl) * IS;
+                    T P0[K], P1[K];  // P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
+#pragma unroll
+                    for (int m = 0; m < K; ++m) P0[m] = P1[m] = T(0);
+                    const bool store = own && !mine;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) {
+                        T cv[VE], vv[VE];
+                        vload<T>(rowp + q * VE, cv);
+                        vload<T>(rowj + q * VE, vv);
+#pragma unroll
+                        for (int e = 0; e < VE; e += 2) {
+                            const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
+                            vv[e] = nv.x;
+                            vv[e + 1] = nv.y;
+                        }
+                        if (store) vstore<T>(rowj + q * VE, vv);
+#pragma unroll
+                        for (int e = 0; e < VE; ++e) {
+                            const int i = q * VE + e;
+                            if (i < n) {
+                                P0[PO.m0[i]] = fmaT(av[PO.m1[i]], vv[e], P0[PO.m0[i]]);
+                                P1[PO.m1[i]] = fmaT(au[PO.m0[i]], vv[e], P1[PO.m1[i]]);
+                            }
+                        }
+                    }
+                    if (own) {
+                        T gx = T(0), gy2 = T(0), sx = T(0), sy = T(0);
+#pragma unroll
+                        for (int m = 1; m < K; ++m) {
+                            gx = fmaT(au[m - 1], P0[m], gx);
+                            gy2 = fmaT(av[m - 1], P1[m], gy2);
+                        }
+#pragma unroll
+                        for (int m = 2; m < K; ++m) {
+                            sx = fmaT(au[m - 2], P0[m], sx);
+                            sy = fmaT(av[m - 2], P1[m], sy);
+                        }
+                        const T g1 = sig_new * sq2, g2s = sig_new * T(2);
+                        if (b) {
+                            DD[0].y = g1 * gx;
+                            DD[1].y = g1 * gy2;
+                            SD[0].y = g2s * sx;
+                            SD[1].y = g2s * sy;
+                        } else {
+                            DD[0].x = g1 * gx;
+                            DD[1].x = g1 * gy2;
+                            SD[0].x = g2s * sx;
+                            SD[1].x = g2s * sy;
+                        }
+                    }
+                    kp = publish();
+                    __syncwarp();
+                }
+                // ---- 4. this step's sample, taken with the next step's reduce-scatter
+                if (it_step >= a.burn_in) {
+                    pend = true;
+                    pend_acc = accept;
+                    pend_win = it_step > a.win_lo && it_step < a.win_hi;
+                }
+            }
+            if constexpr (F32) {
+                if (pend) {  // the block's last step: its kinetic sum by a reduction of its own
+                    sample(seg_sum<32>(kp));
+                    pend = false;
+                }
+                fold();
+            }
+        }
+        if (pend) sample(seg_sum<32>(kp));
+
+        // ---- write the walker back
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (own) {
+                T *dst = rec + L.off_inv + (size_t)(h * n + l) * L.inv_stride;
+                const T *src = inv + (h * n + l) * IS;
+                const T sg = h ? SIG.y : SIG.x;
+                T v[IS];
+#pragma unroll
+                for (int q = 0; q < IS / VE; ++q) vload<T>(src + q * VE, v + q * VE);
+#pragma unroll
+                for (int i = 0; i < n; ++i) dst[PO.orb[i]] = v[i] * (sg * T(1.0 / PO.scale[i]));
+            }
+        }
+        if (own) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int ka = 2 * l + c, kb = 2 * (n + l) + c;
+                rec[L.off_x + ka] = X[c].x;
+                rec[L.off_x + kb] = X[c].y;
+                rec[L.off_dd + ka] = DD[c].x;
+                rec[L.off_dd + kb] = DD[c].y;
+                rec[L.off_sdd + ka] = SD[c].x;
+                rec[L.off_sdd + kb] = SD[c].y;
+                rec[L.off_gj + ka] = GJ[c].x;
+                rec[L.off_gj + kb] = GJ[c].y;
+            }
+        }
+        for (int i = l; i < D; i += 32) rec[L.off_fc + i] = fcs[i];
+        if (mdirty)
+            for (int j = l; j < N; j += 32) P.mask[(size_t)w * N + j] = msk[j];
+        if (l == 0) {
+            double *so = P.scal + (size_t)w * NSCAL;
+            so[SC_SUMX2] = sumx2;
+            so[SC_LAPJ] = lapj;
+            so[SC_BH2] = bh2;
+            so[SC_VINT] = vint;
+            P.counter[w] = ctr;
+        }
+        if (l < P.nacc) {
+            P.acc[((size_t)w * P.nacc + l) * 2] = acc_s;
+            P.acc[((size_t)w * P.nacc + l) * 2 + 1] = acc_c;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) status |= __shfl_xor_sync(FULL, status, o);
+        if (l == 0 && status) P.status[w] |= status;
+        __syncwarp();
+    }
+}
+
+}  // namespace vmc

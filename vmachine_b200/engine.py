@@ -31,9 +31,11 @@ class Info(ctypes.Structure):
         "n_particles", "n_dimensions", "n_coords", "n_elements", "p_max", "n_walkers",
         "precision", "sampling", "steps_per_walker", "burn_in", "batches", "n_iterations",
         "compat", "n_accumulators", "walkers_per_block", "refresh_interval")] + [
-        ("element_kind", ctypes.c_int * 8), ("kernel_variant", ctypes.c_int), ("walkers_per_warp", ctypes.c_int)]
+        ("element_kind", ctypes.c_int * 8), ("kernel_variant", ctypes.c_int), ("walkers_per_warp", ctypes.c_int),
+        ("sweep_form", ctypes.c_int)]
 
 KERNEL_RUNTIME_FLAGS, KERNEL_DOT, KERNEL_GENERAL = 0, 1, 2
+SWEEP_STAGED, SWEEP_OWNER = 1, 2
 
 
 class Sums(ctypes.Structure):
