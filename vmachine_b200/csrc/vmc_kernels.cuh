@@ -108,8 +108,28 @@ struct Params {
     int mlp_cache_stride;
 };
 
+// Per-launch constants of the owner sweep, computed by the host in FP64 and passed in
+// both precisions, so the kernel reads them as constant operands
+enum : int {
+    OC_WA = 0,    // omega alpha
+    OC_HDT,       // dt / 2
+    OC_SDT,       // sqrt(dt)
+    OC_GAM,       // Pade gamma
+    OC_GAMP,      // the previous gamma (stale pairs)
+    OC_M2GAM,     // -2 gamma
+    OC_BSAME,     // Pade beta, equal spins
+    OC_BANTI,     // Pade beta, opposite spins
+    OC_W2H,       // omega^2 / 2
+    OC_MHOM,      // -omega / 2
+    OC_DGK,       // dlnPsi/dgamma per sum beta h^2 (-1, or -1/2 under the reference quirk)
+    OC_LAPC,      // omega alpha D, the Gaussian's -Laplacian
+    OC_N = 16
+};
+
 struct SweepArgs {
     Params P;
+    double oc[OC_N];  // owner sweep constants (OC_*)
+    float ocf[OC_N];  // the same in FP32
     int steps, step_offset, burn_in, win_lo, win_hi;
     unsigned long long seed;
     const double *replay;  // W x replay_stride x 3 or null

@@ -56,6 +56,7 @@ namespace vmc {
 struct PairTable {
     int m0[32], m1[32], orb[32];
     double scale[32];
+    int np;  // transposed pairs (slots 0 .. 2 np - 1)
 };
 
 __host__ __device__ constexpr double owner_factorial(int m) { return m <= 1 ? 1.0 : m * owner_factorial(m - 1); }
@@ -79,6 +80,7 @@ template <int K> __host__ __device__ constexpr PairTable make_pair_table()
             t.m1[i + 1] = a;
             i += 2;
         }
+    t.np = i / 2;
     for (int d = 0; 2 * d < K; ++d) {
         t.m0[i] = d;
         t.m1[i] = d;
@@ -106,18 +108,58 @@ __device__ __forceinline__ void hermite_pe(T u, T (&h)[K])
     for (int m = 1; m + 1 < K; ++m) h[m + 1] = (u * h[m] - h[m - 1]) * T(1.0 / (m + 1));
 }
 
+// hh_0..hh_{K-1} at both coordinates of U: H[m] = (hh_m(U.x), hh_m(U.y))
+template <int K, typename T>
+__device__ __forceinline__ void hermite_pe2(Two<T> U, Two<T> (&H)[K])
+{
+    H[0] = two(T(1), T(1));
+    if (K > 1) H[1] = U;
+#pragma unroll
+    for (int m = 1; m + 1 < K; ++m) {
+        const T c = T(1.0 / (m + 1));
+        H[m + 1] = mul2(fma2(U, H[m], two(-H[m - 1].x, -H[m - 1].y)), two(c, c));
+    }
+}
+
+template <typename T> __device__ __forceinline__ T oconst(const SweepArgs &a, int i);
+template <> __device__ __forceinline__ float oconst<float>(const SweepArgs &a, int i) { return a.ocf[i]; }
+template <> __device__ __forceinline__ double oconst<double>(const SweepArgs &a, int i) { return a.oc[i]; }
+
+#ifndef OWNER_PACK_DOT
+#define OWNER_PACK_DOT 1
+#endif
+#ifndef OWNER_PACK_ACC
+#define OWNER_PACK_ACC 1
+#endif
+#ifndef OWNER_SHM64
+#define OWNER_SHM64 1
+#endif
+#ifndef OWNER_UNIFORM_ACC
+#define OWNER_UNIFORM_ACC 1
+#endif
+
 constexpr int OWNER_WPB = 4;  // walkers (warps) per CTA
+// CTAs per SM the FP32 form is compiled for (its register budget: 65536 / (128 x this))
+#ifndef OWNER_MIN_CTAS_F32
+#define OWNER_MIN_CTAS_F32 4
+#endif
+
+// FP64 values of the FP32 form that only the 32-step folds touch, kept in shared memory:
+// the lanes' accumulators (sums, compensations), the walker's running sums and energies
+// at the start of the launch
+constexpr int OWNER_FOLD_DOUBLES = 72;
+enum : int { OF_ACCS = 0, OF_ACCC = 32, OF_LAPJ = 64, OF_BH2, OF_VINT, OF_SUMX2, OF_T0, OF_V0, OF_I0, OF_E0 };
 
 // Shared bytes per warp: the inverse blocks, then per coordinate the positions, drift
-// gradients and force cache, then the Pade pair masks.
+// gradients and force cache, then the Pade pair masks and the fold values.
 __host__ __device__ constexpr int owner_smem_per_warp(int K, int elem_bytes)
 {
     const int n = K * (K + 1) / 2, D = 4 * n;
-    return (2 * n * inv_row_stride(n, elem_bytes) + 3 * D) * elem_bytes + 2 * n * 8;
+    return (2 * n * inv_row_stride(n, elem_bytes) + 3 * D) * elem_bytes + 2 * n * 8 + OWNER_FOLD_DOUBLES * 8;
 }
 
 template <typename T, int K, int FX>
-__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_sweep_kernel(const SweepArgs a)
+__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTAS_F32 : 3) owner_sweep_kernel(const SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr PairTable PO = make_pair_table<K>();
@@ -144,17 +186,16 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
     T *inv = reinterpret_cast<T *>(ws);
     T *xs = inv + 2 * n * IS, *gs = xs + D, *fcs = gs + D;
     unsigned long long *msk = reinterpret_cast<unsigned long long *>(fcs + D);
+    double *fd = reinterpret_cast<double *>(msk + N);  // fold values (OF_*)
 
-    const T wa = T(P.omega * P.alpha);
-    const T hdt = T(0.5 * P.step), sdt = T(sqrt(P.step));
-    const T gam = T(P.gamma), gamp = T(P.gamma_prev);
-    const T2 gam2 = two(gam, gam), m2gam = two(T(-2) * gam, T(-2) * gam), one2 = two(T(1), T(1));
-    const T2 mwa2 = two(-wa, -wa);
-    const T bsame = T(P.beta_same), banti = T(P.beta_anti);
+    constexpr bool SHM = F32 && OWNER_SHM64;
+    const T wa = oconst<T>(a, OC_WA), hdt = oconst<T>(a, OC_HDT), sdt = oconst<T>(a, OC_SDT);
+    const T gam = oconst<T>(a, OC_GAM), gamp = oconst<T>(a, OC_GAMP);
+    const T bsame = oconst<T>(a, OC_BSAME), banti = oconst<T>(a, OC_BANTI);
+    const T2 gam2 = two(gam, gam), m2gam = two(oconst<T>(a, OC_M2GAM), oconst<T>(a, OC_M2GAM));
+    const T2 one2 = two(T(1), T(1)), mwa2 = two(-wa, -wa);
     const T sq2 = T(1.4142135623730951);
-    const double dgk = (FX & Q_PADE_DGAMMA) ? -0.5 : -1.0;  // dlnPsi/dgamma = dgk sum beta h^2
-    const double lapc = P.omega * P.alpha * D;              // the Gaussian's -Laplacian
-    const double w2h = 0.5 * P.omega * P.omega;
+    const double dgk = a.oc[OC_DGK], lapc = a.oc[OC_LAPC], w2h = a.oc[OC_W2H];
     // accumulator slot of this lane: 0..7 energy moments, 8 accepts, then the parameter
     // gradients (1 alpha, 2 gamma) and the same times E_L
     int pk = 0;
@@ -246,28 +287,85 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
         T dlap = T(0), dbh2 = T(0), dvint = T(0), dsx2 = T(0);    // FP32 changes since the fold
         T accf = T(0);
         int ns = 0;
+        // FP32 form, uniform partial sums over the steps since the fold (every lane the
+        // same): (T, V_ext), (V_int, accepts), their squares (T, V_ext), (V_int, E), the
+        // windowed parameter gradients (alpha, gamma) and the same times E
+        T2 u_tv = two(T(0), T(0)), u_ia = u_tv, u_tv2 = u_tv, u_ie2 = u_tv, u_g = u_tv, u_eg = u_tv;
+        if constexpr (SHM) {
+            if (l == 0) {
+                fd[OF_LAPJ] = lapj;
+                fd[OF_BH2] = bh2;
+                fd[OF_VINT] = vint;
+                fd[OF_SUMX2] = sumx2;
+                fd[OF_T0] = T0;
+                fd[OF_V0] = V0;
+                fd[OF_I0] = I0;
+                fd[OF_E0] = E0;
+            }
+            fd[OF_ACCS + l] = acc_s;
+            fd[OF_ACCC + l] = acc_c;
+            __syncwarp();
+        }
         auto fp32_bases = [&]() {
-            cT = T(-0.5 * lapj + 0.5 * lapc - T0);
-            cV = T(w2h * sumx2 - V0);
-            cI = T(vint - I0);
-            gA = T(-0.5 * P.omega * sumx2);
-            gG = T(dgk * bh2);
+            if constexpr (SHM) {
+                cT = T(-0.5 * fd[OF_LAPJ] + 0.5 * lapc - fd[OF_T0]);
+                cV = T(w2h * fd[OF_SUMX2] - fd[OF_V0]);
+                cI = T(fd[OF_VINT] - fd[OF_I0]);
+                gA = T(a.oc[OC_MHOM] * fd[OF_SUMX2]);
+                gG = T(dgk * fd[OF_BH2]);
+            } else {
+                cT = T(-0.5 * lapj + 0.5 * lapc - T0);
+                cV = T(w2h * sumx2 - V0);
+                cI = T(vint - I0);
+                gA = T(a.oc[OC_MHOM] * sumx2);
+                gG = T(dgk * bh2);
+            }
         };
         auto fold = [&]() {
             if constexpr (F32) {
-                const T part = __shfl_xor_sync(FULL, accf, 1);  // odd energy slots: the linear sum
-                const T gsum = __shfl_sync(FULL, accf, te ? l - P.ep : l);
+                T part, gsum;
+                if constexpr (OWNER_UNIFORM_ACC) {
+                    // this lane's slot from the uniform partials
+                    const T lin = eg == 0 ? u_tv.x + u_tv.y + u_ia.x : eg == 1 ? u_tv.x : eg == 2 ? u_tv.y : u_ia.x;
+                    const T sq = eg == 0 ? u_ie2.y : eg == 1 ? u_tv2.x : eg == 2 ? u_tv2.y : u_ie2.x;
+                    gsum = pk == 1 ? u_g.x : pk == 2 ? u_g.y : T(0);
+                    const T eg_ = pk == 1 ? u_eg.x : pk == 2 ? u_eg.y : T(0);
+                    part = lin;
+                    accf = l < 8 ? ((l & 1) ? sq : lin) : l == 8 ? u_ia.y : te ? eg_ : gsum;
+                    u_tv = u_ia = u_tv2 = u_ie2 = u_g = u_eg = two(T(0), T(0));
+                } else {
+                    part = __shfl_xor_sync(FULL, accf, 1);  // odd energy slots: the linear sum
+                    gsum = __shfl_sync(FULL, accf, te ? l - P.ep : l);
+                }
+                const double ref = SHM ? fd[l < 8 ? (eg == 0 ? OF_E0 : OF_T0 + eg - 1) : OF_E0] : myref;
                 double v = (double)accf;
-                if (l < 8) v += (l & 1) ? ns * myref * myref + 2.0 * myref * (double)part : ns * myref;
-                else if (te) v += myref * (double)gsum;
-                kadd(acc_s, acc_c, v);
+                if (l < 8) v += (l & 1) ? ns * ref * ref + 2.0 * ref * (double)part : ns * ref;
+                else if (te) v += ref * (double)gsum;
                 accf = T(0);
                 ns = 0;
                 // the FP32 running-sum changes into the FP64 sums
-                lapj += (double)dlap;
-                bh2 += (double)dbh2;
-                vint += (double)dvint;
-                sumx2 += (double)dsx2;
+                if constexpr (SHM) {
+                    double s_ = fd[OF_ACCS + l], c_ = fd[OF_ACCC + l];
+                    kadd(s_, c_, v);
+                    fd[OF_ACCS + l] = s_;
+                    fd[OF_ACCC + l] = c_;
+                    const double nl = fd[OF_LAPJ] + (double)dlap, nb = fd[OF_BH2] + (double)dbh2;
+                    const double nv = fd[OF_VINT] + (double)dvint, nx = fd[OF_SUMX2] + (double)dsx2;
+                    __syncwarp();
+                    if (l == 0) {
+                        fd[OF_LAPJ] = nl;
+                        fd[OF_BH2] = nb;
+                        fd[OF_VINT] = nv;
+                        fd[OF_SUMX2] = nx;
+                    }
+                    __syncwarp();
+                } else {
+                    kadd(acc_s, acc_c, v);
+                    lapj += (double)dlap;
+                    bh2 += (double)dbh2;
+                    vint += (double)dvint;
+                    sumx2 += (double)dsx2;
+                }
                 dlap = dbh2 = dvint = dsx2 = T(0);
                 fp32_bases();
             }
@@ -283,12 +381,28 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
         auto sample = [&](T ks) {
             if constexpr (F32) {
                 const T Ts = fmaT(T(-0.5), ks + dlap, cT);
-                const T Vs = fmaT(T(w2h), dsx2, cV);
+                const T Vs = fmaT(oconst<T>(a, OC_W2H), dsx2, cV);
                 const T Is = cI + dvint;
                 const T Es = Ts + Vs + Is;
                 if (Es != Es) status |= ST_NAN_ENERGY;
+                if constexpr (OWNER_UNIFORM_ACC) {
+                    const T ga = fmaT(oconst<T>(a, OC_MHOM), dsx2, gA), gg = fmaT(oconst<T>(a, OC_DGK), dbh2, gG);
+                    const T wf = pend_win ? T(1) : T(0);
+                    const T2 tv = two(Ts, Vs), ie = two(Is, Es);
+                    u_tv = add2(u_tv, tv);
+                    u_ia = add2(u_ia, two(Is, pend_acc ? T(1) : T(0)));
+                    u_tv2 = fma2(tv, tv, u_tv2);
+                    u_ie2 = fma2(ie, ie, u_ie2);
+                    const T2 G = mul2(two(ga, gg), two(wf, wf));
+                    u_g = add2(u_g, G);
+                    u_eg = fma2(two(Es, Es), G, u_eg);
+                    ++ns;
+                    return;
+                }
                 const T eb = eg == 0 ? Es : eg == 1 ? Ts : eg == 2 ? Vs : Is;
-                const T gl = pk == 1 ? fmaT(T(-0.5 * P.omega), dsx2, gA) : pk == 2 ? fmaT(T(dgk), dbh2, gG) : T(0);
+                const T gl = pk == 1   ? fmaT(oconst<T>(a, OC_MHOM), dsx2, gA)
+                             : pk == 2 ? fmaT(oconst<T>(a, OC_DGK), dbh2, gG)
+                                       : T(0);
                 const T gq = pend_win ? (te ? Es * gl : gl) : T(0);
                 accf += l < 8 ? ((l & 1) ? eb * eb : eb) : l == 8 ? (pend_acc ? T(1) : T(0)) : gq;
                 ++ns;
@@ -298,7 +412,7 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                 if (el != el) status |= ST_NAN_ENERGY;
                 const double base = eg == 0 ? el : eg == 1 ? ekin : eg == 2 ? vext : vint;
                 const double qe = (l & 1) ? base * base : base;
-                const double g = pk == 1 ? -0.5 * P.omega * sumx2 : pk == 2 ? dgk * bh2 : 0.0;
+                const double g = pk == 1 ? a.oc[OC_MHOM] * sumx2 : pk == 2 ? dgk * bh2 : 0.0;
                 const double qp = pend_win ? (te ? g * el : g) : 0.0;
                 kadd(acc_s, acc_c, l < 8 ? qe : l == 8 ? (pend_acc ? 1.0 : 0.0) : qp);
             }
@@ -350,11 +464,45 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                 const T qx = adim ? xp.x : xn, qy = adim ? xn : xp.y;  // proposed position of p
 
                 // ---- 2a. Slater: s_l = phi(r_p') . staged row l of block b (lane l), R = sigma_p s_pl
+                T sl, gl_ = T(0);
+                if constexpr (GREEN_Q && OWNER_PACK_DOT) {
+                    // packed: Qd[a] = (sum_b hh_b(y) v(a,b), sum_b hh_b(x) v(b,a)) over the
+                    // transposed pairs, s = sum_a (hh_a(x), hh_a(y)) . Qd[a] + the diagonals
+                    T2 H[K];
+                    hermite_pe2<K, T>(two(sq2 * qx, sq2 * qy), H);
+                    const T *row = inv + (b * n + lc) * IS;
+                    T2 Qd[K];
+#pragma unroll
+                    for (int m = 0; m < K; ++m) Qd[m] = two(T(0), T(0));
+                    T dsum = T(0);
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) {
+                        T v[VE];
+                        vload<T>(row + q * VE, v);
+#pragma unroll
+                        for (int e = 0; e < VE; e += 2) {
+                            const int i = q * VE + e;
+                            if (i < 2 * PO.np) {
+                                const int pa = PO.m0[i], pb = PO.m1[i];
+                                Qd[pa] = fma2(two(H[pb].y, H[pb].x), two(v[e], v[e + 1]), Qd[pa]);
+                            } else {
+#pragma unroll
+                                for (int t = 0; t < 2; ++t)
+                                    if (i + t < n) {
+                                        const int d = PO.m0[i + t];
+                                        dsum = fmaT(H[d].x * H[d].y, v[e + t], dsum);
+                                    }
+                            }
+                        }
+                    }
+                    T2 s2 = two(T(0), T(0));
+#pragma unroll
+                    for (int m = 0; 2 * m + 2 <= K; ++m) s2 = fma2(H[m], Qd[m], s2);
+                    sl = s2.x + s2.y + dsum;
+                } else {
                 T hu[K], hv[K];
                 hermite_pe<K>(sq2 * qx, hu);
                 hermite_pe<K>(sq2 * qy, hv);
-                T sl, gl_ = T(0);
-                {
                     const T *row = inv + (b * n + lc) * IS;
                     T part[K];
 #pragma unroll
@@ -409,7 +557,7 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                 {
                     const T2 pxo = two(-xp.x, -xp.x), pyo = two(-xp.y, -xp.y);
                     const T2 pxn = two(-qx, -qx), pyn = two(-qy, -qy);
-                    const T2 dxo = add2(X[0], pxo), dyo = add2(X[1], pyo);
+                    const T2 dxo = add2(X[0], pxo), dyo = add2(X[1], pyo);  // partner minus moved
                     const T2 dxn = add2(X[0], pxn), dyn = add2(X[1], pyn);
                     const T2 r2o = fma2(dyo, dyo, mul2(dxo, dxo)), r2n = fma2(dyn, dyn, mul2(dxn, dxn));
                     // partners: particle l (block 0) and n + l (block 1), not the moved one
@@ -434,9 +582,11 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                     T2 dh = add2(hn, two(-ho.x, -ho.y));
                     if constexpr (RATIO_Q) dh = two(l > p ? dh.x : T(0), n + l > p ? dh.y : T(0));
                     const T2 sr = mul2(B, dh);
+                    // d J / d x_j = beta f1^2 (x_j - x_p) / r for the partner j, the negative
+                    // for the moved particle: the partners' change is new minus old
                     const T2 tnx = mul2(fin, dxn), tny = mul2(fin, dyn);
-                    gdx = fma2(fio, dxo, two(-tnx.x, -tnx.y));
-                    gdy = fma2(fio, dyo, two(-tny.x, -tny.y));
+                    gdx = fma2(fio, two(-dxo.x, -dxo.y), tnx);
+                    gdy = fma2(fio, two(-dyo.x, -dyo.y), tny);
                     // 2 f (DIM - (1 + 2 gamma h)) / r, new minus old (DIM = 2)
                     const T2 lqo = mul2(fio, fma2(m2gam, ho, one2)), lqn = mul2(fin, fma2(m2gam, hn, one2));
                     const T2 dl = add2(lqn, two(-lqo.x, -lqo.y));
@@ -447,8 +597,8 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                     vals[1] = T(2) * (dl.x + dl.y);
                     vals[2] = db.x + db.y;
                     vals[3] = dv.x + dv.y;
-                    vals[4] = tnx.x + tnx.y;
-                    vals[5] = tny.x + tny.y;
+                    vals[4] = -(tnx.x + tnx.y);
+                    vals[5] = -(tny.x + tny.y);
                     vals[6] = kp;  // the previous step's kinetic terms
                     vals[7] = T(0);
                 }
@@ -538,38 +688,98 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                     if (b) SIG.y = sig_new;
                     else SIG.x = sig_new;
                     const T ux = sq2 * (b ? X[0].y : X[0].x), uy = sq2 * (b ? X[1].y : X[1].x);
-                    T au[K], av[K];
-                    hermite_pe<K>(ux, au);
-                    hermite_pe<K>(uy, av);
                     T *rowj = inv + (b * n + lc) * IS;
                     const T *rowp = inv + (b * n + pl) * IS;
-                    T P0[K], P1[K];  // P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
-#pragma unroll
-                    for (int m = 0; m < K; ++m) P0[m] = P1[m] = T(0);
                     const bool store = own && !mine;
+                    T gx, gy2, sx, sy;
+                    if constexpr (OWNER_PACK_ACC) {
+                        // packed: with Hj[m] = (hh_m(x), hh_m(y)) of the lane's particle and a
+                        // staged pair S = (v(a,b), v(b,a)):
+                        //   Q[a] = (P0[a], P1[a]) += (hh_b(y), hh_b(x)) . S
+                        //   R[b] = (P1[b], P0[b]) += (hh_a(x), hh_a(y)) . S
+                        // where P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
+                        constexpr int QN = (K + 1) / 2;  // first indices of the pairs and diagonals
+                        T2 Hj[K];
+                        hermite_pe2<K, T>(two(ux, uy), Hj);
+                        T2 Q[QN], Rb[K];
 #pragma unroll
-                    for (int q = 0; q < NQ; ++q) {
-                        T cv[VE], vv[VE];
-                        vload<T>(rowp + q * VE, cv);
-                        vload<T>(rowj + q * VE, vv);
+                        for (int m = 0; m < QN; ++m) Q[m] = two(T(0), T(0));
 #pragma unroll
-                        for (int e = 0; e < VE; e += 2) {
-                            const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
-                            vv[e] = nv.x;
-                            vv[e + 1] = nv.y;
-                        }
-                        if (store) vstore<T>(rowj + q * VE, vv);
+                        for (int m = 0; m < K; ++m) Rb[m] = two(T(0), T(0));
 #pragma unroll
-                        for (int e = 0; e < VE; ++e) {
-                            const int i = q * VE + e;
-                            if (i < n) {
-                                P0[PO.m0[i]] = fmaT(av[PO.m1[i]], vv[e], P0[PO.m0[i]]);
-                                P1[PO.m1[i]] = fmaT(au[PO.m0[i]], vv[e], P1[PO.m1[i]]);
+                        for (int q = 0; q < NQ; ++q) {
+                            T cv[VE], vv[VE];
+                            vload<T>(rowp + q * VE, cv);
+                            vload<T>(rowj + q * VE, vv);
+#pragma unroll
+                            for (int e = 0; e < VE; e += 2) {
+                                const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
+                                vv[e] = nv.x;
+                                vv[e + 1] = nv.y;
+                            }
+                            if (store) vstore<T>(rowj + q * VE, vv);
+#pragma unroll
+                            for (int e = 0; e < VE; e += 2) {
+                                const int i = q * VE + e;
+                                if (i < 2 * PO.np) {
+                                    const int pa = PO.m0[i], pb = PO.m1[i];
+                                    const T2 S = two(vv[e], vv[e + 1]);
+                                    Q[pa] = fma2(two(Hj[pb].y, Hj[pb].x), S, Q[pa]);
+                                    Rb[pb] = fma2(Hj[pa], S, Rb[pb]);
+                                } else {
+#pragma unroll
+                                    for (int t = 0; t < 2; ++t)
+                                        if (i + t < n) {
+                                            const int d = PO.m0[i + t];
+                                            Q[d] = fma2(two(Hj[d].y, Hj[d].x), two(vv[e + t], vv[e + t]), Q[d]);
+                                        }
+                                }
                             }
                         }
-                    }
-                    if (own) {
-                        T gx = T(0), gy2 = T(0), sx = T(0), sy = T(0);
+                        // d/dx: sum_m hh_{m-1}(x) P0[m], d/dy: sum_m hh_{m-1}(y) P1[m]; the second
+                        // derivatives with hh_{m-2}
+                        T2 G1 = two(T(0), T(0)), G2 = G1, S1 = G1, S2 = G1;
+#pragma unroll
+                        for (int m = 1; m < QN; ++m) G1 = fma2(Hj[m - 1], Q[m], G1);
+#pragma unroll
+                        for (int m = 1; m < K; ++m) G2 = fma2(two(Hj[m - 1].y, Hj[m - 1].x), Rb[m], G2);
+#pragma unroll
+                        for (int m = 2; m < QN; ++m) S1 = fma2(Hj[m - 2], Q[m], S1);
+#pragma unroll
+                        for (int m = 2; m < K; ++m) S2 = fma2(two(Hj[m - 2].y, Hj[m - 2].x), Rb[m], S2);
+                        gx = G1.x + G2.y;
+                        gy2 = G1.y + G2.x;
+                        sx = S1.x + S2.y;
+                        sy = S1.y + S2.x;
+                    } else {
+                        T au[K], av[K];
+                        hermite_pe<K>(ux, au);
+                        hermite_pe<K>(uy, av);
+                        T P0[K], P1[K];  // P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
+#pragma unroll
+                        for (int m = 0; m < K; ++m) P0[m] = P1[m] = T(0);
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            T cv[VE], vv[VE];
+                            vload<T>(rowp + q * VE, cv);
+                            vload<T>(rowj + q * VE, vv);
+#pragma unroll
+                            for (int e = 0; e < VE; e += 2) {
+                                const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
+                                vv[e] = nv.x;
+                                vv[e + 1] = nv.y;
+                            }
+                            if (store) vstore<T>(rowj + q * VE, vv);
+#pragma unroll
+                            for (int e = 0; e < VE; ++e) {
+                                const int i = q * VE + e;
+                                if (i < n) {
+                                    P0[PO.m0[i]] = fmaT(av[PO.m1[i]], vv[e], P0[PO.m0[i]]);
+                                    P1[PO.m1[i]] = fmaT(au[PO.m0[i]], vv[e], P1[PO.m1[i]]);
+                                }
+                            }
+                        }
+                        gx = gy2 = sx = sy = T(0);
 #pragma unroll
                         for (int m = 1; m < K; ++m) {
                             gx = fmaT(au[m - 1], P0[m], gx);
@@ -580,7 +790,10 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
                             sx = fmaT(au[m - 2], P0[m], sx);
                             sy = fmaT(av[m - 2], P1[m], sy);
                         }
-                        const T g1 = sig_new * sq2, g2s = sig_new * T(2);
+                    }
+                    {
+                        // lanes without particles keep zeros
+                        const T g1 = own ? sig_new * sq2 : T(0), g2s = own ? sig_new * T(2) : T(0);
                         if (b) {
                             DD[0].y = g1 * gx;
                             DD[1].y = g1 * gy2;
@@ -645,6 +858,14 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? 4 : 3) owner_
         for (int i = l; i < D; i += 32) rec[L.off_fc + i] = fcs[i];
         if (mdirty)
             for (int j = l; j < N; j += 32) P.mask[(size_t)w * N + j] = msk[j];
+        if constexpr (SHM) {
+            sumx2 = fd[OF_SUMX2];
+            lapj = fd[OF_LAPJ];
+            bh2 = fd[OF_BH2];
+            vint = fd[OF_VINT];
+            acc_s = fd[OF_ACCS + l];
+            acc_c = fd[OF_ACCC + l];
+        }
         if (l == 0) {
             double *so = P.scal + (size_t)w * NSCAL;
             so[SC_SUMX2] = sumx2;
