@@ -3,7 +3,8 @@
 A walker of a small dot fills few of a warp's 32 lanes (one per orbital row, partner
 or coordinate group), so the production sweep gives each walker an 8-lane quarter
 (N <= 6) or a 16-lane half (N = 12 to 30) of the warp; N = 42 and 56 keep one walker
-per warp by default and take two on request (`walkersPerWarp: 2`, rows of the 21 x 21
+per warp by default (the owner form, test_owner_sweep_gpu.py) and take two on request
+in the staged form (`walkersPerWarp: 2`, rows of the 21 x 21
 and 28 x 28 inverse blocks in two passes).  The walkers see the same random numbers and the same
 arithmetic either way, so the iterations of a population swept several per warp
 equal those swept one per warp (`walkersPerWarp: 1`).  A population of 37 leaves
@@ -34,7 +35,9 @@ def run(text, iterations):
 @pytest.mark.parametrize("compat", ["reference", "corrected"])
 def test_walkers_per_warp_equal_one(N, omega, per_warp, precision, compat):
     from vmachine_b200.batch import dot_text
-    text = dot_text(N, omega, 37, 300, precision, seed=11, compat=compat)
+    # both arms in the staged form (one walker per warp would otherwise take the owner
+    # form at N = 42 and 56; tests/test_owner_sweep_gpu.py compares the two forms)
+    text = dot_text(N, omega, 37, 300, precision, seed=11, compat=compat) + "sweepForm: staged\n"
     i2, two, p2 = run(text + f"walkersPerWarp: {per_warp}\n", 3)
     i1, one, p1 = run(text + "walkersPerWarp: 1\n", 3)
     assert i2.walkers_per_warp == per_warp and i1.walkers_per_warp == 1
