@@ -7,8 +7,12 @@ Workload (one "step" = one optimisation iteration of the whole walker population
   sampled after every move (the reference's definition of a step), device-reduced
   sums, ADAM update.  Mixed precision (FP32 sweep, FP64 rebuild every refresh
   interval, compensated FP64 sums); an FP64 engine run of the same workload is
-  reported beside it.  Synthetic: walker start positions from per-walker Philox
-  streams, RandomNormal as in the reference.
+  reported beside it, and both arms are compared at equal sigma_E: one more iteration
+  of each at the same parameters records every walker's local energy per step and
+  blocks the series on the device (the reference's Blocker), and the time each arm
+  needs to reach the same error bar follows from its iteration time and its sigma_E
+  (sigma_E^2 falls as 1 / samples).  Synthetic: walker start positions from
+  per-walker Philox streams, RandomNormal as in the reference.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -49,14 +53,18 @@ def workload_text(walkers, steps_per_walker, precision, seed, refresh="auto"):
     ]) + "\n"
 
 
-def sweep_traffic():
-    """DRAM bytes (read + write) of one sweep launch, from the committed ncu summary."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                        "sweep_kernel_f32_n56_dot.md")
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the mixed
+# owner sweep on this workload's 16 384 walkers, from an ncu capture of a 448-step
+# launch (not this run: the walker state is read and written once per launch, so the
+# figure does not depend on the launch's step count)
+SWEEP_TRAFFIC_BYTES = 232_538_112
+
+
+def cpu_model():
     try:
-        for line in open(path):
-            if "dram_bytes_per_launch:" in line:
-                return int(line.split("dram_bytes_per_launch:")[1].split("|")[0].strip())
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
     except OSError:
         pass
     return None
@@ -206,6 +214,7 @@ def run_reference_arm(args, rank):
                                "process, E_L every move", "processes": cores,
                    "steps_per_process": steps},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "cpu_model": cpu_model(), "samples": values,
                          "sample": f"{cores} concurrent one-rank runs of the reference built "
                                    f"from its sources, {steps} moves each, CPU_time column"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -318,8 +327,40 @@ def run_engine_arm(args):
         mv64 = W * (spw + eng64.info.burn_in) * world
         fp64 = {"value": mv64 / (ms64 * 1e-3), "ms_per_step": ms64, "steps": args.fp64_steps,
                 "energy": e64[-1][0], "sigma_e_walkers": e64[-1][1],
-                "mixed_energy_same_iteration": energies[args.fp64_steps - 1][0],
-                "mixed_sigma_same_iteration": energies[args.fp64_steps - 1][1]}
+                "mixed_energy_same_iteration": energies[min(args.fp64_steps, args.steps) - 1][0],
+                "mixed_sigma_same_iteration": energies[min(args.fp64_steps, args.steps) - 1][1]}
+        if not args.no_sigma:
+            # equal sigma_E: both arms start from the mixed arm's current walkers and
+            # parameters (held fixed), make args.equil_passes sampling passes with their
+            # own Philox streams (no optimiser step), then one recorded pass each (spw
+            # sampled moves per walker), blocked on the device
+            theta, pos = eng.parameters(), eng.positions()
+            equil = {"mixed": [], "fp64": []}
+            for name, e_ in (("mixed", eng), ("fp64", eng64)):
+                e_.set_parameters(theta)
+                e_.init_walkers(pos, seed=seed)
+                for i in range(args.equil_passes):
+                    s_, _, _ = e_.sample(0, spw + burn, burn)
+                    equil[name].append(s_.energy / s_.n_samples)
+            b32 = eng.blocking(spw + burn, burn)
+            b64 = eng64.blocking(spw + burn, burn)
+            t32, t64 = ms / args.steps * 1e-3, ms64 * 1e-3
+            s32, s64 = b32.energy.std_error, b64.energy.std_error
+            fp64["equal_sigma"] = {
+                "blocking": "reference Blocker (automatic blocking, blocker.cpp) of every walker's "
+                            "per-step E_L concatenated walker by walker, %d samples per walker; both "
+                            "arms from the same walkers at the same fixed parameters, after %d "
+                            "equilibration passes"
+                            % (b32.samples_per_walker, args.equil_passes),
+                "mixed": {"energy": b32.energy.mean, "sigma_e": s32, "sigma_e_walkers": b32.energy_walkers.std_error,
+                          "s_per_iteration": t32},
+                "fp64": {"energy": b64.energy.mean, "sigma_e": s64, "sigma_e_walkers": b64.energy_walkers.std_error,
+                         "s_per_iteration": t64},
+                "equilibration_pass_energies": equil,
+                "energy_difference_in_error_bars": abs(b32.energy.mean - b64.energy.mean) / (s32 * s32 + s64 * s64) ** 0.5,
+                "time_to_fp64_sigma_s": {"mixed": t32 * (s32 / s64) ** 2, "fp64": t64},
+                "time_ratio": t64 / (t32 * (s32 / s64) ** 2),
+            }
         eng64.close()
 
     # the heterogeneous multi-system batch (every rank takes part)
@@ -347,6 +388,7 @@ def run_engine_arm(args):
                    "inverse_drift": {"max": max_drift, "q99": q99_drift},
                    "walkers_per_block": eng.info.walkers_per_block,
                    "kernel": ["runtime-flags", "compiled-in dot flags", "general"][eng.info.kernel_variant],
+                   "sweep_form": {1: "staged", 2: "owner"}.get(eng.info.sweep_form),
                    "l2": "walker state %.0f MB per GPU > 126 MB L2, streamed every launch"
                          % (W * (eng.info.n_coords * 5 * 4 + 2 * 28 * 28 * 4 + 56 * 8 + 64) / 1e6)},
         "el_samples_per_s": value * spw / (spw + burn),
@@ -354,14 +396,16 @@ def run_engine_arm(args):
         "gpu_launches": int(args.steps * (2 * launches + 1)),
         "roofline": {"bound": "fp32-pipe", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                     "traffic": sweep_traffic(),
-                     "traffic_note": "dram read + write bytes of one sweep launch from the ncu "
-                                     "capture in profiles/sweep_kernel_f32_n56_dot.md (448 steps; "
-                                     "the walker state is streamed once per launch whatever its "
-                                     "length, so the figure holds for these launches)",
+                     "traffic": SWEEP_TRAFFIC_BYTES,
+                     "traffic_note": "stale capture: dram read + write bytes of one 448-step launch "
+                                     "of the same kernel on the same 16 384 walkers under ncu, not "
+                                     "measured in this run (the walker state is read and written once "
+                                     "per launch whatever its length)",
                      "peak_source": "vmc_measure_fma_peak (FP32 FMA loop, this GPU, this run); "
                                     "MEASURED_PEAKS.json has no FP32 pipe figure",
-                     "flops_per_move": fl, "kernel": "sweep_kernel<float,2,7>",
+                     "flops_per_move": fl,
+                     "kernel": ("owner_sweep_kernel<float,7,reference flags>" if eng.info.sweep_form == 2
+                                else "sweep_kernel<float,2,7>"),
                      "avg_launch_ms": avg_launch * 1e3},
     }
     if e2e:
@@ -378,6 +422,7 @@ def run_engine_arm(args):
         cores = host_cores()
         v, err = reference_sample(cores, args.ref_steps)
         line["cpu_baseline"] = ({"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                                 "cpu_model": cpu_model(),
                                  "sample": f"{cores} concurrent one-rank reference runs, "
                                            f"{args.ref_steps} moves each"}
                                 if v else {"value": None, "unavailable": err})
@@ -415,13 +460,16 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--walkers", type=int, default=16384)
     ap.add_argument("--steps-per-walker", type=int, default=20000)
-    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--fp64-steps", type=int, default=5)
     ap.add_argument("--refresh-interval", default="auto")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-steps", type=int, default=60000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sigma", action="store_true", help="skip the equal-sigma_E blocking runs")
+    ap.add_argument("--equil-passes", type=int, default=3,
+                    help="sampling passes at fixed parameters before the equal-sigma_E blocking runs")
     ap.add_argument("--batch-iterations", type=int, default=16,
                     help="iterations of the 64-system heterogeneous batch (0: skip)")
     ap.add_argument("--learned", type=float, default=0.0,
