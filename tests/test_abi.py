@@ -47,6 +47,17 @@ def test_library_exports_every_declared_symbol():
     ("numParticles: 4\nhamiltonian: harmonicOscillator\nwaveFunctionElement: slaterDeterminant\n"
      "basis: hermite\n", -2),
     ("numParticles: 2\nwaveFunctionElement: gaussian\n", -2),
+    # hydrogen orbitals with n = 4 or l = 2 (hydrogenorbital.cpp:111-394: Ca, Z = 20, and
+    # beyond) are not on the engine: only the closed shells up to Ar
+    ("numParticles: 20\nnumDimensions: 3\natomicNumber: 20\nhamiltonian: atomicNucleus\n"
+     "interactionStyle: coulomb\nwaveFunctionElement: slaterDeterminant\nbasis: hydrogenOrbital\n", -2),
+    ("numParticles: 36\nnumDimensions: 3\natomicNumber: 36\nhamiltonian: atomicNucleus\n"
+     "interactionStyle: coulomb\nwaveFunctionElement: slaterDeterminant\nbasis: hydrogenOrbital\n", -2),
+    # the owner form of the production sweep covers the dots of N = 20 to 56
+    ("numParticles: 12\nhamiltonian: harmonicOscillator\nwaveFunctionElement: slaterDeterminant\n"
+     "waveFunctionElement: gaussian\nbasis: hermite\nsweepForm: owner\n", -2),
+    ("numParticles: 12\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
+     "sweepForm: fastest\n", -1),
 ])
 def test_create_rejects(text, code):
     from vmachine_b200 import library
