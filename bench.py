@@ -263,8 +263,11 @@ def run_engine_arm(args):
     from vmachine_b200 import Engine, measure_fma_peak
     from vmachine_b200 import distributed as vd
     W, spw = args.walkers, args.steps_per_walker
-    seed = 1000 + rank
-    text = workload_text(W, spw, "mixed", seed, args.refresh_interval)
+    # one population of world x W walkers, rank r holding walkers rW .. rW + W - 1 (their
+    # random streams keyed by the population index: the shards are one engine's chains)
+    seed = 1000
+    shard = f"walkerOffset: {rank * W}\n"
+    text = workload_text(W, spw, "mixed", seed, args.refresh_interval) + shard
     eng = Engine(text, device=local)
     eng.init_walkers(None, seed=seed)
     burn = eng.info.burn_in
@@ -313,7 +316,7 @@ def run_engine_arm(args):
     fp64 = None
     if not args.no_fp64:
         # same walkers, seeds and schedule as the mixed arm: energies comparable
-        eng64 = Engine(workload_text(W, spw, "fp64", seed), device=local)
+        eng64 = Engine(workload_text(W, spw, "fp64", seed) + shard, device=local)
         eng64.init_walkers(None, seed=seed)
         for it in range(args.warmup):
             vd.run_iteration(eng64, it)

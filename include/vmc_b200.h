@@ -203,6 +203,13 @@ int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history);
  * records the stop, waits for it and writes the elapsed milliseconds. */
 int vmc_stopwatch(vmc_engine *e, int mode, double *ms);
 
+/* FP64 rebuild cadence of a mixed-precision engine, in steps (>= 1): engines that
+ * share one population (walker shards on several GPUs) set the same cadence after
+ * each iteration, so every shard refreshes where one engine over all walkers would;
+ * with `refreshInterval: auto` the drift test goes on tuning from this value.  No
+ * counterpart in the reference (which never re-inverts). */
+int vmc_set_refresh_interval(vmc_engine *e, int steps);
+
 /* FMA throughput of a device, FP32 (VMC_PRECISION_MIXED) or FP64, measured with a
  * register-resident loop over all SMs; TFLOP/s counting an FMA as 2 flops.  The
  * roofline denominator of the CUDA-core-bound sweep kernel. */

@@ -286,6 +286,9 @@ std::string parse_config(const std::string &text, Config &c)
                 }
             } else if (key == "numWalkers") {
                 c.walkers = std::stoi(v0);
+            } else if (key == "walkerOffset") {
+                c.walker_offset = std::stoi(v0);
+                if (c.walker_offset < 0) return err("walkerOffset must be >= 0");
             } else if (key == "precision") {
                 if (v0 == "fp64") c.precision = 0;
                 else if (v0 == "mixed") c.precision = 1;

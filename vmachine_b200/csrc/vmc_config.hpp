@@ -54,6 +54,7 @@ struct Config {
     std::string path;
     // engine keys (new)
     int walkers = 1;
+    int walker_offset = 0;       // this engine's first walker in a sharded population (random streams)
     int precision = 0;           // 0 fp64, 1 mixed
     int refresh_interval = -1;   // -1 auto
     int compat = 1;              // 1 reference quirks, 0 corrected

@@ -185,6 +185,7 @@ Params make_params(const vmc_engine *e)
     P.n_elem = e->E;
     P.ep = e->EP;
     P.nacc = e->nacc_dev;
+    P.walker_offset = e->cfg.walker_offset;
     for (int i = 0; i < e->E && i < MAX_ELEM; ++i) P.elem_kind[i] = e->cfg.elements[i];
     P.flags = e->flags;
     P.sampling = e->sampling;
@@ -752,7 +753,8 @@ int vmc_init_walkers(vmc_engine *e, const double *pos, uint64_t seed)
         unsigned long long sd_seed = seed;
         int nrm = normal ? 1 : 0;
         double sdv = sd;
-        void *args[] = {&L, &Wi, &st, &sd_seed, &nrm, &sdv};
+        int off = e->cfg.walker_offset;
+        void *args[] = {&L, &Wi, &st, &sd_seed, &nrm, &sdv, &off};
         CUDA_TRY(cudaLaunchKernel(e->ks.initpos, dim3((n + 255) / 256), dim3(256), args, 0, e->stream));
     }
     CUDA_TRY(cudaMemsetAsync(e->d_counter, 0, W * sizeof(unsigned long long), e->stream));
@@ -1204,6 +1206,14 @@ int vmc_set_replay(vmc_engine *e, const double *stream, int length)
     CUDA_TRY(cudaMalloc(&e->d_replay, bytes));
     CUDA_TRY(cudaMemcpyAsync(e->d_replay, stream, bytes, cudaMemcpyHostToDevice, e->stream));
     e->replay_len = length;
+    return VMC_OK;
+}
+
+int vmc_set_refresh_interval(vmc_engine *e, int steps)
+{
+    if (!e || steps < 1) return fail(VMC_E_ARG, "bad argument");
+    if (e->precision != VMC_PRECISION_MIXED) return fail(VMC_E_STATE, "the FP64 engine has no refresh cadence");
+    e->refresh_interval = steps;
     return VMC_OK;
 }
 

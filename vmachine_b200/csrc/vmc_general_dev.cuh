@@ -909,7 +909,8 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                 r1 = q[1];
                 r2 = q[2];
             } else {
-                const uint4 v = philox(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)w, 0u),
+                const uint4 v = philox(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32),
+                                                  (uint32_t)(w + a.P.walker_offset), 0u),
                                        make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
                 ++ctr;
                 k = (int)__umulhi(v.x, (unsigned)D);

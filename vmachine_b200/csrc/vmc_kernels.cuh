@@ -86,6 +86,9 @@ constexpr int MAX_N = 64;
 struct Params {
     Layout L;
     int W, N, n_elem, ep, nacc;
+    // index of this engine's first walker in a population sharded over engines: walker
+    // w's random streams are keyed by w + walker_offset, so shards reproduce one engine
+    int walker_offset;
     int elem_kind[MAX_ELEM];  // element kinds in configuration order
     int flags, sampling;
     double omega, alpha, gamma, gamma_prev, alpha_h, Z;
@@ -655,12 +658,12 @@ __global__ void eval_kernel(const EvalArgs a)
 // sd = 1/omega) or RandomUniform U[0, 1) (randomuniform.cpp:18).
 template <typename T>
 __global__ void initial_positions_kernel(Layout L, int W, void *state, unsigned long long seed,
-                                         int normal, double sd)
+                                         int normal, double sd, int walker_offset)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= W * L.D) return;
     const int w = i / L.D, c = i - w * L.D;
-    const uint4 v = philox(make_uint4((uint32_t)c, 0u, (uint32_t)w, 1u),
+    const uint4 v = philox(make_uint4((uint32_t)c, 0u, (uint32_t)(w + walker_offset), 1u),
                            make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
     double val;
     if (normal) {

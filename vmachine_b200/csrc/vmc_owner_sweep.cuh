@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
             unsigned rng_u;
             {
                 const unsigned long long c = ctr + (unsigned long long)l;
-                const uint4 v = philox(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)w, 0u),
+                const uint4 v = philox(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)(w + P.walker_offset), 0u),
                                        make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
                 rng_k = (int)__umulhi(v.x, (unsigned)D);
                 if constexpr (F32) {

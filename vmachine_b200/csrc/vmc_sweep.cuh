@@ -379,7 +379,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             // (the same per-step stream as a serial draw); each step of this block
             // takes its triple from lane (step - s0) by shuffle.
             const unsigned long long c = ctr + (unsigned long long)lane;
-            const uint4 v = philox(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)w, 0u),
+            const uint4 v = philox(make_uint4((uint32_t)c, (uint32_t)(c >> 32), (uint32_t)(w + P.walker_offset), 0u),
                                    make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32)));
             rng_k = (int)__umulhi(v.x, (unsigned)D);
             if (is) {

@@ -85,7 +85,7 @@ EXPORTS = ["vmc_abi_version", "vmc_create", "vmc_destroy", "vmc_get_info", "vmc_
            "vmc_batch_init_walkers", "vmc_batch_set_tile", "vmc_batch_run_iteration",
            "vmc_batch_last_sums", "vmc_batch_tuning", "vmc_block_series", "vmc_blocking",
            "vmc_format_weights", "vmc_write_weights", "vmc_read_weights", "vmc_save_state", "vmc_load_state",
-           "vmc_last_blocking", "vmc_densities"]
+           "vmc_last_blocking", "vmc_densities", "vmc_set_refresh_interval"]
 
 
 def library():
@@ -118,6 +118,7 @@ def library():
     L.vmc_get_status.argtypes = [vp, vp]
     L.vmc_run_simulation.argtypes = [vp, ctypes.POINTER(Averages), ip]
     L.vmc_stopwatch.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double)]
+    L.vmc_set_refresh_interval.argtypes = [vp, ip]
     L.vmc_measure_fma_peak.argtypes = [ip, ip, ctypes.POINTER(ctypes.c_double)]
     L.vmc_format_weights.argtypes = [vp, ip, ip, ip, ctypes.c_char_p, ctypes.c_longlong]
     L.vmc_write_weights.argtypes = [vp, ctypes.c_char_p, ip]
@@ -309,6 +310,10 @@ class Engine:
         info = Info()
         self._check(library().vmc_get_info(self._h, ctypes.byref(info)))
         return info.refresh_interval
+
+    def set_refresh_interval(self, steps):
+        """Set the FP64 rebuild cadence (mixed precision; vmc_set_refresh_interval)."""
+        self._check(library().vmc_set_refresh_interval(self._h, int(steps)))
 
     # --- checkpoints
     def write_weights(self, path, digits=0):
