@@ -367,6 +367,89 @@ long vmref_iteration(void *hp, int iter, double *out)
     return h->rng->exhausted ? -1 : long(h->rng->pos);
 }
 
+// System::runSimulation's iteration loop (system.cpp:91-137) without terminal or file
+// output: adaptive steps from System::adaptiveSteps, the convergence check by
+// System::checkingConvergence, set up as the API calls setConvergenceTools and
+// setAdaptiveStepTools set them up (userinput.cpp:194-222) when check / adaptive are
+// non-zero (the input.in keys alone leave the convergence window unsized).  Per
+// iteration: the sampled steps (m_stepsWOEqui), the average energy, and 1 for the
+// iteration that counts the densities and writes the instant energies.  Returns the
+// iterations run, or -1 if the stream ran out.
+long vmref_simulation(void *hp, int check, int n_energies, double tolerance, int adaptive, int range,
+                      int additional, int additional_last, int *steps_out, double *energy_out, int *last_out)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    Sampler *sm = s->m_sampler;
+    if (check) s->setConvergenceTools(n_energies, tolerance);
+    if (adaptive) s->setAdaptiveStepTools(range, additional, additional_last);
+    s->m_numberOfNormalIterations = s->m_numberOfIterations - s->m_rangeOfAdaptiveSteps - 1;
+    long n = 0;
+    for (s->m_iter = 0; s->m_iter < s->m_numberOfIterations; s->m_iter++, n++) {
+        if (s->m_applyAdaptiveSteps) {
+            s->m_stepsWOEqui = s->m_initialStepsWOEqui * s->adaptiveSteps();
+            s->m_stepsWEqui = s->m_stepsWOEqui + s->m_equilibriationSteps;
+            s->m_totalStepsWOEqui = s->m_initialTotalStepsWOEqui * s->adaptiveSteps();
+            s->m_totalStepsWEqui = s->m_totalStepsWOEqui + s->m_totalEquilibriationSteps;
+        }
+        sm->m_iter = s->m_iter;
+        sm->setNumberOfSteps(s->m_stepsWOEqui, s->m_totalStepsWOEqui, s->m_totalStepsWEqui);
+        steps_out[n] = s->m_stepsWOEqui;
+        last_out[n] = s->m_iter == s->m_numberOfNormalIterations + s->m_rangeOfAdaptiveSteps ? 1 : 0;
+        s->runMetropolisCycles();
+        sm->computeTotals();
+        sm->computeAverages();
+        s->m_parameters -= s->m_optimization->updateParameters();
+        energy_out[n] = sm->m_averageEnergy;
+        if (s->m_checkConvergence) s->checkingConvergence();
+        s->updateAllParameters(s->m_parameters);
+    }
+    return h->rng->exhausted ? -1 : n;
+}
+
+// nsteps Metropolis steps as vmref_steps, counting after every step the Sampler's
+// electron densities from System's copies, as System::runMetropolisCycles does in the
+// last iteration (system.cpp:157-160; Sampler::computeOneBodyDensity,
+// computeOneBodyDensity2, computeTwoBodyDensity, sampler.cpp:639-692), on a grid of
+// `bins` bins up to max_radius.  Outputs (each may be NULL, then not counted):
+// radial[bins], spatial[bins][bins] (row = the y index), pair[bins][bins] (row = the
+// bin of the lower-index particle).  Returns the random numbers consumed, or -1 if
+// the stream ran out.
+long vmref_densities(void *hp, int nsteps, int bins, double max_radius, long long *radial,
+                     long long *spatial, long long *pair)
+{
+    Handle *h = static_cast<Handle *>(hp);
+    System *s = h->sys;
+    Sampler *sm = s->m_sampler;
+    sm->m_computeOneBodyDensity = radial != nullptr;
+    sm->m_computeOneBodyDensity2 = spatial != nullptr;
+    sm->m_computeTwoBodyDensity = pair != nullptr;
+    sm->m_numberOfBins = bins;
+    sm->m_numberOfBinsHalf = bins / 2;
+    sm->m_maxRadius = max_radius;
+    sm->m_radialStep = max_radius / bins;
+    sm->m_particlesPerBin = Eigen::VectorXi::Zero(bins);
+    sm->m_densityGrid = Eigen::MatrixXi::Zero(bins, bins);
+    sm->m_particlesPerBinPairwise = Eigen::MatrixXi::Zero(bins, bins);
+    for (int i = 0; i < nsteps; i++) {
+        s->m_metropolis->acceptMove();
+        s->m_positions = s->m_metropolis->updatePositions();
+        s->m_distanceMatrix = s->m_metropolis->updateDistanceMatrix();
+        s->m_radialVector = s->m_metropolis->updateRadialVector();
+        sm->computeOneBodyDensity(s->m_radialVector);
+        sm->computeTwoBodyDensity(s->m_radialVector);
+        sm->computeOneBodyDensity2(s->m_positions);
+    }
+    for (int r = 0; r < bins; r++) {
+        if (radial) radial[r] = sm->m_particlesPerBin(r);
+        for (int c = 0; c < bins; c++) {
+            if (spatial) spatial[(size_t)r * bins + c] = sm->m_densityGrid(r, c);
+            if (pair) pair[(size_t)r * bins + c] = sm->m_particlesPerBinPairwise(r, c);
+        }
+    }
+    return h->rng->exhausted ? -1 : long(h->rng->pos);
+}
+
 // Blocker on a series of length 2^k (include/block/blocker.cpp:15-33):
 // out = {mean, stdErr}.
 int vmref_blocking(const double *x, long n, double *out)

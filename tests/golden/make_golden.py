@@ -9,6 +9,8 @@ reference nor its build.
     python tests/golden/make_golden.py hydrogen   # only hydrogen_orbitals.npz
     python tests/golden/make_golden.py hydrogen_sj   # only hydrogen_simplejastrow.npz
     python tests/golden/make_golden.py weights    # only weights_format.npz
+    python tests/golden/make_golden.py densities  # only densities.npz
+    python tests/golden/make_golden.py schedules  # only schedules.npz
 
 Every input is seeded synthetic data: walker positions ~ N(0, 1/sqrt(omega)),
 replayed uniforms/normals from numpy's PCG64 with fixed seeds.
@@ -267,6 +269,92 @@ def make_hydrogen_sj():
     np.savez_compressed(os.path.join(HERE, "hydrogen_simplejastrow.npz"), **out)
 
 
+DENSITY_CASES = [
+    # atoms: the Metropolis keeps System's radial vector current (the atomic Hamiltonian
+    # needs it), so all three of the reference's densities count the walker as it moves
+    ("he_horb_sj", SystemSpec(N=2, Z=2, elements=(S, SIMPLEJASTROW), step=0.05, **H_ORB), 3, 500, 40, 4.0),
+    ("be_horb_pade", SystemSpec(N=4, Z=4, elements=(S, P), step=0.02, **H_ORB), 2, 400, 30, 5.0),
+    # a dot: only the spatial density (the reference's radial densities of a dot count the
+    # initial radii, its radial vector not being updated: elementoperation.cpp:130-170)
+    ("n6_slater_gauss_pade", SystemSpec(N=6, elements=(S, G, P), step=0.05), 3, 500, 40, 4.0),
+]
+
+
+def make_densities():
+    """Per case, walkers each with its own replayed stream through the reference's
+    Metropolis, densities counted after every step (no burn-in), summed over walkers."""
+    rng = np.random.default_rng(20261207)
+    out = {}
+    for name, spec, walkers, steps, bins, rmax in DENSITY_CASES:
+        pos = np.stack([rng.normal(0.0, 1.0, spec.D) for _ in range(walkers)])
+        streams = np.stack([make_stream(spec, steps, rng) for _ in range(walkers)])
+        radial = np.zeros(bins, np.int64)
+        spatial = np.zeros((bins, bins), np.int64)
+        pair = np.zeros((bins, bins), np.int64)
+        # one parameter set for every walker (random initial weights would otherwise be
+        # drawn from each walker's own stream)
+        R0 = RefHarness(spec, pos[0], None, streams[0])
+        theta = R0.params()
+        R0.close()
+        for w in range(walkers):
+            R = RefHarness(spec, pos[w], theta, streams[w])
+            r, sp, pr, used = R.densities(steps, bins, rmax)
+            assert used == 3 * steps, (name, used)
+            R.close()
+            radial += r
+            spatial += sp
+            pair += pr
+        for k, v in dict(pos=pos, stream=streams, theta=theta, bins=np.array(bins), max_radius=np.array(rmax),
+                         radial=radial, spatial=spatial, pair=pair).items():
+            out[f"{name}/{k}"] = v
+        for k, v in spec_fields(spec).items():
+            out[f"{name}/spec_{k}"] = np.array(v)
+    np.savez_compressed(os.path.join(HERE, "densities.npz"), **out)
+
+
+SCHEDULE_TOOLS = dict(check=1, n_energies=3, tolerance=0.05, adaptive=1, range_=3, additional=1,
+                      additional_last=2)
+SCHEDULE_CASES = [
+    # converges at iteration 2 (|E_0 - E_2| < 0.05), so `normal` = 3, the density
+    # iteration is 6 (x4 steps), 3-5 and the ones after it take x2 steps; the loop goes on
+    # to numIterations (system.cpp:93 has no exit at the last iteration)
+    ("n2_converge", SystemSpec(N=2, elements=(G, P), step=0.1, sampling="bruteForce", num_steps=2000,
+                               extra=["numIterations: 14", "checkConvergence: true", "numberOfEnergies: 3",
+                                      "tolerance: 0.05", "applyAdaptiveSteps: true", "rangeOfAdaptiveSteps: 3",
+                                      "additionalSteps: 1", "additionalStepsLastIter: 2"]), 14),
+    # no convergence (tolerance 0): the last iteration is numIterations - 1
+    ("n2_no_converge", SystemSpec(N=2, elements=(G, P), step=0.1, sampling="bruteForce", num_steps=2000,
+                                  extra=["numIterations: 8", "checkConvergence: true", "numberOfEnergies: 3",
+                                         "tolerance: 0.0", "applyAdaptiveSteps: true", "rangeOfAdaptiveSteps: 3",
+                                         "additionalSteps: 1", "additionalStepsLastIter: 2"]), 8),
+]
+
+
+def make_schedules():
+    """System::runSimulation's schedule on one walker with a replayed stream: per
+    iteration the sampled steps, the energy and the density iteration, under the
+    convergence check and adaptive steps."""
+    rng = np.random.default_rng(20261208)
+    out = {}
+    for name, spec, iters in SCHEDULE_CASES:
+        tools = dict(SCHEDULE_TOOLS)
+        if name == "n2_no_converge":
+            tools["tolerance"] = 0.0
+        pos = rng.normal(0.0, 1.0, spec.D)
+        stream = make_stream(spec, 2000 * 4 * iters + 100, rng)
+        R = RefHarness(spec, pos, None, stream)
+        theta = R.params()
+        n, steps, energy, last = R.simulation(iters, **tools)
+        R.close()
+        assert n == iters, (name, n)
+        for k, v in dict(pos=pos, stream=stream, theta=theta, steps=steps, energy=energy, last=last).items():
+            out[f"{name}/{k}"] = v
+        for k, v in spec_fields(spec).items():
+            out[f"{name}/spec_{k}"] = np.array(v)
+        out[f"{name}/extra"] = np.array("\n".join(spec.extra))
+    np.savez_compressed(os.path.join(HERE, "schedules.npz"), **out)
+
+
 def make_hydrogen():
     rng = np.random.default_rng(20261204)
     out = make_eval(rng, HYDROGEN_EVAL)
@@ -281,12 +369,20 @@ def main():
     if sys.argv[1:] == ["hydrogen_sj"]:
         make_hydrogen_sj()
         return
+    if sys.argv[1:] == ["schedules"]:
+        make_schedules()
+        return
+    if sys.argv[1:] == ["densities"]:
+        make_densities()
+        return
     if sys.argv[1:] == ["weights"]:
         np.savez_compressed(os.path.join(HERE, "weights_format.npz"),
                             **make_weights(np.random.default_rng(20261205)))
         return
     make_hydrogen()
     make_hydrogen_sj()
+    make_densities()
+    make_schedules()
     rng = np.random.default_rng(20261203)
     np.savez_compressed(os.path.join(HERE, "eval_fixed.npz"), **make_eval(rng))
     np.savez_compressed(os.path.join(HERE, "chains.npz"), **make_chains(rng))

@@ -292,6 +292,33 @@ class RefHarness:
         used = self.lib.vmref_steps(self.h, n, _ptr(acc), _ptr(en), _ptr(pg))
         return acc, en, pg, used
 
+    def densities(self, n, bins, max_radius, radial=True, spatial=True, pair=True):
+        """n steps counting the Sampler's densities after each (vmref_densities)."""
+        L = self.lib
+        L.vmref_densities.restype = ctypes.c_long
+        L.vmref_densities.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        r = np.zeros(bins, np.int64) if radial else None
+        sp = np.zeros((bins, bins), np.int64) if spatial else None
+        pr = np.zeros((bins, bins), np.int64) if pair else None
+        used = L.vmref_densities(self.h, n, bins, max_radius, _ptr(r), _ptr(sp), _ptr(pr))
+        return r, sp, pr, used
+
+    def simulation(self, max_iters, check=0, n_energies=5, tolerance=1e-6, adaptive=0, range_=10, additional=4,
+                   additional_last=8):
+        """System::runSimulation's loop with the convergence and adaptive-step tools
+        (vmref_simulation): per iteration the sampled steps, the energy and the
+        density-iteration flag."""
+        L = self.lib
+        L.vmref_simulation.restype = ctypes.c_long
+        L.vmref_simulation.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]
+        steps, energy, last = np.zeros(max_iters, np.int32), np.zeros(max_iters), np.zeros(max_iters, np.int32)
+        n = L.vmref_simulation(self.h, check, n_energies, tolerance, adaptive, range_, additional, additional_last,
+                               _ptr(steps), _ptr(energy), _ptr(last))
+        return n, steps[:max(n, 0)], energy[:max(n, 0)], last[:max(n, 0)]
+
     def iteration(self, it):
         EP = self.E * self.P
         out = np.zeros(6 + 3 * EP)

@@ -51,3 +51,27 @@ def test_not_power_of_two_and_constant():
     assert b.mean == -1.0 and b.std_error == -1.0 and b.n_k == 0
     c = block_series(np.full(256, 2.0))
     assert c.mean == 2.0 and c.std_error == 0.0
+
+
+def test_reference_resampling_example():
+    """The reference's own Blocker fixture: examples/resampling/523861_0.dat, the
+    instant energies (2^17) of that example's last iteration, whose blocked result the
+    example's log prints as 'Total energy : 3.0111013667 (with STD = 0.0030690608)';
+    also against the reference's Blocker compiled from its sources (oracle/_ref)."""
+    import ctypes
+    from vmachine_b200 import block_series
+    ref = os.environ.get("VMC_REFERENCE_DIR", "/root/reference")
+    path = os.path.join(ref, "examples", "resampling", "523861_0.dat")
+    if not os.path.exists(path):
+        pytest.skip("the reference's example files are not on this machine")
+    x = np.loadtxt(path)
+    assert len(x) == 1 << 17
+    b = block_series(x)
+    assert round(b.mean, 10) == 3.0111013667 and round(b.std_error, 10) == 0.0030690608
+    so = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libvmref.so")
+    if os.path.exists(so):
+        lib = ctypes.CDLL(so)
+        lib.vmref_blocking.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+        out = np.zeros(2)
+        lib.vmref_blocking(x.ctypes.data_as(ctypes.c_void_p), len(x), out.ctypes.data_as(ctypes.c_void_p))
+        assert abs(b.mean - out[0]) < 1e-14 * abs(out[0]) and abs(b.std_error - out[1]) < 1e-12 * out[1]

@@ -3,7 +3,12 @@ system.cpp:81-139) and its electron densities (sampler.cpp:639-692), on the GPU.
 
 - vmc_densities counts, step by step, exactly the bins a host computes from the
   walkers' positions after each step (FP64 engine; the binning restated here from
-  sampler.cpp:639-692);
+  sampler.cpp:639-692), and on replayed random numbers exactly the counts the
+  reference's own Sampler makes along the same chains (tests/golden/densities.npz:
+  He and Be on hydrogen orbitals, all three densities; a dot, the spatial density:
+  the reference never updates a dot's radial vector, elementoperation.cpp:130-170,
+  so its radial densities count the starting radii, where the engine counts the
+  current ones);
 - vmc_run_simulation: the convergence check ends the run rangeOfAdaptiveSteps + 1
   iterations after convergence, adaptive steps lengthen the last iterations, the
   energy files get one line per iteration, the last iteration writes the density
@@ -48,6 +53,62 @@ def host_bins(pos, N, bins, max_radius):
                 if bi < bins and bj < bins:
                     pair[bi, bj] += 1
     return radial, grid, pair
+
+
+DENS = None
+
+
+def density_cases():
+    global DENS
+    if DENS is None:
+        from oracle_bind import load_cases
+        DENS = load_cases(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "densities.npz"))
+    return DENS
+
+
+@pytest.mark.parametrize("name", ["he_horb_sj", "be_horb_pade", "n6_slater_gauss_pade"])
+def test_densities_match_reference_sampler(name):
+    from oracle_bind import spec_from_case
+    from vmachine_b200 import Engine
+    c = density_cases()[name]
+    spec = spec_from_case(c)
+    pos, stream = c["pos"], c["stream"]
+    W, steps = pos.shape[0], stream.shape[1]
+    bins, rmax = int(c["bins"]), float(c["max_radius"])
+    with Engine(spec.input_in(), walkers=W, precision=0, compat=1) as e:
+        e.set_parameters(c["theta"])
+        e.init_walkers(pos)
+        e.set_replay(stream)
+        r, sp, tb = e.densities(steps, 0, bins, rmax, radial=True, spatial=True, two_body=True)
+    assert np.array_equal(sp.astype(np.int64), c["spatial"])
+    if spec.atom:
+        assert np.array_equal(r.astype(np.int64), c["radial"])
+        assert np.array_equal(tb.astype(np.int64), c["pair"])
+    else:
+        # the same number of counts, binned at the current radii
+        assert r.sum() <= c["radial"].sum() and tb.sum() > 0
+
+
+@pytest.mark.parametrize("name", ["n2_converge", "n2_no_converge"])
+def test_simulation_schedule_matches_reference(name):
+    """vmc_run_simulation on one walker against the reference's own System::runSimulation
+    loop (tests/golden/schedules.npz: adaptiveSteps, checkingConvergence) on the same
+    replayed numbers: the same iterations with the same step counts, so the same
+    energies, including the iterations after the density iteration that the
+    reference's loop still runs."""
+    from oracle_bind import load_cases, spec_from_case
+    from vmachine_b200 import Engine
+    c = load_cases(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "schedules.npz"))[name]
+    spec = spec_from_case(c)
+    spec.extra = str(c["extra"]).split("\n")
+    with Engine(spec.input_in(), walkers=1, precision=0, compat=1) as e:
+        e.set_parameters(c["theta"])
+        e.init_walkers(c["pos"][None, :])
+        e.set_replay(c["stream"][None, :, :])
+        hist = e.run_simulation()
+    energy = np.array([a.energy for a in hist])
+    assert len(energy) == len(c["energy"])
+    assert np.allclose(energy, c["energy"], rtol=1e-10, atol=0), np.abs(energy - c["energy"]).max()
 
 
 def test_densities_match_host_binning():
@@ -100,13 +161,17 @@ def test_run_simulation_driver(tmp_path):
     del burn
 
 
-@pytest.mark.parametrize("tol,expect", [(1e9, 4), (1e-30, 6)])
-def test_convergence_check(tol, expect):
+@pytest.mark.parametrize("tol,compat,expect", [(1e9, "corrected", 4), (1e9, "reference", 6),
+                                               (1e-30, "corrected", 6), (1e-30, "reference", 6)])
+def test_convergence_check(tol, compat, expect):
     """numberOfEnergies 5, rangeOfAdaptiveSteps 2: with a huge tolerance the run
-    converges at iteration 0 and ends at iteration 0 + 1 + 2; with none it runs all 6."""
+    converges at iteration 0, so its density iteration is 0 + 1 + 2; the corrected
+    driver ends there, the reference's loop runs on to numIterations (the schedule
+    itself is held to the reference's in test_simulation_schedule_matches_reference);
+    with no tolerance it runs all 6."""
     from vmachine_b200 import Engine
     extra = ["numIterations: 6", "rangeOfAdaptiveSteps: 2", "checkConvergence: true", f"tolerance: {tol!r}",
-             "numberOfEnergies: 5"]
+             "numberOfEnergies: 5", f"compat: {compat}"]
     with Engine(text(32, 200, extra)) as e:
         e.init_walkers(None, seed=1)
         assert len(e.run_simulation()) == expect

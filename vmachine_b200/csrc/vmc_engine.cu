@@ -974,7 +974,11 @@ int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)
     // on sample 2^additionalSteps times the steps and the last 2^additionalStepsLastIter
     // times (system.cpp:214-224); the convergence check moves `normal` to the next
     // iteration once the energy of numberOfEnergies iterations ago is within
-    // `tolerance` of the latest (system.cpp:197-207)
+    // `tolerance` of the latest (system.cpp:197-207).  The reference's loop has no exit
+    // at the last iteration (system.cpp:93): after it the remaining iterations up to
+    // numIterations run with 2^additionalSteps times the steps; compat: corrected ends
+    // the run there.  The convergence window starts at zeros, as setConvergenceTools
+    // sizes it (userinput.cpp:194-200).
     const Config &c = e->cfg;
     int normal = c.iterations - c.range_adaptive - 1;
     bool check = c.check_convergence;
@@ -1063,7 +1067,7 @@ int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history)
             ef[2] << a.external << std::endl;
             ef[3] << a.interaction << std::endl;
         }
-        if (last) {
+        if (last && !e->compat) {
             ++it;
             break;
         }
