@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -103,6 +104,34 @@ bool select_set(int precision, int dim, int K, int flags, KernelSet &out)
                                             : select_kernels_f64(dim, K, flags, out);
 }
 
+}  // namespace
+
+// Unique identifier of the calling thread's current CUDA context (cuCtxGetId through
+// the runtime's driver entry points, so the library needs no link to the driver
+// library), or 0 when it cannot be told.
+unsigned long long vmc::current_context_id()
+{
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+    return 0;
+}
+
+namespace {
+
 uint4 host_philox(uint4 c, uint2 k)
 {
     for (int r = 0; r < 10; ++r) {
@@ -115,15 +144,21 @@ uint4 host_philox(uint4 c, uint2 k)
     return c;
 }
 
+// Constant-memory tables belong to the context the modules were loaded in: the
+// upload is redone whenever the device's current context is not the one uploaded to
+// (a context created after cudaDeviceReset starts with empty tables).
 int hermite_init_device(int device)
 {
-    static bool done[64] = {false};
-    if (device < 64 && done[device]) return VMC_OK;
+    static std::mutex mu;
+    static unsigned long long done[64] = {0};
+    std::lock_guard<std::mutex> lock(mu);
+    const unsigned long long ctx = current_context_id();
+    if (device < 64 && ctx != 0 && done[device] == ctx) return VMC_OK;
     const HermiteCoef h = hermite_coefficients();
     CUDA_TRY(upload_hermite_f32(h));
     CUDA_TRY(upload_hermite_f64(h));
     CUDA_TRY(upload_hermite_gen(h));
-    if (device < 64) done[device] = true;
+    if (device < 64) done[device] = ctx;
     return VMC_OK;
 }
 

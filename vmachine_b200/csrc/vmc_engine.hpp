@@ -11,6 +11,8 @@
 
 namespace vmc {
 int set_last_error(int code, const char *msg);
+// identifier of the current CUDA context (0: unknown), for per-context set-up
+unsigned long long current_context_id();
 }  // namespace vmc
 
 struct vmc_engine {

@@ -35,6 +35,7 @@ namespace vmc {
 bool select_kernels_f64(int dim, int K, int flags, KernelSet &out);
 cudaError_t upload_hermite_f64(const HermiteCoef &h);
 int set_last_error(int code, const char *msg);  // vmc_engine.cu: message for vmc_last_error
+unsigned long long current_context_id();        // vmc_engine.cu: 0 when it cannot be told
 }  // namespace vmc
 
 using namespace vmc;
@@ -48,6 +49,7 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char *g_scratch_ptr[kMaxDevices] = {nullptr};
+unsigned long long g_setup_ctx[kMaxDevices] = {0};  // the context the set-up was made in
 
 int err(int code, const std::string &msg) { return set_last_error(code, msg.c_str()); }
 
@@ -56,13 +58,17 @@ int cuda_err(const char *what, cudaError_t e)
     return err(VMC_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// Once per device, with that device current: address of the scratch array and
-// the Hermite recurrence coefficients of the FP64 kernels (synchronous copies,
-// which is why the first call on a device must not come during stream capture).
+// Once per device and context, with that device current: address of the scratch
+// array and the Hermite recurrence coefficients of the FP64 kernels (synchronous
+// copies, which is why the first call on a device must not come during stream
+// capture).  A new context on the device (after cudaDeviceReset, the module loaded
+// again) gets the set-up again: the array's address and the constant tables are the
+// context's.
 int setup_device(int device, unsigned char **scratch)
 {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_ptr[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (g_scratch_ptr[device] && ctx != 0 && g_setup_ctx[device] == ctx) {
         *scratch = g_scratch_ptr[device];
         return VMC_OK;
     }
@@ -84,6 +90,7 @@ int setup_device(int device, unsigned char **scratch)
     ce = upload_hermite_f64(h);
     if (ce != cudaSuccess) return cuda_err("Hermite coefficient upload", ce);
     g_scratch_ptr[device] = static_cast<unsigned char *>(ptr);
+    g_setup_ctx[device] = ctx;
     *scratch = g_scratch_ptr[device];
     return VMC_OK;
 }
