@@ -52,6 +52,23 @@ def evaluate(eng, eval_steps, burn_steps=200):
     return float(np.mean(e)), float(np.std(e, ddof=1) / np.sqrt(len(e))), int(info.n_walkers)
 
 
+def evaluate_blocked(eng, eval_steps, burn_steps=200):
+    """The frozen wave function with every walker's local-energy series blocked on the
+    device (vmc_blocking: the reference's Blocker per walker, include/block/blocker.cpp):
+    the energy with its independent-chains error bar (each walker's own blocked
+    variance of its mean, summed over walkers / W^2, so a walker that sits near a node
+    for the whole pass weighs by its own fluctuation, not by its distance from the
+    others), the concatenated-series Blocker result, and the variance of the local
+    energy, the variational principle's second criterion."""
+    eng.sample(10 ** 6, burn_steps + 1, burn_steps)
+    b = eng.blocking(eval_steps + 1, 1)
+    s, _, _ = eng.sample(10 ** 6, eval_steps + 1, 1)
+    var = s.energy2 / s.n_samples - (s.energy / s.n_samples) ** 2
+    return {"energy": b.energy_walkers.mean, "error": b.energy_walkers.std_error,
+            "energy_blocker": b.energy.mean, "error_blocker": b.energy.std_error,
+            "variance": float(var), "samples_per_walker": int(b.samples_per_walker)}
+
+
 def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps=4000,
             lr_pade=0.01, lr_mlp=3e-4, seed=7, mlp_iterations=None):
     """Pade against MLP Jastrow at equal wall time: both train for budget_s seconds,
@@ -72,11 +89,16 @@ def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps
             eng, hist = train(text, budget_s, seed=seed)
         energy, err, W = evaluate(eng, eval_steps)
         out[name] = {"iterations": len(hist), "train_seconds": hist[-1][0], "lr": lr,
-                     "last_iteration_energy": hist[-1][1], "energy": energy, "error": err}
+                     "last_iteration_energy": hist[-1][1], "energy": energy, "error": err,
+                     "blocked": evaluate_blocked(eng, eval_steps)}
         eng.close()
     d = out["pade"]["energy"] - out["mlp"]["energy"]
     out["gain"] = d
     out["gain_sigma"] = d / np.hypot(out["pade"]["error"], out["mlp"]["error"])
+    bp, bm = out["pade"]["blocked"], out["mlp"]["blocked"]
+    out["gain_blocked"] = bp["energy"] - bm["energy"]
+    out["gain_blocked_sigma"] = out["gain_blocked"] / np.hypot(bp["error"], bm["error"])
+    out["variance_ratio"] = bm["variance"] / bp["variance"]
     return out
 
 
