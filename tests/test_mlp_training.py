@@ -4,12 +4,15 @@ forward and backward kernels (N = 20, omega = 0.5 quantum dot).
 - Training lowers the energy of the MLP wave function far below its untrained
   start (the network's output layers start at zero, so the untrained factor is the
   cusp term alone, with alpha = 1).
-- At equal wall time the trained MLP is not worse than the Pade-Jastrow trained by
-  the same engine (the difference is printed; the 150 s run of
-  vmachine_b200.learned.compare measured the MLP 0.072 +- 0.008 lower).
+- At equal wall time the trained MLP has a lower energy than the Pade-Jastrow trained
+  by the same engine, by more than 3 sigma: both frozen wave functions are evaluated
+  by brute-force Metropolis in FP64 on fresh walkers with every walker's series
+  blocked on the device (learned.evaluate_frozen), sigma the two blocked error bars
+  in quadrature.  The variances of the local energy are printed.
 Both factors run on the mixed-precision dot sweep.
-Energies are of the frozen wave functions, with error bars over walkers.
 """
+import math
+
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -19,7 +22,7 @@ BUDGET_S = 40.0
 
 def test_trained_network_gains():
     from vmachine_b200 import Engine
-    from vmachine_b200.learned import dot_config, evaluate, train
+    from vmachine_b200.learned import dot_config, evaluate, evaluate_frozen, train
     N, omega, W, steps = 20, 0.5, 2048, 800
     mlp_text = dot_config(N, omega, "mlpJastrow", W, steps, 3e-4)
     untrained = Engine(mlp_text)
@@ -27,12 +30,16 @@ def test_trained_network_gains():
     e0, s0, _ = evaluate(untrained, 2000, burn_steps=1000)
     untrained.close()
     eng, hist = train(mlp_text, BUDGET_S)
-    e_mlp, s_mlp, _ = evaluate(eng, 2000)
+    b_mlp = evaluate_frozen(eng, mlp_text, 2000, 1000)
     eng.close()
-    pade, _ = train(dot_config(N, omega, "padeJastrow", W, steps, 0.01), BUDGET_S)
-    e_pade, s_pade, _ = evaluate(pade, 2000)
+    pade_text = dot_config(N, omega, "padeJastrow", W, steps, 0.01)
+    pade, phist = train(pade_text, BUDGET_S)
+    b_pade = evaluate_frozen(pade, pade_text, 2000, 1000)
     pade.close()
-    print(f"untrained {e0:.4f}+-{s0:.4f}  trained MLP {e_mlp:.4f}+-{s_mlp:.4f} ({len(hist)} iterations)  "
-          f"Pade {e_pade:.4f}+-{s_pade:.4f}")
-    assert e_mlp < e0 - 5 * (s0 + s_mlp)
-    assert e_mlp < e_pade + 3 * (s_mlp + s_pade)
+    gap = b_pade["energy"] - b_mlp["energy"]
+    sigma = math.hypot(b_pade["error"], b_mlp["error"])
+    print(f"untrained {e0:.4f}+-{s0:.4f}  trained MLP {b_mlp['energy']:.4f}+-{b_mlp['error']:.4f} "
+          f"var {b_mlp['variance']:.3f} ({len(hist)} iterations)  Pade {b_pade['energy']:.4f}+-{b_pade['error']:.4f} "
+          f"var {b_pade['variance']:.3f} ({len(phist)} iterations)  gap {gap:.4f} = {gap / sigma:.1f} sigma")
+    assert b_mlp["energy"] < e0 - 5 * (s0 + b_mlp["error"])
+    assert gap > 3 * sigma

@@ -6,8 +6,7 @@
 // Lane l < n (n = N / 2 orbitals per spin block) owns particle l (spin up, row l of the
 // first inverse block) and particle n + l (spin down, row l of the second block).  For
 // those two particles it keeps, in registers, one pair (particle l, particle n + l) per
-// coordinate of: the positions, d ln det / dx, (d^2 det / dx^2) / det and the Pade
-// gradient.  The pair terms of a move (the moved particle against both of a lane's
+// coordinate of: the positions, d ln det / dx and the Pade gradient.  The pair terms of a move (the moved particle against both of a lane's
 // particles), the Jastrow gradient update and the kinetic energy are therefore packed
 // two-wide instructions on register operands.  Shared memory holds what the whole warp
 // reads at one index: the inverse blocks and, per coordinate, the position, the drift
@@ -22,8 +21,9 @@
 //      particle's block), the Pade / Coulomb pair terms of both own particles against the
 //      moved one, one reduce-scatter of the pair sums (which also carries the previous
 //      step's per-lane kinetic terms, so the kinetic energy costs no reduction of its own);
-//   3. accept: Sherman-Morrison through the row scales (below), the block's derivative
-//      vectors recomputed from the updated rows, the Pade gradient, the running sums;
+//   3. accept: Sherman-Morrison through the row scales (below), the block's gradient
+//      vectors d ln det / dx recomputed from the updated rows, the Pade gradient, the
+//      running sums;
 //   4. E_L and dlnPsi/dtheta of every step after burn-in (one step late: the kinetic sum of
 //      step s is the total carried by the reduce-scatter of step s + 1).
 //
@@ -38,19 +38,33 @@
 // row by R through its sigma alone, so the rank-1 pass updates every other row from a
 // row that nobody writes (no warp barrier between the reads and the writes).
 //
+// Laplacian of the determinants.  The kinetic energy needs only the sum over particles of
+// (d^2 det / dx^2) / det, and for Hermite orbitals that sum follows from the gradients:
+// with u = sqrt(2) x, hh_m'' = u hh_m' - m hh_m (He_m'' - u He_m' + m He_m = 0), so
+//   (d^2 det / dx_j^2) / det = 2 x_j d ln det / dx_j - 2 sum_i m0_i phi_i(r_j) Binv_ij
+// and summed over the particles of a block (sum_j phi_i(r_j) Binv_ij = 1) the second
+// terms give 2 sum_i (m0_i + m1_i), twice the sum of the occupied shells.  Each lane adds
+// 2 x.d ln det / dx minus its share of that constant, 4 (K - 1) / 3 per particle; the
+// per-particle second derivatives are written to the walker record once, at the end.
+//
 // Sums.  The running pair sums (Pade Laplacian, sum beta h^2, Coulomb) and sum x^2 are
 // FP64 per walker.  In the FP32 form the per-step changes go to FP32 partial sums that
-// are added to the FP64 values every 32 steps, and each lane's accumulator slot adds its
-// per-step sample, shifted by the walker's value at the start of the launch, to an FP32
-// partial sum folded into the lane's FP64 Neumaier accumulator every 32 steps.  The FP64
-// form adds to the FP64 sums and accumulators every step, as the staged sweep does.
+// are added to the FP64 values every 32 steps.  Its samples are taken 32 steps at a
+// time: every step leaves in shared memory its kinetic sum, the partial sums' values and
+// its accept / window / after-burn-in bits (three stores by single lanes), and every 32
+// steps lane i evaluates step i's energies and gradients, shifted by the walker's values
+// at the start of the launch, the warp sums the twelve moments, and each lane folds the
+// one of its accumulator slot into its FP64 Neumaier accumulator.  The FP64 form adds to
+// the FP64 sums and accumulators every step, as the staged sweep does.
 #pragma once
 
 namespace vmc {
 
-// Orbital order of the staged inverse rows: slot 2q holds orbital (a, b) and slot 2q + 1
-// orbital (b, a) of the q-th transposed pair (a < b, a + b < K, by a then b); the
-// diagonal orbitals (d, d), 2d < K, follow.  Per slot: the Hermite degrees along x (m0)
+// Orbital order of the staged inverse rows: slot 2q holds orbital (b, a) and slot 2q + 1
+// orbital (a, b) of the q-th transposed pair (a < b, a + b < K, by b then a); the
+// diagonal orbitals (d, d), 2d < K, follow.  (m0, m1) are the degrees along (x, y), so a
+// slot pair times (hh_b(x), hh_b(y)) gives the two orbitals' partial sums over the
+// larger index without exchanging the halves of a packed register pair.  Per slot: the Hermite degrees along x (m0)
 // and y (m1), the orbital's index in the record (the reference's order: shell s = m0 + m1,
 // then m1) and the staging scale sqrt(m0! m1!).
 struct PairTable {
@@ -72,12 +86,12 @@ template <int K> __host__ __device__ constexpr PairTable make_pair_table()
 {
     PairTable t{};
     int i = 0;
-    for (int a = 0; a < K; ++a)
-        for (int b = a + 1; a + b < K; ++b) {
-            t.m0[i] = a;
-            t.m1[i] = b;
-            t.m0[i + 1] = b;
-            t.m1[i + 1] = a;
+    for (int b = 1; b < K; ++b)
+        for (int a = 0; a < b && a + b < K; ++a) {
+            t.m0[i] = b;
+            t.m1[i] = a;
+            t.m0[i + 1] = a;
+            t.m1[i + 1] = b;
             i += 2;
         }
     t.np = i / 2;
@@ -134,14 +148,24 @@ template <> __device__ __forceinline__ double oconst<double>(const SweepArgs &a,
 #ifndef OWNER_SHM64
 #define OWNER_SHM64 1
 #endif
-#ifndef OWNER_UNIFORM_ACC
-#define OWNER_UNIFORM_ACC 1
-#endif
 
-constexpr int OWNER_WPB = 4;  // walkers (warps) per CTA
-// CTAs per SM the FP32 form is compiled for (its register budget: 65536 / (128 x this))
+// One walker (warp) per CTA, and the register budget of 20 resident warps per SM for
+// the FP32 form (5 per scheduler: 102 registers, 94 used without spills) and 12 for the
+// FP64 form.  The register file is split between the four schedulers, so occupancy
+// moves in steps of four warps; against 4-warp CTAs at 16 warps (128 registers), 20
+// one-warp CTAs ran the N = 56 sweep 11 % faster (1.62 against 1.46 x 10^9 walker-moves/s;
+// 4-warp CTAs at 96 or 80 registers spilled and ran at 1.47 and 1.13).  Shared memory:
+// 20 x (8.6 KB + the 1 KB every CTA reserves) for the FP32 form at N = 56.
+#ifndef OWNER_WALKERS_PER_CTA
+#define OWNER_WALKERS_PER_CTA 1
+#endif
+constexpr int OWNER_WPB = OWNER_WALKERS_PER_CTA;  // walkers (warps) per CTA
+// CTAs per SM each form is compiled for (register budget: 65536 / (32 OWNER_WPB x this))
 #ifndef OWNER_MIN_CTAS_F32
-#define OWNER_MIN_CTAS_F32 4
+#define OWNER_MIN_CTAS_F32 20
+#endif
+#ifndef OWNER_MIN_CTAS_F64
+#define OWNER_MIN_CTAS_F64 12
 #endif
 
 // FP64 values of the FP32 form that only the 32-step folds touch, kept in shared memory:
@@ -150,16 +174,23 @@ constexpr int OWNER_WPB = 4;  // walkers (warps) per CTA
 constexpr int OWNER_FOLD_DOUBLES = 72;
 enum : int { OF_ACCS = 0, OF_ACCC = 32, OF_LAPJ = 64, OF_BH2, OF_VINT, OF_SUMX2, OF_T0, OF_V0, OF_I0, OF_E0 };
 
+// Per step of a 32-step block, FP32 form: the partial sums (lap, sum x^2, V_int,
+// sum beta h^2) after the step, its kinetic sum and its bits
+constexpr int OWNER_STEP_BYTES = 16 + 4 + 4;
+enum : unsigned { SB_ACCEPT = 1u, SB_WINDOW = 2u, SB_SAMPLED = 4u };
+
 // Shared bytes per warp: the inverse blocks, then per coordinate the positions, drift
-// gradients and force cache, then the Pade pair masks and the fold values.
+// gradients and force cache, then the Pade pair masks, the fold values and (FP32) the
+// 32-step sample buffer.
 __host__ __device__ constexpr int owner_smem_per_warp(int K, int elem_bytes)
 {
     const int n = K * (K + 1) / 2, D = 4 * n;
-    return (2 * n * inv_row_stride(n, elem_bytes) + 3 * D) * elem_bytes + 2 * n * 8 + OWNER_FOLD_DOUBLES * 8;
+    return (2 * n * inv_row_stride(n, elem_bytes) + 3 * D) * elem_bytes + 2 * n * 8 + OWNER_FOLD_DOUBLES * 8 +
+           (elem_bytes == 4 ? 32 * OWNER_STEP_BYTES : 0);
 }
 
 template <typename T, int K, int FX>
-__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTAS_F32 : 3) owner_sweep_kernel(const SweepArgs a)
+__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTAS_F32 : OWNER_MIN_CTAS_F64) owner_sweep_kernel(const SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr PairTable PO = make_pair_table<K>();
@@ -187,6 +218,10 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
     T *xs = inv + 2 * n * IS, *gs = xs + D, *fcs = gs + D;
     unsigned long long *msk = reinterpret_cast<unsigned long long *>(fcs + D);
     double *fd = reinterpret_cast<double *>(msk + N);  // fold values (OF_*)
+    // FP32 form: the block's per-step records
+    float4 *sbd = reinterpret_cast<float4 *>(fd + OWNER_FOLD_DOUBLES);
+    float *sbk = reinterpret_cast<float *>(sbd + 32);
+    unsigned *sbf = reinterpret_cast<unsigned *>(sbk + 32);
 
     constexpr bool SHM = F32 && OWNER_SHM64;
     const T wa = oconst<T>(a, OC_WA), hdt = oconst<T>(a, OC_HDT), sdt = oconst<T>(a, OC_SDT);
@@ -222,14 +257,13 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
 #pragma unroll
                 for (int q = 0; q < IS / VE; ++q) vstore<T>(dst + q * VE, v + q * VE);
         }
-        T2 X[2], DD[2], SD[2], GJ[2];
+        T2 X[2], DD[2], GJ[2];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             const int ka = 2 * lc + c, kb = 2 * (n + lc) + c;
             const T z = T(0);
             X[c] = own ? two(rec[L.off_x + ka], rec[L.off_x + kb]) : two(z, z);
             DD[c] = own ? two(rec[L.off_dd + ka], rec[L.off_dd + kb]) : two(z, z);
-            SD[c] = own ? two(rec[L.off_sdd + ka], rec[L.off_sdd + kb]) : two(z, z);
             GJ[c] = own ? two(rec[L.off_gj + ka], rec[L.off_gj + kb]) : two(z, z);
         }
         for (int i = l; i < D; i += 32) {
@@ -254,15 +288,19 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
         T2 SIG = two(T(1), T(1));
 
         // drift gradient G = -omega alpha x + d ln det + Pade gradient of the own particles
-        // into shared memory, and this lane's kinetic terms (G^2 + d2det/det - dd^2)
+        // into shared memory, and this lane's kinetic terms: G^2 - dd^2 + the determinants'
+        // Laplacian as 2 x dd - 4 (K - 1) / 3 per particle (the Hermite identity above)
+        const T shell_share = T(4.0 * (K - 1) / 3.0);
+        const T2 kc2 = own ? two(-shell_share, -shell_share) : two(T(0), T(0));
+        const T2 two2 = two(T(2), T(2));
         auto publish = [&]() -> T {
-            T2 k2 = add2(SD[0], SD[1]);
+            T2 k2 = kc2;
             T2 G[2];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 G[c] = fma2(mwa2, X[c], add2(DD[c], GJ[c]));
                 k2 = fma2(G[c], G[c], k2);
-                k2 = fma2(two(-DD[c].x, -DD[c].y), DD[c], k2);
+                k2 = fma2(DD[c], fma2(two2, X[c], two(-DD[c].x, -DD[c].y)), k2);
             }
             if (own) {
                 reinterpret_cast<T2 *>(gs)[l] = two(G[0].x, G[1].x);
@@ -285,12 +323,6 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
         const double myref = l < 8 ? (eg == 0 ? E0 : eg == 1 ? T0 : eg == 2 ? V0 : I0) : E0;
         T cT = T(0), cV = T(0), cI = T(0), gA = T(0), gG = T(0);  // FP32 shifted bases at the fold
         T dlap = T(0), dbh2 = T(0), dvint = T(0), dsx2 = T(0);    // FP32 changes since the fold
-        T accf = T(0);
-        int ns = 0;
-        // FP32 form, uniform partial sums over the steps since the fold (every lane the
-        // same): (T, V_ext), (V_int, accepts), their squares (T, V_ext), (V_int, E), the
-        // windowed parameter gradients (alpha, gamma) and the same times E
-        T2 u_tv = two(T(0), T(0)), u_ia = u_tv, u_tv2 = u_tv, u_ie2 = u_tv, u_g = u_tv, u_eg = u_tv;
         if constexpr (SHM) {
             if (l == 0) {
                 fd[OF_LAPJ] = lapj;
@@ -321,28 +353,53 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                 gG = T(dgk * bh2);
             }
         };
-        auto fold = [&]() {
+        unsigned status = 0;
+        // the samples of a block's nb steps (FP32 form): lane i evaluates step i from its
+        // record, the warp sums (T, V_ext), (V_int, accepts), their squares (T, V_ext),
+        // (V_int, E), the windowed parameter gradients (alpha, gamma) and the same times
+        // E, and each lane adds its accumulator slot's value
+        auto fold = [&](int nb) {
             if constexpr (F32) {
-                T part, gsum;
-                if constexpr (OWNER_UNIFORM_ACC) {
-                    // this lane's slot from the uniform partials
-                    const T lin = eg == 0 ? u_tv.x + u_tv.y + u_ia.x : eg == 1 ? u_tv.x : eg == 2 ? u_tv.y : u_ia.x;
-                    const T sq = eg == 0 ? u_ie2.y : eg == 1 ? u_tv2.x : eg == 2 ? u_tv2.y : u_ie2.x;
-                    gsum = pk == 1 ? u_g.x : pk == 2 ? u_g.y : T(0);
-                    const T eg_ = pk == 1 ? u_eg.x : pk == 2 ? u_eg.y : T(0);
-                    part = lin;
-                    accf = l < 8 ? ((l & 1) ? sq : lin) : l == 8 ? u_ia.y : te ? eg_ : gsum;
-                    u_tv = u_ia = u_tv2 = u_ie2 = u_g = u_eg = two(T(0), T(0));
-                } else {
-                    part = __shfl_xor_sync(FULL, accf, 1);  // odd energy slots: the linear sum
-                    gsum = __shfl_sync(FULL, accf, te ? l - P.ep : l);
+                __syncwarp();
+                const unsigned fl = l < nb ? sbf[l] : 0u;
+                T2 u_tv = two(T(0), T(0)), u_ia = u_tv, u_tv2 = u_tv, u_ie2 = u_tv, u_g = u_tv, u_eg = u_tv;
+                if (fl & SB_SAMPLED) {
+                    const float4 d = sbd[l];
+                    const T Ts = fmaT(T(-0.5), sbk[l] + d.x, cT);
+                    const T Vs = fmaT(oconst<T>(a, OC_W2H), d.y, cV);
+                    const T Is = cI + d.z;
+                    const T Es = Ts + Vs + Is;
+                    const T wf = (fl & SB_WINDOW) ? T(1) : T(0);
+                    u_tv = two(Ts, Vs);
+                    u_ia = two(Is, (fl & SB_ACCEPT) ? T(1) : T(0));
+                    u_tv2 = mul2(u_tv, u_tv);
+                    u_ie2 = mul2(two(Is, Es), two(Is, Es));
+                    u_g = mul2(two(fmaT(oconst<T>(a, OC_MHOM), d.y, gA), fmaT(oconst<T>(a, OC_DGK), d.w, gG)), two(wf, wf));
+                    u_eg = mul2(two(Es, Es), u_g);
                 }
+                const int ns = __popc(__ballot_sync(FULL, (fl & SB_SAMPLED) != 0u));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    u_tv = add2(u_tv, two(__shfl_xor_sync(FULL, u_tv.x, o), __shfl_xor_sync(FULL, u_tv.y, o)));
+                    u_ia = add2(u_ia, two(__shfl_xor_sync(FULL, u_ia.x, o), __shfl_xor_sync(FULL, u_ia.y, o)));
+                    u_tv2 = add2(u_tv2, two(__shfl_xor_sync(FULL, u_tv2.x, o), __shfl_xor_sync(FULL, u_tv2.y, o)));
+                    u_ie2 = add2(u_ie2, two(__shfl_xor_sync(FULL, u_ie2.x, o), __shfl_xor_sync(FULL, u_ie2.y, o)));
+                    u_g = add2(u_g, two(__shfl_xor_sync(FULL, u_g.x, o), __shfl_xor_sync(FULL, u_g.y, o)));
+                    u_eg = add2(u_eg, two(__shfl_xor_sync(FULL, u_eg.x, o), __shfl_xor_sync(FULL, u_eg.y, o)));
+                }
+                // a NaN energy reaches the sum of E^2
+                if (u_ie2.y != u_ie2.y) status |= ST_NAN_ENERGY;
+                // this lane's slot
+                const T lin = eg == 0 ? u_tv.x + u_tv.y + u_ia.x : eg == 1 ? u_tv.x : eg == 2 ? u_tv.y : u_ia.x;
+                const T sq = eg == 0 ? u_ie2.y : eg == 1 ? u_tv2.x : eg == 2 ? u_tv2.y : u_ie2.x;
+                const T gsum = pk == 1 ? u_g.x : pk == 2 ? u_g.y : T(0);
+                const T eg_ = pk == 1 ? u_eg.x : pk == 2 ? u_eg.y : T(0);
+                const T part = lin;
+                const T accf = l < 8 ? ((l & 1) ? sq : lin) : l == 8 ? u_ia.y : te ? eg_ : gsum;
                 const double ref = SHM ? fd[l < 8 ? (eg == 0 ? OF_E0 : OF_T0 + eg - 1) : OF_E0] : myref;
                 double v = (double)accf;
                 if (l < 8) v += (l & 1) ? ns * ref * ref + 2.0 * ref * (double)part : ns * ref;
                 else if (te) v += ref * (double)gsum;
-                accf = T(0);
-                ns = 0;
                 // the FP32 running-sum changes into the FP64 sums
                 if constexpr (SHM) {
                     double s_ = fd[OF_ACCS + l], c_ = fd[OF_ACCC + l];
@@ -373,40 +430,12 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
         if constexpr (F32) fp32_bases();
 
         unsigned long long ctr = P.counter[w];
-        unsigned status = 0;
         // the step whose sample is pending (taken with the next step's reduce-scatter)
         bool pend = false, pend_acc = false, pend_win = false;
 
-        // E_L and dlnPsi/dtheta of the pending step from its kinetic sum ks
+        // FP64 form: E_L and dlnPsi/dtheta of the pending step from its kinetic sum ks
         auto sample = [&](T ks) {
-            if constexpr (F32) {
-                const T Ts = fmaT(T(-0.5), ks + dlap, cT);
-                const T Vs = fmaT(oconst<T>(a, OC_W2H), dsx2, cV);
-                const T Is = cI + dvint;
-                const T Es = Ts + Vs + Is;
-                if (Es != Es) status |= ST_NAN_ENERGY;
-                if constexpr (OWNER_UNIFORM_ACC) {
-                    const T ga = fmaT(oconst<T>(a, OC_MHOM), dsx2, gA), gg = fmaT(oconst<T>(a, OC_DGK), dbh2, gG);
-                    const T wf = pend_win ? T(1) : T(0);
-                    const T2 tv = two(Ts, Vs), ie = two(Is, Es);
-                    u_tv = add2(u_tv, tv);
-                    u_ia = add2(u_ia, two(Is, pend_acc ? T(1) : T(0)));
-                    u_tv2 = fma2(tv, tv, u_tv2);
-                    u_ie2 = fma2(ie, ie, u_ie2);
-                    const T2 G = mul2(two(ga, gg), two(wf, wf));
-                    u_g = add2(u_g, G);
-                    u_eg = fma2(two(Es, Es), G, u_eg);
-                    ++ns;
-                    return;
-                }
-                const T eb = eg == 0 ? Es : eg == 1 ? Ts : eg == 2 ? Vs : Is;
-                const T gl = pk == 1   ? fmaT(oconst<T>(a, OC_MHOM), dsx2, gA)
-                             : pk == 2 ? fmaT(oconst<T>(a, OC_DGK), dbh2, gG)
-                                       : T(0);
-                const T gq = pend_win ? (te ? Es * gl : gl) : T(0);
-                accf += l < 8 ? ((l & 1) ? eb * eb : eb) : l == 8 ? (pend_acc ? T(1) : T(0)) : gq;
-                ++ns;
-            } else {
+            if constexpr (!F32) {
                 const double lap = (double)ks + lapj - lapc;
                 const double ekin = -0.5 * lap, vext = w2h * sumx2, el = ekin + vext + vint;
                 if (el != el) status |= ST_NAN_ENERGY;
@@ -466,15 +495,17 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                 // ---- 2a. Slater: s_l = phi(r_p') . staged row l of block b (lane l), R = sigma_p s_pl
                 T sl, gl_ = T(0);
                 if constexpr (GREEN_Q && OWNER_PACK_DOT) {
-                    // packed: Qd[a] = (sum_b hh_b(y) v(a,b), sum_b hh_b(x) v(b,a)) over the
-                    // transposed pairs, s = sum_a (hh_a(x), hh_a(y)) . Qd[a] + the diagonals
+                    // packed: for the pair (a < b) in slots (b, a), (a, b),
+                    //   Qd[a] += (hh_b(x), hh_b(y)) * (v(b,a), v(a,b)),
+                    // a diagonal (d, d) adds hh_d(x) v to Qd[d].x, and
+                    //   s = sum_a hh_a(y) Qd[a].x + hh_a(x) Qd[a].y
+                    constexpr int QN = (K + 1) / 2;  // smaller indices of the pairs and diagonals
                     T2 H[K];
                     hermite_pe2<K, T>(two(sq2 * qx, sq2 * qy), H);
                     const T *row = inv + (b * n + lc) * IS;
-                    T2 Qd[K];
+                    T2 Qd[QN];
 #pragma unroll
-                    for (int m = 0; m < K; ++m) Qd[m] = two(T(0), T(0));
-                    T dsum = T(0);
+                    for (int m = 0; m < QN; ++m) Qd[m] = two(T(0), T(0));
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
                         T v[VE];
@@ -483,22 +514,22 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                         for (int e = 0; e < VE; e += 2) {
                             const int i = q * VE + e;
                             if (i < 2 * PO.np) {
-                                const int pa = PO.m0[i], pb = PO.m1[i];
-                                Qd[pa] = fma2(two(H[pb].y, H[pb].x), two(v[e], v[e + 1]), Qd[pa]);
+                                const int qa = PO.m1[i], qb = PO.m0[i];
+                                Qd[qa] = fma2(H[qb], two(v[e], v[e + 1]), Qd[qa]);
                             } else {
 #pragma unroll
                                 for (int t = 0; t < 2; ++t)
                                     if (i + t < n) {
                                         const int d = PO.m0[i + t];
-                                        dsum = fmaT(H[d].x * H[d].y, v[e + t], dsum);
+                                        Qd[d].x = fmaT(H[d].x, v[e + t], Qd[d].x);
                                     }
                             }
                         }
                     }
-                    T2 s2 = two(T(0), T(0));
+                    T s = T(0);
 #pragma unroll
-                    for (int m = 0; 2 * m + 2 <= K; ++m) s2 = fma2(H[m], Qd[m], s2);
-                    sl = s2.x + s2.y + dsum;
+                    for (int m = 0; m < QN; ++m) s = fmaT(H[m].x, Qd[m].y, fmaT(H[m].y, Qd[m].x, s));
+                    sl = s;
                 } else {
                 T hu[K], hv[K];
                 hermite_pe<K>(sq2 * qx, hu);
@@ -605,7 +636,11 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                 // one reduce-scatter: lane L ends with the total of value L / 4
                 const T tot = warp_reduce_scatter8<T, 32>(vals, l);
                 const T sum_ratio = __shfl_sync(FULL, tot, 0);
-                if (pend) sample(__shfl_sync(FULL, tot, 24));  // E_L of the previous step
+                if constexpr (F32) {
+                    if (pend && l == 24) sbk[slot - 1] = tot;  // the previous step's kinetic sum
+                } else {
+                    if (pend) sample(__shfl_sync(FULL, tot, 24));  // E_L of the previous step
+                }
                 pend = false;
 
                 // ---- 2c/2d. ratio, Green's ratio, accept
@@ -679,7 +714,7 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                     }
                     // Sherman-Morrison on block b (slaterdeterminant.cpp:165-175) through the
                     // row scales: row l += t_l row p with t_l = -s_l sigma_p / R (staged
-                    // rows), sigma_p /= R; then the block's derivative vectors
+                    // rows), sigma_p /= R; then the block's gradient vectors
                     // (slaterdeterminant.cpp:155-163) from the updated rows
                     const T sig_p = __shfl_sync(FULL, sig_l, pl);
                     const T rinv = Fs::rcp(R);
@@ -691,16 +726,20 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                     T *rowj = inv + (b * n + lc) * IS;
                     const T *rowp = inv + (b * n + pl) * IS;
                     const bool store = own && !mine;
-                    T gx, gy2, sx, sy;
+                    T gx, gy2;
                     if constexpr (OWNER_PACK_ACC) {
-                        // packed: with Hj[m] = (hh_m(x), hh_m(y)) of the lane's particle and a
-                        // staged pair S = (v(a,b), v(b,a)):
-                        //   Q[a] = (P0[a], P1[a]) += (hh_b(y), hh_b(x)) . S
-                        //   R[b] = (P1[b], P0[b]) += (hh_a(x), hh_a(y)) . S
-                        // where P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
-                        constexpr int QN = (K + 1) / 2;  // first indices of the pairs and diagonals
+                        // packed, with Hj[m] = (hh_m(x), hh_m(y)) of the lane's particle, its
+                        // swaps Hs[a] = (hh_a(y), hh_a(x)), P0[m0] = sum_m1 hh_m1(y) v(m0, m1)
+                        // and P1[m1] = sum_m0 hh_m0(x) v(m0, m1): for the pair (a < b) with
+                        // S = (v(b,a), v(a,b)),
+                        //   Q[a] = (P1[a], P0[a]) += Hj[b] * S,  Rb[b] = (P0[b], P1[b]) += Hs[a] * S,
+                        // and a diagonal (d, d) adds Hj[d] * (v, v) to Q[d]
+                        constexpr int QN = (K + 1) / 2;
                         T2 Hj[K];
                         hermite_pe2<K, T>(two(ux, uy), Hj);
+                        T2 Hs[QN];
+#pragma unroll
+                        for (int m = 0; m < QN; ++m) Hs[m] = two(Hj[m].y, Hj[m].x);
                         T2 Q[QN], Rb[K];
 #pragma unroll
                         for (int m = 0; m < QN; ++m) Q[m] = two(T(0), T(0));
@@ -722,35 +761,28 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                             for (int e = 0; e < VE; e += 2) {
                                 const int i = q * VE + e;
                                 if (i < 2 * PO.np) {
-                                    const int pa = PO.m0[i], pb = PO.m1[i];
+                                    const int qa = PO.m1[i], qb = PO.m0[i];
                                     const T2 S = two(vv[e], vv[e + 1]);
-                                    Q[pa] = fma2(two(Hj[pb].y, Hj[pb].x), S, Q[pa]);
-                                    Rb[pb] = fma2(Hj[pa], S, Rb[pb]);
+                                    Q[qa] = fma2(Hj[qb], S, Q[qa]);
+                                    Rb[qb] = fma2(Hs[qa], S, Rb[qb]);
                                 } else {
 #pragma unroll
                                     for (int t = 0; t < 2; ++t)
                                         if (i + t < n) {
                                             const int d = PO.m0[i + t];
-                                            Q[d] = fma2(two(Hj[d].y, Hj[d].x), two(vv[e + t], vv[e + t]), Q[d]);
+                                            Q[d] = fma2(Hj[d], two(vv[e + t], vv[e + t]), Q[d]);
                                         }
                                 }
                             }
                         }
-                        // d/dx: sum_m hh_{m-1}(x) P0[m], d/dy: sum_m hh_{m-1}(y) P1[m]; the second
-                        // derivatives with hh_{m-2}
-                        T2 G1 = two(T(0), T(0)), G2 = G1, S1 = G1, S2 = G1;
+                        // d/dx = sum_m hh_{m-1}(x) P0[m], d/dy = sum_m hh_{m-1}(y) P1[m]
+                        T2 GR = two(T(0), T(0)), GQ = GR;
 #pragma unroll
-                        for (int m = 1; m < QN; ++m) G1 = fma2(Hj[m - 1], Q[m], G1);
+                        for (int m = 1; m < K; ++m) GR = fma2(Hj[m - 1], Rb[m], GR);
 #pragma unroll
-                        for (int m = 1; m < K; ++m) G2 = fma2(two(Hj[m - 1].y, Hj[m - 1].x), Rb[m], G2);
-#pragma unroll
-                        for (int m = 2; m < QN; ++m) S1 = fma2(Hj[m - 2], Q[m], S1);
-#pragma unroll
-                        for (int m = 2; m < K; ++m) S2 = fma2(two(Hj[m - 2].y, Hj[m - 2].x), Rb[m], S2);
-                        gx = G1.x + G2.y;
-                        gy2 = G1.y + G2.x;
-                        sx = S1.x + S2.y;
-                        sy = S1.y + S2.x;
+                        for (int m = 1; m < QN; ++m) GQ = fma2(Hs[m - 1], Q[m], GQ);
+                        gx = GR.x + GQ.y;
+                        gy2 = GR.y + GQ.x;
                     } else {
                         T au[K], av[K];
                         hermite_pe<K>(ux, au);
@@ -779,49 +811,48 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                                 }
                             }
                         }
-                        gx = gy2 = sx = sy = T(0);
+                        gx = gy2 = T(0);
 #pragma unroll
                         for (int m = 1; m < K; ++m) {
                             gx = fmaT(au[m - 1], P0[m], gx);
                             gy2 = fmaT(av[m - 1], P1[m], gy2);
                         }
-#pragma unroll
-                        for (int m = 2; m < K; ++m) {
-                            sx = fmaT(au[m - 2], P0[m], sx);
-                            sy = fmaT(av[m - 2], P1[m], sy);
-                        }
                     }
                     {
                         // lanes without particles keep zeros
-                        const T g1 = own ? sig_new * sq2 : T(0), g2s = own ? sig_new * T(2) : T(0);
+                        const T g1 = own ? sig_new * sq2 : T(0);
                         if (b) {
                             DD[0].y = g1 * gx;
                             DD[1].y = g1 * gy2;
-                            SD[0].y = g2s * sx;
-                            SD[1].y = g2s * sy;
                         } else {
                             DD[0].x = g1 * gx;
                             DD[1].x = g1 * gy2;
-                            SD[0].x = g2s * sx;
-                            SD[1].x = g2s * sy;
                         }
                     }
                     kp = publish();
                     __syncwarp();
                 }
                 // ---- 4. this step's sample, taken with the next step's reduce-scatter
-                if (it_step >= a.burn_in) {
+                const bool sampled = it_step >= a.burn_in, win = it_step > a.win_lo && it_step < a.win_hi;
+                if (sampled) {
                     pend = true;
                     pend_acc = accept;
-                    pend_win = it_step > a.win_lo && it_step < a.win_hi;
+                    pend_win = win;
+                }
+                if constexpr (F32) {
+                    if (l == 0) {
+                        sbd[slot] = make_float4(dlap, dsx2, dvint, dbh2);
+                        sbf[slot] = (sampled ? SB_SAMPLED : 0u) | (accept ? SB_ACCEPT : 0u) | (win ? SB_WINDOW : 0u);
+                    }
                 }
             }
             if constexpr (F32) {
                 if (pend) {  // the block's last step: its kinetic sum by a reduction of its own
-                    sample(seg_sum<32>(kp));
+                    const T ks = seg_sum<32>(kp);
+                    if (l == 0) sbk[s_end - 1 - s0] = ks;
                     pend = false;
                 }
-                fold();
+                fold(s_end - s0);
             }
         }
         if (pend) sample(seg_sum<32>(kp));
@@ -849,10 +880,35 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                 rec[L.off_x + kb] = X[c].y;
                 rec[L.off_dd + ka] = DD[c].x;
                 rec[L.off_dd + kb] = DD[c].y;
-                rec[L.off_sdd + ka] = SD[c].x;
-                rec[L.off_sdd + kb] = SD[c].y;
                 rec[L.off_gj + ka] = GJ[c].x;
                 rec[L.off_gj + kb] = GJ[c].y;
+            }
+            // (d^2 det / dx^2) / det of both own particles from their final rows:
+            // 2 sigma sum_m hh_{m-2}(x) P0[m] and 2 sigma sum_m hh_{m-2}(y) P1[m]
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                T au[K], av[K];
+                hermite_pe<K>(sq2 * (h ? X[0].y : X[0].x), au);
+                hermite_pe<K>(sq2 * (h ? X[1].y : X[1].x), av);
+                const T *src = inv + (h * n + l) * IS;
+                T P0[K], P1[K];
+#pragma unroll
+                for (int m = 0; m < K; ++m) P0[m] = P1[m] = T(0);
+#pragma unroll
+                for (int i = 0; i < n; ++i) {
+                    const T v = src[i];
+                    P0[PO.m0[i]] = fmaT(av[PO.m1[i]], v, P0[PO.m0[i]]);
+                    P1[PO.m1[i]] = fmaT(au[PO.m0[i]], v, P1[PO.m1[i]]);
+                }
+                T sx = T(0), sy = T(0);
+#pragma unroll
+                for (int m = 2; m < K; ++m) {
+                    sx = fmaT(au[m - 2], P0[m], sx);
+                    sy = fmaT(av[m - 2], P1[m], sy);
+                }
+                const T g2 = T(2) * (h ? SIG.y : SIG.x);
+                rec[L.off_sdd + 2 * (h * n + l)] = g2 * sx;
+                rec[L.off_sdd + 2 * (h * n + l) + 1] = g2 * sy;
             }
         }
         for (int i = l; i < D; i += 32) rec[L.off_fc + i] = fcs[i];

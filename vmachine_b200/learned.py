@@ -8,6 +8,7 @@ budget each, then evaluated with their parameters frozen: every walker samples
 energies over sqrt(walkers) (the walkers are independent Markov chains).  The
 variational principle decides: the lower energy at comparable error bars wins.
 """
+import re
 import time
 
 import numpy as np
@@ -52,28 +53,66 @@ def evaluate(eng, eval_steps, burn_steps=200):
     return float(np.mean(e)), float(np.std(e, ddof=1) / np.sqrt(len(e))), int(info.n_walkers)
 
 
-def evaluate_blocked(eng, eval_steps, burn_steps=200):
+def evaluate_blocked(eng, eval_steps, burn_steps=200, fresh_seed=None):
     """The frozen wave function with every walker's local-energy series blocked on the
     device (vmc_blocking: the reference's Blocker per walker, include/block/blocker.cpp):
     the energy with its independent-chains error bar (each walker's own blocked
     variance of its mean, summed over walkers / W^2, so a walker that sits near a node
     for the whole pass weighs by its own fluctuation, not by its distance from the
     others), the concatenated-series Blocker result, and the variance of the local
-    energy, the variational principle's second criterion."""
+    energy, the variational principle's second criterion.
+
+    fresh_seed: start from new walkers drawn from the configured initial state with
+    this seed (then burn_steps of equilibration) instead of the training's walkers.  A
+    walker that importance sampling has left stuck next to a node of the determinant
+    (a persistent configuration: its drift overshoots and nearly every move is
+    rejected, with local energies of thousands) would otherwise carry over from
+    training and dominate both the mean and the variance.
+    flagged_walkers counts walkers whose status bits were set during the evaluation
+    (2: a NaN acceptance weight, the mark of such a configuration)."""
+    if fresh_seed is not None:
+        eng.init_walkers(None, seed=fresh_seed)
     eng.sample(10 ** 6, burn_steps + 1, burn_steps)
     b = eng.blocking(eval_steps + 1, 1)
     s, _, _ = eng.sample(10 ** 6, eval_steps + 1, 1)
     var = s.energy2 / s.n_samples - (s.energy / s.n_samples) ** 2
+    e = eng.walker_energies()
     return {"energy": b.energy_walkers.mean, "error": b.energy_walkers.std_error,
             "energy_blocker": b.energy.mean, "error_blocker": b.energy.std_error,
-            "variance": float(var), "samples_per_walker": int(b.samples_per_walker)}
+            "variance": float(var), "samples_per_walker": int(b.samples_per_walker),
+            "walker_median": float(np.median(e)), "walker_max_deviation": float(np.max(np.abs(e - np.median(e)))),
+            "flagged_walkers": int(np.count_nonzero(eng.status()))}
+
+
+def evaluate_frozen(eng, text, eval_steps=4000, burn_steps=2000, step_length=1.0, seed=1007):
+    """The trained parameters of `eng` evaluated by brute-force Metropolis in FP64 on
+    fresh walkers (a second engine from `text` with sampling: bruteForce,
+    stepLength: step_length, precision: fp64), every walker's series blocked
+    (evaluate_blocked).  The expectation value of a frozen wave function does not
+    depend on the sampler, and brute-force moves carry no drift: importance sampling
+    at dt = 0.01 leaves a few walkers stuck next to a node of the determinant (the
+    drift, about 2 / distance there, throws every proposal far off, and nearly every
+    move is rejected), and such a walker's mean local energy, in the thousands, would
+    dominate the estimate and its variance."""
+    t = re.sub(r"^sampling:.*$", "sampling: bruteForce", text, flags=re.M)
+    t = re.sub(r"^stepLength:.*$", f"stepLength: {step_length!r}", t, flags=re.M)
+    t = re.sub(r"^precision:.*$", "precision: fp64", t, flags=re.M)
+    ev = Engine(t)
+    try:
+        ev.set_parameters(eng.parameters())
+        return evaluate_blocked(ev, eval_steps, burn_steps, fresh_seed=seed)
+    finally:
+        ev.close()
 
 
 def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps=4000,
-            lr_pade=0.01, lr_mlp=3e-4, seed=7, mlp_iterations=None):
+            lr_pade=0.01, lr_mlp=3e-4, seed=7, mlp_iterations=None, eval_burn=2000):
     """Pade against MLP Jastrow at equal wall time: both train for budget_s seconds,
     or, with mlp_iterations, the MLP trains for that many iterations and the Pade
-    factor for the MLP's wall time; then each frozen wave function is evaluated."""
+    factor for the MLP's wall time; then each frozen wave function is evaluated, on
+    the training's walkers ("energy", "error": walker means) and blocked on fresh
+    walkers after eval_burn steps of equilibration ("blocked"), and by brute-force
+    Metropolis in FP64 on fresh walkers ("frozen", evaluate_frozen)."""
     out = {"system": f"2D dot N={N} omega={omega}", "walkers": walkers, "steps_per_iteration": steps,
            "budget_s": budget_s, "eval_steps_per_walker": eval_steps}
     runs = (("pade", "padeJastrow", lr_pade), ("mlp", "mlpJastrow", lr_mlp))
@@ -90,7 +129,8 @@ def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps
         energy, err, W = evaluate(eng, eval_steps)
         out[name] = {"iterations": len(hist), "train_seconds": hist[-1][0], "lr": lr,
                      "last_iteration_energy": hist[-1][1], "energy": energy, "error": err,
-                     "blocked": evaluate_blocked(eng, eval_steps)}
+                     "blocked": evaluate_blocked(eng, eval_steps, eval_burn, fresh_seed=seed + 1000),
+                     "frozen": evaluate_frozen(eng, text, eval_steps, eval_burn, seed=seed + 1000)}
         eng.close()
     d = out["pade"]["energy"] - out["mlp"]["energy"]
     out["gain"] = d
@@ -99,6 +139,10 @@ def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps
     out["gain_blocked"] = bp["energy"] - bm["energy"]
     out["gain_blocked_sigma"] = out["gain_blocked"] / np.hypot(bp["error"], bm["error"])
     out["variance_ratio"] = bm["variance"] / bp["variance"]
+    fp, fm = out["pade"]["frozen"], out["mlp"]["frozen"]
+    out["gain_frozen"] = fp["energy"] - fm["energy"]
+    out["gain_frozen_sigma"] = out["gain_frozen"] / np.hypot(fp["error"], fm["error"])
+    out["variance_ratio_frozen"] = fm["variance"] / fp["variance"]
     return out
 
 
@@ -144,12 +188,13 @@ def main(argv=None):
     c.add_argument("--iterations", type=int, default=0,
                    help="train the MLP for this many iterations and the Pade factor for the same wall time")
     c.add_argument("--lr-mlp", type=float, default=3e-4)
+    c.add_argument("--lr-pade", type=float, default=0.01)
     a = ap.parse_args(argv)
     if a.cmd == "speed":
         print(json.dumps(sweep_speed(a.walkers, a.steps, tensor_cores=not a.cuda_cores, precision=a.precision)))
     else:
         print(json.dumps(compare(walkers=a.walkers, steps=a.steps, budget_s=a.budget, lr_mlp=a.lr_mlp,
-                                 mlp_iterations=a.iterations or None)))
+                                 lr_pade=a.lr_pade, mlp_iterations=a.iterations or None)))
 
 
 if __name__ == "__main__":
