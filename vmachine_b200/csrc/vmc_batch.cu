@@ -322,6 +322,9 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
                 return reject(VMC_E_UNSUPPORTED, "more than " + std::to_string(BATCH_MAX_GEN) + " general-path systems");
             kind = BATCH_GENERAL;
             b->gen_of.push_back(b->n_gen++);
+            // the batch runs its general-path walkers in FP64 (its kernels call the FP64
+            // sweep, and general systems take no refresh there), whatever the precision
+            e->gen.f32 = 0;
         } else {
             const bool dot = e->dim == 2 && e->K >= 1 && e->K <= 7 &&
                              (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED);

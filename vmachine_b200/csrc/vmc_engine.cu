@@ -277,8 +277,10 @@ int sweep_smem_per_warp(const vmc_engine *e)
 int run_rebuild(vmc_engine *e, int mode, double *drift)
 {
     if (e->general) {
-        CUDA_TRY(gen_launch_state(make_params(e), e->gen, mode == RB_INIT ? GEN_INIT : GEN_STATE, nullptr,
-                                  nullptr, nullptr, nullptr, e->stream));
+        // the FP32 sweep's refresh re-inverts in FP64; otherwise the FP64 inverse is
+        // carried and only the evaluation is redone
+        const int gm = mode == RB_INIT ? GEN_INIT : (e->gen.f32 && mode == RB_REFRESH) ? GEN_REFRESH : GEN_STATE;
+        CUDA_TRY(gen_launch_state(make_params(e), e->gen, gm, nullptr, nullptr, nullptr, nullptr, e->stream));
         return VMC_OK;
     }
     RebuildArgs a{};
@@ -585,11 +587,18 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
         e->gen.mlp_tc = c.mlp_tc ? 1 : 0;
     }
     if (general) {
-        if (e->precision == VMC_PRECISION_MIXED)
-            return reject("mixed precision covers Gaussian, Hermite Slater, Pade and hydrogen-like "
-                          "systems; this system runs with precision: fp64");
         const std::string why = gen_configure(c, e->E, e->Pmax, e->gen);
         if (!why.empty()) return reject(why);
+        // mixed precision on the general path: the compiled atom form (3D hydrogen-orbital
+        // Slater determinants with SimpleJastrow / Pade), FP32 sweeps between FP64
+        // re-inversions
+        if (e->precision == VMC_PRECISION_MIXED) {
+            if (e->gen.variant != GV_ATOM)
+                return reject("mixed precision covers the dots, hydrogen-like systems and the atoms' "
+                              "hydrogen-orbital Slater x SimpleJastrow / Pade form; this system runs with "
+                              "precision: fp64");
+            e->gen.f32 = 1;
+        }
         e->n_orb = e->gen.n;
         e->nacc_dev = 0;  // set below from the active parameters
         for (int i = 0; i < e->E; ++i)
@@ -611,7 +620,8 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     if (e->steps_per_walker < 1) return reject("numSteps smaller than numWalkers");
     e->burn_in = (int)(e->steps_per_walker * c.eq_fraction);
     e->batches = c.optimization == "adam" ? 10 : 1;  // adam.h:15, gradientdescent.h:13
-    e->elem_bytes = e->precision == VMC_PRECISION_MIXED ? 4 : 8;
+    // the general path keeps its record in FP64 (its FP32 sweep stages it in FP32)
+    e->elem_bytes = e->precision == VMC_PRECISION_MIXED && !general ? 4 : 8;
     e->L = make_layout(e->N, e->dim, e->n_orb, (int)e->elem_bytes);
     if (general) {  // positions first in the general record (vmc_general.hpp)
         e->L.off_x = 0;
@@ -646,7 +656,8 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     // auto: start at 4 D steps (at least 512) and let the drift test tune it
     e->refresh_interval = c.refresh_interval >= 0 ? c.refresh_interval
                           : (e->precision == VMC_PRECISION_MIXED ? std::max(4 * e->D, 512) : 0);
-    e->refresh_auto = c.refresh_interval < 0 && e->precision == VMC_PRECISION_MIXED;
+    // the general path's refresh measures no drift: its cadence stays as configured
+    e->refresh_auto = c.refresh_interval < 0 && e->precision == VMC_PRECISION_MIXED && !general;
     e->seed = c.have_seed ? (unsigned long long)c.seed : 0x5eedULL;
 
     int rc;

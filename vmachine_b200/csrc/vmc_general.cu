@@ -25,8 +25,9 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
     double *rec = reinterpret_cast<double *>(P.state) + (size_t)w * g.rec;
     unsigned long long *mask = P.mask + (size_t)w * P.N;
     unsigned status = 0;
-    if (mode == GEN_INIT) {
+    if (mode == GEN_INIT)
         for (int j = lane; j < P.N; j += 32) mask[j] = ~0ull;
+    if (mode != GEN_STATE) {
         if (P.flags & F_SLATER) status = gen_invert(P, g, dim, rec, inv_area + (size_t)wib * g.n * 2 * g.n, lane);
         __syncwarp();
     }
@@ -42,11 +43,11 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_state_kernel(const Params P,
 
 // G walkers per warp (compiled forms only): each takes a 32 / G-lane segment, a
 // GEN_SCR / G slice of the warp's scratch and its own staging area.
-template <bool TC, int GV, int G = 1>
+template <bool TC, int GV, int G = 1, typename R = double>
 __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs a, const GenParams g)
 {
     extern __shared__ __align__(16) double gsm[];
-    __shared__ double scratch[GEN_WPB][GEN_SCR];
+    __shared__ R scratch[GEN_WPB][GEN_SCR];
     __shared__ float pre[GEN_WPB][3 * 32];  // TC: u, du/dr, d2u/dr2 of each partner of the proposal
     __shared__ __align__(8) unsigned long long tc_bar;
     __shared__ uint32_t tc_slot;
@@ -62,9 +63,11 @@ __global__ void __launch_bounds__(32 * GEN_WPB) gen_sweep_kernel(const SweepArgs
     if (TC) tc_ready(tc, &tc_slot);
     const bool active = w < P.W;
     if (!TC && !active) return;
-    const int nst = gen_stage_doubles(g, P.nacc);  // 0 with the MLP (gsm holds its weights)
-    gen_sweep_walker<TC, GV, 32 / G>(a, a.steps, a.step_offset, g, w, active, scratch[wib] + seg * (GEN_SCR / G), mw,
-                                     tc, pre[wib], nst ? gsm + (size_t)(wib * G + seg) * nst : nullptr);
+    const int nst = gen_stage_bytes(g, P.nacc, (int)sizeof(R));  // 0 with the MLP (gsm holds its weights)
+    R *stage = nst ? reinterpret_cast<R *>(reinterpret_cast<unsigned char *>(gsm) + (size_t)(wib * G + seg) * nst)
+                   : nullptr;
+    gen_sweep_walker<TC, GV, 32 / G, R>(a, a.steps, a.step_offset, g, w, active, scratch[wib] + seg * (GEN_SCR / G),
+                                        mw, tc, pre[wib], stage);
     if (TC) tc_teardown(tc, wib);
 }
 
@@ -726,7 +729,7 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
                              double *o_pg, double *o_en, cudaStream_t st)
 {
     const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) +
-                        (mode == GEN_INIT ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0);
+                        (mode != GEN_STATE ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0);
     cudaError_t e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     gen_state_kernel<<<(P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(P, g, mode, o_grad, o_lap, o_pg,
@@ -741,16 +744,25 @@ cudaError_t gen_launch_sweep(const SweepArgs &a, const GenParams &g, cudaStream_
     // four walkers per warp for the small atoms (not while sampling densities, whose
     // histogram code takes a whole warp per walker)
     const int G = atom && g.seg == 4 && a.dens_bins == 0 ? 4 : 1;
+    // the FP32 sweep: the compiled atom form with its record staged (every atom's is)
+    const bool f32 = g.f32 && atom && gen_stage_doubles(g, a.P.nacc) > 0;
+    if (g.f32 && !f32) return cudaErrorInvalidConfiguration;
     const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) + (tc ? TC_SMEM : 0) +
-                        (size_t)GEN_WPB * G * gen_stage_doubles(g, a.P.nacc) * sizeof(double);
-    const void *fn = tc       ? (const void *)gen_sweep_kernel<true, GV_ANY>
-                     : G == 4 ? (const void *)gen_sweep_kernel<false, GV_ATOM, 4>
-                     : atom   ? (const void *)gen_sweep_kernel<false, GV_ATOM>
-                              : (const void *)gen_sweep_kernel<false, GV_ANY>;
+                        (size_t)GEN_WPB * G * gen_stage_bytes(g, a.P.nacc, f32 ? 4 : 8);
+    const void *fn = tc            ? (const void *)gen_sweep_kernel<true, GV_ANY>
+                     : f32 && G == 4 ? (const void *)gen_sweep_kernel<false, GV_ATOM, 4, float>
+                     : f32           ? (const void *)gen_sweep_kernel<false, GV_ATOM, 1, float>
+                     : G == 4        ? (const void *)gen_sweep_kernel<false, GV_ATOM, 4>
+                     : atom          ? (const void *)gen_sweep_kernel<false, GV_ATOM>
+                                     : (const void *)gen_sweep_kernel<false, GV_ANY>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned grid = (a.P.W + GEN_WPB * G - 1) / (GEN_WPB * G);
-    if (tc)
+    if (f32 && G == 4)
+        gen_sweep_kernel<false, GV_ATOM, 4, float><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
+    else if (f32)
+        gen_sweep_kernel<false, GV_ATOM, 1, float><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
+    else if (tc)
         gen_sweep_kernel<true, GV_ANY><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);
     else if (G == 4)
         gen_sweep_kernel<false, GV_ATOM, 4><<<grid, 32 * GEN_WPB, smem, st>>>(a, g);

@@ -1,5 +1,6 @@
 // General walker path (vmc_general.cu): FP64 kernels for every wave-function
-// element, used when a system has SimpleJastrow, RBM or hydrogen-orbital parts.
+// element, used when a system has SimpleJastrow, RBM or hydrogen-orbital parts, and an
+// FP32 sweep of the compiled atom form for mixed precision.
 #pragma once
 #include <string>
 
@@ -9,7 +10,10 @@
 namespace vmc {
 
 enum : int { BASIS_HERMITE = 1, BASIS_HYDROGEN = 2 };
-enum : int { GEN_INIT = 0, GEN_STATE = 1 };
+// GEN_INIT: fresh walkers (masks, inverse, evaluation, force cache); GEN_STATE:
+// evaluation; GEN_REFRESH: FP64 re-inversion from the positions and evaluation (the
+// refresh of the atoms' FP32 sweep)
+enum : int { GEN_INIT = 0, GEN_STATE = 1, GEN_REFRESH = 2 };
 // Compiled variants of the general path: GV_ANY takes every element, basis and
 // dimension at run time; GV_ATOM is the atoms' form (3D, a Slater determinant of
 // hydrogen orbitals with SimpleJastrow and/or Pade-Jastrow) with the dimension and the
@@ -38,6 +42,7 @@ struct GenParams {
     int mlp_tc;                 // MLP sweep with the second layer on the tensor cores
     int variant;                // GV_*: the compiled sweep that takes this system
     int seg;                    // walkers per warp of the sweep (4: atoms of at most 4 electrons)
+    int f32;                    // the sweep in FP32 (mixed precision, compiled atom form only)
     unsigned char orb[32][3];   // Hermite degrees (m0, m1, m2) or hydrogen (n, l, m + 1)
 };
 
