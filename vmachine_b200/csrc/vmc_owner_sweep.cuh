@@ -672,163 +672,172 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
 
                 if (accept) {
                     // ---- 3. state update
-                    const bool mine = l == pl;
-                    if (adim == 0) {
-                        if (mine) X[0] = b ? two(X[0].x, xn) : two(xn, X[0].y);
-                    } else {
-                        if (mine) X[1] = b ? two(X[1].x, xn) : two(xn, X[1].y);
-                    }
-                    if (l == 0) {
-                        xs[k] = xn;
-                        fcs[k] = Fn;
-                    }
-                    // running sums (the pair totals sit in lanes 4, 8, 12; the new
-                    // gradient of the moved particle in lanes 16, 20)
-                    const T tl = __shfl_sync(FULL, tot, 4), tb = __shfl_sync(FULL, tot, 8);
-                    const T tv = __shfl_sync(FULL, tot, 12);
-                    const T tgx = __shfl_sync(FULL, tot, 16), tgy = __shfl_sync(FULL, tot, 20);
-                    if constexpr (F32) {
-                        dlap += tl;
-                        dbh2 += tb;
-                        dvint += tv;
-                        dsx2 += (xn - xo) * (xn + xo);
-                    } else {
-                        sumx2 += (double)xn * (double)xn - (double)xo * (double)xo;
-                        lapj += (double)tl;
-                        bh2 += (double)tb;
-                        vint += (double)tv;
-                    }
-                    // Pade gradients: partners by their change, the moved particle anew
-                    GJ[0] = add2(GJ[0], gdx);
-                    GJ[1] = add2(GJ[1], gdy);
-                    if (mine) {
-                        GJ[0] = b ? two(GJ[0].x, tgx) : two(tgx, GJ[0].y);
-                        GJ[1] = b ? two(GJ[1].x, tgy) : two(tgy, GJ[1].y);
-                    }
-                    if constexpr (STALE) {
-                        if (!allcur) {
-                            if (own && l != p) msk[l] |= 1ull << p;
-                            if (own && n + l != p) msk[n + l] |= 1ull << p;
-                            if (mine) msk[p] = ~0ull;
-                        }
-                    }
-                    // Sherman-Morrison on block b (slaterdeterminant.cpp:165-175) through the
-                    // row scales: row l += t_l row p with t_l = -s_l sigma_p / R (staged
-                    // rows), sigma_p /= R; then the block's gradient vectors
-                    // (slaterdeterminant.cpp:155-163) from the updated rows
-                    const T sig_p = __shfl_sync(FULL, sig_l, pl);
-                    const T rinv = Fs::rcp(R);
-                    const T tcoef = (own && !mine) ? -(sl * sig_p * rinv) : T(0);
-                    const T sig_new = mine ? sig_l * rinv : sig_l;
-                    if (b) SIG.y = sig_new;
-                    else SIG.x = sig_new;
-                    const T ux = sq2 * (b ? X[0].y : X[0].x), uy = sq2 * (b ? X[1].y : X[1].x);
-                    T *rowj = inv + (b * n + lc) * IS;
-                    const T *rowp = inv + (b * n + pl) * IS;
-                    const bool store = own && !mine;
-                    T gx, gy2;
-                    if constexpr (OWNER_PACK_ACC) {
-                        // packed, with Hj[m] = (hh_m(x), hh_m(y)) of the lane's particle, its
-                        // swaps Hs[a] = (hh_a(y), hh_a(x)), P0[m0] = sum_m1 hh_m1(y) v(m0, m1)
-                        // and P1[m1] = sum_m0 hh_m0(x) v(m0, m1): for the pair (a < b) with
-                        // S = (v(b,a), v(a,b)),
-                        //   Q[a] = (P1[a], P0[a]) += Hj[b] * S,  Rb[b] = (P0[b], P1[b]) += Hs[a] * S,
-                        // and a diagonal (d, d) adds Hj[d] * (v, v) to Q[d]
-                        constexpr int QN = (K + 1) / 2;
-                        T2 Hj[K];
-                        hermite_pe2<K, T>(two(ux, uy), Hj);
-                        T2 Hs[QN];
-#pragma unroll
-                        for (int m = 0; m < QN; ++m) Hs[m] = two(Hj[m].y, Hj[m].x);
-                        T2 Q[QN], Rb[K];
-#pragma unroll
-                        for (int m = 0; m < QN; ++m) Q[m] = two(T(0), T(0));
-#pragma unroll
-                        for (int m = 0; m < K; ++m) Rb[m] = two(T(0), T(0));
-#pragma unroll
-                        for (int q = 0; q < NQ; ++q) {
-                            T cv[VE], vv[VE];
-                            vload<T>(rowp + q * VE, cv);
-                            vload<T>(rowj + q * VE, vv);
-#pragma unroll
-                            for (int e = 0; e < VE; e += 2) {
-                                const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
-                                vv[e] = nv.x;
-                                vv[e + 1] = nv.y;
-                            }
-                            if (store) vstore<T>(rowj + q * VE, vv);
-#pragma unroll
-                            for (int e = 0; e < VE; e += 2) {
-                                const int i = q * VE + e;
-                                if (i < 2 * PO.np) {
-                                    const int qa = PO.m1[i], qb = PO.m0[i];
-                                    const T2 S = two(vv[e], vv[e + 1]);
-                                    Q[qa] = fma2(Hj[qb], S, Q[qa]);
-                                    Rb[qb] = fma2(Hs[qa], S, Rb[qb]);
-                                } else {
-#pragma unroll
-                                    for (int t = 0; t < 2; ++t)
-                                        if (i + t < n) {
-                                            const int d = PO.m0[i + t];
-                                            Q[d] = fma2(Hj[d], two(vv[e + t], vv[e + t]), Q[d]);
-                                        }
-                                }
-                            }
-                        }
-                        // d/dx = sum_m hh_{m-1}(x) P0[m], d/dy = sum_m hh_{m-1}(y) P1[m]
-                        T2 GR = two(T(0), T(0)), GQ = GR;
-#pragma unroll
-                        for (int m = 1; m < K; ++m) GR = fma2(Hj[m - 1], Rb[m], GR);
-#pragma unroll
-                        for (int m = 1; m < QN; ++m) GQ = fma2(Hs[m - 1], Q[m], GQ);
-                        gx = GR.x + GQ.y;
-                        gy2 = GR.y + GQ.x;
-                    } else {
-                        T au[K], av[K];
-                        hermite_pe<K>(ux, au);
-                        hermite_pe<K>(uy, av);
-                        T P0[K], P1[K];  // P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
-#pragma unroll
-                        for (int m = 0; m < K; ++m) P0[m] = P1[m] = T(0);
-#pragma unroll
-                        for (int q = 0; q < NQ; ++q) {
-                            T cv[VE], vv[VE];
-                            vload<T>(rowp + q * VE, cv);
-                            vload<T>(rowj + q * VE, vv);
-#pragma unroll
-                            for (int e = 0; e < VE; e += 2) {
-                                const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
-                                vv[e] = nv.x;
-                                vv[e + 1] = nv.y;
-                            }
-                            if (store) vstore<T>(rowj + q * VE, vv);
-#pragma unroll
-                            for (int e = 0; e < VE; ++e) {
-                                const int i = q * VE + e;
-                                if (i < n) {
-                                    P0[PO.m0[i]] = fmaT(av[PO.m1[i]], vv[e], P0[PO.m0[i]]);
-                                    P1[PO.m1[i]] = fmaT(au[PO.m0[i]], vv[e], P1[PO.m1[i]]);
-                                }
-                            }
-                        }
-                        gx = gy2 = T(0);
-#pragma unroll
-                        for (int m = 1; m < K; ++m) {
-                            gx = fmaT(au[m - 1], P0[m], gx);
-                            gy2 = fmaT(av[m - 1], P1[m], gy2);
-                        }
-                    }
-                    {
-                        // lanes without particles keep zeros
-                        const T g1 = own ? sig_new * sq2 : T(0);
-                        if (b) {
-                            DD[0].y = g1 * gx;
-                            DD[1].y = g1 * gy2;
+                    // the moved particle's block as a compile-time constant: its rows, row
+                    // scale and register halves are fixed offsets and halves, not selections
+                    auto update = [&](auto block) {
+                        constexpr int b = decltype(block)::value;
+                        const bool mine = l == pl;
+                        if (adim == 0) {
+                            if (mine) X[0] = b ? two(X[0].x, xn) : two(xn, X[0].y);
                         } else {
-                            DD[0].x = g1 * gx;
-                            DD[1].x = g1 * gy2;
+                            if (mine) X[1] = b ? two(X[1].x, xn) : two(xn, X[1].y);
                         }
-                    }
+                        if (l == 0) {
+                            xs[k] = xn;
+                            fcs[k] = Fn;
+                        }
+                        // running sums (the pair totals sit in lanes 4, 8, 12; the new
+                        // gradient of the moved particle in lanes 16, 20)
+                        const T tl = __shfl_sync(FULL, tot, 4), tb = __shfl_sync(FULL, tot, 8);
+                        const T tv = __shfl_sync(FULL, tot, 12);
+                        const T tgx = __shfl_sync(FULL, tot, 16), tgy = __shfl_sync(FULL, tot, 20);
+                        if constexpr (F32) {
+                            dlap += tl;
+                            dbh2 += tb;
+                            dvint += tv;
+                            dsx2 += (xn - xo) * (xn + xo);
+                        } else {
+                            sumx2 += (double)xn * (double)xn - (double)xo * (double)xo;
+                            lapj += (double)tl;
+                            bh2 += (double)tb;
+                            vint += (double)tv;
+                        }
+                        // Pade gradients: partners by their change, the moved particle anew
+                        GJ[0] = add2(GJ[0], gdx);
+                        GJ[1] = add2(GJ[1], gdy);
+                        if (mine) {
+                            GJ[0] = b ? two(GJ[0].x, tgx) : two(tgx, GJ[0].y);
+                            GJ[1] = b ? two(GJ[1].x, tgy) : two(tgy, GJ[1].y);
+                        }
+                        if constexpr (STALE) {
+                            if (!allcur) {
+                                if (own && l != p) msk[l] |= 1ull << p;
+                                if (own && n + l != p) msk[n + l] |= 1ull << p;
+                                if (mine) msk[p] = ~0ull;
+                            }
+                        }
+                        // Sherman-Morrison on block b (slaterdeterminant.cpp:165-175) through the
+                        // row scales: row l += t_l row p with t_l = -s_l sigma_p / R (staged
+                        // rows), sigma_p /= R; then the block's gradient vectors
+                        // (slaterdeterminant.cpp:155-163) from the updated rows
+                        const T sig_p = __shfl_sync(FULL, sig_l, pl);
+                        const T rinv = Fs::rcp(R);
+                        const T tcoef = (own && !mine) ? -(sl * sig_p * rinv) : T(0);
+                        const T sig_new = mine ? sig_l * rinv : sig_l;
+                        if (b) SIG.y = sig_new;
+                        else SIG.x = sig_new;
+                        const T ux = sq2 * (b ? X[0].y : X[0].x), uy = sq2 * (b ? X[1].y : X[1].x);
+                        T *rowj = inv + (b * n + lc) * IS;
+                        const T *rowp = inv + (b * n + pl) * IS;
+                        const bool store = own && !mine;
+                        T gx, gy2;
+                        if constexpr (OWNER_PACK_ACC) {
+                            // packed, with Hj[m] = (hh_m(x), hh_m(y)) of the lane's particle, its
+                            // swaps Hs[a] = (hh_a(y), hh_a(x)), P0[m0] = sum_m1 hh_m1(y) v(m0, m1)
+                            // and P1[m1] = sum_m0 hh_m0(x) v(m0, m1): for the pair (a < b) with
+                            // S = (v(b,a), v(a,b)),
+                            //   Q[a] = (P1[a], P0[a]) += Hj[b] * S,  Rb[b] = (P0[b], P1[b]) += Hs[a] * S,
+                            // and a diagonal (d, d) adds Hj[d] * (v, v) to Q[d]
+                            constexpr int QN = (K + 1) / 2;
+                            T2 Hj[K];
+                            hermite_pe2<K, T>(two(ux, uy), Hj);
+                            T2 Hs[QN];
+    #pragma unroll
+                            for (int m = 0; m < QN; ++m) Hs[m] = two(Hj[m].y, Hj[m].x);
+                            T2 Q[QN], Rb[K];
+    #pragma unroll
+                            for (int m = 0; m < QN; ++m) Q[m] = two(T(0), T(0));
+    #pragma unroll
+                            for (int m = 0; m < K; ++m) Rb[m] = two(T(0), T(0));
+    #pragma unroll
+                            for (int q = 0; q < NQ; ++q) {
+                                T cv[VE], vv[VE];
+                                vload<T>(rowp + q * VE, cv);
+                                vload<T>(rowj + q * VE, vv);
+    #pragma unroll
+                                for (int e = 0; e < VE; e += 2) {
+                                    const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
+                                    vv[e] = nv.x;
+                                    vv[e + 1] = nv.y;
+                                }
+                                if (store) vstore<T>(rowj + q * VE, vv);
+    #pragma unroll
+                                for (int e = 0; e < VE; e += 2) {
+                                    const int i = q * VE + e;
+                                    if (i < 2 * PO.np) {
+                                        const int qa = PO.m1[i], qb = PO.m0[i];
+                                        const T2 S = two(vv[e], vv[e + 1]);
+                                        Q[qa] = fma2(Hj[qb], S, Q[qa]);
+                                        Rb[qb] = fma2(Hs[qa], S, Rb[qb]);
+                                    } else {
+    #pragma unroll
+                                        for (int t = 0; t < 2; ++t)
+                                            if (i + t < n) {
+                                                const int d = PO.m0[i + t];
+                                                Q[d] = fma2(Hj[d], two(vv[e + t], vv[e + t]), Q[d]);
+                                            }
+                                    }
+                                }
+                            }
+                            // d/dx = sum_m hh_{m-1}(x) P0[m], d/dy = sum_m hh_{m-1}(y) P1[m]
+                            T2 GR = two(T(0), T(0)), GQ = GR;
+    #pragma unroll
+                            for (int m = 1; m < K; ++m) GR = fma2(Hj[m - 1], Rb[m], GR);
+    #pragma unroll
+                            for (int m = 1; m < QN; ++m) GQ = fma2(Hs[m - 1], Q[m], GQ);
+                            gx = GR.x + GQ.y;
+                            gy2 = GR.y + GQ.x;
+                        } else {
+                            T au[K], av[K];
+                            hermite_pe<K>(ux, au);
+                            hermite_pe<K>(uy, av);
+                            T P0[K], P1[K];  // P0[m0] = sum_m1 hh_m1(y) v, P1[m1] = sum_m0 hh_m0(x) v
+    #pragma unroll
+                            for (int m = 0; m < K; ++m) P0[m] = P1[m] = T(0);
+    #pragma unroll
+                            for (int q = 0; q < NQ; ++q) {
+                                T cv[VE], vv[VE];
+                                vload<T>(rowp + q * VE, cv);
+                                vload<T>(rowj + q * VE, vv);
+    #pragma unroll
+                                for (int e = 0; e < VE; e += 2) {
+                                    const T2 nv = fma2(two(cv[e], cv[e + 1]), two(tcoef, tcoef), two(vv[e], vv[e + 1]));
+                                    vv[e] = nv.x;
+                                    vv[e + 1] = nv.y;
+                                }
+                                if (store) vstore<T>(rowj + q * VE, vv);
+    #pragma unroll
+                                for (int e = 0; e < VE; ++e) {
+                                    const int i = q * VE + e;
+                                    if (i < n) {
+                                        P0[PO.m0[i]] = fmaT(av[PO.m1[i]], vv[e], P0[PO.m0[i]]);
+                                        P1[PO.m1[i]] = fmaT(au[PO.m0[i]], vv[e], P1[PO.m1[i]]);
+                                    }
+                                }
+                            }
+                            gx = gy2 = T(0);
+    #pragma unroll
+                            for (int m = 1; m < K; ++m) {
+                                gx = fmaT(au[m - 1], P0[m], gx);
+                                gy2 = fmaT(av[m - 1], P1[m], gy2);
+                            }
+                        }
+                        {
+                            // lanes without particles keep zeros
+                            const T g1 = own ? sig_new * sq2 : T(0);
+                            if (b) {
+                                DD[0].y = g1 * gx;
+                                DD[1].y = g1 * gy2;
+                            } else {
+                                DD[0].x = g1 * gx;
+                                DD[1].x = g1 * gy2;
+                            }
+                        }
+                    };
+                    if (b)
+                        update(std::integral_constant<int, 1>{});
+                    else
+                        update(std::integral_constant<int, 0>{});
                     kp = publish();
                     __syncwarp();
                 }
