@@ -84,6 +84,32 @@ def test_two_calls_match_engine_eval(name):
             assert rel(got, want) < TOL, (call, rel(got, want))
 
 
+def test_call_leaves_device_memory_unchanged():
+    """After the first call on the device (its one-time set-up), a call changes the
+    device's free memory by nothing: the entry point allocates no device memory."""
+    import torch
+    spec, theta, W = CASES["dot56"]
+    theta = np.asarray(theta, np.float64).reshape(len(theta), 1)
+    lib, f = entry()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(5)
+    d_pos = torch.from_numpy(positions(rng, W, spec.N * spec.d, 1.0 / np.sqrt(spec.omega))).to(dev)
+    energies = torch.zeros((W, 3), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    args = (spec.input_in().encode(), theta.ctypes.data, theta.shape[0], theta.shape[1], d_pos.data_ptr(), W,
+            energies.data_ptr(), stream.cuda_stream)
+    assert f(*args) == 0, lib.vmc_last_error()  # first call: the per-device set-up
+    stream.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(3):
+        assert f(*args) == 0, lib.vmc_last_error()
+    stream.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(dev)
+    assert free_after == free_before
+    assert np.all(np.isfinite(energies.cpu().numpy()))
+
+
 def test_rejects_walker_counts_beyond_the_array():
     import torch
     spec, theta, _ = CASES["dot56"]
