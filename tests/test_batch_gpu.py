@@ -89,6 +89,25 @@ def test_batch_tuner_keeps_results():
         assert np.allclose(params[s], th_ref, rtol=TOL, atol=TOL), (s, params[s], th_ref)
 
 
+def test_batch_fp32_atoms_equal_alone():
+    """He and Ne in mixed precision inside a batch: the FP32 atom sweep in the batch
+    kernel with the FP64 re-inversion after each launch computes what an engine alone
+    computes with the same cadence (refreshInterval = the batch's 2 048-step launches).
+    FP32 arithmetic in two compilations of the same code: energies to 1e-6 relative;
+    parameters to 1e-5 absolute, a thousandth of an ADAM step at lr 0.01 (ADAM divides
+    by the root of the squared-gradient average, so parameters whose gradient is near
+    zero amplify FP32 differences in it; measured 5e-7)."""
+    texts = [atom_text(2, 40, 300, seed=14, precision="mixed"), atom_text(10, 24, 300, seed=16, precision="mixed"),
+             dot_text(6, 0.5, 96, 300, "mixed", seed=12)]
+    seeds = [5, 6, 7]
+    en, params, info, _ = batched(texts, seeds, 3, tile=(4, 1))
+    ref = alone([t + "refreshInterval: 2048\n" if "atomicNumber" in t else t for t in texts], seeds, 3)
+    for s, (e_ref, th_ref) in enumerate(ref):
+        assert np.allclose(en[:, s], e_ref, rtol=1e-6, atol=0), (s, en[:, s], e_ref)
+        print(s, np.max(np.abs(np.asarray(params[s]) - np.asarray(th_ref))))
+        assert np.allclose(params[s], th_ref, rtol=0, atol=1e-5), s
+
+
 def test_mixed_workload_runs():
     """The 64-system workload (62 dots N = 2..56, He, Ne) at a few steps per walker:
     tuned, replayed, finite, no NaN energy or singular walker."""

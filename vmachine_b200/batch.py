@@ -5,8 +5,9 @@ closed-shell quantum dots with N in {2, 6, 12, 20, 30, 42, 56} (cycled), omega
 drawn from U[0.1, 1] and a walker count from U{256..4096}, Slater(Hermite) x
 Gaussian x Pade-Jastrow with importance sampling; plus the helium and neon atoms
 (Z = 2 and 10; Slater determinants of hydrogen orbitals, 1x1 and 5x5 blocks, times
-the SimpleJastrow factor) on the general FP64 path.  Everything is drawn from one
-seed, so the workload is reproducible.
+the SimpleJastrow factor) on the general path, in the workload's precision (mixed:
+the atoms' FP32 sweep with the Slater inverse in FP64, re-inverted in FP64 after each
+launch).  Everything is drawn from one seed, so the workload is reproducible.
 
 `partition` spreads systems over ranks by cost (walkers x steps x work per step,
 longest first onto the least loaded rank); the systems are independent, so ranks
@@ -30,13 +31,13 @@ def dot_text(N, omega, walkers, steps, precision="mixed", seed=1, lr=0.01, compa
         f"seed: {seed}", f"compat: {compat}"]) + "\n"
 
 
-def atom_text(Z, walkers, steps, seed=1, lr=0.01, compat="corrected"):
+def atom_text(Z, walkers, steps, seed=1, lr=0.01, compat="corrected", precision="fp64"):
     return "\n".join([
         f"numParticles: {Z}", "numDimensions: 3", f"atomicNumber: {Z}", "hamiltonian: atomicNucleus",
         "interactionStyle: coulomb", "waveFunctionElement: slaterDeterminant",
         "waveFunctionElement: simpleJastrow", "basis: hydrogenOrbital", "sampling: importanceSampling",
         "stepLength: 0.01", "optimization: adam", f"learningRate: {lr!r}", f"numSteps: {walkers * steps}",
-        f"numWalkers: {walkers}", "precision: fp64", f"seed: {seed}", f"compat: {compat}"]) + "\n"
+        f"numWalkers: {walkers}", f"precision: {precision}", f"seed: {seed}", f"compat: {compat}"]) + "\n"
 
 
 def mixed_systems(seed=5, steps=2000, n_dots=62, precision="mixed", atoms=True, max_walkers=4096):
@@ -52,7 +53,7 @@ def mixed_systems(seed=5, steps=2000, n_dots=62, precision="mixed", atoms=True, 
     if atoms:
         for j, Z in enumerate((2, 10)):
             W = int(rng.integers(256, max_walkers + 1))
-            texts.append(atom_text(Z, W, steps, seed=2000 + j))
+            texts.append(atom_text(Z, W, steps, seed=2000 + j, precision=precision))
             desc.append({"kind": "atom", "Z": Z, "N": Z, "walkers": W})
     return texts, desc
 

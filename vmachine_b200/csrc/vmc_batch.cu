@@ -39,6 +39,9 @@ struct vmc_batch {
     std::vector<int> kind, gen_of;  // per system: Hermite shells or BATCH_GENERAL; index into gen
     std::vector<double> cost;       // work per walker-step (ordering only)
     std::vector<char> theta_dirty;  // parameters changed since the last sweep
+    // per system: the rounds after which an FP32 general-path system (the atoms in mixed
+    // precision) takes its FP64 re-inversion, this iteration
+    std::vector<int> gen_rounds;
     int n_gen = 0;
     BatchOps ops{};
     const void *sweep_fn = nullptr;
@@ -217,6 +220,12 @@ int enqueue(vmc_batch *b, const vmc_batch::Cand &c, int rounds, const std::vecto
             void *rargs[] = {&R};
             if ((rc = launch(b->ops.rebuild, dim3(b->rebuild_grid), dim3(128), rb_smem, st, rargs))) return rc;
         }
+        // the FP32 atoms: FP64 re-inversion and evaluation after each of their launches
+        for (int s = 0; s < n; ++s)
+            if (b->gen_rounds[s] > r) {
+                vmc_engine *e = b->sys[s];
+                BCUDA(gen_launch_state(engine_params(e), e->gen, GEN_REFRESH, nullptr, nullptr, nullptr, nullptr, st));
+            }
     }
     double *out = b->d_out, *drift = b->d_drift_all;
     long long *doff = b->d_drift_off;
@@ -322,9 +331,6 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
                 return reject(VMC_E_UNSUPPORTED, "more than " + std::to_string(BATCH_MAX_GEN) + " general-path systems");
             kind = BATCH_GENERAL;
             b->gen_of.push_back(b->n_gen++);
-            // the batch runs its general-path walkers in FP64 (its kernels call the FP64
-            // sweep, and general systems take no refresh there), whatever the precision
-            e->gen.f32 = 0;
         } else {
             const bool dot = e->dim == 2 && e->K >= 1 && e->K <= 7 &&
                              (e->flags == FX_DOT_COMPAT || e->flags == FX_DOT_CORRECTED);
@@ -379,7 +385,10 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
         int cap = 1;
         for (vmc_engine *e : b->sys) {
             const int steps = e->steps_per_walker + e->burn_in;
-            const int chunk_min = e->refresh_auto ? e->D
+            // general-path systems run in launches of sweep_chunk steps (the FP32 atoms
+            // re-invert in FP64 after each)
+            const int chunk_min = e->general ? e->sweep_chunk
+                                  : e->refresh_auto ? e->D
                                   : e->refresh_interval > 0 ? e->refresh_interval : e->sweep_chunk;
             cap = std::max(cap, (steps + chunk_min - 1) / chunk_min);
         }
@@ -484,7 +493,7 @@ int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *avg)
     for (int s = 0; s < n; ++s) {
         vmc_engine *e = b->sys[s];
         const int steps = e->steps_per_walker + e->burn_in, burn = e->burn_in;
-        const int chunk = e->refresh_interval > 0 ? e->refresh_interval : e->sweep_chunk;
+        const int chunk = e->general ? e->sweep_chunk : e->refresh_interval > 0 ? e->refresh_interval : e->sweep_chunk;
         n_launch[s] = (steps + chunk - 1) / chunk;
         rounds = std::max(rounds, n_launch[s]);
         const int bs = (steps - burn) / e->batches, m = iteration % e->batches;
@@ -515,6 +524,9 @@ int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *avg)
     for (int s = 0; s < n; ++s)
         if (b->h_sys[s].refresh)
             for (int r = 0; r < n_launch[s]; ++r) rebuild_round[r] = 1;
+    b->gen_rounds.assign(n, 0);
+    for (int s = 0; s < n; ++s)
+        if (b->kind[s] == BATCH_GENERAL && b->sys[s]->gen.f32) b->gen_rounds[s] = n_launch[s];
     const bool tuning = b->chosen < 0;
     const vmc_batch::Cand c = tuning ? b->cands[b->next_cand % b->cands.size()] : b->cands[b->chosen];
     if ((rc = build_items(b, c.per_item))) return rc;
@@ -523,6 +535,7 @@ int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *avg)
         std::vector<long long> key = {rounds, c.wpb, c.per_item, c.grid, b->n_items, theta_refresh ? 1 : 0,
                                       (long long)(size_t)b->d_items};
         for (char f : rebuild_round) key.push_back(f);
+        for (int g : b->gen_rounds) key.push_back(g);
         if (key != b->key || !b->exec) {
             if (b->exec) cudaGraphExecDestroy(b->exec);
             if (b->graph) cudaGraphDestroy(b->graph);

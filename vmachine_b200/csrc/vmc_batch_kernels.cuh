@@ -68,10 +68,43 @@ __device__ __forceinline__ bool batch_next(const BatchLaunch &b, int lane, int2 
 // The warp's slice (`slice` doubles): GEN_SCR scratch doubles, then the staged record
 // and, when they fit too, the accumulators (the slice is sized by the batch's largest
 // dot record, so a large general-path walker stages less or nothing).
+// The atoms' FP32 sweep (g.f32): the same slice, with FP32 scratch and staged records
+// (the FP64 Slater inverse and the accumulators after each record).  Returns false when
+// the staged records do not fit the slice; the caller then runs the FP64 sweep on the
+// FP64 records.
+static __device__ __noinline__ bool batch_gen_walkers_f32(const SweepArgs &a, int steps, int off, const GenParams &g,
+                                                          int w0, int w_end, double *scr, int slice)
+{
+    TcMlp tc{};
+    const int full = gen_stage_bytes(g, a.P.nacc, 4);
+    float *scr32 = reinterpret_cast<float *>(scr);
+    unsigned char *base = reinterpret_cast<unsigned char *>(scr + GEN_SCR);
+    const long long room = (long long)(slice - GEN_SCR) * 8;
+    if (g.variant != GV_ATOM || full == 0) return false;
+    if (g.seg == 4) {
+        if (4LL * full > room) return false;
+        const int seg = (threadIdx.x & 31) >> 3;
+        float *st4 = reinterpret_cast<float *>(base + seg * full);
+        for (int wb = w0; wb < w_end; wb += 4) {
+            const int w = wb + seg;
+            if (w < w_end)
+                gen_sweep_walker<false, GV_ATOM, 8, float>(a, steps, off, g, w, true, scr32 + seg * (GEN_SCR / 4),
+                                                           nullptr, tc, nullptr, st4, true);
+        }
+        return true;
+    }
+    if (full > room) return false;
+    for (int w = w0; w < w_end; ++w)
+        gen_sweep_walker<false, GV_ATOM, 32, float>(a, steps, off, g, w, true, scr32, nullptr, tc, nullptr,
+                                                    reinterpret_cast<float *>(base), true);
+    return true;
+}
+
 static __device__ __noinline__ void batch_gen_walkers(const SweepArgs &a, int steps, int off, const GenParams &g, int w0,
                                                int w_end, double *scr, int slice)
 {
     TcMlp tc{};  // the general systems of a batch have no MLP factor
+    if (g.f32 && batch_gen_walkers_f32(a, steps, off, g, w0, w_end, scr, slice)) return;
     const int full = gen_stage_doubles(g, a.P.nacc);
     const bool rec_fits = !g.mlp && GEN_SCR + g.rec <= slice, acc_fits = full && GEN_SCR + full <= slice;
     double *stage = rec_fits ? scr + GEN_SCR : nullptr;

@@ -730,8 +730,11 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
 {
     const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) +
                         (mode != GEN_STATE ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0);
-    cudaError_t e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    // above the default 48 KB only (the batch launches the refresh inside a graph capture)
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
     gen_state_kernel<<<(P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(P, g, mode, o_grad, o_lap, o_pg,
                                                                                 o_en);
     return cudaGetLastError();
