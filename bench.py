@@ -448,8 +448,9 @@ def batch_line(args, pg, rank, local, world):
     secs = max_over_ranks(pg, local, r["ms_per_iteration"] * 1e-3)
     moves = sum(desc[i]["walkers"] for i in range(len(desc))) * 2000.0
     return {"workload": "64 systems: 62 2D closed-shell dots N in {2,6,12,20,30,42,56}, omega ~ U[0.1, 1], "
-                        "256-4096 walkers each; He and Ne atoms (hydrogen orbitals x SimpleJastrow, FP64 general "
-                        "path); 2000 steps per walker per iteration, seed 5",
+                        "256-4096 walkers each; He and Ne atoms (hydrogen orbitals x SimpleJastrow, general "
+                        "path: FP32 sweep, FP64 Slater inverse); mixed precision, 2000 steps per walker per "
+                        "iteration, seed 5",
             "walker_moves_per_s": moves / secs, "ms_per_iteration": secs * 1e3, "systems_per_rank": len(mine),
             "tile": r["tile"], "graph_captures": r["graph_captures"], "replayed_iterations": r["replayed_iterations"],
             "tuning_ns_per_move": [t[3] for t in r["tuning"]], "scaling": "strong"}
