@@ -84,6 +84,32 @@ def test_two_calls_match_engine_eval(name):
             assert rel(got, want) < TOL, (call, rel(got, want))
 
 
+def test_matches_reference_fixture_n56():
+    """The headline system's energies at the reference-generated fixed positions
+    (tests/golden/eval_fixed.npz, the reference's own evaluation): kinetic, external
+    and interaction energy of three walkers, 1e-10 relative."""
+    import os
+
+    import torch
+    from oracle_bind import load_cases, spec_from_case
+    c = load_cases(os.path.join(os.path.dirname(__file__), "golden", "eval_fixed.npz"))["n56_w028_slater_gauss_pade"]
+    spec = spec_from_case(c)
+    pos = np.ascontiguousarray(c["pos"], np.float64)
+    theta = np.ascontiguousarray(c["theta"], np.float64)
+    W = pos.shape[0]
+    lib, f = entry()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    d_pos = torch.from_numpy(pos).to(dev)
+    energies = torch.full((W, 3), float("nan"), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    rc = f(spec.input_in().encode(), theta.ctypes.data, theta.shape[0], theta.shape[1], d_pos.data_ptr(), W,
+           energies.data_ptr(), stream.cuda_stream)
+    assert rc == 0, lib.vmc_last_error()
+    stream.synchronize()
+    assert rel(energies.cpu().numpy(), c["energies"]) < 1e-10
+
+
 def test_call_leaves_device_memory_unchanged():
     """After the first call on the device (its one-time set-up), a call changes the
     device's free memory by nothing: the entry point allocates no device memory."""
