@@ -19,6 +19,10 @@
 // restatement in oracle/vmc_oracle.c function for function (eval_impl,
 // ratio_impl, vmo_run).
 //
+// The device functions are templated on the walker's real type R: double is the FP64
+// path; float is the compiled atom form's mixed-precision sweep, whose record is staged
+// in FP32 while the Slater inverse, its contractions and the accumulators stay FP64.
+//
 // This header holds the path's device functions; vmc_general.cu has its kernels and
 // launchers, and the multi-system kernel (vmc_batch.cu) calls gen_sweep_walker.
 #pragma once
@@ -37,7 +41,7 @@ namespace {
 
 
 constexpr int GEN_WPB = 4;     // warps per CTA
-constexpr int GEN_SCR = 256;   // shared doubles per warp (a warp of G walkers: GEN_SCR / G each)
+constexpr int GEN_SCR = 256;   // shared reals (R) per warp (a warp of G walkers: GEN_SCR / G each)
 // shared scratch of a walker: orbital values at the proposal | moved row | RBM visible
 // (sorted) | RBM hidden p_j = 1/(1+e^v) | RBM hidden e^v/(1+e^v); the pair elements'
 // per-pair terms reuse it from offset 0 during an evaluation (the compiled atom form
