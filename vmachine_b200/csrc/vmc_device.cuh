@@ -89,12 +89,28 @@ __device__ __forceinline__ void kadd(double &s, double &c, double v)
 }
 
 // ------------------------------------------------------------------ math
-__device__ __forceinline__ float fast_rcp(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ double fast_rcp(double x) { return 1.0 / x; }
-__device__ __forceinline__ float vsqrt(float x) { return sqrtf(x); }
-__device__ __forceinline__ double vsqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float vexp(float x) { return expf(x); }
-__device__ __forceinline__ double vexp(double x) { return exp(x); }
+// FP32 PTX approximate instructions with subnormals flushed, one MUFU each (the
+// non-flushing forms add a rescaling of subnormal operands around it): for the FP32
+// sweeps' distances, denominators and exponents, which stay far from that range.
+// exp(x) = 2^(x log2 e).
+__device__ __forceinline__ float approx_rsqrt(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float approx_rcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float approx_exp(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x * 1.4426950408889634f));
+    return r;
+}
 
 // Coefficients of the normalised Hermite functions h_m = H_m / sqrt(2^m m!):
 //   h_{m+1} = A_m x h_m - B_m h_{m-1},  A_m = sqrt(2/(m+1)), B_m = sqrt(m/(m+1))

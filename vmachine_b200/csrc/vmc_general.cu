@@ -730,9 +730,13 @@ cudaError_t gen_launch_state(const Params &P, const GenParams &g, int mode, doub
 {
     const size_t smem = (g.mlp ? MLP_SMEM_DOUBLES * sizeof(double) : 0) +
                         (mode != GEN_STATE ? (size_t)GEN_WPB * gen_smem_per_warp(g) : 0);
-    // above the default 48 KB only (the batch launches the refresh inside a graph capture)
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // not while the stream is being captured (the batch's refresh of its FP32 atoms, a
+    // few KB, within the default limit): the attribute is set outside any capture
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return e;
+    if (cap == cudaStreamCaptureStatusNone) {
+        e = cudaFuncSetAttribute(gen_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     gen_state_kernel<<<(P.W + GEN_WPB - 1) / GEN_WPB, 32 * GEN_WPB, smem, st>>>(P, g, mode, o_grad, o_lap, o_pg,

@@ -527,13 +527,13 @@ __device__ void gen_evaluate(const Params &P, const GenParams &g, int dim_rt, R 
                         dv[c] = xi[c] - (float)x[j * dim + c];
                         r2 += dv[c] * dv[c];
                     }
-                    const float ir = rsqrtf(r2), du = (float)c3[1];
+                    const float ir = approx_rsqrt(r2), du = (float)c3[1];
                     for (int c = 0; c < dim; ++c) gi[c] += du * dv[c] * ir;
                     if (j > i) li += 2.0f * ((float)c3[2] + (dim - 1) * du * ir);
                 }
                 float r2i = 0.0f;
                 for (int c = 0; c < dim; ++c) r2i += xi[c] * xi[c];
-                const float iri = rsqrtf(r2i), dc = (float)oc[i * 3 + 1];
+                const float iri = approx_rsqrt(r2i), dc = (float)oc[i * 3 + 1];
                 for (int c = 0; c < dim; ++c) gi[c] += dc * xi[c] * iri;
                 lap_l += (R)li + oc[i * 3 + 2] + (dim - 1) * dc * iri;
                 for (int c = 0; c < dim; ++c) {

@@ -33,7 +33,7 @@ constexpr int MLP_SMEM_DOUBLES = (MLP_SMEM_FLOATS + 3) / 4 * 2;  // 16-byte mult
 __device__ __forceinline__ float mlp_tanh(float x)
 {
     x = fminf(fmaxf(x, -9.0f), 9.0f);  // tanh(9) = 1 in FP32
-    return 1.0f - __fdividef(2.0f, __expf(2.0f * x) + 1.0f);
+    return 1.0f - 2.0f * approx_rcp(approx_exp(2.0f * x) + 1.0f);
 }
 
 // Cooperative copy of the weights into shared memory (all threads of the CTA);

@@ -30,10 +30,11 @@
 namespace vmc {
 
 template <typename T> struct Fast;
+// FP32: the PTX approximate instructions (vmc_device.cuh)
 template <> struct Fast<float> {
-    static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
-    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
-    static __device__ __forceinline__ float exp(float x) { return __expf(x); }
+    static __device__ __forceinline__ float rsqrt(float x) { return approx_rsqrt(x); }
+    static __device__ __forceinline__ float rcp(float x) { return approx_rcp(x); }
+    static __device__ __forceinline__ float exp(float x) { return approx_exp(x); }
 };
 template <> struct Fast<double> {
     static __device__ __forceinline__ double rsqrt(double x) { return ::rsqrt(x); }
@@ -520,7 +521,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                     r2o = fmaf(dvo[c], dvo[c], r2o);
                     r2n = fmaf(dvn[c], dvn[c], r2n);
                 }
-                const float iro = pv ? rsqrtf(r2o) : 0.0f, irn = pv ? rsqrtf(r2n) : 0.0f;
+                const float iro = pv ? approx_rsqrt(r2o) : 0.0f, irn = pv ? approx_rsqrt(r2n) : 0.0f;
                 const bool same = same_spin(p, j, N);
                 const unsigned tst = tc_pair_layer(*mctx->tc, mctx->w, pv, r2n * irn, same ? 1.0f : 0.0f,
                                                    mlp_cusp(DIM, same), lane, wib_l, mctx->pre);
