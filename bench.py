@@ -57,7 +57,7 @@ def workload_text(walkers, steps_per_walker, precision, seed, refresh="auto"):
 # owner sweep on this workload's 16 384 walkers, from an ncu capture of a 448-step
 # launch (not this run: the walker state is read and written once per launch, so the
 # figure does not depend on the launch's step count)
-SWEEP_TRAFFIC_BYTES = 225_377_536
+SWEEP_TRAFFIC_BYTES = 225_813_760
 
 
 def cpu_model():
