@@ -89,6 +89,20 @@ def test_batch_tuner_keeps_results():
         assert np.allclose(params[s], th_ref, rtol=TOL, atol=TOL), (s, params[s], th_ref)
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batch_owner_form_equals_alone(precision):
+    """N = 42 and 56 run the owner-form sweep inside the batch kernel, as they do alone:
+    the same energies and parameters as each system alone."""
+    texts = [dot_text(42, 0.5, 40, 300, precision, seed=31), dot_text(56, 0.28, 33, 300, precision, seed=32),
+             dot_text(12, 0.9, 50, 300, precision, seed=33)]
+    seeds = [8, 9, 10]
+    en, params, info, _ = batched(texts, seeds, 3, tile=(4, 1))
+    ref = alone(texts, seeds, 3)
+    for s, (e_ref, th_ref) in enumerate(ref):
+        assert np.allclose(en[:, s], e_ref, rtol=TOL, atol=0), (s, en[:, s], e_ref)
+        assert np.allclose(params[s], th_ref, rtol=TOL, atol=TOL), (s, params[s], th_ref)
+
+
 def test_batch_fp32_atoms_equal_alone():
     """He and Ne in mixed precision inside a batch: the FP32 atom sweep in the batch
     kernel with the FP64 re-inversion after each launch computes what an engine alone

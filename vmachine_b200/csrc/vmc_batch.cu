@@ -358,6 +358,8 @@ int vmc_batch_create(const char *const *texts, int n_systems, const vmc_options 
             b->rebuild_smem = std::max(b->rebuild_smem, engine_rebuild_smem_per_warp(e));
         b->sweep_smem = std::max(b->sweep_smem, e->general ? (int)(GEN_SCR * sizeof(double))
                                                            : batch_walkers_per_warp(e, kind) * engine_sweep_smem_per_warp(e));
+        // N = 42 and 56 run the owner-form sweep in the batch too (as they do alone)
+        if (!e->general && e->owner) b->sweep_smem = std::max(b->sweep_smem, e->ks.owner_smem);
     }
     if (dot_precision < 0)  // general-path systems only: slices as large as their staging
         for (vmc_engine *e : b->sys)
@@ -512,6 +514,8 @@ int vmc_batch_run_iteration(vmc_batch *b, int iteration, vmc_averages *avg)
         h.theta_refresh = (b->kind[s] != BATCH_GENERAL && b->theta_dirty[s]) ? 1 : 0;
         h.samples = steps - burn;
         h.seg = batch_walkers_per_warp(e, b->kind[s]);
+        h.owner = (b->kind[s] == 6 || b->kind[s] == 7) && e->owner ? 1 : 0;
+        if (h.owner) owner_constants(e, h.a);
         h.drift = e->d_drift;
         theta_refresh |= h.theta_refresh != 0;
         if (b->kind[s] == BATCH_GENERAL) {

@@ -39,6 +39,7 @@ struct BatchSys {
     int theta_refresh;  // parameters changed: re-derive the walkers before round 0
     int samples;        // sampled steps per walker (total_steps - burn-in)
     int seg;            // walkers per warp in the sweep: the engine's for N <= 30, else 1
+    int owner;          // N = 42, 56: the owner-form sweep (a.oc / a.ocf hold its constants)
     double *drift;      // W: inverse drift of the refreshes
 };
 
@@ -167,8 +168,14 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3) batch_sweep_ker
             if (sy.seg == 2) sweep_walkers<T, 2, 5, FX, true, 2>(sy.a, steps, off, ws, item.y, w_end, 2, nullptr, seg_stride);
             else sweep_walkers<T, 2, 5, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
-        case 6: sweep_walkers<T, 2, 6, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
-        case 7: sweep_walkers<T, 2, 7, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1); break;
+        case 6:
+            if (sy.owner) owner_sweep_walkers<T, 6, FX>(sy.a, steps, off, ws, item.y, w_end, 1);
+            else sweep_walkers<T, 2, 6, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
+        case 7:
+            if (sy.owner) owner_sweep_walkers<T, 7, FX>(sy.a, steps, off, ws, item.y, w_end, 1);
+            else sweep_walkers<T, 2, 7, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
+            break;
         default:
             batch_gen_walkers(sy.a, steps, off, c_gen[sy.gen], item.y, w_end, reinterpret_cast<double *>(ws),
                               b.smem_per_warp / (int)sizeof(double));

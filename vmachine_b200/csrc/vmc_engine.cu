@@ -297,6 +297,24 @@ int run_rebuild(vmc_engine *e, int mode, double *drift)
     return rc;
 }
 
+void fill_owner_constants(const vmc_engine *e, SweepArgs &a)
+{
+    const Params &P = a.P;
+    a.oc[OC_WA] = P.omega * P.alpha;
+    a.oc[OC_HDT] = 0.5 * P.step;
+    a.oc[OC_SDT] = std::sqrt(P.step);
+    a.oc[OC_GAM] = P.gamma;
+    a.oc[OC_GAMP] = P.gamma_prev;
+    a.oc[OC_M2GAM] = -2.0 * P.gamma;
+    a.oc[OC_BSAME] = P.beta_same;
+    a.oc[OC_BANTI] = P.beta_anti;
+    a.oc[OC_W2H] = 0.5 * P.omega * P.omega;
+    a.oc[OC_MHOM] = -0.5 * P.omega;
+    a.oc[OC_DGK] = (e->flags & Q_PADE_DGAMMA) ? -0.5 : -1.0;
+    a.oc[OC_LAPC] = P.omega * P.alpha * e->D;
+    for (int i = 0; i < OC_N; ++i) a.ocf[i] = (float)a.oc[i];
+}
+
 int run_sweep(vmc_engine *e, SweepArgs &a)
 {
     a.P = make_params(e);
@@ -306,20 +324,7 @@ int run_sweep(vmc_engine *e, SweepArgs &a)
     }
     const bool plain = !a.probe_k && !a.replay && !a.rec_en && !a.rec_acc && !a.dens_bins;
     if (plain && e->owner) {
-        const Params &P = a.P;
-        a.oc[OC_WA] = P.omega * P.alpha;
-        a.oc[OC_HDT] = 0.5 * P.step;
-        a.oc[OC_SDT] = std::sqrt(P.step);
-        a.oc[OC_GAM] = P.gamma;
-        a.oc[OC_GAMP] = P.gamma_prev;
-        a.oc[OC_M2GAM] = -2.0 * P.gamma;
-        a.oc[OC_BSAME] = P.beta_same;
-        a.oc[OC_BANTI] = P.beta_anti;
-        a.oc[OC_W2H] = 0.5 * P.omega * P.omega;
-        a.oc[OC_MHOM] = -0.5 * P.omega;
-        a.oc[OC_DGK] = (e->flags & Q_PADE_DGAMMA) ? -0.5 : -1.0;
-        a.oc[OC_LAPC] = P.omega * P.alpha * e->D;
-        for (int i = 0; i < OC_N; ++i) a.ocf[i] = (float)a.oc[i];
+        fill_owner_constants(e, a);
         a.wpb = OWNER_WPB;
         a.smem_per_warp = e->ks.owner_smem;
         const size_t smem = (size_t)OWNER_WPB * a.smem_per_warp;
@@ -1396,6 +1401,7 @@ HermiteCoef hermite_coefficients()
 }
 
 Params engine_params(const vmc_engine *e) { return make_params(e); }
+void owner_constants(const vmc_engine *e, SweepArgs &a) { fill_owner_constants(e, a); }
 int upload_parameters(vmc_engine *e) { return upload_theta(e); }
 int engine_sweep_smem_per_warp(const vmc_engine *e) { return sweep_smem_per_warp(e); }
 int engine_rebuild_smem_per_warp(const vmc_engine *e) { return rebuild_smem_per_warp(e->N, e->dim, e->n_orb); }

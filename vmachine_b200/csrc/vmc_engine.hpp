@@ -99,6 +99,8 @@ constexpr double INSTANT_FILE_LINES = 1.0e8;
 HermiteCoef hermite_coefficients();
 // Kernel parameters of the engine's current state (parameters, gamma history,
 // device buffers).
+// the owner-form sweep's per-launch constants (SweepArgs::oc, ocf) from a.P
+void owner_constants(const vmc_engine *e, SweepArgs &a);
 Params engine_params(const vmc_engine *e);
 // Shared bytes per warp of the sweep (the staged record, Pade mask and scalars) and
 // of the FP64 rebuild.

@@ -189,10 +189,14 @@ __host__ __device__ constexpr int owner_smem_per_warp(int K, int elem_bytes)
            (elem_bytes == 4 ? 32 * OWNER_STEP_BYTES : 0);
 }
 
+// Steps step_offset .. step_offset + steps - 1 of walkers w0, w0 + w_stride, ... < w_end
+// by the calling warp, whose owner_smem_per_warp bytes of shared memory start at ws.
+// The sweep kernel below runs it over a launch's walkers; the multi-system batch kernel
+// over a work item's.
 template <typename T, int K, int FX>
-__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTAS_F32 : OWNER_MIN_CTAS_F64) owner_sweep_kernel(const SweepArgs a)
+__device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int steps, int step_offset, unsigned char *ws,
+                                                    int w0, int w_end, int w_stride)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr PairTable PO = make_pair_table<K>();
     using T2 = Two<T>;
     using Fs = Fast<T>;
@@ -210,10 +214,9 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
 
     const Params &P = a.P;
     const Layout L = P.L;
-    const int l = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int l = threadIdx.x & 31;
     const bool own = l < n;
     const int lc = own ? l : n - 1;  // lanes without particles shadow the last row and store nothing
-    unsigned char *ws = smem_raw + (size_t)wib * a.smem_per_warp;
     T *inv = reinterpret_cast<T *>(ws);
     T *xs = inv + 2 * n * IS, *gs = xs + D, *fcs = gs + D;
     unsigned long long *msk = reinterpret_cast<unsigned long long *>(fcs + D);
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
     }
     const int eg = (l >> 1) & 3;  // energy slots: 0 E, 1 T, 2 V_ext, 3 V_int
 
-    for (int w = blockIdx.x * OWNER_WPB + wib; w < P.W; w += gridDim.x * OWNER_WPB) {
+    for (int w = w0; w < w_end; w += w_stride) {
         T *rec = reinterpret_cast<T *>(P.state) + (size_t)w * L.rec;
         // ---- stage the walker: inverse rows reordered and rescaled, own particles' arrays
 #pragma unroll
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
             }
         };
 
-        for (int s0 = 0; s0 < a.steps; s0 += 32) {
+        for (int s0 = 0; s0 < steps; s0 += 32) {
             // lane i draws the numbers of step ctr + i; step s0 + i reads them by shuffle
             int rng_k;
             T rng_z;
@@ -473,9 +476,9 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
                     allcur = __all_sync(FULL, mm == ~0ull);
                 }
             }
-            const int s_end = min(s0 + 32, a.steps);
+            const int s_end = min(s0 + 32, steps);
             for (int s = s0; s < s_end; ++s) {
-                const int it_step = a.step_offset + s;
+                const int it_step = step_offset + s;
                 const int slot = (s - s0) & 31;
                 ++ctr;
                 const int k = __shfl_sync(FULL, rng_k, slot);
@@ -948,6 +951,15 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
         if (l == 0 && status) P.status[w] |= status;
         __syncwarp();
     }
+}
+
+template <typename T, int K, int FX>
+__global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTAS_F32 : OWNER_MIN_CTAS_F64) owner_sweep_kernel(const SweepArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5;
+    owner_sweep_walkers<T, K, FX>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
+                                  blockIdx.x * OWNER_WPB + wib, a.P.W, gridDim.x * OWNER_WPB);
 }
 
 }  // namespace vmc
