@@ -131,8 +131,13 @@ static __device__ __noinline__ void batch_gen_walkers(const SweepArgs &a, int st
     }
 }
 
+// CTAs per SM the batch sweep is compiled for, its register budget (3: 80 registers
+// at 256 threads; 2, 128 registers, ran the 64-system workload 5 % slower)
+#ifndef BATCH_MIN_BLOCKS
+#define BATCH_MIN_BLOCKS 3
+#endif
 template <typename T, int FX>
-__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, 3) batch_sweep_kernel(const BatchLaunch b)
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, BATCH_MIN_BLOCKS) batch_sweep_kernel(const BatchLaunch b)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
