@@ -592,6 +592,15 @@ void vmo_initial_positions(uint64_t seed, uint32_t walker, int D, int normal, do
 
 /* ------------------------------------------------------------ sampling loop */
 
+/* The drift limiter of the corrected mode (Umrigar, Nightingale and Runge, J. Chem.
+ * Phys. 99, 2865 (1993)): v (-1 + sqrt(1 + 2 a dt v^2)) / (a dt v^2), written as
+ * 2 v / (1 + sqrt(1 + 2 a dt v^2)); a = 0 leaves v alone. */
+static double drift_limited(const vmo_system *s, double v)
+{
+    if (!(s->drift_limit > 0.0) || (s->quirks & VMO_Q_IS_GREEN)) return v;
+    return 2.0 * v / (1.0 + sqrt(1.0 + 2.0 * s->drift_limit * s->step * v * v));
+}
+
 int vmo_run(const vmo_system *s, const double *theta, int W, double *pos, double *fcache,
             double *gpair, int steps, int burn_in, int iter, int batches, const double *stream, uint64_t seed,
             uint64_t *counter, unsigned char *accepted, double *energies, double *sums)
@@ -620,7 +629,7 @@ int vmo_run(const vmo_system *s, const double *theta, int W, double *pos, double
                 if ((rc = eval_impl(s, theta, x, gp, grad, lap, pg, en))) break;
                 double gk = 0.0;
                 for (int e = 0; e < E; e++) gk += grad[e * D + k];
-                fn = 2.0 * gk;
+                fn = 2.0 * drift_limited(s, gk);
                 fo = (s->quirks & VMO_Q_IS_GREEN) ? fc[k] : fn;
                 dx = 0.5 * dt * fn + rnd[1] * sqdt;
             } else { /* bruteforce.cpp:34 */
@@ -640,7 +649,7 @@ int vmo_run(const vmo_system *s, const double *theta, int W, double *pos, double
                     if ((rc = eval_impl(s, theta, y, gp, grad, lap, pg, en))) break;
                     double gk = 0.0;
                     for (int e = 0; e < E; e++) gk += grad[e * D + k];
-                    double fy = 2.0 * gk;
+                    double fy = 2.0 * drift_limited(s, gk);
                     wgt = p * exp(0.5 * (fo + fy) * (0.25 * dt * (fo - fy) - dx));
                 }
             }

@@ -60,6 +60,7 @@ typedef struct {
     int quirks;               /* VMO_Q_* bits */
     double omega, Z, step;    /* omega, atomic number, stepLength (dt for IS) */
     double sigma;             /* RBM width (1/sqrt(omega) after the omega key) */
+    double drift_limit;       /* corrected IS: drift limiter a (0: off), v -> 2v / (1 + sqrt(1 + 2 a dt v^2)) */
 } vmo_system;
 
 /* Per-element parameter count (the reference's getNumberOfParameters after setConstants). */

@@ -41,6 +41,7 @@ class VmoSystem(ctypes.Structure):
         ("coulomb", ctypes.c_int), ("sampling", ctypes.c_int), ("hidden", ctypes.c_int),
         ("p_max", ctypes.c_int), ("quirks", ctypes.c_int), ("omega", ctypes.c_double),
         ("Z", ctypes.c_double), ("step", ctypes.c_double), ("sigma", ctypes.c_double),
+        ("drift_limit", ctypes.c_double),
     ]
 
 
@@ -58,6 +59,7 @@ class SystemSpec:
     atom: bool = False                     # atomicNucleus Hamiltonian instead of harmonic oscillator
     basis: str = "hermite"
     sorting: bool = False
+    drift_limit: float = 0.0               # corrected importance sampling: drift limiter a (0: off)
     optimization: str = "adam"
     learning_rate: float = 0.1
     num_steps: int = 1000
@@ -102,6 +104,8 @@ class SystemSpec:
         L.append(f"sorting: {'true' if self.sorting else 'false'}")
         L.append(f"sampling: {self.sampling}")
         L.append(f"stepLength: {self.step!r}")
+        if self.drift_limit > 0:
+            L.append(f"driftLimit: {self.drift_limit!r}")
         L.append(f"optimization: {self.optimization}")
         L.append(f"learningRate: {self.learning_rate!r}")
         L.append(f"numSteps: {self.num_steps}")
@@ -127,6 +131,7 @@ class SystemSpec:
         s.Z = float(self.Z)
         s.step = self.step
         s.sigma = 1.0 / np.sqrt(self.omega) if not self.atom else 1.0
+        s.drift_limit = self.drift_limit
         return s
 
 

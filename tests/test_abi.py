@@ -58,6 +58,13 @@ def test_library_exports_every_declared_symbol():
      "waveFunctionElement: gaussian\nbasis: hermite\nsweepForm: owner\n", -2),
     ("numParticles: 12\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
      "sweepForm: fastest\n", -1),
+    # the drift limiter: importance sampling in the corrected mode only
+    ("numParticles: 2\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
+     "sampling: importanceSampling\ndriftLimit: 0.5\n", -2),
+    ("numParticles: 2\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
+     "sampling: bruteForce\ncompat: corrected\ndriftLimit: 0.5\n", -2),
+    ("numParticles: 2\nhamiltonian: harmonicOscillator\nwaveFunctionElement: gaussian\n"
+     "compat: corrected\ndriftLimit: -1\n", -1),
 ])
 def test_create_rejects(text, code):
     from vmachine_b200 import library

@@ -138,10 +138,12 @@ def test_noninteracting_exact_energy():
             assert a.std_error < (1e-7 if precision == 0 else 1e-4)
 
 
-def test_corrected_mode_matches_oracle_chain():
-    """compat: corrected (full Pade ratio, Fokker-Planck Green's ratio) against the oracle."""
+@pytest.mark.parametrize("drift_limit", [0.0, 0.5])
+def test_corrected_mode_matches_oracle_chain(drift_limit):
+    """compat: corrected (full Pade ratio, Fokker-Planck Green's ratio) against the oracle,
+    without and with the drift limiter."""
     from oracle_bind import Q_RBM_SORT
-    spec = SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, quirks=0)
+    spec = SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, quirks=0, drift_limit=drift_limit)
     O = Oracle()
     rng = np.random.default_rng(11)
     steps = 300
@@ -160,15 +162,16 @@ def test_corrected_mode_matches_oracle_chain():
     del Q_RBM_SORT
 
 
-@pytest.mark.parametrize("Z,elements,compat", [
-    (2, (SLATER, SIMPLEJASTROW), 1), (10, (SLATER, SIMPLEJASTROW), 1),
-    (10, (SLATER, SIMPLEJASTROW), 0), (10, (SLATER, PADE, SIMPLEJASTROW), 0)])
-def test_atom_sweep_matches_oracle_chain(Z, elements, compat):
+@pytest.mark.parametrize("Z,elements,compat,drift_limit", [
+    (2, (SLATER, SIMPLEJASTROW), 1, 0.0), (10, (SLATER, SIMPLEJASTROW), 1, 0.0),
+    (10, (SLATER, SIMPLEJASTROW), 0, 0.0), (10, (SLATER, PADE, SIMPLEJASTROW), 0, 0.0),
+    (10, (SLATER, SIMPLEJASTROW), 0, 0.5)])
+def test_atom_sweep_matches_oracle_chain(Z, elements, compat, drift_limit):
     """Atoms (hydrogen-orbital Slater determinant with SimpleJastrow and Pade-Jastrow
     factors) take the general path's compiled 3D form: replayed chains of four
     walkers against the oracle, reference Green's ratio and corrected."""
     spec = SystemSpec(N=Z, d=3, Z=Z, atom=True, basis="hydrogenOrbital", elements=elements, step=0.01,
-                      quirks=SystemSpec().quirks if compat else 0)
+                      quirks=SystemSpec().quirks if compat else 0, drift_limit=drift_limit)
     rng = np.random.default_rng(Z + 7 * compat)
     W, steps = 4, 300
     pos = rng.normal(size=(W, spec.D))

@@ -57,6 +57,33 @@ def test_owner_sweep_matches_oracle(n, walkers, compat):
     assert abs(s.energy - out["sums"][:, 0].sum()) < 1e-10 * abs(out["sums"][:, 0].sum())
 
 
+@pytest.mark.parametrize("n,walkers", [(20, 19), (56, 5)])
+def test_owner_sweep_drift_limit_matches_oracle(n, walkers):
+    """The corrected mode's drift limiter (driftLimit: 0.5) in the FP64 owner sweep
+    against the oracle on Philox streams, as above."""
+    from vmachine_b200 import Engine
+    from vmachine_b200.engine import SWEEP_OWNER
+    steps, seed = 300, 1234
+    spec = spec_for(n, walkers, steps, 0, "owner")
+    spec.drift_limit = 0.5
+    rng = np.random.default_rng(n + 1)
+    pos = rng.normal(0, 1 / np.sqrt(OMEGA[n]), size=(walkers, spec.D))
+    theta = np.array([[0.0], [1.0], [0.5]])
+    with Engine(spec.input_in(), walkers=walkers, precision=0, compat=0) as eng:
+        assert eng.info.sweep_form == SWEEP_OWNER
+        eng.set_parameters(theta)
+        eng.init_walkers(pos, seed=seed)
+        s, _, _ = eng.sample(0, steps, 0)
+        final = eng.positions()
+    O = Oracle()
+    p = pos.copy()
+    f = np.stack([O.quantum_force(spec, theta, pos[w]) for w in range(walkers)])
+    out = O.run(spec, theta, p, f, steps, 0, 0, 10, stream=None, seed=seed, counter=np.zeros(walkers, np.uint64))
+    assert rel(final, p) < 1e-11
+    assert abs(s.accepts - out["sums"][:, 8].sum()) < 0.5
+    assert abs(s.energy - out["sums"][:, 0].sum()) < 1e-10 * abs(out["sums"][:, 0].sum())
+
+
 @pytest.mark.parametrize("n", [20, 56])
 @pytest.mark.parametrize("compat", [1, 0])
 def test_owner_mixed_tracks_staged(n, compat):

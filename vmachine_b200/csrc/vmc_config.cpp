@@ -286,6 +286,9 @@ std::string parse_config(const std::string &text, Config &c)
                 }
             } else if (key == "numWalkers") {
                 c.walkers = std::stoi(v0);
+            } else if (key == "driftLimit") {
+                c.drift_limit = std::stod(v0);
+                if (!(c.drift_limit >= 0.0)) return err("driftLimit must be >= 0");
             } else if (key == "walkerOffset") {
                 c.walker_offset = std::stoi(v0);
                 if (c.walker_offset < 0) return err("walkerOffset must be >= 0");

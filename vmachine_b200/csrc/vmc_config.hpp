@@ -55,6 +55,10 @@ struct Config {
     // engine keys (new)
     int walkers = 1;
     int walker_offset = 0;       // this engine's first walker in a sharded population (random streams)
+    // importance sampling, corrected mode: drift limiter constant a (0: off), the drift
+    // v = d ln Psi / dx scaled to 2 v / (1 + sqrt(1 + 2 a dt v^2)) in the proposal and
+    // in the Green's ratio (Umrigar, Nightingale and Runge, J. Chem. Phys. 99, 2865 (1993))
+    double drift_limit = 0.0;
     int precision = 0;           // 0 fp64, 1 mixed
     int refresh_interval = -1;   // -1 auto
     int compat = 1;              // 1 reference quirks, 0 corrected

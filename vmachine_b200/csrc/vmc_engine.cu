@@ -221,6 +221,7 @@ Params make_params(const vmc_engine *e)
     P.ep = e->EP;
     P.nacc = e->nacc_dev;
     P.walker_offset = e->cfg.walker_offset;
+    P.drift_limit = e->cfg.drift_limit;
     for (int i = 0; i < e->E && i < MAX_ELEM; ++i) P.elem_kind[i] = e->cfg.elements[i];
     P.flags = e->flags;
     P.sampling = e->sampling;
@@ -559,6 +560,10 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
     if (c.coulomb) flags |= F_COULOMB;
     if (c.hamiltonian == "atomicNucleus") flags |= F_ATOM;
     if (c.compat) flags |= Q_PADE_RATIO | Q_PADE_DGAMMA | Q_IS_GREEN | Q_PADE_STALE;
+    // the drift limiter changes the proposal and needs the Fokker-Planck Green's ratio:
+    // importance sampling in the corrected mode only
+    if (c.drift_limit > 0.0 && (c.compat || c.sampling == "bruteForce"))
+        return reject("driftLimit needs importanceSampling with compat: corrected");
     // quirk bits of the general-path elements only where those elements are present,
     // so a quantum dot keeps its compiled-in flag set
     if (c.compat && (flags & F_SIMPLEJ)) flags |= Q_SJ_RATIO;

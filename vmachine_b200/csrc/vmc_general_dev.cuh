@@ -978,7 +978,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
             if (a.probe_k) {
                 dx = a.probe_x[w] - xo;
             } else if (is) {
-                fn = 2.0 * rec[g.off_g + k];
+                fn = R(2) * limited_drift<R>(rec[g.off_g + k], P);
                 dx = 0.5 * dt * fn + r1 * sqdt;
             } else {
                 dx = 10.0 * (r1 - 0.5) * P.step;
@@ -1019,7 +1019,7 @@ __device__ __forceinline__ void gen_sweep_walker(const SweepArgs &a, int steps, 
                     if (P.flags & Q_IS_GREEN) {
                         wgt = (exp(0.5 * (fc[k] - fn) * dx) + 1.0) * prob;  // importancesampling.cpp:43-47
                     } else {
-                        const double fy = 2.0 * (double)gy, fnd = fn;
+                        const double fy = 2.0 * (double)limited_drift<R>(gy, P), fnd = fn;
                         wgt = prob * exp(0.5 * (fnd + fy) * (0.25 * dt * (fnd - fy) - (double)dx));
                     }
                 }

@@ -93,6 +93,7 @@ struct Params {
     int flags, sampling;
     double omega, alpha, gamma, gamma_prev, alpha_h, Z;
     double step;               // stepLength (brute force) or dt (importance sampling)
+    double drift_limit;        // importance sampling, corrected mode: the limiter's a (0: off)
     int idx_alpha, idx_gamma, idx_alpha_h;  // parameter slots (e*p_max + j) or -1
     double beta_same, beta_anti;            // Pade spin coefficients
     // device buffers
@@ -110,6 +111,20 @@ struct Params {
     float *mlp_cache;
     int mlp_cache_stride;
 };
+
+// The corrected mode's drift limiter (Umrigar, Nightingale and Runge, J. Chem. Phys. 99,
+// 2865 (1993)): v = d ln Psi / dx_k becomes v (-1 + sqrt(1 + 2 a dt v^2)) / (a dt v^2),
+// written as 2 v / (1 + sqrt(1 + 2 a dt v^2)), in the proposal and in the Green's ratio
+// alike, so the chain stays exact; a = P.drift_limit, 0 leaves v alone.  It bounds the
+// step a walker next to a node of the determinant takes, where v grows like 1 / distance.
+template <typename T>
+__device__ __forceinline__ T limited_drift(T v, const Params &P)
+{
+    if (!(P.drift_limit > 0.0)) return v;
+    const T c = T(2.0 * P.drift_limit * P.step);
+    return T(2) * v / (T(1) + sqrt(T(1) + c * v * v));
+}
+
 
 // Per-launch constants of the owner sweep, computed by the host in FP64 and passed in
 // both precisions, so the kernel reads them as constant operands

@@ -490,7 +490,7 @@ __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int step
                 const int pl = p - b * n;
                 const T2 xp = reinterpret_cast<const T2 *>(xs)[p];
                 const T xo = adim ? xp.y : xp.x;
-                const T Fn = T(2) * gs[k];
+                const T Fn = T(2) * limited_drift<T>(gs[k], P);
                 const T dx = hdt * Fn + zr * sdt;
                 const T xn = xo + dx;
                 const T qx = adim ? xp.x : xn, qy = adim ? xn : xp.y;  // proposed position of p
@@ -667,7 +667,7 @@ __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int step
                     const T gsl = __shfl_sync(FULL, sig_l * gl_, pl) * sq2;
                     const T gy = -wa * xn + __shfl_sync(FULL, tot, 16 + 4 * adim) + gsl / R;
                     const double prob = (double)(R * R) * (double)rat_g * (double)rat_p;
-                    const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
+                    const double fy = 2.0 * (double)limited_drift<T>(gy, P), fo2 = (double)Fn;
                     const double wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
                     if (wgt != wgt) status |= ST_BAD_RATIO;
                     accept = wgt >= ur * TWO_M32;

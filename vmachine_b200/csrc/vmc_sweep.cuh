@@ -439,7 +439,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             if (probe_k) {
                 dx = T(a.probe_x[w]) - xo;
             } else if (is) {
-                Fn = T(2) * Gk;
+                Fn = T(2) * limited_drift<T>(Gk, P);
                 dx = T(0.5 * P.step) * Fn + r1 * T(sqrt(P.step));
             } else {
                 dx = T(10) * (r1 - T(0.5)) * T(P.step);
@@ -660,7 +660,7 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                         if (jas) gy += __shfl_sync(FULL, pair_total, VL * (4 + adim), SEG);
                         if (flags & F_HYDROGENLIKE) gy += -T(P.alpha_h * P.Z) * xn / rpn;
                         if constexpr (K > 0) gy += Gs / R;
-                        const double fy = 2.0 * (double)gy, fo2 = (double)Fn;
+                        const double fy = 2.0 * (double)limited_drift<T>(gy, P), fo2 = (double)Fn;
                         wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
                     }
                 }

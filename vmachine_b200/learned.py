@@ -95,6 +95,7 @@ def evaluate_frozen(eng, text, eval_steps=4000, burn_steps=2000, step_length=1.0
     move is rejected), and such a walker's mean local energy, in the thousands, would
     dominate the estimate and its variance."""
     t = re.sub(r"^sampling:.*$", "sampling: bruteForce", text, flags=re.M)
+    t = re.sub(r"^driftLimit:.*\n?", "", t, flags=re.M)
     t = re.sub(r"^stepLength:.*$", f"stepLength: {step_length!r}", t, flags=re.M)
     t = re.sub(r"^precision:.*$", "precision: fp64", t, flags=re.M)
     ev = Engine(t)
@@ -106,20 +107,23 @@ def evaluate_frozen(eng, text, eval_steps=4000, burn_steps=2000, step_length=1.0
 
 
 def compare(N=20, omega=0.5, walkers=4096, steps=800, budget_s=120.0, eval_steps=4000,
-            lr_pade=0.01, lr_mlp=3e-4, seed=7, mlp_iterations=None, eval_burn=2000):
+            lr_pade=0.01, lr_mlp=3e-4, seed=7, mlp_iterations=None, eval_burn=2000, drift_limit=0.0):
     """Pade against MLP Jastrow at equal wall time: both train for budget_s seconds,
     or, with mlp_iterations, the MLP trains for that many iterations and the Pade
     factor for the MLP's wall time; then each frozen wave function is evaluated, on
     the training's walkers ("energy", "error": walker means) and blocked on fresh
     walkers after eval_burn steps of equilibration ("blocked"), and by brute-force
-    Metropolis in FP64 on fresh walkers ("frozen", evaluate_frozen)."""
+    Metropolis in FP64 on fresh walkers ("frozen", evaluate_frozen).  drift_limit > 0
+    trains both with the corrected mode's drift limiter (driftLimit)."""
     out = {"system": f"2D dot N={N} omega={omega}", "walkers": walkers, "steps_per_iteration": steps,
+           "drift_limit": drift_limit,
            "budget_s": budget_s, "eval_steps_per_walker": eval_steps}
     runs = (("pade", "padeJastrow", lr_pade), ("mlp", "mlpJastrow", lr_mlp))
     if mlp_iterations:
         runs = runs[::-1]
     for name, jastrow, lr in runs:
-        text = dot_config(N, omega, jastrow, walkers, steps, lr, seed=seed)
+        text = dot_config(N, omega, jastrow, walkers, steps, lr, seed=seed,
+                          extra=[f"driftLimit: {drift_limit!r}"] if drift_limit > 0 else ())
         if name == "mlp" and mlp_iterations:
             eng, hist = train(text, float("inf"), max_iterations=mlp_iterations, seed=seed)
             budget_s = hist[-1][0]
@@ -189,12 +193,14 @@ def main(argv=None):
                    help="train the MLP for this many iterations and the Pade factor for the same wall time")
     c.add_argument("--lr-mlp", type=float, default=3e-4)
     c.add_argument("--lr-pade", type=float, default=0.01)
+    c.add_argument("--drift-limit", type=float, default=0.0, help="train with the corrected mode's drift limiter")
     a = ap.parse_args(argv)
     if a.cmd == "speed":
         print(json.dumps(sweep_speed(a.walkers, a.steps, tensor_cores=not a.cuda_cores, precision=a.precision)))
     else:
         print(json.dumps(compare(walkers=a.walkers, steps=a.steps, budget_s=a.budget, lr_mlp=a.lr_mlp,
-                                 lr_pade=a.lr_pade, mlp_iterations=a.iterations or None)))
+                                 lr_pade=a.lr_pade, mlp_iterations=a.iterations or None,
+                                 drift_limit=a.drift_limit)))
 
 
 if __name__ == "__main__":
