@@ -490,7 +490,10 @@ __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int step
                 const int pl = p - b * n;
                 const T2 xp = reinterpret_cast<const T2 *>(xs)[p];
                 const T xo = adim ? xp.y : xp.x;
-                const T Fn = T(2) * limited_drift<T>(gs[k], P);
+                // the drift limiter is a corrected-mode option: compiled out of the reference form
+                T Fn;
+                if constexpr (GREEN_Q) Fn = T(2) * gs[k];
+                else Fn = T(2) * limited_drift<T>(gs[k], P);
                 const T dx = hdt * Fn + zr * sdt;
                 const T xn = xo + dx;
                 const T qx = adim ? xp.x : xn, qy = adim ? xn : xp.y;  // proposed position of p

@@ -439,7 +439,8 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
             if (probe_k) {
                 dx = T(a.probe_x[w]) - xo;
             } else if (is) {
-                Fn = T(2) * limited_drift<T>(Gk, P);
+                // the drift limiter is a corrected-mode option (no cost in the reference form)
+                Fn = T(2) * ((flags & Q_IS_GREEN) ? Gk : limited_drift<T>(Gk, P));
                 dx = T(0.5 * P.step) * Fn + r1 * T(sqrt(P.step));
             } else {
                 dx = T(10) * (r1 - T(0.5)) * T(P.step);
