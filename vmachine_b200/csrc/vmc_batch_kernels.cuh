@@ -69,6 +69,20 @@ __device__ __forceinline__ bool batch_next(const BatchLaunch &b, int lane, int2 
 // The warp's slice (`slice` doubles): GEN_SCR scratch doubles, then the staged record
 // and, when they fit too, the accumulators (the slice is sized by the batch's largest
 // dot record, so a large general-path walker stages less or nothing).
+// N = 42, 56: the owner-form sweep, with the drift limiter's instance where it is on
+template <typename T, int K, int FX>
+__device__ __forceinline__ void batch_owner_walkers(const BatchSys &sy, int steps, int off, unsigned char *ws, int w0,
+                                                    int w_end)
+{
+    if constexpr ((FX & Q_IS_GREEN) == 0) {
+        if (sy.a.P.drift_limit > 0.0) {
+            owner_sweep_walkers<T, K, FX, true>(sy.a, steps, off, ws, w0, w_end, 1);
+            return;
+        }
+    }
+    owner_sweep_walkers<T, K, FX>(sy.a, steps, off, ws, w0, w_end, 1);
+}
+
 // The atoms' FP32 sweep (g.f32): the same slice, with FP32 scratch and staged records
 // (the FP64 Slater inverse and the accumulators after each record).  Returns false when
 // the staged records do not fit the slice; the caller then runs the FP64 sweep on the
@@ -174,11 +188,11 @@ __global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, BATCH_MIN_BLOCKS) 
             else sweep_walkers<T, 2, 5, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
         case 6:
-            if (sy.owner) owner_sweep_walkers<T, 6, FX>(sy.a, steps, off, ws, item.y, w_end, 1);
+            if (sy.owner) batch_owner_walkers<T, 6, FX>(sy, steps, off, ws, item.y, w_end);
             else sweep_walkers<T, 2, 6, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
         case 7:
-            if (sy.owner) owner_sweep_walkers<T, 7, FX>(sy.a, steps, off, ws, item.y, w_end, 1);
+            if (sy.owner) batch_owner_walkers<T, 7, FX>(sy, steps, off, ws, item.y, w_end);
             else sweep_walkers<T, 2, 7, FX, true>(sy.a, steps, off, ws, item.y, w_end, 1);
             break;
         default:

@@ -193,7 +193,9 @@ __host__ __device__ constexpr int owner_smem_per_warp(int K, int elem_bytes)
 // by the calling warp, whose owner_smem_per_warp bytes of shared memory start at ws.
 // The sweep kernel below runs it over a launch's walkers; the multi-system batch kernel
 // over a work item's.
-template <typename T, int K, int FX>
+// LIMIT: the corrected mode's drift limiter (P.drift_limit > 0) compiled in; the callers
+// pick the instance per launch, so the default sweep carries none of it.
+template <typename T, int K, int FX, bool LIMIT = false>
 __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int steps, int step_offset, unsigned char *ws,
                                                     int w0, int w_end, int w_stride)
 {
@@ -492,7 +494,7 @@ __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int step
                 const T xo = adim ? xp.y : xp.x;
                 // the drift limiter is a corrected-mode option: compiled out of the reference form
                 T Fn;
-                if constexpr (GREEN_Q) Fn = T(2) * gs[k];
+                if constexpr (!LIMIT) Fn = T(2) * gs[k];
                 else Fn = T(2) * limited_drift<T>(gs[k], P);
                 const T dx = hdt * Fn + zr * sdt;
                 const T xn = xo + dx;
@@ -670,7 +672,7 @@ __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int step
                     const T gsl = __shfl_sync(FULL, sig_l * gl_, pl) * sq2;
                     const T gy = -wa * xn + __shfl_sync(FULL, tot, 16 + 4 * adim) + gsl / R;
                     const double prob = (double)(R * R) * (double)rat_g * (double)rat_p;
-                    const double fy = 2.0 * (double)limited_drift<T>(gy, P), fo2 = (double)Fn;
+                    const double fy = 2.0 * (double)(LIMIT ? limited_drift<T>(gy, P) : gy), fo2 = (double)Fn;
                     const double wgt = prob * exp(0.5 * (fo2 + fy) * (0.25 * P.step * (fo2 - fy) - (double)dx));
                     if (wgt != wgt) status |= ST_BAD_RATIO;
                     accept = wgt >= ur * TWO_M32;
@@ -961,8 +963,15 @@ __global__ void __launch_bounds__(OWNER_WPB * 32, sizeof(T) == 4 ? OWNER_MIN_CTA
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5;
-    owner_sweep_walkers<T, K, FX>(a, a.steps, a.step_offset, smem_raw + (size_t)wib * a.smem_per_warp,
-                                  blockIdx.x * OWNER_WPB + wib, a.P.W, gridDim.x * OWNER_WPB);
+    unsigned char *ws = smem_raw + (size_t)wib * a.smem_per_warp;
+    const int w0 = blockIdx.x * OWNER_WPB + wib, stride = gridDim.x * OWNER_WPB;
+    if constexpr ((FX & Q_IS_GREEN) == 0) {  // the limiter is a corrected-mode option
+        if (a.P.drift_limit > 0.0) {
+            owner_sweep_walkers<T, K, FX, true>(a, a.steps, a.step_offset, ws, w0, a.P.W, stride);
+            return;
+        }
+    }
+    owner_sweep_walkers<T, K, FX>(a, a.steps, a.step_offset, ws, w0, a.P.W, stride);
 }
 
 }  // namespace vmc
