@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from oracle_bind import Oracle, load_cases, spec_from_case
+from oracle_bind import GAUSSIAN, PADE, SLATER, Oracle, SystemSpec, load_cases, spec_from_case
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
@@ -132,3 +132,30 @@ def test_blocking(name):
     mean, var = oracle().blocking(c["x"])
     assert abs(mean - float(c["mean"])) < 1e-12 * max(1.0, abs(float(c["mean"])))
     assert abs(np.sqrt(var) - float(c["std_error"])) < 1e-9 * float(c["std_error"])
+
+
+def test_drift_limiter_in_the_oracle():
+    """The corrected mode's drift limiter in the oracle (driftLimit: a): a tiny a leaves
+    a replayed chain as it is without the limiter, a = 0.5 changes it, and the
+    reference mode ignores the constant (its proposal is the reference's)."""
+    spec0 = SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, quirks=0)
+    rng = np.random.default_rng(3)
+    steps = 200
+    pos = rng.normal(size=(1, spec0.D))
+    stream = np.stack([rng.random(steps), rng.normal(size=steps), rng.random(steps)], -1)[None]
+    theta = np.array([[0.0], [0.95], [0.6]])
+    O = Oracle()
+
+    def chain(spec):
+        p = pos.copy()
+        return O.run(spec, theta, p, np.zeros_like(p), steps, 0, 0, 1, stream=stream), p
+
+    (base, p0) = chain(spec0)
+    tiny, p1 = chain(SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, quirks=0, drift_limit=1e-12))
+    assert np.array_equal(base["accepted"], tiny["accepted"])
+    assert np.allclose(p0, p1, rtol=1e-9, atol=1e-12)
+    lim, p2 = chain(SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, quirks=0, drift_limit=0.5))
+    assert not np.allclose(p0, p2)
+    ref0, r0 = chain(SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05))
+    ref1, r1 = chain(SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, drift_limit=0.5))
+    assert np.array_equal(ref0["accepted"], ref1["accepted"]) and np.array_equal(r0, r1)
