@@ -29,7 +29,8 @@ enum {
     VMC_E_UNSUPPORTED = -2, /* a configuration the engine does not implement                   */
     VMC_E_CUDA = -3,        /* CUDA runtime error                                              */
     VMC_E_ARG = -4,         /* bad argument (size, NULL)                                       */
-    VMC_E_NAN = -5,         /* NaN kinetic energy (sampler.cpp:219-225 aborts with 143)        */
+    VMC_E_NAN = -5,         /* NaN kinetic energy (sampler.cpp:219-225 aborts with 143), or a NaN
+                               energy average: no optimiser step is taken                     */
     VMC_E_SINGULAR = -6,    /* singular Slater block at (re)initialisation                     */
     VMC_E_STATE = -7,       /* call out of order (e.g. sampling before walkers exist)          */
     VMC_E_TIMEOUT = -8,     /* a bounded device wait gave up: the pass is incomplete, its sums

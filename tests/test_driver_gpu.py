@@ -175,3 +175,23 @@ def test_convergence_check(tol, compat, expect):
     with Engine(text(32, 200, extra)) as e:
         e.init_walkers(None, seed=1)
         assert len(e.run_simulation()) == expect
+
+
+def test_nan_energy_average_takes_no_step():
+    """A pass whose energy average is NaN while its kinetic average is finite (a NaN
+    from the potential alone) returns VMC_E_NAN and leaves the parameters as they
+    were; the same pass with its genuine totals then takes the step."""
+    from vmachine_b200 import Engine
+    from vmachine_b200.engine import Sums, VmcError
+    with Engine(text(16, 100)) as e:
+        e.init_walkers(None, seed=1)
+        s, g, ge = e.sample(0, 200, 20)
+        before = e.parameters().copy()
+        bad = Sums.from_buffer_copy(s)
+        bad.energy = float("nan")
+        with pytest.raises(VmcError) as err:
+            e.apply_sums(bad, g, ge)
+        assert err.value.code == -5
+        assert np.array_equal(e.parameters(), before)
+        a = e.apply_sums(s, g, ge)
+        assert np.isfinite(a.energy) and not np.array_equal(e.parameters(), before)

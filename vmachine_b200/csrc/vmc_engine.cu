@@ -61,6 +61,15 @@ __global__ void reduce_acc_kernel(const double *acc, int W, int nacc, double *ou
         out[a] = S + C;
     }
 }
+
+// Per-walker mean energy (accumulator 0: sum plus its compensation) gathered into one
+// contiguous array, so that the host reads W doubles in one copy instead of W strided
+// 16-byte rows.
+__global__ void walker_means_kernel(const double *acc, int W, int nacc, double inv_n, double *out)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < W) out[w] = (acc[(size_t)w * nacc * 2] + acc[(size_t)w * nacc * 2 + 1]) * inv_n;
+}
 }  // namespace vmc
 
 namespace {
@@ -175,6 +184,7 @@ void free_engine(vmc_engine *e)
     cudaFree(e->d_acc);
     cudaFree(e->d_out);
     cudaFree(e->d_drift);
+    cudaFree(e->d_wmean);
     cudaFree(e->d_mask);
     cudaFree(e->d_counter);
     cudaFree(e->d_status);
@@ -685,6 +695,7 @@ int vmc_create(const char *text, const vmc_options *opt, vmc_engine **out)
             CUDA_TRY(cudaMalloc(&e->d_acc, W * e->nacc_dev * 2 * sizeof(double)));
             CUDA_TRY(cudaMalloc(&e->d_out, std::max(64, e->nacc_dev) * sizeof(double)));
             CUDA_TRY(cudaMalloc(&e->d_drift, W * sizeof(double)));
+            CUDA_TRY(cudaMalloc(&e->d_wmean, W * sizeof(double)));
             CUDA_TRY(cudaMalloc(&e->d_mask, W * e->N * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_counter, W * sizeof(unsigned long long)));
             CUDA_TRY(cudaMalloc(&e->d_status, W * sizeof(unsigned)));
@@ -992,12 +1003,13 @@ int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy)
 {
     if (!e || !mean_energy) return fail(VMC_E_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(e->device));
-    std::vector<double> col((size_t)e->W * 2);
-    CUDA_TRY(cudaMemcpy2DAsync(col.data(), 2 * sizeof(double), e->d_acc, e->nacc_dev * 2 * sizeof(double),
-                               2 * sizeof(double), e->W, cudaMemcpyDeviceToHost, e->stream));
-    CUDA_TRY(cudaStreamSynchronize(e->stream));
     const double n = std::max(1.0, e->last_samples_per_walker);
-    for (int w = 0; w < e->W; ++w) mean_energy[w] = (col[2 * w] + col[2 * w + 1]) / n;
+    walker_means_kernel<<<(e->W + 255) / 256, 256, 0, e->stream>>>(e->d_acc, e->W, e->nacc_dev, 1.0 / n,
+                                                                   e->d_wmean);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(mean_energy, e->d_wmean, (size_t)e->W * sizeof(double), cudaMemcpyDeviceToHost,
+                             e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
     return VMC_OK;
 }
 
@@ -1449,6 +1461,12 @@ int apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum, con
     if (std::isnan(a.kinetic)) {
         if (out) *out = a;
         return fail(VMC_E_NAN, "Energy exploded, please decrease the learning rate");
+    }
+    // a NaN local energy from the potential alone (the kinetic average finite) would
+    // otherwise reach the parameters through the gradient: no optimiser step either
+    if (std::isnan(a.energy)) {
+        if (out) *out = a;
+        return fail(VMC_E_NAN, "NaN local energy; the parameters are left unchanged");
     }
     // Optimization::getEnergyGradient (optimization.cpp:10-16)
     const size_t P = e->theta.size();

@@ -59,7 +59,7 @@ struct vmc_engine {
     int opt_step = 0;
     // device buffers
     void *d_state = nullptr;
-    double *d_scal = nullptr, *d_acc = nullptr, *d_out = nullptr, *d_drift = nullptr;
+    double *d_scal = nullptr, *d_acc = nullptr, *d_out = nullptr, *d_drift = nullptr, *d_wmean = nullptr;
     unsigned long long *d_mask = nullptr, *d_counter = nullptr;
     unsigned *d_status = nullptr;
     double *d_pos = nullptr;  // W x D positions staged for the host link

@@ -652,14 +652,23 @@ __device__ __forceinline__ void owner_sweep_walkers(const SweepArgs &a, int step
                 pend = false;
 
                 // ---- 2c/2d. ratio, Green's ratio, accept
-                const T rat_g = Fs::exp(wa * (xo * xo - xn * xn));
-                const T rat_p = Fs::exp(T(2) * sum_ratio);
+                // the Gaussian and Pade factors of the ratio: FP32 takes them as one
+                // exponential of the summed exponents; FP64 keeps the reference's two
+                // factors (and so its rounding)
+                T rat_g, rat_p;
+                if constexpr (F32) {
+                    rat_g = Fs::exp(fmaf(wa, (xo - xn) * (xo + xn), 2.0f * sum_ratio));
+                    rat_p = 1.0f;
+                } else {
+                    rat_g = Fs::exp(wa * (xo * xo - xn * xn));
+                    rat_p = Fs::exp(T(2) * sum_ratio);
+                }
                 bool accept;
                 if constexpr (GREEN_Q) {
                     // importancesampling.cpp:43-47: exp(0.5 (F_old(k) - F_new(k)) dx) + 1
                     const T ex = Fs::exp(T(0.5) * (fcs[k] - Fn) * dx);
                     if constexpr (F32) {
-                        const float wgt = (ex + 1.0f) * (R * R * rat_g * rat_p);
+                        const float wgt = (ex + 1.0f) * (R * R * rat_g);
                         if (wgt != wgt) status |= ST_BAD_RATIO;
                         accept = wgt >= __uint2float_rn(ur) * 2.3283064365386963e-10f;
                     } else {

@@ -797,21 +797,21 @@ __device__ __forceinline__ void sweep_walkers(const SweepArgs &a, int steps, int
                 constexpr int NV = VEC ? DK / VW : 1;
                 T ks = T(0);
                 auto coord_term = [&](int c, T xc, T g_s, T s_s, T g_j) {
-                    T G = T(0), lc = T(0);
-                    if (flags & F_GAUSS) G += -wa * xc;
+                    T Gc = T(0), lc = T(0);
+                    if (flags & F_GAUSS) Gc += -wa * xc;
                     if (K > 0) {
-                        G += g_s;
+                        Gc += g_s;
                         lc += s_s - g_s * g_s;
                     }
-                    if (jas) G += g_j;
+                    if (jas) Gc += g_j;
                     if (flags & F_HYDROGENLIKE) {
                         const int q = c / DIM;
                         T r2s = T(0);
 #pragma unroll
                         for (int e2 = 0; e2 < DIM; ++e2) r2s += x[q * DIM + e2] * x[q * DIM + e2];
-                        G += -T(P.alpha_h * P.Z) * xc * F::rsqrt(r2s);
+                        Gc += -T(P.alpha_h * P.Z) * xc * F::rsqrt(r2s);
                     }
-                    ks += G * G + lc;
+                    ks += Gc * Gc + lc;
                 };
                 if constexpr (VEC) {
                     using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
