@@ -276,9 +276,17 @@ def run_engine_arm(args):
         vd.run_iteration(eng, it)
     barrier(pg, local)
     sweep_s, launches, sig, energies = 0.0, 0.0, [], []
+    kernels = 0
     with ClockSampler(local) as clk:
         eng.stopwatch_start()
         for it in range(args.steps):
+            # this iteration's kernels: a sweep and an FP64 re-inversion per launch of
+            # refresh-interval steps, the accumulator reduction, two per-walker mean
+            # gathers (the engine's spread estimate and the shard's copy) and the
+            # re-inversion after the parameter step
+            interval = eng.refresh_interval()
+            n_launch = -(-(spw + burn) // interval) if interval > 0 else None
+            kernels += 2 * n_launch + 4 if n_launch else 0
             a = vd.run_iteration(eng, args.warmup + it)  # all-reduce of the sums when N > 1
             sig.append(a.walker_std_error)
             energies.append((a.energy, a.walker_std_error))
@@ -396,7 +404,7 @@ def run_engine_arm(args):
                          % (W * (eng.info.n_coords * 5 * 4 + 2 * 28 * 28 * 4 + 56 * 8 + 64) / 1e6)},
         "el_samples_per_s": value * spw / (spw + burn),
         "energy": energy, "sigma_e_walkers": sig[-1] if sig else None,
-        "gpu_launches": int(args.steps * (2 * launches + 1)),
+        "gpu_launches": int(kernels) if kernels else int(args.steps * (2 * launches + 4)),
         "roofline": {"bound": "fp32-pipe", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "traffic": SWEEP_TRAFFIC_BYTES,
@@ -460,7 +468,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    # the mixed engine's FP64 re-inversion cadence settles in the warm-up: it starts at
+    # 512 steps, the first passes from the starting distribution halve it to 256, and it
+    # doubles per pass while the inverse drift stays small, reaching its 8 192-step cap
+    # by the eighth pass
+    ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--walkers", type=int, default=16384)
     ap.add_argument("--steps-per-walker", type=int, default=20000)
