@@ -4,6 +4,7 @@
 // resets the hidden-node count and Z.  Errors are returned, not aborted on.
 #include "vmc_config.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <sstream>
 
@@ -51,35 +52,28 @@ const char *element_label(int e)
     }
 }
 
-// System::searchShortning (parser.cpp:340-390): rename the concatenated label
-// string when it is one of the orderings of `labels`.
+// System::searchShortning (parser.cpp:340-390) as a rule on the labels: the
+// concatenated string "_l1_l2..." takes the short name when it holds as many labels as
+// `labels` (at most four), each of them one of `labels`, and they are not all the same
+// one (a one-label list matches itself).  Repeats are allowed otherwise: the
+// reference's loops accept e.g. "_Gaussian_Gaussian_Pade-Jastrow" for three labels.
 void shortening(const std::vector<std::string> &labels, const std::string &name, std::string &all)
 {
-    const size_t n = labels.size();
-    if (n == 1 && all == "_" + labels[0]) all = name;
-    if (n == 2) {
-        for (auto &i : labels)
-            for (auto &j : labels)
-                if (i != j && all == "_" + i + "_" + j) { all = name; return; }
-    } else if (n == 3) {
-        for (auto &i : labels)
-            for (auto &j : labels)
-                for (auto &k : labels)
-                    if ((i != j || i != k || j != k) && all == "_" + i + "_" + j + "_" + k) {
-                        all = name;
-                        return;
-                    }
-    } else if (n == 4) {
-        for (auto &i : labels)
-            for (auto &j : labels)
-                for (auto &k : labels)
-                    for (auto &l : labels)
-                        if ((i != j || i != k || i != l || j != k || j != l || k != l) &&
-                            all == "_" + i + "_" + j + "_" + k + "_" + l) {
-                            all = name;
-                            return;
-                        }
+    if (all.empty() || all[0] != '_' || labels.size() > 4) return;
+    std::vector<std::string> parts;
+    for (size_t a = 1; a <= all.size();) {
+        size_t b = all.find('_', a);
+        if (b == std::string::npos) b = all.size();
+        parts.push_back(all.substr(a, b - a));
+        a = b + 1;
     }
+    if (parts.size() != labels.size()) return;
+    bool uniform = true;
+    for (const std::string &p : parts) {
+        if (std::find(labels.begin(), labels.end(), p) == labels.end()) return;
+        uniform = uniform && p == parts[0];
+    }
+    if (labels.size() == 1 || !uniform) all = name;
 }
 
 // System::collectAllLabels (parser.cpp:396-520)
