@@ -301,11 +301,14 @@ def run_engine_arm(args):
     value = total_moves / (ms * 1e-3)
     energy = a.energy
 
-    # e2e through the C ABI with host buffers: walkers uploaded, one iteration,
-    # walkers read back, every step
+    # e2e through the C ABI with pinned host buffers: walkers uploaded, one iteration,
+    # walkers read back, every step (each step's result is the next step's input)
     e2e = None
     if not args.no_e2e:
-        pos = eng.positions()
+        import torch
+        pinned = [torch.empty((eng.W, eng.D), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+        pos, nxt = (t.numpy() for t in pinned)
+        eng.positions(out=pos)
         h2d = pos.nbytes + 8 * eng.E * eng.P
         d2h = pos.nbytes + 8 * 16
         barrier(pg, local)
@@ -313,12 +316,13 @@ def run_engine_arm(args):
         for it in range(args.e2e_steps):
             eng.init_walkers(pos, seed=seed)
             vd.run_iteration(eng, 1000 + it)
-            pos = eng.positions()
+            eng.positions(out=nxt)
+            pos, nxt = nxt, pos
         e2e_ms = max_over_ranks(pg, local, eng.stopwatch_stop())
         e2e = {"value": moves_per_step * args.e2e_steps * world / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "vmc_init_walkers(host positions) + vmc_sample + vmc_apply_sums + "
-                       "vmc_get_positions per step"}
+               "path": "vmc_init_walkers(pinned host positions) + vmc_sample + vmc_apply_sums + "
+                       "vmc_get_positions(into pinned host memory) per step"}
 
     # FP64 engine on the same workload (same walkers, fewer steps per iteration)
     fp64 = None

@@ -207,8 +207,13 @@ class Engine:
             self.W, self.D)
         self._check(library().vmc_init_walkers(self._h, _p(pos), int(seed)))
 
-    def positions(self):
-        out = np.zeros((self.W, self.D))
+    def positions(self, out=None):
+        """Walker positions (W x D, FP64), into `out` when given (a C-contiguous float64
+        array of that shape, e.g. a pinned host buffer)."""
+        if out is None:
+            out = np.zeros((self.W, self.D))
+        elif out.shape != (self.W, self.D) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("positions: out must be a C-contiguous float64 array of shape (W, D)")
         self._check(library().vmc_get_positions(self._h, _p(out)))
         return out
 
