@@ -159,3 +159,83 @@ def test_drift_limiter_in_the_oracle():
     ref0, r0 = chain(SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05))
     ref1, r1 = chain(SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), step=0.05, drift_limit=0.5))
     assert np.array_equal(ref0["accepted"], ref1["accepted"]) and np.array_equal(r0, r1)
+
+
+DENS = load_cases(os.path.join(GOLD, "densities.npz"))
+SCHED = load_cases(os.path.join(GOLD, "schedules.npz"))
+
+
+@pytest.mark.parametrize("name", sorted(DENS))
+def test_densities(name):
+    """The oracle's chains, binned after every step by the host restatement of the
+    Sampler's densities, give exactly the reference's counts (tests/golden/densities.npz:
+    its own Sampler on the same replayed numbers, summed over walkers).  An atom's
+    densities see the current radii; a dot's radial densities the starting ones."""
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from oracle.vmc_oracle_host import DensityCounts, radial_vector_updated, radii
+    from oracle_bind import HYDROGENLIKE
+    c = DENS[name]
+    spec = spec_from_case(c)
+    O = oracle()
+    counts = DensityCounts(int(c["bins"]), float(c["max_radius"]))
+    moving = radial_vector_updated(spec.atom, HYDROGENLIKE in spec.elements)
+    W, steps = c["stream"].shape[:2]
+    for w in range(W):
+        pos = c["pos"][w][None].copy()
+        f = O.quantum_force(spec, c["theta"], c["pos"][w])[None].copy()
+        r0 = radii(pos[0], spec.d)
+        for s in range(steps):
+            O.run(spec, c["theta"], pos, f, 1, 0, 0, 1, stream=c["stream"][w:w + 1, s:s + 1], want_steps=False)
+            counts.add(pos[0], radii(pos[0], spec.d) if moving else r0, spec.d)
+    assert np.array_equal(counts.spatial, c["spatial"])
+    assert np.array_equal(counts.radial, c["radial"])
+    assert np.array_equal(counts.pair, c["pair"])
+
+
+@pytest.mark.parametrize("name", sorted(SCHED))
+def test_simulation_schedule(name):
+    """System::runSimulation's schedule (convergence check, adaptive steps) restated on
+    the host around the oracle's iterations gives the reference's step counts, density
+    iteration and energies on the same replayed numbers (tests/golden/schedules.npz)."""
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from oracle.vmc_oracle_host import Adam, Schedule, averages, energy_gradient
+    c = SCHED[name]
+    spec = spec_from_case(c)
+    keys = dict(line.split(": ", 1) for line in str(c["extra"]).split("\n") if line)
+    on = {"true": True, "false": False}
+    sched = Schedule(int(keys["numIterations"]), spec.num_steps,
+                     adaptive=on[keys["applyAdaptiveSteps"]], range_=int(keys["rangeOfAdaptiveSteps"]),
+                     additional=int(keys["additionalSteps"]), additional_last=int(keys["additionalStepsLastIter"]),
+                     check=on[keys["checkConvergence"]], n_energies=int(keys["numberOfEnergies"]),
+                     tolerance=float(keys["tolerance"]))
+    assert spec.optimization == "adam" and spec.sampling == "bruteForce"
+    O = oracle()
+    theta = c["theta"].copy()
+    E, P = theta.shape
+    optim = Adam(theta.shape, spec.learning_rate)
+    pos = c["pos"][None].copy()
+    f = np.zeros_like(pos)
+    gpair = np.zeros((1, spec.N, spec.N))
+    if PADE in spec.elements:
+        gpair[:] = theta[list(spec.elements).index(PADE), 0]
+    # burn-in: the equilibration fraction main() sets, 0.001 (main.cpp:10), of the
+    # initial step count, the same in every iteration (userinput.cpp:74)
+    burn = int(spec.num_steps * 0.001)
+    off, steps, energy, last = 0, [], [], []
+    for it in range(sched.n_iterations):
+        n = sched.steps(it)
+        stream = c["stream"][off:off + n + burn][None]
+        off += n + burn
+        out = O.run(spec, theta, pos, f, n + burn, burn, it, optim.batches, stream=stream, want_steps=False,
+                    gpair=gpair)
+        avg = averages(out["sums"].sum(0), n, n // optim.batches, (E, P))
+        theta = theta - optim.update(energy_gradient(avg))
+        steps.append(n)
+        last.append(int(sched.is_density_iteration(it)))
+        energy.append(avg["energy"])
+        sched.after(it, avg["energy"])
+    assert steps == [int(v) for v in c["steps"]]
+    assert last == [int(v) for v in c["last"]]
+    assert rel(energy, c["energy"]) < TOL
