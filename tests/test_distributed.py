@@ -5,9 +5,10 @@ MPI_Reduce + MPI_Bcast, src/sampler.cpp:111-187, src/system.cpp:130-135); the
 walkers' error bar and status bits are those of all walkers; a rank whose pass
 fails makes every rank raise (after the same collectives, so none waits).
 
-The engines here are host fakes (no GPU): sample() returns rank-dependent
-totals; apply_sums() restates the averages and ADAM step with the CPU checker.
-Real engines on a GPU: tests/test_distributed_gpu.py.
+The engines here run on the host (no GPU): fakes whose sample() returns
+rank-dependent totals, and shards of one walker population whose chains the C oracle
+runs on replayed random numbers; apply_sums() restates the averages and ADAM step with
+the CPU checker.  Real engines on a GPU: tests/test_distributed_gpu.py.
 """
 import os
 import socket
@@ -179,3 +180,110 @@ def test_a_failing_rank_fails_every_rank():
             p.join(timeout=120)
             assert p.exitcode == 0
         assert out[0] == [0, -8, 0] and out[1] == [0, -8, 0]
+
+
+class OracleShard:
+    """A slice of one walker population run by the C oracle (oracle/vmc_oracle.c),
+    with the engine's interface as distributed.run_iteration uses it.  Every walker
+    has its own replayed random stream, the population's row for that walker, so a
+    slice walks exactly the chains the whole population walks."""
+
+    STEPS, BURN = 200, 2
+
+    def __init__(self, lo, hi, n_walkers=6, iterations=3):
+        sys.path.insert(0, HERE)
+        sys.path.insert(0, ROOT)
+        from oracle.vmc_oracle_host import Adam
+        from oracle_bind import GAUSSIAN, PADE, Oracle, SystemSpec
+        from vmachine_b200.engine import Info
+        self.spec = SystemSpec(N=2, elements=(GAUSSIAN, PADE), step=0.05, omega=1.0)
+        self.O = Oracle()
+        rng = np.random.default_rng(11)
+        D, per = self.spec.D, self.STEPS + self.BURN
+        pos = rng.normal(0.0, 1.0, (n_walkers, D))
+        stream = np.empty((n_walkers, per * iterations, 3))
+        stream[..., 0] = rng.random(stream.shape[:2])
+        stream[..., 1] = rng.normal(size=stream.shape[:2])
+        stream[..., 2] = rng.random(stream.shape[:2])
+        self.pos, self.stream = pos[lo:hi].copy(), stream[lo:hi]
+        self.theta = np.array([[1.0], [0.5]])
+        self.E, self.P = self.theta.shape
+        self.f = np.stack([self.O.quantum_force(self.spec, self.theta, p) for p in self.pos])
+        self.opt = Adam(self.theta.shape, 0.05)
+        self.info = Info()
+        self.info.steps_per_walker, self.info.burn_in, self.info.precision = self.STEPS, self.BURN, 0
+        self.off, self.means = 0, None
+
+    def sample(self, iteration, steps, burn_in):
+        from vmachine_b200.engine import Sums
+        W = len(self.pos)
+        out = self.O.run(self.spec, self.theta, self.pos, self.f, steps, burn_in, iteration,
+                         self.opt.batches, stream=self.stream[:, self.off:self.off + steps], want_steps=False)
+        self.off += steps
+        per_walker = out["sums"]
+        n = steps - burn_in
+        self.means = per_walker[:, 0] / n
+        S = per_walker.sum(0)
+        s = Sums()
+        for i, f in enumerate(("energy", "energy2", "kinetic", "kinetic2", "external", "external2",
+                               "interaction", "interaction2", "accepts")):
+            setattr(s, f, S[i])
+        s.n_samples, s.n_window = W * n, W * (n // self.opt.batches)
+        ep = self.E * self.P
+        return s, S[9:9 + ep].reshape(self.E, self.P), S[9 + ep:9 + 2 * ep].reshape(self.E, self.P)
+
+    def walker_energies(self):
+        return self.means
+
+    def apply_sums(self, s, g, ge):
+        from oracle.vmc_oracle_host import averages, energy_gradient
+        vec = [s.energy, s.energy2, s.kinetic, s.kinetic2, s.external, s.external2, s.interaction,
+               s.interaction2, s.accepts]
+        avg = averages(np.concatenate([vec, g.ravel(), ge.ravel()]), s.n_samples, s.n_window,
+                       (self.E, self.P))
+        self.theta = self.theta - self.opt.update(energy_gradient(avg))
+        return avg
+
+
+def _oracle_rank(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    from vmachine_b200 import distributed as vd
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    eng = OracleShard(3 * rank, 3 * rank + 3)
+    hist = []
+    for it in range(3):
+        a = vd.run_iteration(eng, it)
+        hist.append((a["energy"], a["walker_std_error"]))
+    out[rank] = (eng.theta.copy(), hist)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_of_oracle_chains_equal_one_population():
+    """Two ranks, each running three walkers' chains in the C oracle, all-reduce their
+    totals through distributed.run_iteration: every iteration's energy and walker
+    error bar and the parameters after three ADAM steps equal those of one process
+    running all six walkers (the reference's one-rank computeTotals and update)."""
+    sys.path.insert(0, ROOT)
+    from vmachine_b200 import distributed as vd
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_oracle_rank, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+        (theta0, hist0), (theta1, hist1) = out[0], out[1]
+    assert np.array_equal(theta0, theta1) and hist0 == hist1
+    one = OracleShard(0, 6)
+    for it in range(3):
+        a = vd.run_iteration(one, it)
+        assert abs(a["energy"] - hist0[it][0]) <= 1e-13 * abs(a["energy"])
+        # the spread from summed moments cancels: a few units in the 12th digit
+        assert abs(a["walker_std_error"] - hist0[it][1]) <= 1e-10 * a["walker_std_error"]
+    assert np.allclose(theta0, one.theta, rtol=1e-12, atol=0)
