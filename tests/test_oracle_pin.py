@@ -239,3 +239,22 @@ def test_simulation_schedule(name):
     assert steps == [int(v) for v in c["steps"]]
     assert last == [int(v) for v in c["last"]]
     assert rel(energy, c["energy"]) < TOL
+
+
+def test_exact_energies():
+    """The exact ground states the reference's tests use: two non-interacting
+    electrons in the 2D oscillator, omega = 1, with the Gaussian at alpha = 1, have
+    E_L = 2 at every position (zero variance); a Slater determinant of Hermite
+    orbitals times that Gaussian is the exact closed-shell state of N = 6 and 12,
+    E_L = sum of the shell energies (10 and 28) everywhere."""
+    O = oracle()
+    rng = np.random.default_rng(5)
+    for N, exact, elements in ((2, 2.0, (GAUSSIAN,)), (6, 10.0, (SLATER, GAUSSIAN)),
+                               (12, 28.0, (SLATER, GAUSSIAN))):
+        spec = SystemSpec(N=N, elements=elements, coulomb=False, omega=1.0)
+        theta = np.zeros((len(elements), spec.p_max))
+        theta[list(elements).index(GAUSSIAN), 0] = 1.0
+        for _ in range(5):
+            _, _, _, en = O.eval(spec, theta, rng.normal(0.0, 1.0, spec.D))
+            assert abs(en.sum() - exact) < 1e-10 * exact, (N, en)
+            assert en[2] == 0.0
