@@ -5,7 +5,8 @@ forward and backward kernels (N = 20, omega = 0.5 quantum dot).
   start (the network's output layers start at zero, so the untrained factor is the
   cusp term alone, with alpha = 1).
 - At equal wall time the trained MLP's energy is not above the Pade-Jastrow's trained
-  by the same engine by more than 3 sigma: both frozen wave functions are evaluated
+  by the same engine by more than 3 sigma or 0.02 (0.02 %), whichever is larger: both
+  frozen wave functions are evaluated
   by brute-force Metropolis in FP64 on fresh walkers with every walker's series
   blocked on the device (learned.evaluate_frozen), sigma the two blocked error bars
   in quadrature.  The gap and the variances of the local energy are printed.
@@ -15,7 +16,9 @@ The gap itself is not asserted: it depends on the training run.  Importance samp
 at dt = 0.01 leaves a few walkers stuck next to a node of the determinant, and the
 MLP's gradient sums are accumulated with atomic additions, so two runs of the same
 configuration part during training.  Runs of this test have ended with the MLP below
-the Pade by 0.060 (18 sigma) and level with it (-0.0001, 0.0 sigma).
+the Pade by 0.060 (18 sigma) and level with it (-0.0001, 0.0 sigma); in the second the
+Pade itself ended 0.013 higher than in the first, so a run that perturbs only the MLP
+could leave it a few sigma above.
 """
 import math
 
@@ -48,4 +51,4 @@ def test_trained_network_gains():
           f"var {b_mlp['variance']:.3f} ({len(hist)} iterations)  Pade {b_pade['energy']:.4f}+-{b_pade['error']:.4f} "
           f"var {b_pade['variance']:.3f} ({len(phist)} iterations)  gap {gap:.4f} = {gap / sigma:.1f} sigma")
     assert b_mlp["energy"] < e0 - 5 * (s0 + b_mlp["error"])
-    assert gap > -3 * sigma
+    assert gap > -max(3 * sigma, 0.02)
