@@ -481,4 +481,15 @@ long vmref_format_weights(const double *theta, int E, int P, char *buf, long cap
     return (long)t.size();
 }
 
+// System's trial wave-function label (System::collectAllLabels, parser.cpp:396-520),
+// the name Automatize reads to choose the initial weights.  Writes it NUL-terminated
+// into buf and returns its length, or -1 if cap is too small.
+long vmref_trial_label(void *hp, char *buf, long cap)
+{
+    const std::string t = static_cast<Handle *>(hp)->sys->getTrialWaveFunction();
+    if ((long)t.size() + 1 > cap) return -1;
+    std::memcpy(buf, t.c_str(), t.size() + 1);
+    return (long)t.size();
+}
+
 }  // extern "C"

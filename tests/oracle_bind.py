@@ -297,6 +297,16 @@ class RefHarness:
         used = self.lib.vmref_steps(self.h, n, _ptr(acc), _ptr(en), _ptr(pg))
         return acc, en, pg, used
 
+    def trial_label(self):
+        """System's trial wave-function label (vmref_trial_label)."""
+        L = self.lib
+        L.vmref_trial_label.restype = ctypes.c_long
+        L.vmref_trial_label.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_long]
+        buf = ctypes.create_string_buffer(512)
+        n = L.vmref_trial_label(self.h, buf, len(buf))
+        assert n >= 0
+        return buf.raw[:n].decode()
+
     def densities(self, n, bins, max_radius, radial=True, spatial=True, pair=True):
         """n steps counting the Sampler's densities after each (vmref_densities)."""
         L = self.lib
