@@ -481,6 +481,30 @@ long vmref_format_weights(const double *theta, int E, int P, char *buf, long cap
     return (long)t.size();
 }
 
+// System's settings after parsing and set-up, as doubles in this order: particles,
+// dimensions, omega, sigma, Z, hidden units, learning rate, iterations, equilibration
+// fraction, total steps without burn-in, step length, sorting, max radius, bins,
+// tolerance, energies kept by the convergence check, range of adaptive steps,
+// additional steps, additional steps in the last iteration, checkpoint frequency, and
+// the convergence-check, adaptive-steps and three density switches.  Returns 25.
+int vmref_settings(void *hp, double *out)
+{
+    const System *s = static_cast<Handle *>(hp)->sys;
+    const double v[] = {double(s->m_numberOfParticles), double(s->m_numberOfDimensions), s->m_omega,
+                        s->m_sigma, double(s->m_Z), double(s->m_numberOfHiddenUnits), s->m_eta,
+                        double(s->m_numberOfIterations), s->m_equilibrationFraction,
+                        double(s->m_initialTotalStepsWOEqui), s->m_stepLength, double(s->m_sorting),
+                        s->m_maxRadius, double(s->m_numberOfBins), s->m_tolerance,
+                        double(s->m_numberOfEnergies), double(s->m_rangeOfAdaptiveSteps),
+                        double(s->m_additionalSteps), double(s->m_additionalStepsLastIter),
+                        double(s->m_checkpointFreq), double(s->m_checkConvergence),
+                        double(s->m_applyAdaptiveSteps), double(s->m_computeOneBodyDensity),
+                        double(s->m_computeOneBodyDensity2), double(s->m_computeTwoBodyDensity)};
+    const int n = int(sizeof(v) / sizeof(v[0]));
+    for (int i = 0; i < n; i++) out[i] = v[i];
+    return n;
+}
+
 // System's trial wave-function label (System::collectAllLabels, parser.cpp:396-520),
 // the name Automatize reads to choose the initial weights.  Writes it NUL-terminated
 // into buf and returns its length, or -1 if cap is too small.

@@ -227,7 +227,7 @@ class Oracle:
 class RefHarness:
     """One reference System (one walker) at fixed positions with a replayed stream."""
 
-    def __init__(self, spec, pos, theta=None, stream=None, path=REF_SO):
+    def __init__(self, spec, pos, theta=None, stream=None, path=REF_SO, text=None):
         self.lib = ctypes.CDLL(path)
         L = self.lib
         L.vmref_create.restype = ctypes.c_void_p
@@ -249,7 +249,8 @@ class RefHarness:
         pos = np.ascontiguousarray(pos, np.float64)
         th = None if theta is None else np.ascontiguousarray(theta, np.float64).ravel()
         st = None if stream is None else np.ascontiguousarray(stream, np.float64).ravel()
-        self.h = L.vmref_create(spec.input_in().encode(), _ptr(pos), len(pos), _ptr(th),
+        config = text if text is not None else spec.input_in()
+        self.h = L.vmref_create(config.encode(), _ptr(pos), len(pos), _ptr(th),
                                 0 if th is None else len(th), _ptr(st),
                                 0 if st is None else len(st))
         assert self.h, "reference harness failed to build the system"
@@ -296,6 +297,15 @@ class RefHarness:
         pg = np.zeros((n, self.E, self.P))
         used = self.lib.vmref_steps(self.h, n, _ptr(acc), _ptr(en), _ptr(pg))
         return acc, en, pg, used
+
+    def settings(self):
+        """System's parsed settings (vmref_settings)."""
+        L = self.lib
+        L.vmref_settings.restype = ctypes.c_int
+        L.vmref_settings.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        out = np.zeros(32)
+        n = L.vmref_settings(self.h, _ptr(out))
+        return out[:n]
 
     def trial_label(self):
         """System's trial wave-function label (vmref_trial_label)."""

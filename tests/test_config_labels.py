@@ -1,5 +1,9 @@
-"""The engine's input.in parser against the reference's on the host: for every
-element set the engine runs, the trial wave-function label (System::collectAllLabels,
+"""The engine's input.in parser against the reference's on the host.
+
+The parsed settings (system size, omega and what it resets, Z and the hidden units and
+what resets them, learning rate, steps, burn-in fraction, the driver's keys) equal the
+reference System's after it parses the same text.  For every element set the engine
+runs, the trial wave-function label (System::collectAllLabels,
 parser.cpp:396-520: the element labels joined, then renamed by searchShortning,
 :340-390), which Automatize reads to pick the initial weights
 (InitialWeights/automatize.cpp), is the one the reference's own System builds from the
@@ -75,3 +79,57 @@ def test_trial_label_matches_reference(name, spec):
     finally:
         ref.close()
     assert ours == theirs, (name, ours, theirs)
+
+
+SETTINGS = ("particles", "dimensions", "omega", "sigma", "Z", "hidden units", "learning rate",
+            "iterations", "equilibration fraction", "total steps", "step length", "sorting",
+            "max radius", "bins", "tolerance", "energies", "range of adaptive steps",
+            "additional steps", "additional steps last", "checkpoint frequency", "check convergence",
+            "adaptive steps", "one-body density", "spatial density", "two-body density")
+
+BODY = ["hamiltonian: harmonicOscillator", "interactionStyle: coulomb", "waveFunctionElement: gaussian",
+        "waveFunctionElement: padeJastrow", "sampling: importanceSampling", "optimization: adam",
+        "numSteps: 1000", "numIterations: 12"]
+
+SETTING_CASES = [
+    # main.cpp's defaults and system.h's
+    ("defaults", ["numParticles: 2", "numDimensions: 2"]),
+    # omega: resets stepLength to 0.1 / sqrt(omega) and the RBM width (parser.cpp:57-60)
+    ("omega_then_step", ["numParticles: 2", "omega: 0.5", "stepLength: 0.2"]),
+    ("step_then_omega", ["numParticles: 2", "stepLength: 0.2", "omega: 0.5"]),
+    # numParticles: resets Z and the hidden units (parser.cpp:51-54)
+    ("hidden_then_particles", ["numHiddenNodes: 3", "numParticles: 6"]),
+    ("particles_then_hidden", ["numParticles: 6", "numHiddenNodes: 3"]),
+    ("z_then_particles", ["atomicNumber: 3", "numParticles: 4"]),
+    ("particles_then_z", ["numParticles: 4", "atomicNumber: 3"]),
+    # the driver's keys
+    ("driver", ["numParticles: 2", "learningRate: 0.02", "equilibration: 0.01", "sorting: false",
+                "maxRadius: 3.0", "numberOfBins: 50", "checkConvergence: true", "numberOfEnergies: 7",
+                "tolerance: 1e-5", "applyAdaptiveSteps: true", "rangeOfAdaptiveSteps: 4",
+                "additionalSteps: 2", "additionalStepsLastIter: 3", "checkpointFreq: 10",
+                "computeOneBodyDensity: true", "computeOneBodyDensity2: true",
+                "computeTwoBodyDensity: true"]),
+]
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.exists(REF_SO),
+                    reason="needs g++ and the reference harness")
+@pytest.mark.parametrize("name,lines", SETTING_CASES, ids=[c[0] for c in SETTING_CASES])
+def test_parsed_settings_match_reference(name, lines):
+    """The same input.in text through the engine's parser and the reference's
+    (System::parser and its set-up) gives the same settings, key side effects included."""
+    text = "\n".join(lines + BODY) + "\n"
+    lib = shim()
+    lib.cfg_settings.restype = ctypes.c_int
+    lib.cfg_settings.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    ours = np.zeros(len(SETTINGS))
+    assert lib.cfg_settings(text.encode(), ours.ctypes.data) == len(SETTINGS)
+    N = int(ours[0])
+    ref = RefHarness(None, np.random.default_rng(1).normal(0.0, 1.0, 2 * N), text=text)
+    try:
+        theirs = ref.settings()
+    finally:
+        ref.close()
+    assert len(theirs) == len(SETTINGS)
+    diff = [(k, a, b) for k, a, b in zip(SETTINGS, ours, theirs) if not np.isclose(a, b, rtol=1e-15, atol=0)]
+    assert not diff, (name, diff)
