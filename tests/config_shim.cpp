@@ -31,3 +31,14 @@ extern "C" int cfg_settings(const char *text, double *out)
     for (int i = 0; i < n; i++) out[i] = v[i];
     return n;
 }
+
+// Per-element parameter counts of the parsed configuration, in element order.
+// Returns the number of elements, or -1 if the text does not parse.
+extern "C" int cfg_parameter_counts(const char *text, int *out, int cap)
+{
+    vmc::Config c;
+    if (!vmc::parse_config(text, c).empty()) return -1;
+    const int n = (int)c.elements.size();
+    for (int i = 0; i < n && i < cap; i++) out[i] = vmc::element_parameters(c, c.elements[i]);
+    return n;
+}

@@ -81,6 +81,28 @@ def test_trial_label_matches_reference(name, spec):
     assert ours == theirs, (name, ours, theirs)
 
 
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.exists(REF_SO),
+                    reason="needs g++ and the reference harness")
+@pytest.mark.parametrize("name,spec", CASES, ids=[c[0] for c in CASES])
+def test_parameter_counts_match_reference(name, spec):
+    """The parameter matrix has the reference's shape: as many rows as elements and
+    as many columns as the largest element's parameter count (System::setMaxParameters,
+    elementoperation.cpp:173-186), with each element's count from the engine's
+    element_parameters."""
+    lib = shim()
+    lib.cfg_parameter_counts.restype = ctypes.c_int
+    lib.cfg_parameter_counts.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int]
+    counts = np.zeros(16, np.int32)
+    n = lib.cfg_parameter_counts(spec.input_in().encode(), counts.ctypes.data, len(counts))
+    assert n == len(spec.elements)
+    ref = RefHarness(spec, np.random.default_rng(1).normal(0.0, 1.0, spec.D))
+    try:
+        E, P = ref.E, ref.P
+    finally:
+        ref.close()
+    assert (n, int(counts[:n].max())) == (E, P), (name, counts[:n], E, P)
+
+
 SETTINGS = ("particles", "dimensions", "omega", "sigma", "Z", "hidden units", "learning rate",
             "iterations", "equilibration fraction", "total steps", "step length", "sorting",
             "max radius", "bins", "tolerance", "energies", "range of adaptive steps",
