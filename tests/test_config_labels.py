@@ -46,31 +46,34 @@ CASES = [
     ("he_hydrogenlike_pade", SystemSpec(N=2, d=3, Z=2, elements=(H, P), atom=True)),
 ]
 
-SHIM = None
+NEEDS = pytest.mark.skipif(shutil.which("g++") is None or not os.path.exists(REF_SO),
+                           reason="needs g++ and the reference harness")
 
 
-def shim():
-    global SHIM
-    if SHIM is None:
-        import tempfile
-        out = os.path.join(tempfile.mkdtemp(prefix="cfgshim_"), "libcfgshim.so")
-        src = os.path.join(ROOT, "vmachine_b200", "csrc")
-        subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", "-I", src,
-                        os.path.join(HERE, "config_shim.cpp"), os.path.join(src, "vmc_config.cpp"),
-                        "-o", out], check=True)
-        SHIM = ctypes.CDLL(out)
-        SHIM.cfg_trial_label.restype = ctypes.c_long
-        SHIM.cfg_trial_label.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_long]
-    return SHIM
+@pytest.fixture(scope="module")
+def shim(tmp_path_factory):
+    """The engine's parser (vmc_config.cpp) and tests/config_shim.cpp built for the host."""
+    out = str(tmp_path_factory.mktemp("cfgshim") / "libcfgshim.so")
+    src = os.path.join(ROOT, "vmachine_b200", "csrc")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", "-I", src,
+                    os.path.join(HERE, "config_shim.cpp"), os.path.join(src, "vmc_config.cpp"),
+                    "-o", out], check=True)
+    lib = ctypes.CDLL(out)
+    lib.cfg_trial_label.restype = ctypes.c_long
+    lib.cfg_trial_label.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_long]
+    lib.cfg_settings.restype = ctypes.c_int
+    lib.cfg_settings.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    lib.cfg_parameter_counts.restype = ctypes.c_int
+    lib.cfg_parameter_counts.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int]
+    return lib
 
 
-@pytest.mark.skipif(shutil.which("g++") is None or not os.path.exists(REF_SO),
-                    reason="needs g++ and the reference harness")
+@NEEDS
 @pytest.mark.parametrize("name,spec", CASES, ids=[c[0] for c in CASES])
-def test_trial_label_matches_reference(name, spec):
+def test_trial_label_matches_reference(shim, name, spec):
     text = spec.input_in()
     buf = ctypes.create_string_buffer(512)
-    n = shim().cfg_trial_label(text.encode(), buf, len(buf))
+    n = shim.cfg_trial_label(text.encode(), buf, len(buf))
     assert n >= 0, f"the engine's parser rejected {name}"
     ours = buf.raw[:n].decode()
     ref = RefHarness(spec, np.random.default_rng(1).normal(0.0, 1.0, spec.D))
@@ -81,17 +84,14 @@ def test_trial_label_matches_reference(name, spec):
     assert ours == theirs, (name, ours, theirs)
 
 
-@pytest.mark.skipif(shutil.which("g++") is None or not os.path.exists(REF_SO),
-                    reason="needs g++ and the reference harness")
+@NEEDS
 @pytest.mark.parametrize("name,spec", CASES, ids=[c[0] for c in CASES])
-def test_parameter_counts_match_reference(name, spec):
+def test_parameter_counts_match_reference(shim, name, spec):
     """The parameter matrix has the reference's shape: as many rows as elements and
     as many columns as the largest element's parameter count (System::setMaxParameters,
     elementoperation.cpp:173-186), with each element's count from the engine's
     element_parameters."""
-    lib = shim()
-    lib.cfg_parameter_counts.restype = ctypes.c_int
-    lib.cfg_parameter_counts.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int]
+    lib = shim
     counts = np.zeros(16, np.int32)
     n = lib.cfg_parameter_counts(spec.input_in().encode(), counts.ctypes.data, len(counts))
     assert n == len(spec.elements)
@@ -134,16 +134,13 @@ SETTING_CASES = [
 ]
 
 
-@pytest.mark.skipif(shutil.which("g++") is None or not os.path.exists(REF_SO),
-                    reason="needs g++ and the reference harness")
+@NEEDS
 @pytest.mark.parametrize("name,lines", SETTING_CASES, ids=[c[0] for c in SETTING_CASES])
-def test_parsed_settings_match_reference(name, lines):
+def test_parsed_settings_match_reference(shim, name, lines):
     """The same input.in text through the engine's parser and the reference's
     (System::parser and its set-up) gives the same settings, key side effects included."""
     text = "\n".join(lines + BODY) + "\n"
-    lib = shim()
-    lib.cfg_settings.restype = ctypes.c_int
-    lib.cfg_settings.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    lib = shim
     ours = np.zeros(len(SETTINGS))
     assert lib.cfg_settings(text.encode(), ours.ctypes.data) == len(SETTINGS)
     N = int(ours[0])
