@@ -291,3 +291,37 @@ def test_interacting_pair_optimises_toward_exact():
         theta = theta - opt.update(energy_gradient(avg))
     assert energies[0] - energies[-1] > 0.01
     assert abs(energies[-1] - 3.0) < 0.01
+
+
+def test_importance_sampling_stationary_distribution():
+    """Detailed balance of the oracle's importance sampling, measured: two
+    non-interacting electrons in the 2D oscillator (omega = 1) under a Gaussian of
+    alpha = 0.8 have <E_L> = alpha + 1/alpha exactly when the chain samples |Psi|^2.
+    32 chains of 38 000 steps at dt = 0.2:
+    - the corrected Fokker-Planck Green's ratio samples it (within 4 error bars), and so
+      does the drift-limited form (driftLimit 0.5: limited drift in the proposal and in
+      the ratio);
+    - the reference's Green's ratio (importancesampling.cpp:43-47, reproduced under
+      compat: reference) does not: its chains sit more than 20 error bars low, the
+      bias that compat: corrected removes."""
+    from oracle_bind import Q_ALL
+    O = oracle()
+    alpha = 0.8
+    exact = alpha + 1.0 / alpha
+    W, steps, burn = 32, 40000, 2000
+    theta = np.array([[alpha]])
+    res = {}
+    for name, quirks, a in (("corrected", 0, 0.0), ("limited", 0, 0.5), ("reference", Q_ALL, 0.0)):
+        spec = SystemSpec(N=2, elements=(GAUSSIAN,), coulomb=False, omega=1.0,
+                          sampling="importanceSampling", step=0.2, quirks=quirks, drift_limit=a)
+        pos = np.random.default_rng(2).normal(0.0, 1.0, (W, spec.D))
+        f = np.stack([O.quantum_force(spec, theta, p) for p in pos])
+        out = O.run(spec, theta, pos, f, steps, burn, 0, 1, seed=11, counter=np.zeros(W, np.uint64),
+                    want_steps=False)
+        means = out["sums"][:, 0] / (steps - burn)
+        res[name] = (means.mean(), means.std(ddof=1) / np.sqrt(W))
+    for name in ("corrected", "limited"):
+        e, err = res[name]
+        assert abs(e - exact) < 4 * err, (name, e, err)
+    e, err = res["reference"]
+    assert exact - e > 20 * err, res
