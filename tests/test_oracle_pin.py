@@ -303,7 +303,8 @@ def test_importance_sampling_stationary_distribution():
       the ratio);
     - the reference's Green's ratio (importancesampling.cpp:43-47, reproduced under
       compat: reference) does not: its chains sit more than 20 error bars low, the
-      bias that compat: corrected removes."""
+      bias that compat: corrected removes;
+    - brute-force moves (bruteforce.cpp:26-52, stepLength 0.2) sample it."""
     from oracle_bind import Q_ALL
     O = oracle()
     alpha = 0.8
@@ -311,16 +312,18 @@ def test_importance_sampling_stationary_distribution():
     W, steps, burn = 32, 40000, 2000
     theta = np.array([[alpha]])
     res = {}
-    for name, quirks, a in (("corrected", 0, 0.0), ("limited", 0, 0.5), ("reference", Q_ALL, 0.0)):
+    for name, quirks, a in (("corrected", 0, 0.0), ("limited", 0, 0.5), ("reference", Q_ALL, 0.0),
+                            ("brute force", Q_ALL, 0.0)):
+        sampling = "bruteForce" if name == "brute force" else "importanceSampling"
         spec = SystemSpec(N=2, elements=(GAUSSIAN,), coulomb=False, omega=1.0,
-                          sampling="importanceSampling", step=0.2, quirks=quirks, drift_limit=a)
+                          sampling=sampling, step=0.2, quirks=quirks, drift_limit=a)
         pos = np.random.default_rng(2).normal(0.0, 1.0, (W, spec.D))
         f = np.stack([O.quantum_force(spec, theta, p) for p in pos])
         out = O.run(spec, theta, pos, f, steps, burn, 0, 1, seed=11, counter=np.zeros(W, np.uint64),
                     want_steps=False)
         means = out["sums"][:, 0] / (steps - burn)
         res[name] = (means.mean(), means.std(ddof=1) / np.sqrt(W))
-    for name in ("corrected", "limited"):
+    for name in ("corrected", "limited", "brute force"):
         e, err = res[name]
         assert abs(e - exact) < 4 * err, (name, e, err)
     e, err = res["reference"]
