@@ -105,14 +105,17 @@ typedef struct {
     double walker_std_error; /* std of per-walker means / sqrt(W): independent chains */
 } vmc_averages;
 
-/* Version of this ABI, for a binding to check. */
+/* Version of this ABI, for a binding to check (no counterpart in the reference). */
 int vmc_abi_version(void);
 
 /* Parse input.in text and build an engine on a device.  Replaces
  * System::parser + System::initializeSystem (parser.cpp:25-333, system.cpp:50-73).
  * `opt` may be NULL.  Walkers are created by vmc_init_walkers. */
 int vmc_create(const char *input_in_text, const vmc_options *opt, vmc_engine **out);
+/* Frees the engine and its device memory (System::~System, system.cpp:231). */
 void vmc_destroy(vmc_engine *e);
+/* Sizes and choices of the engine (System's getters, system.h:171-181, plus the
+ * engine's own: walkers, precision, kernel form). */
 int vmc_get_info(const vmc_engine *e, vmc_info *out);
 /* Last error message (static storage, for the calling thread's last failure). */
 const char *vmc_last_error(void);
@@ -127,6 +130,7 @@ int vmc_get_parameters(const vmc_engine *e, double *theta, int n_elements, int p
  * (WaveFunction::initializeArrays) and the importance-sampling force cache
  * (ImportanceSampling::initialize, importancesampling.cpp:11-32). */
 int vmc_init_walkers(vmc_engine *e, const double *pos, uint64_t seed);
+/* Every walker's positions (System::getPositions, system.h:212). */
 int vmc_get_positions(const vmc_engine *e, double *pos /* W x D */);
 
 /* One sampling pass of every walker: `burn_in` unsampled then sampled steps,
@@ -152,7 +156,9 @@ int vmc_run_iteration(vmc_engine *e, int iteration, vmc_averages *out);
 int vmc_apply_sums(vmc_engine *e, const vmc_sums *total, const double *grad_sum,
                    const double *egrad_sum, vmc_averages *out);
 
-/* Per-walker sampled-energy means of the last vmc_sample (W values). */
+/* Per-walker sampled-energy means of the last vmc_sample (W values): each walker's
+ * m_cumulativeEnergy / steps, what one reference rank holds before the MPI_Reduce
+ * (sampler.cpp:111-187). */
 int vmc_get_walker_energies(const vmc_engine *e, double *mean_energy);
 
 /* Oracle entry (a): evaluate every walker at its current positions after an FP64
@@ -183,7 +189,8 @@ int vmc_replay(vmc_engine *e, const double *stream, int steps, uint8_t *accepted
  * replayed against the reference's ReplayRNG-driven run. */
 int vmc_set_replay(vmc_engine *e, const double *stream, int length);
 
-/* Per-walker status words (OR of VMC status bits) since creation. */
+/* Per-walker status words (OR of VMC status bits) since creation (no counterpart in
+ * the reference, which aborts or carries on instead). */
 int vmc_get_status(const vmc_engine *e, uint32_t *status /* W */);
 
 /* Full run as System::runSimulation (system.cpp:81-139) without terminal output:
@@ -201,7 +208,8 @@ int vmc_get_status(const vmc_engine *e, uint32_t *status /* W */);
 int vmc_run_simulation(vmc_engine *e, vmc_averages *history, int n_history);
 
 /* Device-side stopwatch on the engine's stream: mode 0 records the start; mode 1
- * records the stop, waits for it and writes the elapsed milliseconds. */
+ * records the stop, waits for it and writes the elapsed milliseconds (the
+ * reference times each iteration with MPI_Wtime, system.cpp:101-104). */
 int vmc_stopwatch(vmc_engine *e, int mode, double *ms);
 
 /* FP64 rebuild cadence of a mixed-precision engine, in steps (>= 1): engines that
@@ -213,7 +221,8 @@ int vmc_set_refresh_interval(vmc_engine *e, int steps);
 
 /* FMA throughput of a device, FP32 (VMC_PRECISION_MIXED) or FP64, measured with a
  * register-resident loop over all SMs; TFLOP/s counting an FMA as 2 flops.  The
- * roofline denominator of the CUDA-core-bound sweep kernel. */
+ * roofline denominator of the CUDA-core-bound sweep kernel (no counterpart in the
+ * reference). */
 int vmc_measure_fma_peak(int device, int precision, double *tflops);
 
 /* ---- Blocking analysis (Sampler::doResampling, sampler.cpp:319-405, and the
@@ -302,11 +311,14 @@ int vmc_load_state(vmc_engine *e, const char *path);
  *
  * Systems: 2D closed-shell quantum dots with Slater(Hermite) x Gaussian x Pade,
  * Coulomb, importance sampling (all in the batch's precision and compat mode), and
- * general-path systems in FP64 (hydrogen-orbital atoms, SimpleJastrow, RBM; not
- * the MLP Jastrow).  Up to VMC_BATCH_MAX_SYSTEMS systems, at most 16 of them on the
- * general path; one batch per device at a time (its system table is a device
- * constant).  opt (may be NULL): device, compat and refresh_interval apply to
- * every system, precision to the dots; walker counts come from each text. */
+ * general-path systems: hydrogen-orbital atoms with SimpleJastrow in the batch's
+ * precision (mixed: the FP32 atom sweep with an FP64 Slater inverse, re-inverted in
+ * FP64 after each round), other general-path systems (RBM, SimpleJastrow on other
+ * bases) in FP64; not the MLP Jastrow.  Up to VMC_BATCH_MAX_SYSTEMS systems, at most
+ * 16 of them on the general path; one batch per device at a time (its system table
+ * is a device constant).  opt (may be NULL): device, compat and refresh_interval
+ * apply to every system, precision to the dots and those atoms (NULL or -1: each
+ * text's own); walker counts come from each text. */
 #define VMC_BATCH_MAX_SYSTEMS 64
 typedef struct vmc_batch vmc_batch;
 
