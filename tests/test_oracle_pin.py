@@ -246,7 +246,8 @@ def test_exact_energies():
     electrons in the 2D oscillator, omega = 1, with the Gaussian at alpha = 1, have
     E_L = 2 at every position (zero variance); a Slater determinant of Hermite
     orbitals times that Gaussian is the exact closed-shell state of N = 6 and 12,
-    E_L = sum of the shell energies (10 and 28) everywhere."""
+    E_L = sum of the shell energies (10 and 28) everywhere; and the same holds for
+    hydrogen-orbital determinants of atoms without the repulsion."""
     O = oracle()
     rng = np.random.default_rng(5)
     for N, exact, elements in ((2, 2.0, (GAUSSIAN,)), (6, 10.0, (SLATER, GAUSSIAN)),
@@ -258,6 +259,16 @@ def test_exact_energies():
             _, _, _, en = O.eval(spec, theta, rng.normal(0.0, 1.0, spec.D))
             assert abs(en.sum() - exact) < 1e-10 * exact, (N, en)
             assert en[2] == 0.0
+    # hydrogenic atoms without the electrons' repulsion: a Slater determinant of
+    # hydrogen orbitals is exact, E_L = -sum Z^2 / (2 n^2) everywhere (He 1s^2,
+    # Be 1s^2 2s^2, Ne 1s^2 2s^2 2p^6)
+    for N, Z, exact in ((2, 2, -4.0), (4, 4, -20.0), (10, 10, -200.0)):
+        spec = SystemSpec(N=N, Z=Z, d=3, elements=(SLATER,), atom=True, basis="hydrogenOrbital",
+                          coulomb=False)
+        theta = np.zeros((1, max(spec.p_max, 1)))
+        for _ in range(5):
+            _, _, _, en = O.eval(spec, theta, rng.normal(0.0, 1.0, spec.D))
+            assert abs(en.sum() - exact) < 1e-12 * abs(exact), (N, en)
 
 
 def test_interacting_pair_optimises_toward_exact():
