@@ -56,3 +56,35 @@ def test_bf16_rounding_and_layout():
     p = mj.unpack(t)
     assert np.all(p["w3"] == 0) and np.all(p["v3"] == 0)
     assert np.allclose(mj.pack(p), t)
+
+
+@pytest.mark.parametrize("N,dim", [(6, 2), (8, 3)])
+def test_symmetries(N, dim):
+    """J depends on the pair distances, the pairs' spin and the radii only: exchanging
+    two electrons of the same spin leaves J unchanged and exchanges their gradients;
+    a rotation of all positions leaves J and the Laplacian unchanged and rotates the
+    gradient.  Exchanging electrons of opposite spin changes J."""
+    theta = random_theta(7)
+    rng = np.random.default_rng(8)
+    x = rng.normal(0, 1.2, (N, dim))
+    J, G, lap = mj.jastrow(theta, x.ravel(), N, dim)
+    G = G.reshape(N, dim)
+    h = N // 2
+    # same spin: particles 0 and 1 (both up), h and h + 1 (both down)
+    for a, b in ((0, 1), (h, h + 1)):
+        y = x.copy()
+        y[[a, b]] = y[[b, a]]
+        J2, G2, lap2 = mj.jastrow(theta, y.ravel(), N, dim)
+        G2 = G2.reshape(N, dim)
+        assert abs(J2 - J) < 1e-12 * max(1.0, abs(J))
+        assert abs(lap2 - lap) < 1e-10 * max(1.0, abs(lap))
+        assert np.allclose(G2[[b, a]], G[[a, b]], rtol=1e-12, atol=1e-12)
+    y = x.copy()
+    y[[0, h]] = y[[h, 0]]
+    assert abs(mj.jastrow(theta, y.ravel(), N, dim)[0] - J) > 1e-6
+    # a rotation about the origin
+    q, _ = np.linalg.qr(rng.normal(size=(dim, dim)))
+    Jr, Gr, lapr = mj.jastrow(theta, (x @ q.T).ravel(), N, dim)
+    assert abs(Jr - J) < 1e-11 * max(1.0, abs(J))
+    assert abs(lapr - lap) < 1e-9 * max(1.0, abs(lap))
+    assert np.allclose(Gr.reshape(N, dim), G @ q.T, rtol=1e-10, atol=1e-10)
