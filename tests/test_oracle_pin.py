@@ -339,3 +339,26 @@ def test_importance_sampling_stationary_distribution():
         assert abs(e - exact) < 4 * err, (name, e, err)
     e, err = res["reference"]
     assert exact - e > 20 * err, res
+
+
+def test_local_energy_symmetries():
+    """|Psi|^2 of a closed-shell dot (Slater determinant of Hermite orbitals x Gaussian x
+    Pade) is unchanged by exchanging two electrons of the same spin and by rotating all
+    positions about the origin (the closed shells fill every orbital of a degenerate
+    level), so the oracle's local-energy parts are too."""
+    O = oracle()
+    rng = np.random.default_rng(12)
+    for N in (6, 12):
+        spec = SystemSpec(N=N, elements=(SLATER, GAUSSIAN, PADE), omega=1.0)
+        theta = np.zeros((3, spec.p_max))
+        theta[1, 0], theta[2, 0] = 0.9, 0.4
+        x = rng.normal(0.0, 1.0, (N, 2))
+        en = O.eval(spec, theta, x.ravel())[3]
+        h = N // 2
+        for a, b in ((0, 2), (h, h + 1)):
+            y = x.copy()
+            y[[a, b]] = y[[b, a]]
+            assert rel(O.eval(spec, theta, y.ravel())[3], en) < 1e-11
+        c, s = np.cos(0.7), np.sin(0.7)
+        rot = x @ np.array([[c, -s], [s, c]]).T
+        assert rel(O.eval(spec, theta, rot.ravel())[3], en) < 1e-10
