@@ -362,3 +362,38 @@ def test_local_energy_symmetries():
         c, s = np.cos(0.7), np.sin(0.7)
         rot = x @ np.array([[c, -s], [s, c]]).T
         assert rel(O.eval(spec, theta, rot.ravel())[3], en) < 1e-10
+
+
+@pytest.mark.parametrize("case", ["dot6", "he_sj", "rbm"])
+def test_derivatives_consistent_with_ratios(case):
+    """Each element's gradient and Laplacian of ln Psi equal the central differences
+    of the log of its own |Psi|^2 ratio for single-coordinate moves (corrected mode),
+    and T = -1/2 (lap + |grad|^2) follows.  The one exception is the reference's own:
+    RBMGaussian's ratio is exp(((x_old - a)^2 - (x_new - a)^2) / (2 sigma^2))
+    (rbmgaussian.cpp:43-45), the ratio of the amplitudes, while its gradient
+    -(x - a) / sigma^2 and Laplacian belong to the same Gaussian (RBMProduct squares
+    its ratio, rbmproduct.cpp:115); so the difference quotients give half of them, and
+    a chain with RBMGaussian samples |Psi_G| |Psi_rest|^2."""
+    from oracle_bind import RBMGAUSSIAN, RBMPRODUCT, SIMPLEJASTROW
+    spec = {"dot6": SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), omega=1.0, quirks=0),
+            "he_sj": SystemSpec(N=2, Z=2, d=3, elements=(SLATER, SIMPLEJASTROW), atom=True,
+                                basis="hydrogenOrbital", quirks=0),
+            "rbm": SystemSpec(N=2, elements=(RBMGAUSSIAN, RBMPRODUCT), hidden=2, quirks=0)}[case]
+    O = oracle()
+    rng = np.random.default_rng(3)
+    theta = rng.normal(0.5, 0.1, (len(spec.elements), spec.p_max))
+    x = rng.normal(0.0, 1.0, spec.D)
+    g, lap, _, en = O.eval(spec, theta, x)
+    h = 1e-4
+    gfd, d2 = np.zeros_like(g), np.zeros(len(spec.elements))
+    for k in range(spec.D):
+        rp = np.log(O.ratio(spec, theta, x, k, x[k] + h))
+        rm = np.log(O.ratio(spec, theta, x, k, x[k] - h))
+        gfd[:, k] = (rp - rm) / (4 * h)
+        d2 += (rp + rm) / (2 * h * h)
+    half = np.array([0.5 if e == RBMGAUSSIAN else 1.0 for e in spec.elements])
+    assert rel(gfd, g * half[:, None]) < 1e-6
+    assert rel(d2, lap * half) < 1e-6
+    if RBMGAUSSIAN not in spec.elements:
+        G = g.sum(0)
+        assert abs(-0.5 * (d2.sum() + G @ G) - en[0]) < 1e-6 * max(1.0, abs(en[0]))
