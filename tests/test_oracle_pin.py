@@ -397,3 +397,41 @@ def test_derivatives_consistent_with_ratios(case):
     if RBMGAUSSIAN not in spec.elements:
         G = g.sum(0)
         assert abs(-0.5 * (d2.sum() + G @ G) - en[0]) < 1e-6 * max(1.0, abs(en[0]))
+
+
+@pytest.mark.parametrize("case", ["dot6", "he_sj", "rbm"])
+def test_parameter_gradients_consistent_with_ratios(case):
+    """d ln(ratio) / d theta for a fixed move equals 2 (dlnPsi/dtheta at the new point
+    minus at the old) for every parameter (corrected mode), up to two of the
+    reference's own factors, both reproduced: RBMGaussian's amplitude ratio (1 instead
+    of 2, rbmgaussian.cpp:43-45), and RBMProduct's weight gradient x n, which lacks the
+    1 / sigma^2 its ratio carries (rbmproduct.cpp:95-101 against :106, with
+    sigma = 10 x the width, :15): the reference's ADAM sees the weights' gradient
+    sigma^2 = 100 / omega times too large."""
+    from oracle_bind import RBMGAUSSIAN, RBMPRODUCT, SIMPLEJASTROW
+    spec = {"dot6": SystemSpec(N=6, elements=(SLATER, GAUSSIAN, PADE), omega=1.0, quirks=0),
+            "he_sj": SystemSpec(N=2, Z=2, d=3, elements=(SLATER, SIMPLEJASTROW), atom=True,
+                                basis="hydrogenOrbital", quirks=0),
+            "rbm": SystemSpec(N=2, elements=(RBMGAUSSIAN, RBMPRODUCT), hidden=2, quirks=0)}[case]
+    O = oracle()
+    rng = np.random.default_rng(5)
+    theta = rng.normal(0.5, 0.1, (len(spec.elements), spec.p_max))
+    x = rng.normal(0.0, 1.0, spec.D)
+    k, xn = 1, x[1] + 0.3
+    x2 = x.copy()
+    x2[k] = xn
+    dpg = O.eval(spec, theta, x2)[2] - O.eval(spec, theta, x)[2]
+    sigma2 = (10.0 / np.sqrt(spec.omega)) ** 2
+    h = 1e-6
+    for e, el in enumerate(spec.elements):
+        for p in range(spec.n_params(e)):
+            tp, tm = theta.copy(), theta.copy()
+            tp[e, p] += h
+            tm[e, p] -= h
+            d = (np.log(O.ratio(spec, tp, x, k, xn)[e]) - np.log(O.ratio(spec, tm, x, k, xn)[e])) / (2 * h)
+            want = 2.0 * dpg[e, p]
+            if el == RBMGAUSSIAN:
+                want = dpg[e, p]
+            elif el == RBMPRODUCT and p >= spec.hidden:
+                want /= sigma2
+            assert abs(d - want) < 1e-6 * max(1e-2, abs(want)), (el, p, d, want)
