@@ -1,8 +1,14 @@
-"""Pin the C oracle (oracle/vmc_oracle.c) to the reference's own outputs.
+"""Pin the C oracle (oracle/vmc_oracle.c) to the reference's own outputs, and check it
+against properties that need no reference.
 
 The golden vectors in tests/golden/ were produced by the reference's C++ sources
 (tests/golden/make_golden.py).  Bar: 1e-11 relative (max-abs over each array,
-relative to its max-abs) for FP64 values, identical accept/reject sequences.
+relative to its max-abs) for FP64 values, identical accept/reject sequences.  The
+densities and the driver schedule are restated on the host (oracle/vmc_oracle_host.py)
+around the oracle's chains.  The properties: exact energies (the oscillator's and the
+hydrogenic closed shells), the variational bound on the interacting pair, the
+stationary distribution of each move type, symmetry of the local energy, and
+derivatives against difference quotients of the oracle's own ratios.
 """
 import os
 
